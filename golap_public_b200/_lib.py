@@ -1,0 +1,133 @@
+"""ctypes binding of libgx.so (the C-ABI declared in include/gx.h).
+
+The library is built in-tree by golap_public_b200.build.build().  There is no
+fallback: if libgx.so cannot be loaded, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libgx.so"
+
+P = C.c_void_p
+u8p = C.POINTER(C.c_uint8)
+
+GX_OK, GX_ERR_CUDA, GX_ERR_CORRUPT, GX_ERR_CAPACITY, GX_ERR_TIMEOUT, GX_ERR_NOMEM, GX_ERR_INVALID = range(7)
+GX_CODEC_NONE, GX_CODEC_LZ4, GX_CODEC_CASCADED = 0, 1, 2
+GX_STEP_FILTER, GX_STEP_PROBE, GX_STEP_CARRY, GX_STEP_VALUE = 1, 2, 4, 8
+GX_AGG_SUM, GX_AGG_SUM_PRODUCT, GX_AGG_COUNT = 0, 1, 2
+GX_MAX_STEPS = 8
+
+
+class GxError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_STATUS = {0: "GX_OK", 1: "GX_ERR_CUDA", 2: "GX_ERR_CORRUPT", 3: "GX_ERR_CAPACITY", 4: "GX_ERR_TIMEOUT",
+           5: "GX_ERR_NOMEM", 6: "GX_ERR_INVALID"}
+
+
+class EncodeOpts(C.Structure):
+    _fields_ = [("codec", C.c_uint32), ("rows_per_chunk", C.c_uint32), ("rows_per_block", C.c_uint32),
+                ("lz4_segments", C.c_uint32), ("lz4_min_match", C.c_uint32), ("lz4_search_depth", C.c_uint32),
+                ("casc_rle", C.c_uint32), ("casc_delta", C.c_uint32), ("casc_bitpack", C.c_uint32),
+                ("threads", C.c_uint32)]
+
+
+class ColumnInfo(C.Structure):
+    _fields_ = [("n_rows", C.c_uint64), ("comp_bytes", C.c_uint64), ("uncomp_bytes", C.c_uint64),
+                ("meta_bytes", C.c_uint64), ("codec", C.c_uint32), ("rows_per_chunk", C.c_uint32),
+                ("rows_per_block", C.c_uint32), ("n_chunks", C.c_uint32), ("blocks_per_chunk", C.c_uint32),
+                ("n_blocks", C.c_uint32), ("lz4_segments", C.c_uint32), ("on_device", C.c_uint32)]
+
+
+class BlockInfo(C.Structure):
+    _fields_ = [("offset", C.c_uint64), ("size", C.c_uint64), ("payload", C.c_uint64), ("tuples", C.c_uint64)]
+
+
+class Pred(C.Structure):
+    _fields_ = [("col_dev", P), ("lo", C.c_int32), ("hi", C.c_int32)]
+
+
+class ScanStep(C.Structure):
+    _fields_ = [("col", P), ("flags", C.c_uint32), ("lo", C.c_int32), ("hi", C.c_int32), ("ht", P),
+                ("digit_base", C.c_int32), ("digit_card", C.c_uint32)]
+
+
+class ScanPlan(C.Structure):
+    _fields_ = [("n_steps", C.c_uint32), ("steps", ScanStep * GX_MAX_STEPS), ("agg", C.c_uint32),
+                ("keep_chunks_dev", P), ("groupby", P), ("result_dev", P)]
+
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "gx_status_str": (C.c_char_p, [C.c_int32]),
+    "gx_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "gx_version": (C.c_char_p, []),
+    "gx_device_count": (C.c_int32, [C.POINTER(C.c_int)]),
+    "gx_encode_opts_default": (C.c_int32, [C.POINTER(EncodeOpts)]),
+    "gx_column_encode": (C.c_int32, [P, C.c_uint64, C.POINTER(EncodeOpts), C.POINTER(P)]),
+    "gx_column_free": (C.c_int32, [P]),
+    "gx_column_info_get": (C.c_int32, [P, C.POINTER(ColumnInfo)]),
+    "gx_column_chunk_minmax": (C.c_int32, [P, P, P]),
+    "gx_column_blocks": (C.c_int32, [P, P]),
+    "gx_column_payload": (C.c_int32, [P, C.POINTER(u8p), C.POINTER(C.c_uint64)]),
+    "gx_column_seg_index": (C.c_int32, [P, C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64)]),
+    "gx_column_to_device": (C.c_int32, [P, C.c_int, P]),
+    "gx_column_release_device": (C.c_int32, [P]),
+    "gx_decompress_chunk": (C.c_int32, [P, C.c_uint64, P, P]),
+    "gx_decompress_chunks": (C.c_int32, [P, C.c_uint64, C.c_uint64, P, P]),
+    "gx_lz4_decompress_raw": (C.c_int32, [P, P, P, P, C.c_uint64, P, P]),
+    "gx_check_minmax": (C.c_int32, [P, C.c_int32, C.c_int32, P, P]),
+    "gx_combine_and": (C.c_int32, [P, P, P, C.c_uint64, P]),
+    "gx_prune_minmax": (C.c_int32, [P, P, P, C.c_uint32, P, P]),
+    "gx_hashtable_create": (C.c_int32, [C.c_uint64, C.POINTER(P)]),
+    "gx_hashtable_free": (C.c_int32, [P]),
+    "gx_hashtable_build": (C.c_int32, [P, P, P, C.c_uint64, P, C.c_uint32, P]),
+    "gx_hashtable_count": (C.c_int32, [P, C.POINTER(C.c_uint64), P]),
+    "gx_hashtable_probe": (C.c_int32, [P, P, C.c_uint64, P, P, P]),
+    "gx_groupby_create": (C.c_int32, [C.c_uint64, C.POINTER(P)]),
+    "gx_groupby_free": (C.c_int32, [P]),
+    "gx_groupby_reset": (C.c_int32, [P, P]),
+    "gx_groupby_add": (C.c_int32, [P, P, P, C.c_uint64, P]),
+    "gx_groupby_read": (C.c_int32, [P, P, P, C.c_uint64, C.POINTER(C.c_uint64), P]),
+    "gx_scan": (C.c_int32, [C.POINTER(ScanPlan), P]),
+    "gx_scan_sync": (C.c_int32, [C.POINTER(ScanPlan), P, C.POINTER(C.c_uint64)]),
+    "gx_scan_check": (C.c_int32, [P]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libgx.so (raises if it is missing: there is no non-CUDA path)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is not built; run golap_public_b200.build.build()")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib().gx_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != GX_OK:
+        raise GxError(status, last_error())

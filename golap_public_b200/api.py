@@ -1,0 +1,299 @@
+"""Host-side mirror of the reference operator API for the hot path.
+
+Names follow the GOLAP classes they stand in for:
+  Column            CompInfo/BlockInfo + the compressed chunk store
+                    (core/comp.cuh:23-78) with its MinMaxMeta
+                    (core/metadata.cuh:110-221) collected at ingest
+  ChunkDecompressor ChunkDecompressor::step (core/comp.cuh:151-227)
+  MetaChecker       MetaChecker::add_minmax (core/metadata.cuh:638-658)
+  HashMap           HashMap + hash_map_build_pred_other
+                    (core/dev_structs.cuh:37-132, core/join.cuh:107-135)
+  HashAggregate     HashAggregate with SumAgg (core/dev_structs.cuh:158-253)
+  ScanPlan          the fused per-chunk pipelines pipeline_q1_lineorder /
+                    pipeline_q3 (usecases/ssb/queries/01.cuh:27, 03.cuh:119)
+
+Device buffers are torch CUDA tensors (plumbing only); all compute runs in
+libgx.so.  Errors raise GxError carrying the library's status and message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import check
+
+
+def _stream_handle(stream=None):
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+def _dptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+CODECS = {"none": L.GX_CODEC_NONE, "lz4": L.GX_CODEC_LZ4, "cascaded": L.GX_CODEC_CASCADED}
+
+
+class Column:
+    """One compressed int32 column: chunks of rows_per_chunk rows, blocks of rows_per_block rows."""
+
+    def __init__(self, values: np.ndarray, codec: str = "lz4", rows_per_chunk: int = 1_000_000,
+                 rows_per_block: int = 16384, lz4_segments: int = 32, lz4_min_match: int = 4,
+                 lz4_search_depth: int = 16, threads: int = 0, name: str = ""):
+        values = np.ascontiguousarray(values, dtype=np.int32)
+        o = L.EncodeOpts()
+        check(L.lib().gx_encode_opts_default(C.byref(o)))
+        o.codec = CODECS[codec]
+        o.rows_per_chunk = rows_per_chunk
+        o.rows_per_block = rows_per_block
+        o.lz4_segments = lz4_segments
+        o.lz4_min_match = lz4_min_match
+        o.lz4_search_depth = lz4_search_depth
+        o.threads = threads
+        h = C.c_void_p()
+        check(L.lib().gx_column_encode(values.ctypes.data_as(C.c_void_p), len(values), C.byref(o), C.byref(h)))
+        self.handle = h
+        self.name = name
+        self.codec = codec
+
+    # --- inspection
+    @property
+    def info(self) -> L.ColumnInfo:
+        i = L.ColumnInfo()
+        check(L.lib().gx_column_info_get(self.handle, C.byref(i)))
+        return i
+
+    def minmax(self):
+        n = self.info.n_chunks
+        mins = np.zeros(n, np.int32)
+        maxs = np.zeros(n, np.int32)
+        check(L.lib().gx_column_chunk_minmax(self.handle, mins.ctypes.data_as(C.c_void_p),
+                                             maxs.ctypes.data_as(C.c_void_p)))
+        return mins, maxs
+
+    def blocks(self) -> np.ndarray:
+        n = self.info.n_blocks
+        arr = (L.BlockInfo * max(n, 1))()
+        check(L.lib().gx_column_blocks(self.handle, arr))
+        return np.array([(b.offset, b.size, b.payload, b.tuples) for b in arr[:n]], dtype=np.uint64).reshape(-1, 4)
+
+    def payload(self) -> np.ndarray:
+        p = L.u8p()
+        n = C.c_uint64()
+        check(L.lib().gx_column_payload(self.handle, C.byref(p), C.byref(n)))
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+
+    def seg_index(self) -> np.ndarray:
+        p = C.POINTER(C.c_uint32)()
+        n = C.c_uint64()
+        check(L.lib().gx_column_seg_index(self.handle, C.byref(p), C.byref(n)))
+        if n.value == 0:
+            return np.zeros(0, np.uint32)
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+
+    # --- device residency
+    def to_device(self, residency: str = "hbm", stream=None) -> "Column":
+        check(L.lib().gx_column_to_device(self.handle, 1 if residency == "hbm" else 2, _stream_handle(stream)))
+        return self
+
+    def release_device(self):
+        check(L.lib().gx_column_release_device(self.handle))
+
+    def free(self):
+        if self.handle:
+            L.lib().gx_column_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class ChunkDecompressor:
+    """Decompresses chunks of a device-resident Column into a device buffer."""
+
+    def __init__(self, col: Column):
+        self.col = col
+
+    def step(self, chunk_idx: int, out, stream=None):
+        check(L.lib().gx_decompress_chunk(self.col.handle, chunk_idx, _dptr(out), _stream_handle(stream)))
+
+    def chunks(self, first: int, n: int, out, stream=None):
+        check(L.lib().gx_decompress_chunks(self.col.handle, first, n, _dptr(out), _stream_handle(stream)))
+
+
+class MetaChecker:
+    """Combines min/max predicates into per-chunk keep flags (uint16, 1 = keep)."""
+
+    def __init__(self, n_chunks: int):
+        self.preds: list[tuple[Column, int, int]] = []
+        self.n_chunks = n_chunks
+
+    def add_minmax(self, col: Column, lo: int, hi: int) -> "MetaChecker":
+        self.preds.append((col, lo, hi))
+        return self
+
+    def run(self, keep_out, stream=None):
+        n = len(self.preds)
+        cols = (C.c_void_p * n)(*[c.handle.value for c, _, _ in self.preds])
+        lo = (C.c_int32 * n)(*[p[1] for p in self.preds])
+        hi = (C.c_int32 * n)(*[p[2] for p in self.preds])
+        check(L.lib().gx_prune_minmax(cols, lo, hi, n, _dptr(keep_out), _stream_handle(stream)))
+        return keep_out
+
+
+class HashMap:
+    """Open-addressing join table on the device: key -> payload (row id when no payload)."""
+
+    def __init__(self, max_entries: int):
+        h = C.c_void_p()
+        check(L.lib().gx_hashtable_create(max_entries, C.byref(h)))
+        self.handle = h
+
+    def build(self, keys, payload=None, preds=(), stream=None) -> "HashMap":
+        n = keys.numel()
+        arr = (L.Pred * max(1, len(preds)))()
+        for i, (col, lo, hi) in enumerate(preds):
+            arr[i].col_dev = col.data_ptr()
+            arr[i].lo = lo
+            arr[i].hi = hi
+        check(L.lib().gx_hashtable_build(self.handle, _dptr(keys), _dptr(payload), n, arr, len(preds),
+                                         _stream_handle(stream)))
+        return self
+
+    def count(self, stream=None) -> int:
+        n = C.c_uint64()
+        check(L.lib().gx_hashtable_count(self.handle, C.byref(n), _stream_handle(stream)))
+        return n.value
+
+    def probe(self, keys, payload_out=None, hits=None, stream=None):
+        check(L.lib().gx_hashtable_probe(self.handle, _dptr(keys), keys.numel(), _dptr(payload_out), _dptr(hits),
+                                         _stream_handle(stream)))
+
+    def free(self):
+        if self.handle:
+            L.lib().gx_hashtable_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class HashAggregate:
+    """Device group table: int64 key -> int64 sum."""
+
+    def __init__(self, max_groups: int):
+        h = C.c_void_p()
+        check(L.lib().gx_groupby_create(max_groups, C.byref(h)))
+        self.handle = h
+        self.max_groups = max_groups
+
+    def reset(self, stream=None):
+        check(L.lib().gx_groupby_reset(self.handle, _stream_handle(stream)))
+
+    def add(self, keys, vals, stream=None):
+        check(L.lib().gx_groupby_add(self.handle, _dptr(keys), _dptr(vals), keys.numel(), _stream_handle(stream)))
+
+    def read(self, cap: int | None = None, stream=None) -> dict:
+        cap = cap or self.max_groups
+        k = np.zeros(cap, np.int64)
+        s = np.zeros(cap, np.int64)
+        n = C.c_uint64()
+        check(L.lib().gx_groupby_read(self.handle, k.ctypes.data_as(C.c_void_p), s.ctypes.data_as(C.c_void_p), cap,
+                                      C.byref(n), _stream_handle(stream)))
+        return dict(zip(k[: n.value].tolist(), s[: n.value].tolist()))
+
+    def free(self):
+        if self.handle:
+            L.lib().gx_groupby_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+@dataclass
+class Step:
+    col: Column
+    flags: int
+    lo: int = 0
+    hi: int = 0
+    ht: HashMap | None = None
+    digit_base: int = 0
+    digit_card: int = 0
+
+
+@dataclass
+class ScanPlan:
+    """Ordered column steps of one fused scan (see gx_scan_plan in include/gx.h)."""
+
+    steps: list = field(default_factory=list)
+    agg: int = L.GX_AGG_SUM
+    keep_chunks: object = None      # device uint16 tensor or None
+    groupby: HashAggregate | None = None
+    result: object = None           # device int64 tensor (1 element)
+
+    def filter(self, col, lo, hi, carry=False):
+        self.steps.append(Step(col, L.GX_STEP_FILTER | (L.GX_STEP_CARRY if carry else 0), lo, hi))
+        return self
+
+    def probe(self, col, ht, digit_base=0, digit_card=0):
+        self.steps.append(Step(col, L.GX_STEP_PROBE, ht=ht, digit_base=digit_base, digit_card=digit_card))
+        return self
+
+    def carry(self, col):
+        self.steps.append(Step(col, L.GX_STEP_CARRY))
+        return self
+
+    def value(self, col, lo=None, hi=None):
+        flags = L.GX_STEP_VALUE
+        if lo is not None:
+            flags |= L.GX_STEP_FILTER
+        self.steps.append(Step(col, flags, lo or 0, hi or 0))
+        return self
+
+    def to_c(self) -> L.ScanPlan:
+        p = L.ScanPlan()
+        p.n_steps = len(self.steps)
+        for i, s in enumerate(self.steps):
+            d = p.steps[i]
+            d.col = s.col.handle.value
+            d.flags = s.flags
+            d.lo = s.lo
+            d.hi = s.hi
+            d.ht = s.ht.handle.value if s.ht is not None else None
+            d.digit_base = s.digit_base
+            d.digit_card = s.digit_card
+        p.agg = self.agg
+        p.keep_chunks_dev = self.keep_chunks.data_ptr() if self.keep_chunks is not None else None
+        p.groupby = self.groupby.handle.value if self.groupby is not None else None
+        p.result_dev = self.result.data_ptr() if self.result is not None else None
+        self._c = p  # keep alive
+        return p
+
+    def launch(self, stream=None):
+        check(L.lib().gx_scan(C.byref(self.to_c()), _stream_handle(stream)))
+
+    def run_sync(self, stream=None) -> int:
+        rows = C.c_uint64()
+        check(L.lib().gx_scan_sync(C.byref(self.to_c()), _stream_handle(stream), C.byref(rows)))
+        return rows.value
+
+
+def scan_check(stream=None):
+    check(L.lib().gx_scan_check(_stream_handle(stream)))

@@ -1,0 +1,971 @@
+// kernels.cu -- sm_100a kernels of the hot path and the C-ABI entry points
+// that launch them.
+//
+//   scan_kernel        fused per-tile decode -> filter -> probe -> aggregate
+//                      (replaces ChunkDecompressor + pipeline_q1_lineorder,
+//                      usecases/ssb/queries/01.cuh:27-54, and pipeline_q3,
+//                      usecases/ssb/queries/03.cuh:119-170)
+//   items_kernel       min/max pruning + compaction of surviving chunks
+//                      (check_mmmeta/combine_and, core/metadata.cuh:540-547,632-636)
+//   decompress_kernel  chunk decompression to global memory
+//                      (ChunkDecompressor::step, core/comp.cuh:171-195)
+//   ht_build_kernel / ht_probe_kernel
+//                      (hash_map_build_pred_other core/join.cuh:107-135,
+//                       hash_join_count core/join.cuh:46-59)
+//   groupby_add_kernel (group_by_agg_2col core/group.cuh:15-24 with SumAgg)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../include/gx.h"
+#include "gx_device.cuh"
+#include "gx_internal.h"
+
+using namespace gx;
+
+// First error raised by any kernel of this library on the current device.
+__device__ int g_gx_error;
+
+__device__ __forceinline__ void raise_error(int code) { atomicCAS(&g_gx_error, 0, code); }
+
+#define GX_CK(call)                                                                       \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return gx::set_error(GX_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kDecThreads = 256;
+constexpr uint32_t kBufWords = kMaxRowsPerBlock + kMaxSegments;  // padded segment layout
+constexpr uint32_t kMaskWords = kMaxRowsPerBlock / 32;
+constexpr uint32_t kSmemGroupLog2 = 11;                          // 2048-slot partial table
+
+struct ScanStep {
+    gx_dcol col;
+    uint32_t flags;
+    int32_t lo, hi;
+    const uint64_t* ht;
+    uint32_t ht_log2;
+    int32_t digit_base;
+    uint32_t digit_card;
+    uint32_t first_digit;
+};
+
+struct PrunePred {
+    const int32_t* mins;
+    const int32_t* maxs;
+    int32_t lo, hi;
+};
+
+struct ScanParams {
+    uint32_t n_steps;
+    ScanStep steps[GX_MAX_STEPS];
+    uint32_t agg;
+    uint32_t grouped;       // sums per group key
+    uint32_t need_aux;      // aux array (carry or group key) in shared memory
+    uint32_t blocks_per_chunk;
+    const uint32_t* items;  // surviving chunk ids
+    const uint32_t* n_items;
+    uint32_t* work_counter;
+    int64_t* result;
+    int64_t* g_keys;
+    int64_t* g_sums;
+    uint32_t g_log2;
+    unsigned long long* rows_scanned;
+};
+
+struct ItemsParams {
+    const uint16_t* keep_in;
+    uint16_t* keep_out;
+    PrunePred preds[GX_MAX_STEPS];
+    uint32_t n_preds;
+    uint32_t n_chunks;
+    uint32_t* items;
+    uint32_t* n_items;
+    uint32_t* work_counter;
+};
+
+// Decode block `slot` of column `c` into shared memory.  Returns the
+// layout flag (1 = padded segment layout) or a negative error.
+template <int NT>
+__device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint32_t rows, uint32_t* buf,
+                                           int32_t* run_val, uint32_t* run_start, uint32_t* tmp,
+                                           int* s_err) {
+    const uint32_t tid = threadIdx.x;
+    const gx_dblock d = c.blocks[slot];
+    const uint8_t* blk = c.payload + d.offset;
+    // directory sanity: the tile fits the decode buffer and the stream lies
+    // inside the payload (its slack covers the decoders' word over-read)
+    if (d.n_rows != rows || rows > kMaxRowsPerBlock || d.offset > c.payload_bytes ||
+        (uint64_t)d.comp_bytes + 16 > c.payload_bytes - d.offset) {
+        if (tid == 0) *s_err = kErrCorrupt;
+        __syncthreads();
+        return -1;
+    }
+    if (c.codec == GX_CODEC_NONE) {
+        if (d.comp_bytes != rows * 4) {
+            if (tid == 0) *s_err = kErrCorrupt;
+        } else {
+            const uint4* src = (const uint4*)blk;
+            uint4* dst = (uint4*)buf;
+            const uint32_t nv = rows / 4;
+            for (uint32_t i = tid; i < nv; i += NT) dst[i] = __ldg(src + i);
+            for (uint32_t i = nv * 4 + tid; i < rows; i += NT) buf[i] = __ldg((const uint32_t*)blk + i);
+        }
+        __syncthreads();
+        return 0;
+    }
+    if (c.codec == GX_CODEC_LZ4 && c.S > 1) {
+        const uint32_t seg_rows = 1u << c.seg_shift;
+        if (tid < c.S) {
+            const uint32_t j = tid;
+            const uint32_t ob = min(j * seg_rows, rows) * 4, oe = min((j + 1) * seg_rows, rows) * 4;
+            const uint32_t* e = c.seg + (size_t)2 * c.S * slot + 2 * j;
+            const uint32_t comp_pos = __ldg(e), info = __ldg(e + 1);
+            if (ob < oe) {
+                int rc = lz4_seg_lane(blk, d.comp_bytes, comp_pos, info, ob, oe, buf + j * (seg_rows + 1));
+                if (rc) *s_err = rc;
+            }
+        }
+        __syncthreads();
+        return 1;
+    }
+    if (c.codec == GX_CODEC_LZ4) {
+        if (tid < 32) {
+            int rc = lz4_warp_block(blk, d.comp_bytes, (uint8_t*)buf, rows * 4, tid);
+            if (rc && tid == 0) *s_err = rc;
+        }
+        __syncthreads();
+        return 0;
+    }
+    // cascaded
+    int rc = casc_decode_block<NT>(blk, d.comp_bytes, rows, (int32_t*)buf, run_val, run_start, tmp);
+    if (rc && tid == 0) *s_err = rc;
+    __syncthreads();
+    return 0;
+}
+
+__global__ void __launch_bounds__(kScanThreads, 1) scan_kernel(const __grid_constant__ ScanParams P) {
+    constexpr int NT = kScanThreads;
+    constexpr int NW = NT / 32;
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint32_t* buf = (uint32_t*)smem;
+    uint32_t* aux = buf + kBufWords;
+    uint32_t* mask = aux + (P.need_aux ? kMaxRowsPerBlock : 0);
+    int32_t* run_val = (int32_t*)(mask + kMaskWords);
+    uint32_t* run_start = (uint32_t*)(run_val + kCascMaxRuns);
+    uint32_t* gkeys = run_start + kCascMaxRuns + 4;
+    unsigned long long* gsums = (unsigned long long*)(gkeys + (P.grouped ? (1u << kSmemGroupLog2) : 0));
+
+    __shared__ uint32_t s_item;
+    __shared__ int s_err;
+    __shared__ uint32_t s_alive;
+    __shared__ uint32_t s_tmp[NW + 1];
+    __shared__ unsigned long long s_red[NW];
+
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (P.grouped) {
+        for (uint32_t i = tid; i < (1u << kSmemGroupLog2); i += NT) {
+            gkeys[i] = kEmptyGKey;
+            gsums[i] = 0;
+        }
+    }
+    if (tid == 0) s_err = 0;
+    int64_t local_sum = 0;
+    unsigned long long local_rows = 0;
+    const uint32_t bpc = P.blocks_per_chunk;
+    const uint32_t total = *P.n_items * bpc;
+    __syncthreads();
+
+    while (true) {
+        if (tid == 0) s_item = atomicAdd(P.work_counter, 1u);
+        __syncthreads();
+        const uint32_t it = s_item;
+        __syncthreads();
+        if (it >= total) break;
+        const uint32_t chunk = P.items[it / bpc];
+        const uint32_t slot = chunk * bpc + it % bpc;
+        const uint32_t rows = P.steps[0].col.blocks[slot].n_rows;
+        if (rows == 0) continue;
+        const uint32_t ngroups = (rows + 31) / 32;
+        for (uint32_t g = tid; g < ngroups; g += NT)
+            mask[g] = (g + 1) * 32 <= rows ? 0xFFFFFFFFu : ((1u << (rows & 31)) - 1u);
+        if (tid == 0) local_rows += rows;
+        __syncthreads();
+
+        for (uint32_t si = 0; si < P.n_steps; ++si) {
+            const ScanStep& st = P.steps[si];
+            const int layout = decode_tile<NT>(st.col, slot, rows, buf, run_val, run_start, s_tmp, &s_err);
+            const int derr = s_err;
+            __syncthreads();  // every thread has read s_err before it is reset
+            if (derr) {       // corrupt block: drop the tile, remember the error
+                if (tid == 0) {
+                    raise_error(derr);
+                    s_err = 0;
+                }
+                __syncthreads();
+                break;
+            }
+            const uint32_t shift = st.col.seg_shift;
+            if (tid == 0) s_alive = 0;
+            __syncthreads();
+            uint32_t alive_w = 0;
+            for (uint32_t g = warp; g < ngroups; g += NW) {
+                const uint32_t m = mask[g];
+                if (m == 0) continue;
+                const uint32_t r = g * 32 + lane;
+                bool keep = (m >> lane) & 1u;
+                int32_t v = 0;
+                if (keep) v = (int32_t)buf[layout == 1 ? r + (r >> shift) : r];
+                if ((st.flags & GX_STEP_FILTER) && keep) keep = v >= st.lo && v <= st.hi;
+                if ((st.flags & GX_STEP_PROBE) && keep) {
+                    int32_t p = 0;
+                    keep = ht_probe(st.ht, st.ht_log2, v, &p);
+                    if (keep && st.digit_card) {
+                        uint32_t dgt = (uint32_t)(p - st.digit_base);
+                        if (dgt >= st.digit_card) {
+                            raise_error(kErrInvalid);
+                            keep = false;
+                        } else {
+                            aux[r] = st.first_digit ? dgt : aux[r] * st.digit_card + dgt;
+                        }
+                    }
+                }
+                if ((st.flags & GX_STEP_CARRY) && keep) aux[r] = (uint32_t)v;
+                if (st.flags & GX_STEP_VALUE) {
+                    int64_t val = 0;
+                    if (keep) {
+                        if (P.agg == GX_AGG_SUM_PRODUCT) val = (int64_t)v * (int64_t)(int32_t)aux[r];
+                        else if (P.agg == GX_AGG_COUNT) val = 1;
+                        else val = v;
+                    }
+                    if (!P.grouped) {
+                        local_sum += val;
+                    } else {
+                        const uint32_t gk = keep ? aux[r] : 0;
+                        uint32_t active = __ballot_sync(0xFFFFFFFFu, keep);
+                        while (active) {
+                            const int leader = __ffs(active) - 1;
+                            const uint32_t lk = __shfl_sync(0xFFFFFFFFu, gk, leader);
+                            const bool peer = keep && gk == lk && ((active >> lane) & 1u);
+                            const uint32_t peers = __ballot_sync(0xFFFFFFFFu, peer);
+                            const uint64_t tot = warp_sum_u64(peer ? (uint64_t)val : 0ull);
+                            if ((int)lane == leader) {
+                                if (!group_add_smem(gkeys, gsums, kSmemGroupLog2, lk, tot))
+                                    if (!group_add_global(P.g_keys, P.g_sums, P.g_log2, (int64_t)lk, (int64_t)tot))
+                                        raise_error(kErrCapacity);
+                            }
+                            active &= ~peers;
+                        }
+                    }
+                }
+                const uint32_t nm = __ballot_sync(0xFFFFFFFFu, keep);
+                if (lane == 0) mask[g] = nm;
+                alive_w += __popc(nm);
+            }
+            if (lane == 0 && alive_w) atomicAdd(&s_alive, alive_w);
+            __syncthreads();
+            if (s_alive == 0) break;  // nothing left in this tile
+        }
+        __syncthreads();
+    }
+
+    // scalar result: one atomic per CTA
+    if (!P.grouped && P.result) {
+        unsigned long long u = (unsigned long long)local_sum;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) u += __shfl_down_sync(0xFFFFFFFFu, u, d);
+        if (lane == 0) s_red[warp] = u;
+        __syncthreads();
+        if (tid == 0) {
+            unsigned long long t = 0;
+            for (int w = 0; w < NW; ++w) t += s_red[w];
+            if (t) atomicAdd((unsigned long long*)P.result, t);
+        }
+    }
+    if (tid == 0 && P.rows_scanned && local_rows) atomicAdd(P.rows_scanned, local_rows);
+    if (P.grouped) {
+        __syncthreads();
+        for (uint32_t i = tid; i < (1u << kSmemGroupLog2); i += NT) {
+            if (gkeys[i] != kEmptyGKey)
+                if (!group_add_global(P.g_keys, P.g_sums, P.g_log2, (int64_t)gkeys[i], (int64_t)gsums[i]))
+                    raise_error(kErrCapacity);
+        }
+    }
+}
+
+// One CTA: per-chunk keep flags (AND over min/max predicates), compaction
+// of the surviving chunk ids, reset of the work counter.
+__global__ void __launch_bounds__(1024) items_kernel(const __grid_constant__ ItemsParams P) {
+    __shared__ uint32_t s_count;
+    if (threadIdx.x == 0) s_count = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < P.n_chunks; base += blockDim.x) {
+        const uint32_t c = base + threadIdx.x;
+        bool keep = false;
+        if (c < P.n_chunks) {
+            keep = P.keep_in ? P.keep_in[c] != 0 : true;
+            for (uint32_t p = 0; p < P.n_preds; ++p) {
+                const PrunePred& q = P.preds[p];
+                keep = keep && (q.lo <= q.maxs[c]) && (q.hi >= q.mins[c]);
+            }
+            if (P.keep_out) P.keep_out[c] = keep ? 1 : 0;
+        }
+        // order-preserving compaction within this round
+        const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const uint32_t b = __ballot_sync(0xFFFFFFFFu, keep);
+        __shared__ uint32_t s_warp[32];
+        if (lane == 0) s_warp[warp] = __popc(b);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t run = s_count;
+            for (uint32_t w = 0; w < blockDim.x / 32; ++w) {
+                uint32_t x = s_warp[w];
+                s_warp[w] = run;
+                run += x;
+            }
+            s_count = run;
+        }
+        __syncthreads();
+        if (keep) P.items[s_warp[warp] + __popc(b & ((1u << lane) - 1u))] = c;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        *P.n_items = s_count;
+        *P.work_counter = 0;
+    }
+}
+
+// Decompress slots [slot0, slot0 + gridDim.x) of a column into dst (rows
+// laid out contiguously from the first row of slot0).
+__global__ void __launch_bounds__(kDecThreads) decompress_kernel(const gx_dcol c, uint32_t slot0,
+                                                                 uint64_t row0, int32_t* dst) {
+    constexpr int NT = kDecThreads;
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint32_t* buf = (uint32_t*)smem;
+    int32_t* run_val = (int32_t*)(buf + kBufWords);
+    uint32_t* run_start = (uint32_t*)(run_val + kCascMaxRuns);
+    __shared__ int s_err;
+    __shared__ uint32_t s_tmp[NT / 32 + 1];
+    const uint32_t slot = slot0 + blockIdx.x;
+    const gx_dblock d = c.blocks[slot];
+    if (d.n_rows == 0) return;
+    if (threadIdx.x == 0) s_err = 0;
+    __syncthreads();
+    const int layout = decode_tile<NT>(c, slot, d.n_rows, buf, run_val, run_start, s_tmp, &s_err);
+    if (s_err) {
+        if (threadIdx.x == 0) raise_error(s_err);
+        return;
+    }
+    const uint32_t chunk = slot / c.blocks_per_chunk, j = slot % c.blocks_per_chunk;
+    const uint64_t first = (uint64_t)chunk * c.rows_per_chunk + (uint64_t)j * c.rows_per_block - row0;
+    int32_t* out = dst + first;
+    for (uint32_t r = threadIdx.x; r < d.n_rows; r += NT)
+        out[r] = (int32_t)buf[layout == 1 ? r + (r >> c.seg_shift) : r];
+}
+
+__global__ void raw_lz4_kernel(const uint8_t* comp, const uint64_t* coff, uint8_t* out, const uint64_t* ooff,
+                               uint64_t n_blocks, int32_t* status) {
+    const uint64_t b = (uint64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    if (b >= n_blocks) return;
+    const uint64_t c0 = coff[b], c1 = coff[b + 1], o0 = ooff[b], o1 = ooff[b + 1];
+    int rc = kErrCorrupt;
+    if (c1 >= c0 && o1 >= o0 && c1 - c0 < (1ull << 31) && o1 - o0 < (1ull << 31))
+        rc = lz4_warp_block(comp + c0, (uint32_t)(c1 - c0), out + o0, (uint32_t)(o1 - o0), threadIdx.x & 31);
+    if ((threadIdx.x & 31) == 0) status[b] = rc;
+}
+
+__global__ void check_minmax_kernel(const int32_t* mins, const int32_t* maxs, uint32_t n, int32_t lo, int32_t hi,
+                                    uint16_t* out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (lo <= maxs[i] && hi >= mins[i]) out[i] = 1;
+}
+
+__global__ void combine_and_kernel(uint16_t* out, const uint16_t* a, const uint16_t* b, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = a[i] & b[i];
+}
+
+__global__ void fill_u64_kernel(uint64_t* p, uint64_t n, uint64_t v) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+struct BuildPreds {
+    gx_pred p[4];
+    uint32_t n;
+};
+
+__global__ void ht_build_kernel(uint64_t* slots, uint32_t log2cap, const int32_t* keys, const int32_t* payload,
+                                uint64_t n, const __grid_constant__ BuildPreds preds, unsigned long long* counters) {
+    const uint32_t mask = (1u << log2cap) - 1;
+    unsigned long long ins = 0, dup = 0, bad = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        bool pass = true;
+        for (uint32_t k = 0; k < preds.n; ++k) {
+            int32_t x = preds.p[k].col_dev[i];
+            pass = pass && x >= preds.p[k].lo && x <= preds.p[k].hi;
+        }
+        if (!pass) continue;
+        const int32_t key = keys[i];
+        if (key == kEmptyKey) {
+            ++bad;
+            continue;
+        }
+        const int32_t pay = payload ? payload[i] : (int32_t)i;
+        const unsigned long long e = ((unsigned long long)(uint32_t)pay << 32) | (uint32_t)key;
+        uint32_t s = hash_key32(key, log2cap);
+        bool done = false;
+        for (uint32_t t = 0; t <= mask; ++t) {
+            unsigned long long old = atomicCAS((unsigned long long*)slots + s, (unsigned long long)kEmptySlot, e);
+            if (old == (unsigned long long)kEmptySlot) {
+                ++ins;
+                done = true;
+                break;
+            }
+            if ((int32_t)(uint32_t)old == key) {
+                ++dup;
+                done = true;
+                break;
+            }
+            s = (s + 1) & mask;
+        }
+        if (!done) ++bad;
+    }
+    if (ins) atomicAdd(&counters[0], ins);
+    if (dup) atomicAdd(&counters[1], dup);
+    if (bad) atomicAdd(&counters[2], bad);
+}
+
+__global__ void ht_probe_kernel(const uint64_t* slots, uint32_t log2cap, const int32_t* keys, uint64_t n,
+                                int32_t* out, unsigned long long* hits) {
+    unsigned long long h = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        int32_t p = 0;
+        bool hit = ht_probe(slots, log2cap, keys[i], &p);
+        if (out) out[i] = hit ? p : INT32_MIN;
+        h += hit;
+    }
+    if (hits) {
+        for (int d = 16; d > 0; d >>= 1) h += __shfl_down_sync(0xFFFFFFFFu, h, d);
+        if ((threadIdx.x & 31) == 0 && h) atomicAdd(hits, h);
+    }
+}
+
+__global__ void groupby_add_kernel(int64_t* gk, int64_t* gs, uint32_t log2cap, const int64_t* keys,
+                                   const int64_t* vals, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const int64_t k = keys[i];
+        if (k == kEmptyGroup || !group_add_global(gk, gs, log2cap, k, vals[i])) raise_error(kErrCapacity);
+    }
+}
+
+__global__ void groupby_compact_kernel(const int64_t* gk, const int64_t* gs, uint64_t cap, int64_t* ok, int64_t* os,
+                                       unsigned long long* count, uint64_t out_cap) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cap; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (gk[i] == kEmptyGroup) continue;
+        unsigned long long j = atomicAdd(count, 1ull);
+        if (j < out_cap) {
+            ok[j] = gk[i];
+            os[j] = gs[i];
+        }
+    }
+}
+
+// ------------------------------------------------------------ host helpers
+
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cached[dev]) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = n > 0 ? n : 1;
+    }
+    return cached[dev];
+}
+
+uint32_t log2_ceil(uint64_t x) {
+    uint32_t l = 0;
+    while ((1ull << l) < x) ++l;
+    return l;
+}
+
+size_t scan_smem_bytes(bool need_aux, bool grouped) {
+    size_t b = 4ull * kBufWords;
+    if (need_aux) b += 4ull * kMaxRowsPerBlock;
+    b += 4ull * kMaskWords;
+    b += 4ull * kCascMaxRuns + 4ull * (kCascMaxRuns + 4);
+    if (grouped) b += (4ull + 8ull) * (1u << kSmemGroupLog2);
+    return b;
+}
+
+size_t dec_smem_bytes() { return 4ull * kBufWords + 4ull * kCascMaxRuns + 4ull * (kCascMaxRuns + 4); }
+
+gx_status wait_stream(cudaStream_t s, double timeout_s) {
+    auto t0 = std::chrono::steady_clock::now();
+    while (true) {
+        cudaError_t e = cudaStreamQuery(s);
+        if (e == cudaSuccess) return GX_OK;
+        if (e != cudaErrorNotReady) return set_error(GX_ERR_CUDA, "stream failed: %s", cudaGetErrorString(e));
+        double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > timeout_s) return set_error(GX_ERR_TIMEOUT, "stream did not finish within %.0f s", timeout_s);
+        std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 5 : 200));
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- objects
+
+struct gx_hashtable {
+    uint64_t* slots = nullptr;
+    uint32_t log2cap = 0;
+    uint64_t max_entries = 0;
+    unsigned long long* counters = nullptr;  // inserted, duplicates, dropped
+};
+
+struct gx_groupby {
+    int64_t* keys = nullptr;
+    int64_t* sums = nullptr;
+    uint32_t log2cap = 0;
+    uint64_t max_groups = 0;
+};
+
+extern "C" {
+
+gx_status gx_column_to_device(gx_column* col, int residency, void* stream) {
+    if (!col || (residency != 1 && residency != 2)) return set_error(GX_ERR_INVALID, "gx_column_to_device: bad args");
+    gx_column_release_device(col);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t pb = col->payload.size();
+    if (residency == 1) {
+        GX_CK(cudaMalloc(&col->d_payload, pb));
+        GX_CK(cudaMemcpyAsync(col->d_payload, col->payload.data(), pb, cudaMemcpyHostToDevice, s));
+    } else {
+        GX_CK(cudaHostAlloc(&col->h_pinned, pb, cudaHostAllocMapped | cudaHostAllocPortable));
+        std::memcpy(col->h_pinned, col->payload.data(), pb);
+        GX_CK(cudaHostGetDevicePointer(&col->d_payload, col->h_pinned, 0));
+    }
+    GX_CK(cudaMalloc(&col->d_blocks, sizeof(gx_dblock) * col->blocks.size()));
+    GX_CK(cudaMemcpyAsync(col->d_blocks, col->blocks.data(), sizeof(gx_dblock) * col->blocks.size(),
+                          cudaMemcpyHostToDevice, s));
+    if (!col->seg.empty()) {
+        GX_CK(cudaMalloc(&col->d_seg, 4 * col->seg.size()));
+        GX_CK(cudaMemcpyAsync(col->d_seg, col->seg.data(), 4 * col->seg.size(), cudaMemcpyHostToDevice, s));
+    }
+    GX_CK(cudaMalloc(&col->d_mins, 4 * col->n_chunks));
+    GX_CK(cudaMalloc(&col->d_maxs, 4 * col->n_chunks));
+    GX_CK(cudaMemcpyAsync(col->d_mins, col->mins.data(), 4 * col->n_chunks, cudaMemcpyHostToDevice, s));
+    GX_CK(cudaMemcpyAsync(col->d_maxs, col->maxs.data(), 4 * col->n_chunks, cudaMemcpyHostToDevice, s));
+    GX_CK(cudaStreamSynchronize(s));
+    cudaGetDevice(&col->device);
+    col->residency = residency;
+    return GX_OK;
+}
+
+gx_status gx_column_release_device(gx_column* col) {
+    if (!col) return set_error(GX_ERR_INVALID, "null column");
+    if (col->residency == 1 && col->d_payload) cudaFree(col->d_payload);
+    if (col->h_pinned) cudaFreeHost(col->h_pinned);
+    if (col->d_blocks) cudaFree(col->d_blocks);
+    if (col->d_seg) cudaFree(col->d_seg);
+    if (col->d_mins) cudaFree(col->d_mins);
+    if (col->d_maxs) cudaFree(col->d_maxs);
+    col->d_payload = nullptr;
+    col->h_pinned = nullptr;
+    col->d_blocks = nullptr;
+    col->d_seg = nullptr;
+    col->d_mins = col->d_maxs = nullptr;
+    col->residency = 0;
+    return GX_OK;
+}
+
+gx_status gx_decompress_chunks(const gx_column* col, uint64_t first_chunk, uint64_t n_chunks, void* dst_dev,
+                               void* stream) {
+    if (!col || !dst_dev) return set_error(GX_ERR_INVALID, "gx_decompress_chunks: null argument");
+    if (!col->residency) return set_error(GX_ERR_INVALID, "column is not on the device");
+    if (first_chunk + n_chunks > col->n_chunks) return set_error(GX_ERR_INVALID, "chunk range out of bounds");
+    if (n_chunks == 0) return GX_OK;
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr_set[dev & 63]) {
+        GX_CK(cudaFuncSetAttribute(decompress_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)dec_smem_bytes()));
+        attr_set[dev & 63] = true;
+    }
+    const uint32_t slot0 = (uint32_t)(first_chunk * col->blocks_per_chunk);
+    const uint32_t nslots = (uint32_t)(n_chunks * col->blocks_per_chunk);
+    const uint64_t row0 = first_chunk * (uint64_t)col->rows_per_chunk;
+    decompress_kernel<<<nslots, kDecThreads, dec_smem_bytes(), (cudaStream_t)stream>>>(col->view(), slot0, row0,
+                                                                                        (int32_t*)dst_dev);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+gx_status gx_decompress_chunk(const gx_column* col, uint64_t chunk_idx, void* dst_dev, void* stream) {
+    return gx_decompress_chunks(col, chunk_idx, 1, dst_dev, stream);
+}
+
+gx_status gx_lz4_decompress_raw(const uint8_t* comp_dev, const uint64_t* comp_offsets_dev, uint8_t* out_dev,
+                                const uint64_t* out_offsets_dev, uint64_t n_blocks, int32_t* status_dev,
+                                void* stream) {
+    if (!comp_dev || !comp_offsets_dev || !out_dev || !out_offsets_dev || !status_dev)
+        return set_error(GX_ERR_INVALID, "gx_lz4_decompress_raw: null argument");
+    if (n_blocks == 0) return GX_OK;
+    const uint32_t wpb = 4;
+    raw_lz4_kernel<<<(unsigned)((n_blocks + wpb - 1) / wpb), 32 * wpb, 0, (cudaStream_t)stream>>>(
+        comp_dev, comp_offsets_dev, out_dev, out_offsets_dev, n_blocks, status_dev);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+gx_status gx_check_minmax(const gx_column* col, int32_t lo, int32_t hi, uint16_t* out_dev, void* stream) {
+    if (!col || !out_dev || !col->residency) return set_error(GX_ERR_INVALID, "gx_check_minmax: bad args");
+    uint32_t n = col->n_chunks;
+    check_minmax_kernel<<<std::max(1u, std::min(64u, (n + 511) / 512)), 512, 0, (cudaStream_t)stream>>>(
+        col->d_mins, col->d_maxs, n, lo, hi, out_dev);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+gx_status gx_combine_and(uint16_t* out_dev, const uint16_t* a_dev, const uint16_t* b_dev, uint64_t n, void* stream) {
+    if (!out_dev || !a_dev || !b_dev) return set_error(GX_ERR_INVALID, "gx_combine_and: null argument");
+    if (n == 0) return GX_OK;
+    combine_and_kernel<<<(unsigned)std::min<uint64_t>(64, (n + 511) / 512), 512, 0, (cudaStream_t)stream>>>(
+        out_dev, a_dev, b_dev, n);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+static gx_status launch_items(const gx_column* const* cols, const int32_t* lo, const int32_t* hi, uint32_t n_preds,
+                              uint32_t n_chunks, const uint16_t* keep_in, uint16_t* keep_out, uint32_t* items,
+                              uint32_t* n_items, uint32_t* counter, cudaStream_t s) {
+    ItemsParams ip{};
+    if (n_preds > GX_MAX_STEPS) return set_error(GX_ERR_INVALID, "too many prune predicates");
+    for (uint32_t p = 0; p < n_preds; ++p) {
+        if (!cols[p] || !cols[p]->residency) return set_error(GX_ERR_INVALID, "prune column %u not on device", p);
+        if (cols[p]->n_chunks != n_chunks) return set_error(GX_ERR_INVALID, "prune columns disagree on chunk count");
+        ip.preds[p] = PrunePred{cols[p]->d_mins, cols[p]->d_maxs, lo[p], hi[p]};
+    }
+    ip.n_preds = n_preds;
+    ip.n_chunks = n_chunks;
+    ip.keep_in = keep_in;
+    ip.keep_out = keep_out;
+    ip.items = items;
+    ip.n_items = n_items;
+    ip.work_counter = counter;
+    items_kernel<<<1, 1024, 0, s>>>(ip);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+gx_status gx_prune_minmax(const gx_column* const* cols, const int32_t* lo, const int32_t* hi, uint32_t n_preds,
+                          uint16_t* keep_dev, void* stream) {
+    if (!cols || !lo || !hi || !keep_dev || n_preds == 0) return set_error(GX_ERR_INVALID, "gx_prune_minmax: bad args");
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint32_t n_chunks = cols[0]->n_chunks;
+    uint32_t* scratch = nullptr;
+    GX_CK(cudaMallocAsync(&scratch, 4ull * (n_chunks + 2), s));
+    gx_status st = launch_items(cols, lo, hi, n_preds, n_chunks, nullptr, keep_dev, scratch + 2, scratch, scratch + 1, s);
+    cudaFreeAsync(scratch, s);
+    return st;
+}
+
+// ------------------------------------------------------------ hash tables
+
+gx_status gx_hashtable_create(uint64_t max_entries, gx_hashtable** out) {
+    if (!out || max_entries == 0 || max_entries > (1ull << 30)) return set_error(GX_ERR_INVALID, "gx_hashtable_create: bad args");
+    gx_hashtable* h = new gx_hashtable();
+    h->max_entries = max_entries;
+    h->log2cap = std::max<uint32_t>(4, log2_ceil(2 * max_entries));
+    cudaError_t e = cudaMalloc(&h->slots, 8ull << h->log2cap);
+    if (e == cudaSuccess) e = cudaMalloc(&h->counters, 4 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        cudaFree(h->slots);
+        delete h;
+        return set_error(GX_ERR_NOMEM, "gx_hashtable_create: %s", cudaGetErrorString(e));
+    }
+    *out = h;
+    return GX_OK;
+}
+
+gx_status gx_hashtable_free(gx_hashtable* ht) {
+    if (!ht) return GX_OK;
+    cudaFree(ht->slots);
+    cudaFree(ht->counters);
+    delete ht;
+    return GX_OK;
+}
+
+gx_status gx_hashtable_build(gx_hashtable* ht, const int32_t* keys_dev, const int32_t* payload_dev, uint64_t n,
+                             const gx_pred* preds, uint32_t n_preds, void* stream) {
+    if (!ht || (!keys_dev && n) || n_preds > 4 || (n_preds && !preds)) return set_error(GX_ERR_INVALID, "gx_hashtable_build: bad args");
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint64_t cap = 1ull << ht->log2cap;
+    fill_u64_kernel<<<(unsigned)std::min<uint64_t>(1024, (cap + 255) / 256), 256, 0, s>>>(ht->slots, cap, kEmptySlot);
+    GX_CK(cudaMemsetAsync(ht->counters, 0, 4 * sizeof(unsigned long long), s));
+    if (n == 0) return GX_OK;
+    BuildPreds bp{};
+    for (uint32_t i = 0; i < n_preds; ++i) bp.p[i] = preds[i];
+    bp.n = n_preds;
+    ht_build_kernel<<<(unsigned)std::min<uint64_t>(4 * sm_count(), (n + 255) / 256), 256, 0, s>>>(
+        ht->slots, ht->log2cap, keys_dev, payload_dev, n, bp, ht->counters);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+gx_status gx_hashtable_count(const gx_hashtable* ht, uint64_t* n_entries, void* stream) {
+    if (!ht || !n_entries) return set_error(GX_ERR_INVALID, "gx_hashtable_count: bad args");
+    unsigned long long c[4];
+    GX_CK(cudaMemcpyAsync(c, ht->counters, sizeof(c), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    gx_status st = wait_stream((cudaStream_t)stream, 120.0);
+    if (st) return st;
+    *n_entries = c[0];
+    if (c[2]) return set_error(GX_ERR_CAPACITY, "hash table: %llu rows not inserted (full or reserved key)", c[2]);
+    if (c[0] > ht->max_entries) return set_error(GX_ERR_CAPACITY, "hash table holds %llu > max_entries %llu", c[0],
+                                                 (unsigned long long)ht->max_entries);
+    return GX_OK;
+}
+
+gx_status gx_hashtable_probe(const gx_hashtable* ht, const int32_t* keys_dev, uint64_t n, int32_t* payload_out_dev,
+                             uint64_t* hits_dev, void* stream) {
+    if (!ht || (!keys_dev && n)) return set_error(GX_ERR_INVALID, "gx_hashtable_probe: bad args");
+    if (n == 0) return GX_OK;
+    ht_probe_kernel<<<(unsigned)std::min<uint64_t>(8 * sm_count(), (n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        ht->slots, ht->log2cap, keys_dev, n, payload_out_dev, (unsigned long long*)hits_dev);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+// ---------------------------------------------------------------- groupby
+
+gx_status gx_groupby_create(uint64_t max_groups, gx_groupby** out) {
+    if (!out || max_groups == 0 || max_groups > (1ull << 30)) return set_error(GX_ERR_INVALID, "gx_groupby_create: bad args");
+    gx_groupby* g = new gx_groupby();
+    g->max_groups = max_groups;
+    g->log2cap = std::max<uint32_t>(4, log2_ceil(2 * max_groups));
+    cudaError_t e = cudaMalloc(&g->keys, 8ull << g->log2cap);
+    if (e == cudaSuccess) e = cudaMalloc(&g->sums, 8ull << g->log2cap);
+    if (e != cudaSuccess) {
+        cudaFree(g->keys);
+        delete g;
+        return set_error(GX_ERR_NOMEM, "gx_groupby_create: %s", cudaGetErrorString(e));
+    }
+    *out = g;
+    return gx_groupby_reset(g, nullptr) == GX_OK ? (cudaDeviceSynchronize() == cudaSuccess ? GX_OK : GX_ERR_CUDA)
+                                                  : GX_ERR_CUDA;
+}
+
+gx_status gx_groupby_free(gx_groupby* gb) {
+    if (!gb) return GX_OK;
+    cudaFree(gb->keys);
+    cudaFree(gb->sums);
+    delete gb;
+    return GX_OK;
+}
+
+gx_status gx_groupby_reset(gx_groupby* gb, void* stream) {
+    if (!gb) return set_error(GX_ERR_INVALID, "null groupby");
+    const uint64_t cap = 1ull << gb->log2cap;
+    fill_u64_kernel<<<(unsigned)std::min<uint64_t>(1024, (cap + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        (uint64_t*)gb->keys, cap, (uint64_t)kEmptyGroup);
+    GX_CK(cudaMemsetAsync(gb->sums, 0, 8 * cap, (cudaStream_t)stream));
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+gx_status gx_groupby_add(gx_groupby* gb, const int64_t* keys_dev, const int64_t* vals_dev, uint64_t n, void* stream) {
+    if (!gb || (n && (!keys_dev || !vals_dev))) return set_error(GX_ERR_INVALID, "gx_groupby_add: bad args");
+    if (n == 0) return GX_OK;
+    groupby_add_kernel<<<(unsigned)std::min<uint64_t>(8 * sm_count(), (n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        gb->keys, gb->sums, gb->log2cap, keys_dev, vals_dev, n);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+gx_status gx_groupby_read(gx_groupby* gb, int64_t* keys_host, int64_t* sums_host, uint64_t cap, uint64_t* n_groups,
+                          void* stream) {
+    if (!gb || !n_groups || (cap && (!keys_host || !sums_host))) return set_error(GX_ERR_INVALID, "gx_groupby_read: bad args");
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint64_t tcap = 1ull << gb->log2cap;
+    const uint64_t ocap = std::max<uint64_t>(cap, 1);
+    char* scratch = nullptr;
+    GX_CK(cudaMallocAsync(&scratch, 16 * ocap + 16, s));
+    int64_t* ok = (int64_t*)scratch;
+    int64_t* os = ok + ocap;
+    unsigned long long* cnt = (unsigned long long*)(os + ocap);
+    GX_CK(cudaMemsetAsync(cnt, 0, 8, s));
+    groupby_compact_kernel<<<(unsigned)std::min<uint64_t>(1024, (tcap + 255) / 256), 256, 0, s>>>(
+        gb->keys, gb->sums, tcap, ok, os, cnt, cap);
+    unsigned long long c = 0;
+    GX_CK(cudaMemcpyAsync(&c, cnt, 8, cudaMemcpyDeviceToHost, s));
+    gx_status st = wait_stream(s, 120.0);
+    if (st) {
+        cudaFreeAsync(scratch, s);
+        return st;
+    }
+    *n_groups = c;
+    if (c > cap) {
+        cudaFreeAsync(scratch, s);
+        return set_error(GX_ERR_CAPACITY, "gx_groupby_read: %llu groups > cap %llu", c, (unsigned long long)cap);
+    }
+    if (c) {
+        GX_CK(cudaMemcpyAsync(keys_host, ok, 8 * c, cudaMemcpyDeviceToHost, s));
+        GX_CK(cudaMemcpyAsync(sums_host, os, 8 * c, cudaMemcpyDeviceToHost, s));
+    }
+    cudaFreeAsync(scratch, s);
+    return wait_stream(s, 120.0);
+}
+
+// ------------------------------------------------------------------- scan
+
+static gx_status build_scan_params(const gx_scan_plan* plan, ScanParams* P, const gx_column** ref_col) {
+    if (!plan || plan->n_steps == 0 || plan->n_steps > GX_MAX_STEPS)
+        return set_error(GX_ERR_INVALID, "scan plan needs 1..%d steps", GX_MAX_STEPS);
+    std::memset(P, 0, sizeof(*P));
+    const gx_column* c0 = plan->steps[0].col;
+    if (!c0 || !c0->residency) return set_error(GX_ERR_INVALID, "step 0 column is not on the device");
+    bool any_value = false, any_digit = false, any_carry = false;
+    uint64_t card_prod = 1;
+    for (uint32_t i = 0; i < plan->n_steps; ++i) {
+        const gx_scan_step& s = plan->steps[i];
+        const gx_column* c = s.col;
+        if (!c || !c->residency) return set_error(GX_ERR_INVALID, "step %u column is not on the device", i);
+        if (c->n_rows != c0->n_rows || c->rows_per_chunk != c0->rows_per_chunk ||
+            c->rows_per_block != c0->rows_per_block)
+            return set_error(GX_ERR_INVALID, "step %u column layout differs from step 0", i);
+        if (s.flags == 0 || (s.flags & ~(uint32_t)(GX_STEP_FILTER | GX_STEP_PROBE | GX_STEP_CARRY | GX_STEP_VALUE)))
+            return set_error(GX_ERR_INVALID, "step %u has invalid flags", i);
+        ScanStep& d = P->steps[i];
+        d.col = c->view();
+        d.flags = s.flags;
+        d.lo = s.lo;
+        d.hi = s.hi;
+        if (s.flags & GX_STEP_PROBE) {
+            if (!s.ht) return set_error(GX_ERR_INVALID, "step %u probes a null hash table", i);
+            d.ht = s.ht->slots;
+            d.ht_log2 = s.ht->log2cap;
+            d.digit_base = s.digit_base;
+            d.digit_card = s.digit_card;
+            if (s.digit_card) {
+                d.first_digit = any_digit ? 0 : 1;
+                any_digit = true;
+                card_prod *= s.digit_card;
+                if (card_prod >= 0xFFFFFFFFull) return set_error(GX_ERR_INVALID, "group key space exceeds 2^32-1");
+            }
+        }
+        if (s.flags & GX_STEP_CARRY) any_carry = true;
+        if (s.flags & GX_STEP_VALUE) any_value = true;
+    }
+    if (!any_value) return set_error(GX_ERR_INVALID, "scan plan has no VALUE step");
+    if (plan->agg > GX_AGG_COUNT) return set_error(GX_ERR_INVALID, "unknown aggregate");
+    if (plan->agg == GX_AGG_SUM_PRODUCT && !any_carry) return set_error(GX_ERR_INVALID, "SUM_PRODUCT needs a CARRY step");
+    if (any_carry && any_digit) return set_error(GX_ERR_INVALID, "CARRY and group-key digits cannot be combined");
+    if (plan->groupby && !any_digit) return set_error(GX_ERR_INVALID, "grouped scan needs PROBE steps with digits");
+    if (!plan->groupby && !plan->result_dev) return set_error(GX_ERR_INVALID, "scan plan needs result_dev or groupby");
+    P->n_steps = plan->n_steps;
+    P->agg = plan->agg;
+    P->grouped = plan->groupby ? 1 : 0;
+    P->need_aux = (any_carry || any_digit) ? 1 : 0;
+    P->blocks_per_chunk = c0->blocks_per_chunk;
+    P->result = plan->result_dev;
+    if (plan->groupby) {
+        P->g_keys = plan->groupby->keys;
+        P->g_sums = plan->groupby->sums;
+        P->g_log2 = plan->groupby->log2cap;
+    }
+    *ref_col = c0;
+    return GX_OK;
+}
+
+static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned long long* rows_dev) {
+    ScanParams P;
+    const gx_column* c0 = nullptr;
+    gx_status st = build_scan_params(plan, &P, &c0);
+    if (st) return st;
+    const uint32_t n_chunks = c0->n_chunks;
+    uint32_t* scratch = nullptr;
+    GX_CK(cudaMallocAsync(&scratch, 4ull * (n_chunks + 4), s));
+    uint32_t* n_items = scratch;
+    uint32_t* counter = scratch + 1;
+    uint32_t* items = scratch + 4;
+    st = launch_items(nullptr, nullptr, nullptr, 0, n_chunks, plan->keep_chunks_dev, nullptr, items, n_items, counter, s);
+    if (st) {
+        cudaFreeAsync(scratch, s);
+        return st;
+    }
+    P.items = items;
+    P.n_items = n_items;
+    P.work_counter = counter;
+    P.rows_scanned = rows_dev;
+    const size_t smem = scan_smem_bytes(P.need_aux, P.grouped);
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr_set[dev & 63]) {
+        cudaError_t e = cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)scan_smem_bytes(true, true));
+        if (e != cudaSuccess) {
+            cudaFreeAsync(scratch, s);
+            return set_error(GX_ERR_CUDA, "cudaFuncSetAttribute(scan_kernel): %s", cudaGetErrorString(e));
+        }
+        attr_set[dev & 63] = true;
+    }
+    const uint32_t grid = std::min<uint32_t>((uint32_t)sm_count(), n_chunks * c0->blocks_per_chunk);
+    scan_kernel<<<std::max(1u, grid), kScanThreads, smem, s>>>(P);
+    cudaError_t e = cudaGetLastError();
+    cudaFreeAsync(scratch, s);
+    if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "scan_kernel launch: %s", cudaGetErrorString(e));
+    return GX_OK;
+}
+
+gx_status gx_scan(const gx_scan_plan* plan, void* stream) {
+    return scan_launch(plan, (cudaStream_t)stream, nullptr);
+}
+
+gx_status gx_scan_check(void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    int err = 0, zero = 0;
+    GX_CK(cudaMemcpyFromSymbolAsync(&err, g_gx_error, sizeof(int), 0, cudaMemcpyDeviceToHost, s));
+    gx_status st = wait_stream(s, 120.0);
+    if (st) return st;
+    if (err) {
+        GX_CK(cudaMemcpyToSymbolAsync(g_gx_error, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s));
+        GX_CK(cudaStreamSynchronize(s));
+        return set_error(err, "device reported %s", gx_status_str(err));
+    }
+    return GX_OK;
+}
+
+gx_status gx_scan_sync(const gx_scan_plan* plan, void* stream, uint64_t* rows_scanned) {
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned long long* rows = nullptr;
+    if (rows_scanned) {
+        GX_CK(cudaMallocAsync(&rows, 8, s));
+        GX_CK(cudaMemsetAsync(rows, 0, 8, s));
+    }
+    gx_status st = scan_launch(plan, s, rows);
+    if (!st && rows_scanned) {
+        unsigned long long r = 0;
+        cudaMemcpyAsync(&r, rows, 8, cudaMemcpyDeviceToHost, s);
+        st = wait_stream(s, 300.0);
+        *rows_scanned = r;
+    }
+    if (rows) cudaFreeAsync(rows, s);
+    if (st) return st;
+    return gx_scan_check(stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,144 @@
+"""The two query shapes of the hot path, built on the operator API.
+
+Q1 shape -- usecases/ssb/queries/01.hpp:54-449 (query1) with the kernel
+pipeline_q1_lineorder (01.cuh:27-54):
+    SUM(extended_price * discount) over fact JOIN date
+    WHERE <date predicate> AND discount in [dlo,dhi] AND quantity in [qlo,qhi]
+  pruning: min/max of date_key against the date range of the predicate
+  (the reference prunes with MetaChecker on its date metadata, 01.hpp:263-281)
+
+Q3 shape -- usecases/ssb/queries/03.hpp:80-592 (query3) with pipeline_q3
+(03.cuh:119-170):
+    SUM(revenue) GROUP BY (customer.nation, supplier.nation, year)
+    WHERE customer.region = r AND supplier.region = r AND year in [ylo,yhi]
+  probes in customer -> supplier -> date order, like the reference.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from .api import Column, HashAggregate, HashMap, MetaChecker, ScanPlan, _stream_handle
+
+
+def _dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@dataclass
+class FactTable:
+    cols: dict  # name -> Column (device resident)
+    n_rows: int
+
+
+def encode_fact(data: dict, codecs: dict, rows_per_chunk=1_000_000, rows_per_block=16384, lz4_segments=32,
+                residency="hbm", threads=0, **kw) -> FactTable:
+    cols = {}
+    for name, v in data.items():
+        c = Column(v, codecs.get(name, "lz4"), rows_per_chunk, rows_per_block, lz4_segments, threads=threads,
+                   name=name, **kw)
+        if residency:
+            c.to_device(residency)
+        cols[name] = c
+    return FactTable(cols, len(next(iter(data.values()))))
+
+
+class Q1Query:
+    """Q1-shaped fused scan over a FactTable with columns date_key, discount, quantity, extended_price."""
+
+    def __init__(self, fact: FactTable, date: dict, date_ok: np.ndarray, date_lo: int, date_hi: int,
+                 dlo: int, dhi: int, qlo: int, qhi: int, prune: bool = True):
+        import torch
+
+        self.fact = fact
+        self.ht = HashMap(max(1, int(date_ok.sum())))
+        self._dk = _dev(date["d_key"])
+        self._ok = _dev(date_ok.astype(np.int32))
+        self.ht.build(self._dk, None, preds=[(self._ok, 1, 1)])
+        self.prune = prune
+        n_chunks = fact.cols["date_key"].info.n_chunks
+        self.keep = torch.zeros(n_chunks, dtype=torch.uint16, device="cuda") if prune else None
+        self.checker = MetaChecker(n_chunks).add_minmax(fact.cols["date_key"], date_lo, date_hi)
+        self.result = torch.zeros(1, dtype=torch.int64, device="cuda")
+        c = fact.cols
+        self.plan = ScanPlan(agg=L.GX_AGG_SUM_PRODUCT, keep_chunks=self.keep, result=self.result)
+        self.plan.probe(c["date_key"], self.ht)
+        self.plan.filter(c["discount"], dlo, dhi, carry=True)
+        self.plan.filter(c["quantity"], qlo, qhi)
+        self.plan.value(c["extended_price"])
+        self.plan.to_c()
+
+    def launch(self, stream=None):
+        """Enqueue: clear result, prune, fused scan (no host synchronisation)."""
+        self.result.zero_()
+        if self.prune:
+            self.checker.run(self.keep, stream)
+        self.plan.launch(stream)
+
+    def run(self, stream=None) -> int:
+        self.launch(stream)
+        from .api import scan_check
+
+        scan_check(stream)
+        return int(self.result.item())
+
+
+class Q3Query:
+    """Q3-shaped star join + group-by over a FactTable with cust_key, supp_key, date_key, revenue."""
+
+    def __init__(self, fact: FactTable, customer: dict, supplier: dict, date: dict, region: int, ylo: int, yhi: int,
+                 prune: bool = True, n_nations: int = 25):
+        import torch
+
+        self.fact = fact
+        self.n_nations = n_nations
+        self.ylo, self.yhi = ylo, yhi
+        # tables sized for the rows that pass the dimension filters
+        self.hc = HashMap(max(1, int((customer["region"] == region).sum())))
+        self.hs = HashMap(max(1, int((supplier["region"] == region).sum())))
+        self.hd = HashMap(max(1, int(((date["d_year"] >= ylo) & (date["d_year"] <= yhi)).sum())))
+        self._keep_alive = [_dev(customer["key"]), _dev(customer["nation"]), _dev(customer["region"]),
+                            _dev(supplier["key"]), _dev(supplier["nation"]), _dev(supplier["region"]),
+                            _dev(date["d_key"]), _dev(date["d_year"])]
+        ck, cn, cr, sk, sn, sr, dk, dy = self._keep_alive
+        self.hc.build(ck, cn, preds=[(cr, region, region)])
+        self.hs.build(sk, sn, preds=[(sr, region, region)])
+        self.hd.build(dk, dy, preds=[(dy, ylo, yhi)])
+        n_chunks = fact.cols["date_key"].info.n_chunks
+        self.prune = prune
+        self.keep = torch.zeros(n_chunks, dtype=torch.uint16, device="cuda") if prune else None
+        self.checker = MetaChecker(n_chunks).add_minmax(fact.cols["date_key"], ylo * 10000 + 101, yhi * 10000 + 1231)
+        self.ycard = yhi - ylo + 1
+        self.agg = HashAggregate(n_nations * n_nations * self.ycard)
+        c = fact.cols
+        self.plan = ScanPlan(agg=L.GX_AGG_SUM, keep_chunks=self.keep, groupby=self.agg)
+        self.plan.probe(c["cust_key"], self.hc, 0, n_nations)
+        self.plan.probe(c["supp_key"], self.hs, 0, n_nations)
+        self.plan.probe(c["date_key"], self.hd, ylo, self.ycard)
+        self.plan.value(c["revenue"])
+        self.plan.to_c()
+
+    def launch(self, stream=None):
+        self.agg.reset(stream)
+        if self.prune:
+            self.checker.run(self.keep, stream)
+        self.plan.launch(stream)
+
+    def decode_key(self, k: int):
+        y = k % self.ycard
+        s = (k // self.ycard) % self.n_nations
+        c = k // (self.ycard * self.n_nations)
+        return c, s, self.ylo + y
+
+    def run(self, stream=None) -> dict:
+        """{(c_nation, s_nation, year): sum} after synchronising."""
+        self.launch(stream)
+        from .api import scan_check
+
+        scan_check(stream)
+        raw = self.agg.read(stream=stream)
+        return {self.decode_key(k): v for k, v in raw.items()}

@@ -1,0 +1,258 @@
+/*
+ * gx.h -- C-ABI of the B200-native GOLAP query hot path.
+ *
+ * Plain pointers and sizes only.  Every entry point returns a gx_status
+ * (0 == GX_OK); on failure a thread-local message is available through
+ * gx_last_error().  No entry point exits the process, and no device wait is
+ * unbounded: kernels that spin carry an iteration cap and report
+ * GX_ERR_TIMEOUT through a device error word that the host reads.
+ *
+ * Each declaration names the reference interface it replaces (paths are
+ * relative to the GOLAP source tree).  The C++ drop-in layer in
+ * include/golap_compat/ re-exposes those reference class names on top of
+ * these calls.
+ *
+ * Streams are passed as `void*` (a cudaStream_t); NULL is the legacy default
+ * stream.  "dev" pointers are device (or device-mapped) addresses.
+ */
+#ifndef GX_H
+#define GX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+
+typedef int32_t gx_status;
+enum {
+    GX_OK = 0,
+    GX_ERR_CUDA = 1,     /* a CUDA runtime call failed                         */
+    GX_ERR_CORRUPT = 2,  /* a compressed block failed validation               */
+    GX_ERR_CAPACITY = 3, /* a hash/group table or work list ran out of room    */
+    GX_ERR_TIMEOUT = 4,  /* a bounded device or host wait gave up              */
+    GX_ERR_NOMEM = 5,    /* allocation failed / admission budget exceeded      */
+    GX_ERR_INVALID = 6   /* bad argument                                       */
+};
+
+/* Text for a status code (static storage). */
+const char* gx_status_str(gx_status s);
+/* Copy this thread's last error message into buf (NUL-terminated); returns its length. */
+size_t gx_last_error(char* buf, size_t cap);
+/* Library version string, and the CUDA device count the library sees. */
+const char* gx_version(void);
+gx_status gx_device_count(int* count);
+
+/* ------------------------------------------------------- column encoding
+ * Replaces: CompInfo / BlockInfo (core/comp.cuh:23-78), ChunkCompressor
+ * (core/comp.cuh:81-148), prepare_compressed (core/apps.cuh:149-255) and the
+ * per-chunk MinMaxMeta::init_chunk collection (core/metadata.cuh:157-160).
+ *
+ * A column is split into chunks of rows_per_chunk rows; each chunk into blocks
+ * of rows_per_block rows (blocks never straddle chunks).  Every block of every
+ * column of a table covers the same rows, so a (chunk, block) pair addresses
+ * one row tile across all columns.
+ */
+enum {
+    GX_CODEC_NONE = 0,     /* raw little-endian int32                            */
+    GX_CODEC_LZ4 = 1,      /* LZ4 block format, one block per rows_per_block     */
+    GX_CODEC_CASCADED = 2  /* RLE + delta + frame-of-reference bit-packing       */
+};
+
+typedef struct gx_encode_opts {
+    uint32_t codec;            /* GX_CODEC_*                                             */
+    uint32_t rows_per_chunk;   /* default 1,000,000                                      */
+    uint32_t rows_per_block;   /* default 16,384 (64 KiB of int32)                       */
+    uint32_t lz4_segments;     /* independent decode segments per LZ4 block (1..128);
+                                  1 = plain LZ4 (one serial stream per block)             */
+    uint32_t lz4_min_match;    /* minimum match length in bytes (multiple of 4, >= 4)    */
+    uint32_t lz4_search_depth; /* hash-chain candidates examined per position            */
+    uint32_t casc_rle;         /* cascaded: allow run-length encoding                    */
+    uint32_t casc_delta;       /* cascaded: allow delta encoding                         */
+    uint32_t casc_bitpack;     /* cascaded: allow bit-packing (else 32-bit words)        */
+    uint32_t threads;          /* host encoder threads (0 = hardware concurrency)        */
+} gx_encode_opts;
+
+typedef struct gx_column gx_column;
+
+typedef struct gx_column_info {
+    uint64_t n_rows;
+    uint64_t comp_bytes;       /* payload bytes incl. per-block headers/side indexes   */
+    uint64_t uncomp_bytes;     /* n_rows * 4                                            */
+    uint64_t meta_bytes;       /* block directory + min/max bytes                        */
+    uint32_t codec;
+    uint32_t rows_per_chunk;
+    uint32_t rows_per_block;
+    uint32_t n_chunks;
+    uint32_t blocks_per_chunk;
+    uint32_t n_blocks;
+    uint32_t lz4_segments;
+    uint32_t on_device;        /* 0 none, 1 HBM, 2 pinned host (device-mapped)          */
+} gx_column_info;
+
+/* One compressed block (the reference BlockInfo, core/comp.cuh:23-32). */
+typedef struct gx_block_info {
+    uint64_t offset;   /* byte offset of the block in the column payload */
+    uint64_t size;     /* bytes reserved for the block (16-byte aligned)  */
+    uint64_t payload;  /* bytes actually used by the compressed block     */
+    uint64_t tuples;   /* rows in the block                               */
+} gx_block_info;
+
+gx_status gx_encode_opts_default(gx_encode_opts* opts);
+/* Encode n_rows int32 values from host memory into a new column (host side). */
+gx_status gx_column_encode(const int32_t* host_values, uint64_t n_rows,
+                           const gx_encode_opts* opts, gx_column** out);
+gx_status gx_column_free(gx_column* col);
+gx_status gx_column_info_get(const gx_column* col, gx_column_info* out);
+/* Per-chunk min/max (host arrays of n_chunks entries; MinMaxMeta mins_hst/maxs_hst). */
+gx_status gx_column_chunk_minmax(const gx_column* col, int32_t* mins, int32_t* maxs);
+/* Per-block descriptors (host array of n_blocks entries). */
+gx_status gx_column_blocks(const gx_column* col, gx_block_info* out);
+/* Raw access to the host copy of the compressed payload and the LZ4 segment
+ * index (for CPU-side checkers).  Pointers stay valid until gx_column_free. */
+gx_status gx_column_payload(const gx_column* col, const uint8_t** payload, uint64_t* bytes);
+gx_status gx_column_seg_index(const gx_column* col, const uint32_t** words, uint64_t* n_words);
+/* Copy the compressed column to the device.  residency 1 = HBM, 2 = pinned
+ * host memory mapped into the device address space (zero-copy reads). */
+gx_status gx_column_to_device(gx_column* col, int residency, void* stream);
+gx_status gx_column_release_device(gx_column* col);
+
+/* ------------------------------------------------------------ decompression
+ * Replaces: ChunkDecompressor::step (core/comp.cuh:151-227, nvCOMP decompress
+ * at :186).  Writes the decoded int32 rows of the given chunks to dst_dev. */
+gx_status gx_decompress_chunk(const gx_column* col, uint64_t chunk_idx, void* dst_dev, void* stream);
+gx_status gx_decompress_chunks(const gx_column* col, uint64_t first_chunk, uint64_t n_chunks,
+                               void* dst_dev, void* stream);
+/* Decode independent raw LZ4 blocks produced by any conforming LZ4 encoder
+ * (e.g. liblz4's LZ4_compress_default, as LZ4CPUManager::compress does at
+ * core/comp_cpu.hpp:28-31).  comp_offsets/out_offsets have n_blocks+1 entries
+ * (device arrays).  status_dev (n_blocks int32, device) receives 0 or
+ * GX_ERR_CORRUPT per block. */
+gx_status gx_lz4_decompress_raw(const uint8_t* comp_dev, const uint64_t* comp_offsets_dev,
+                                uint8_t* out_dev, const uint64_t* out_offsets_dev,
+                                uint64_t n_blocks, int32_t* status_dev, void* stream);
+
+/* ------------------------------------------------------------------ pruning
+ * Replaces: MinMaxMeta::check_pred (core/metadata.cuh:203-211), check_mmmeta
+ * (core/metadata.cuh:540-547), combine_and (:632-636) and
+ * MetaChecker::add_minmax (:645-658).  Inclusive overlap test
+ * lo <= chunk_max && hi >= chunk_min; flag 1 = keep. */
+
+/* check_mmmeta semantics: sets out_dev[c] = 1 where the chunk overlaps [lo,hi],
+ * leaves other entries untouched. */
+gx_status gx_check_minmax(const gx_column* col, int32_t lo, int32_t hi,
+                          uint16_t* out_dev, void* stream);
+/* out = a & b over n entries (combine_and). */
+gx_status gx_combine_and(uint16_t* out_dev, const uint16_t* a_dev, const uint16_t* b_dev,
+                         uint64_t n, void* stream);
+/* Whole MetaChecker pass in one launch: keep_dev[c] = AND over predicates. */
+gx_status gx_prune_minmax(const gx_column* const* cols, const int32_t* lo, const int32_t* hi,
+                          uint32_t n_preds, uint16_t* keep_dev, void* stream);
+
+/* --------------------------------------------------------------- hash join
+ * Replaces: HashMap (core/dev_structs.cuh:37-132) with its filtered build
+ * hash_map_build_pred_other (core/join.cuh:107-135) and the probe kernels
+ * hash_join_count / hash_join_rids (core/join.cuh:46-97).  The table is
+ * open addressing with linear probing over 64-bit slots {key, payload};
+ * keys are unique on the build side (dimension keys), as in every reference
+ * use.  Probing returns the payload of the matching key or "miss". */
+typedef struct gx_hashtable gx_hashtable;
+
+/* Conjunctive range predicate on a dimension column (PredInfo, core/dev_structs.cuh:22-26). */
+typedef struct gx_pred {
+    const int32_t* col_dev;
+    int32_t lo;
+    int32_t hi;
+} gx_pred;
+
+gx_status gx_hashtable_create(uint64_t max_entries, gx_hashtable** out);
+gx_status gx_hashtable_free(gx_hashtable* ht);
+/* Clear, then insert (keys[i], payload[i] or i when payload_dev == NULL) for
+ * every row i < n that passes all predicates.  Duplicate keys: the first
+ * inserted wins for probing, later ones are counted as dropped. */
+gx_status gx_hashtable_build(gx_hashtable* ht, const int32_t* keys_dev, const int32_t* payload_dev,
+                             uint64_t n, const gx_pred* preds, uint32_t n_preds, void* stream);
+/* Number of inserted entries (host, synchronises the stream). */
+gx_status gx_hashtable_count(const gx_hashtable* ht, uint64_t* n_entries, void* stream);
+/* For each probe key: payload_out[i] = payload or INT32_MIN on a miss
+ * (payload_out may be NULL); *hits_dev += number of hits (may be NULL). */
+gx_status gx_hashtable_probe(const gx_hashtable* ht, const int32_t* keys_dev, uint64_t n,
+                             int32_t* payload_out_dev, uint64_t* hits_dev, void* stream);
+
+/* ---------------------------------------------------------- hash aggregate
+ * Replaces: HashAggregate (core/dev_structs.cuh:158-253) with SumAgg
+ * (usecases/ssb/queries/query_common.cuh:24-29) and the group_by_agg kernels
+ * (core/group.cuh:15-36).  Open addressing over int64 keys, int64 sums. */
+typedef struct gx_groupby gx_groupby;
+
+gx_status gx_groupby_create(uint64_t max_groups, gx_groupby** out);
+gx_status gx_groupby_free(gx_groupby* gb);
+gx_status gx_groupby_reset(gx_groupby* gb, void* stream);
+/* sums[key] += vals[i] for i < n (device arrays). */
+gx_status gx_groupby_add(gx_groupby* gb, const int64_t* keys_dev, const int64_t* vals_dev,
+                         uint64_t n, void* stream);
+/* Copy the non-empty groups to host arrays (unordered); *n_groups = count.
+ * Fails with GX_ERR_CAPACITY if cap is too small or the table overflowed. */
+gx_status gx_groupby_read(gx_groupby* gb, int64_t* keys_host, int64_t* sums_host, uint64_t cap,
+                          uint64_t* n_groups, void* stream);
+
+/* -------------------------------------------------------------- fused scan
+ * Replaces: ChunkDecompressor + pipeline_q1_lineorder
+ * (usecases/ssb/queries/01.cuh:27-54) and ChunkDecompressor +
+ * pipeline_q3 (usecases/ssb/queries/03.cuh:119-170), driven per chunk by the
+ * worker loops of usecases/ssb/queries/01.hpp:350-424 and 03.hpp:487-547.
+ *
+ * A plan is an ordered list of column steps over one fact table.  For every
+ * row tile that survives pruning, one kernel decodes each referenced column
+ * into shared memory, applies the steps in order, and aggregates.
+ *   FILTER  : keep rows with lo <= v <= hi
+ *   PROBE   : keep rows whose value is a key of ht; if digit_card > 0 the
+ *             payload p extends the group key: g = g*digit_card + (p-digit_base)
+ *   CARRY   : remember v for the product aggregate
+ *   VALUE   : aggregate v (times the carried value when agg == SUM_PRODUCT)
+ * Flags may be OR-ed (FILTER|CARRY).  The aggregate is int64:
+ * a scalar sum (groupby == NULL) or sums per group key. */
+enum {
+    GX_STEP_FILTER = 1,
+    GX_STEP_PROBE = 2,
+    GX_STEP_CARRY = 4,
+    GX_STEP_VALUE = 8
+};
+enum { GX_AGG_SUM = 0, GX_AGG_SUM_PRODUCT = 1, GX_AGG_COUNT = 2 };
+
+#define GX_MAX_STEPS 8
+
+typedef struct gx_scan_step {
+    const gx_column* col;
+    uint32_t flags;              /* GX_STEP_*                                  */
+    int32_t lo, hi;              /* FILTER bounds (inclusive)                  */
+    const gx_hashtable* ht;      /* PROBE table                                */
+    int32_t digit_base;          /* PROBE: payload offset for the group key    */
+    uint32_t digit_card;         /* PROBE: payload cardinality (0 = no digit)  */
+} gx_scan_step;
+
+typedef struct gx_scan_plan {
+    uint32_t n_steps;
+    gx_scan_step steps[GX_MAX_STEPS];
+    uint32_t agg;                     /* GX_AGG_*                                */
+    const uint16_t* keep_chunks_dev;  /* per-chunk keep flags or NULL (scan all) */
+    gx_groupby* groupby;              /* NULL = scalar result                    */
+    int64_t* result_dev;              /* scalar result (int64, device)           */
+} gx_scan_plan;
+
+/* Run the plan on `stream`.  Does not clear result_dev or the group table
+ * (callers accumulate across calls, like the reference's atomics). */
+gx_status gx_scan(const gx_scan_plan* plan, void* stream);
+/* Same, then synchronise and report device-side errors (corrupt blocks,
+ * table overflow).  *rows_scanned (optional) = rows in surviving tiles. */
+gx_status gx_scan_sync(const gx_scan_plan* plan, void* stream, uint64_t* rows_scanned);
+/* Read and clear the device error word of the scan engine. */
+gx_status gx_scan_check(void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GX_H */

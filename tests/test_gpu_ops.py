@@ -1,0 +1,125 @@
+"""GPU operators against the oracle and the reference's own known answers:
+min/max pruning (core/test/metadata_tests.cu), join count/probe
+(core/test/join_tests.cu:71-107), group-by sums
+(core/test/group_by_tests.cu:75-132)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from golap_public_b200 import _lib as L
+from golap_public_b200 import api
+from golap_public_b200._lib import GxError
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def test_check_minmax_and_combine(cuda):
+    rng = np.random.default_rng(4)
+    v = np.sort(rng.integers(0, 10_000, 2_000_000, dtype=np.int32))
+    col = api.Column(v, "cascaded", rows_per_chunk=50_000).to_device()
+    mins, maxs = col.minmax()
+    n = col.info.n_chunks
+    for lo, hi in [(0, 0), (5000, 5000), (-10, -1), (9999, 20000), (1234, 4321), (10_000, 10_000)]:
+        flags = cuda.zeros(n, dtype=cuda.uint16, device="cuda")
+        L.check(L.lib().gx_check_minmax(col.handle, lo, hi, C.c_void_p(flags.data_ptr()), None))
+        cuda.cuda.synchronize()
+        assert flags.cpu().numpy().tolist() == O.minmax_keep(mins, maxs, lo, hi).tolist()
+    a = cuda.zeros(n, dtype=cuda.uint16, device="cuda")
+    b = cuda.zeros(n, dtype=cuda.uint16, device="cuda")
+    L.check(L.lib().gx_check_minmax(col.handle, 0, 6000, C.c_void_p(a.data_ptr()), None))
+    L.check(L.lib().gx_check_minmax(col.handle, 4000, 9000, C.c_void_p(b.data_ptr()), None))
+    L.check(L.lib().gx_combine_and(C.c_void_p(a.data_ptr()), C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()), n, None))
+    cuda.cuda.synchronize()
+    want = O.minmax_keep(mins, maxs, 4000, 9000, keep=O.minmax_keep(mins, maxs, 0, 6000))
+    assert a.cpu().numpy().tolist() == want.tolist()
+
+
+def test_metachecker_known_answers(cuda):
+    # integer version of core/test/metadata_tests.cu:210-272: three chunks of 8
+    # rows, {h0..h7}, {h8..h15}, {Dec1996/Feb1992} -> {0..7}, {8..15}, {1992,1996}
+    v = np.array(list(range(16)) + [1996, 1992] * 4, np.int32)
+    col = api.Column(v, "lz4", rows_per_chunk=8, rows_per_block=8, lz4_segments=1).to_device()
+    keep = cuda.zeros(3, dtype=cuda.uint16, device="cuda")
+    for lo, hi, want in [(5, 5, [1, 0, 0]), (15, 15, [0, 1, 0]), (1997, 1997, [0, 0, 0]), (1992, 1992, [0, 0, 1]),
+                         (7, 1993, [1, 1, 1])]:
+        api.MetaChecker(3).add_minmax(col, lo, hi).run(keep)
+        assert keep.cpu().tolist() == want
+    api.MetaChecker(3).add_minmax(col, 0, 100).add_minmax(col, 8, 2000).run(keep)
+    assert keep.cpu().tolist() == [0, 1, 1]
+
+
+def test_join_count_1to1(cuda):
+    # join_tests.cu:71-107: build 500k ids, probe 10M rows id = i % 500k -> 10M hits
+    build = cuda.arange(500_000, dtype=cuda.int32, device="cuda")
+    probe = (cuda.arange(10_000_000, dtype=cuda.int64, device="cuda") % 500_000).to(cuda.int32)
+    hm = api.HashMap(500_000).build(build)
+    assert hm.count() == 500_000
+    hits = cuda.zeros(1, dtype=cuda.int64, device="cuda")
+    pay = cuda.empty(10_000_000, dtype=cuda.int32, device="cuda")
+    hm.probe(probe, pay, hits)
+    assert int(hits.item()) == 10_000_000
+    assert cuda.equal(pay, probe)  # payload defaults to the build row id
+
+
+def test_filtered_build_and_probe_vs_oracle(cuda):
+    rng = np.random.default_rng(8)
+    n_b, n_p = 200_000, 3_000_000
+    keys = rng.permutation(np.arange(1, 4 * n_b, 4, dtype=np.int32))[:n_b]
+    region = rng.integers(0, 5, n_b, dtype=np.int32)
+    nation = rng.integers(0, 25, n_b, dtype=np.int32)
+    probe = rng.integers(0, 4 * n_b + 10, n_p, dtype=np.int32)
+    kd, rd, nd, pd = (cuda.from_numpy(x).cuda() for x in (keys, region, nation, probe))
+    hm = api.HashMap(n_b).build(kd, nd, preds=[(rd, 2, 3)])
+    ok = (region >= 2) & (region <= 3)
+    assert hm.count() == int(ok.sum())
+    out = cuda.empty(n_p, dtype=cuda.int32, device="cuda")
+    hits = cuda.zeros(1, dtype=cuda.int64, device="cuda")
+    hm.probe(pd, out, hits)
+    rid = O.join_probe(keys, ok, probe)
+    want = np.where(rid >= 0, nation[np.maximum(rid, 0)], np.iinfo(np.int32).min)
+    assert np.array_equal(out.cpu().numpy(), want)
+    assert int(hits.item()) == int((rid >= 0).sum())
+
+
+def test_hashtable_reserved_key_and_capacity(cuda):
+    keys = cuda.tensor([1, 2, np.iinfo(np.int32).min, 3], dtype=cuda.int32, device="cuda")
+    hm = api.HashMap(4).build(keys)
+    with pytest.raises(GxError) as e:
+        hm.count()
+    assert e.value.status == L.GX_ERR_CAPACITY
+    # more keys than max_entries: reported, never hangs
+    many = cuda.arange(100, dtype=cuda.int32, device="cuda")
+    hm2 = api.HashMap(8).build(many)
+    with pytest.raises(GxError):
+        hm2.count()
+
+
+def test_groupby_exact_sums(cuda):
+    # group_by_tests.cu:75-132 at 2^27 rows: 64 groups, each sums to 2^27/64
+    n, g = 1 << 27, 64
+    keys = cuda.arange(n, dtype=cuda.int64, device="cuda") % g
+    vals = cuda.ones(n, dtype=cuda.int64, device="cuda")
+    agg = api.HashAggregate(g)
+    agg.add(keys, vals)
+    res = agg.read()
+    assert len(res) == g and all(v == n // g for v in res.values())
+    del keys, vals
+
+
+def test_groupby_vs_oracle_and_overflow(cuda):
+    rng = np.random.default_rng(12)
+    k = rng.integers(0, 5000, 2_000_000).astype(np.int64)
+    v = rng.integers(-10**9, 10**9, 2_000_000).astype(np.int64)
+    agg = api.HashAggregate(5000)
+    agg.add(cuda.from_numpy(k).cuda(), cuda.from_numpy(v).cuda())
+    got = agg.read()
+    want = np.zeros(5000, np.int64)
+    assert O.lib().or_group_sum_dense(O._ptr(k), O._ptr(v), len(k), O._ptr(want), 5000) == 0
+    assert got == {i: int(want[i]) for i in range(5000) if (k == i).any()}
+    small = api.HashAggregate(10)  # 32 slots
+    small.add(cuda.from_numpy(k[:1000]).cuda(), cuda.from_numpy(v[:1000]).cuda())
+    with pytest.raises(GxError) as e:
+        api.scan_check()
+    assert e.value.status == L.GX_ERR_CAPACITY
