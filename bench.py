@@ -1,0 +1,427 @@
+"""Benchmark of the fused compressed-scan hot path on B200.
+
+Workload (one step = one query): a 60,000,000-row fact table sorted by
+date_key, compressed per 1,000,000-row chunk (date_key cascaded, discount /
+quantity / extended_price LZ4 on 64 KiB blocks), per-chunk min/max; the
+query is SUM(extended_price * discount) over fact JOIN date WHERE the date
+is in January 1994 AND discount BETWEEN 4 AND 6 AND quantity BETWEEN 26 AND
+35.  A step builds the filtered date hash table, prunes chunks on min/max
+and runs the fused scan; the int64 result stays on the device (value) or
+comes back to the host (e2e).  Data is seeded synthetic data with the
+workload's shapes and distributions.
+
+  value     rows/s over the whole table (pruned chunks count, as in the
+            reference's uncompressed-bytes / time definition), compressed
+            columns resident in HBM, device time (CUDA events) per step,
+            L2 flushed between steps.
+  e2e       the same query with the compressed columns in pinned host
+            memory, read by the kernels over PCIe, timed through the public
+            API with the date dimension copied in and the result read back.
+  roofline  the fused scan kernel: algorithmic bytes (compressed bytes of
+            the surviving tiles + their directory/segment index) per launch
+            / launch time, against the measured HBM copy bandwidth.
+  cpu_baseline  the reference's CPU path on the same data: LZ4CPUManager
+            decompression + the query loop over HostHashMap, all host cores.
+
+--impl reference runs only the CPU path (rank 0) and prints its line.
+--gpus N runs N independent replicas (one per GPU; the query does not need
+a collective); value is the total over ranks, time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_ROWS = 60_000_000
+ROWS_PER_CHUNK = 1_000_000
+ROWS_PER_BLOCK = 16384
+DATE_LO, DATE_HI = 19940101, 19940131
+DISC = (4, 6)
+QTY = (26, 35)
+WORKLOAD = ("Q1 shape on 60M rows sorted by date_key: date_key cascaded, discount/quantity/extended_price "
+            "LZ4 on 64 KiB blocks, 1M-row chunks with min/max; month Jan 1994, discount 4..6, quantity 26..35")
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per scan_kernel launch from the committed ncu summary (or None)."""
+    p = ROOT / "profiles" / "scan_kernel_q1_config1.md"
+    if not p.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", p.read_text())
+    return int(m.group(1)) if m else None
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_bench_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 7 and f[0].isdigit():
+                rows.append(f)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [int(r[0]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": int(rows[0][1]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def make_data(seed):
+    from golap_public_b200 import datagen
+
+    return datagen.fact_q1(N_ROWS, True, seed=seed), datagen.date_dim()
+
+
+# ----------------------------------------------------------------- GPU arm
+
+def gpu_arm(args, rank, world):
+    import torch
+    import torch.distributed as dist
+
+    from golap_public_b200 import api, queries
+    from golap_public_b200.build import build
+
+    build()
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    f, dd = make_data(args.seed)
+    ok = dd["d_yearmonthnum"] == 199401
+    fact = queries.encode_fact(f, {"date_key": "cascaded"}, ROWS_PER_CHUNK, ROWS_PER_BLOCK, args.segments)
+    comp = {k: c.info.comp_bytes for k, c in fact.cols.items()}
+
+    q = queries.Q1Query(fact, dd, ok, DATE_LO, DATE_HI, *DISC, *QTY, prune=True)
+    want = None
+    if not args.no_check:
+        from oracle import oracle as O
+
+        want = O.q1(f["date_key"], f["discount"], f["quantity"], f["extended_price"], dd["d_key"], ok, *DISC, *QTY)
+    dk_h = torch.from_numpy(dd["d_key"]).pin_memory()
+    ok_h = torch.from_numpy(ok.astype(np.int32)).pin_memory()
+    dk_d = torch.empty_like(dk_h, device="cuda")
+    ok_d = torch.empty_like(ok_h, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        # the per-query work of the reference's query1 timed region
+        # (01.hpp:235-430): date table build, pruning, fused scan
+        q.ht.build(q._dk, None, preds=[(q._ok, 1, 1)])
+        q.launch()
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    got = q.run()
+    if want is not None and got != want:
+        raise SystemExit(f"result mismatch: gpu {got} oracle {want}")
+    kept = int(q.keep.sum().item())
+    kept_chunks = np.nonzero(q.keep.cpu().numpy())[0].tolist()
+
+    # algorithmic bytes of the scan per launch: compressed bytes of the
+    # surviving tiles of the 4 columns + their block directory and segment
+    # index entries + the date_key min/max read by pruning
+    def alg_bytes(chunks):
+        tot = 0
+        for name, c in fact.cols.items():
+            info = c.info
+            b = c.blocks()
+            per_chunk = info.blocks_per_chunk
+            for ch in chunks:
+                sel = b[ch * per_chunk:(ch + 1) * per_chunk]
+                tot += int(sel[:, 2].sum()) + 16 * len(sel) + (8 * info.lz4_segments * len(sel) if info.lz4_segments > 1 else 0)
+        return tot + 8 * fact.cols["date_key"].info.n_chunks
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(dev) as clk:
+        t_wall = time.perf_counter()
+        for i in range(args.steps):
+            flush.zero_()  # evict the previous step's tiles from L2 (untimed)
+            a, b, c = ev[i]
+            a.record(stream)
+            q.ht.build(q._dk, None, preds=[(q._ok, 1, 1)])
+            q.result.zero_()
+            q.checker.run(q.keep)
+            b.record(stream)
+            q.plan.launch()
+            c.record(stream)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall
+    if world > 1:
+        dist.barrier()
+    step_ms = [a.elapsed_time(c) for a, b, c in ev]
+    scan_ms = [b.elapsed_time(c) for a, b, c in ev]
+    ms = float(np.mean(step_ms))
+    scan_avg = float(np.mean(scan_ms))
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # full-table scan (pruning off): the decode-bound throughput of the same kernel
+    q_all = queries.Q1Query(fact, dd, ok, DATE_LO, DATE_HI, *DISC, *QTY, prune=False)
+    if want is not None:
+        assert q_all.run() == want
+    for _ in range(3):
+        q_all.launch()
+    all_ms = []
+    for _ in range(max(3, min(args.steps, 10))):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        q_all.result.zero_()
+        a.record(stream)
+        q_all.plan.launch()
+        b.record(stream)
+        torch.cuda.synchronize()
+        all_ms.append(a.elapsed_time(b))
+    all_ms_avg = float(np.mean(all_ms))
+    all_bytes = alg_bytes(range(fact.cols["date_key"].info.n_chunks))
+
+    # e2e: pinned-host residency, date dimension in, result out
+    fact_h = queries.encode_fact(f, {"date_key": "cascaded"}, ROWS_PER_CHUNK, ROWS_PER_BLOCK, args.segments,
+                                 residency="pinned")
+    qh = queries.Q1Query(fact_h, dd, ok, DATE_LO, DATE_HI, *DISC, *QTY, prune=True)
+    res_h = torch.zeros(1, dtype=torch.int64).pin_memory()
+    h2d_scan = alg_bytes(kept_chunks) - 8 * fact.cols["date_key"].info.n_chunks
+
+    def e2e_step():
+        dk_d.copy_(dk_h, non_blocking=True)
+        ok_d.copy_(ok_h, non_blocking=True)
+        qh.ht.build(dk_d, None, preds=[(ok_d, 1, 1)])
+        qh.launch()
+        res_h.copy_(qh.result, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    if want is not None and int(res_h.item()) != want:
+        raise SystemExit("e2e result mismatch")
+    e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e2e_step()
+        b.record(stream)
+        b.synchronize()
+        e_ms.append(a.elapsed_time(b))
+    e2e_ms = float(np.mean(e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    pk, pk_kind = peaks()
+    scan_bytes = alg_bytes(kept_chunks)
+    achieved = scan_bytes / (scan_avg * 1e-3) / 1e9
+    line = {
+        "metric": "rows/s & GB/s vs HBM roofline; p50/p99 latency batched vs one-query-at-a-time",
+        "value": N_ROWS * world / (ms * 1e-3),
+        "unit": "rows/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int32",
+        "data": "synthetic (seeded, configs[1] shapes and distributions)",
+        "config": {"workload": WORKLOAD, "rows": N_ROWS, "chunks": 60, "chunks_scanned": kept,
+                   "lz4_segments": args.segments, "residency": "hbm", "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}", "comp_bytes": comp},
+        "result": got,
+        "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
+        "scan_kernel_ms": scan_avg,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk, "unit": "GB/s", "frac": achieved / pk,
+                     "traffic": profile_traffic(), "peak_kind": pk_kind,
+                     "algorithmic_bytes_per_launch": scan_bytes},
+        "full_scan": {"ms": all_ms_avg, "rows_per_s": N_ROWS / (all_ms_avg * 1e-3),
+                      "comp_gbs": all_bytes / (all_ms_avg * 1e-3) / 1e9,
+                      "roofline_frac": all_bytes / (all_ms_avg * 1e-3) / 1e9 / pk,
+                      "uncomp_gbs": N_ROWS * 16 / (all_ms_avg * 1e-3) / 1e9},
+        "e2e": {"value": N_ROWS * world / (e2e_ms * 1e-3), "unit": "rows/s",
+                "h2d_bytes_per_step": int(h2d_scan + dd["d_key"].nbytes + ok.astype(np.int32).nbytes),
+                "d2h_bytes_per_step": 8, "ms_per_step": e2e_ms, "residency": "pinned host (zero-copy reads)"},
+        "gpu_launches": 5 * args.steps,
+        "clocks": clk.summary(),
+        "wall_s_timed": t_wall,
+    }
+    return line, f, dd
+
+
+# ----------------------------------------------------------------- CPU arm
+
+def cpu_baseline(f, dd, steps=3, warmup=1, threads=None):
+    """The reference's CPU path on the same data (see ref_cpu_q1 in oracle/ref_harness.cu)."""
+    from oracle import oracle as O
+
+    threads = threads or os.cpu_count() or 1
+    ok = (dd["d_yearmonthnum"] == 199401).astype(np.uint8)
+    n_chunks = N_ROWS // ROWS_PER_CHUNK
+    bpc = -(-ROWS_PER_CHUNK // ROWS_PER_BLOCK)
+    mins, maxs = O.chunk_minmax(f["date_key"], ROWS_PER_CHUNK)
+    kind = "reference" if O.ref_available() else "port"
+    if kind == "port":
+        t = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            keep = O.minmax_keep(mins, maxs, DATE_LO, DATE_HI)
+            r = O.q1(f["date_key"], f["discount"], f["quantity"], f["extended_price"], dd["d_key"], ok, *DISC, *QTY,
+                     keep_chunk=keep, rows_per_chunk=ROWS_PER_CHUNK)
+            t.append(time.perf_counter() - t0)
+        ms = 1e3 * float(np.mean(t))
+        return {"value": N_ROWS / (ms * 1e-3), "unit": "rows/s", "cores": 1, "kind": "port",
+                "sample": "full query (oracle restatement, 1 thread)", "ms": ms, "result": r}
+    R = O.ref()
+    stride = ROWS_PER_BLOCK * 4 + ROWS_PER_BLOCK * 4 // 255 + 64
+    comp, sizes = [], []
+    for name in ("discount", "quantity", "extended_price"):
+        v = f[name]
+        buf = np.zeros(n_chunks * bpc * stride, np.uint8)
+        sz = np.zeros(n_chunks * bpc, np.int32)
+        for c in range(n_chunks):
+            part = np.ascontiguousarray(v[c * ROWS_PER_CHUNK:(c + 1) * ROWS_PER_CHUNK])
+            assert R.ref_lz4_compress_blocks(O._ptr(part), part.nbytes, ROWS_PER_BLOCK * 4,
+                                             O._ptr(buf[c * bpc * stride:]), stride, O._ptr(sz[c * bpc:])) == 0
+        comp.append(buf)
+        sizes.append(sz)
+    import ctypes as C
+
+    comp_ptrs = (C.c_void_p * 3)(*[b.ctypes.data for b in comp])
+    size_ptrs = (C.c_void_p * 3)(*[s.ctypes.data for s in sizes])
+    res = None
+    times = []
+    for i in range(warmup + steps):
+        el = C.c_double()
+        scanned = C.c_uint64()
+        r = R.ref_cpu_q1(threads, N_ROWS, ROWS_PER_CHUNK, ROWS_PER_BLOCK, O._ptr(f["date_key"]), O._ptr(mins),
+                         O._ptr(maxs), comp_ptrs, stride, size_ptrs, O._ptr(dd["d_key"]), O._ptr(ok), len(ok),
+                         DATE_LO, DATE_HI, *DISC, *QTY, C.byref(el), C.byref(scanned))
+        res = r
+        if i >= warmup:
+            times.append(el.value)
+    ms = float(np.mean(times))
+    return {"value": N_ROWS / (ms * 1e-3), "unit": "rows/s", "cores": threads, "kind": "reference",
+            "sample": f"full query: min/max pruning to {scanned.value} of {n_chunks} chunks, LZ4CPUManager decode of "
+                      "discount/quantity/extended_price (liblz4 blocks of 64 KiB), HostHashMap date join; "
+                      "date_key uncompressed (no reference CPU cascaded decoder)",
+            "ms": ms, "result": int(res)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="gx", choices=["gx", "reference"])
+    ap.add_argument("--segments", type=int, default=32)
+    ap.add_argument("--seed", type=int, default=0xBEE5BEE5)
+    ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        f, dd = make_data(args.seed)
+        cb = cpu_baseline(f, dd, steps=args.steps, warmup=args.warmup)
+        line = {
+            "impl": "reference",
+            "metric": "rows/s & GB/s vs HBM roofline; p50/p99 latency batched vs one-query-at-a-time",
+            "value": cb["value"], "unit": "rows/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": cb["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded, configs[1] shapes and distributions)",
+            "config": {"workload": WORKLOAD, "rows": N_ROWS, "chunks": 60},
+            "result": cb["result"],
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    line, f, dd = gpu_arm(args, rank, world)
+    if rank == 0 and not args.no_cpu:
+        cb = cpu_baseline(f, dd, steps=3, warmup=1)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        line["cpu_baseline"]["ms"] = cb["ms"]
+        if cb["result"] != line["result"]:
+            raise SystemExit(f"cpu baseline result {cb['result']} != gpu {line['result']}")
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -9,6 +9,7 @@
 // and the chunk min/max; blocks are encoded in parallel host threads.
 #include <algorithm>
 #include <cstring>
+#include <atomic>
 #include <thread>
 
 #include "gx_internal.h"
@@ -319,6 +320,7 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
     if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
     threads = std::min<uint32_t>(threads, std::max<uint32_t>(1, col->n_slots));
     std::vector<std::vector<uint8_t>> bufs(threads);
+    std::atomic<bool> overflow{false};
     std::vector<std::vector<uint64_t>> local_off(threads);
     auto work = [&](uint32_t t) {
         uint32_t s0 = (uint32_t)((uint64_t)col->n_slots * t / threads);
@@ -340,6 +342,7 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
                 uint32_t tmp_seg[2 * kMaxSegments];
                 used = lz4_encode_block(vals + r0, rows, S, rows_per_block / S, min_match, depth, buf,
                                         tmp_seg);
+                if (used + 16 > kStageBytes) overflow = true;  // cannot happen for <= 16384 int32 rows
                 if (S > 1) std::memcpy(&col->seg[(size_t)2 * S * s], tmp_seg, 8 * S);
             } else {
                 used = casc_encode_block(vals + r0, rows, rle, delta, bp, buf);
@@ -355,6 +358,7 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
     for (uint32_t t = 1; t < threads; ++t) pool.emplace_back(work, t);
     work(0);
     for (auto& th : pool) th.join();
+    if (overflow) return set_error(GX_ERR_INVALID, "an LZ4 block exceeds the %u-byte staging buffer", kStageBytes);
     size_t total = 0;
     for (auto& b : bufs) total += b.size();
     col->payload.clear();

@@ -17,6 +17,7 @@ namespace gx {
 
 constexpr int kErrCorrupt = 2;   // == GX_ERR_CORRUPT
 constexpr int kErrCapacity = 3;  // == GX_ERR_CAPACITY
+constexpr int kErrTimeout = 4;   // == GX_ERR_TIMEOUT
 constexpr int kErrInvalid = 6;   // == GX_ERR_INVALID
 constexpr uint64_t kEmptySlot = (uint64_t)(uint32_t)kEmptyKey;  // {key=INT32_MIN, payload=0}
 constexpr uint32_t kEmptyGKey = 0xFFFFFFFFu;                    // shared-memory group table
@@ -34,13 +35,68 @@ __device__ __forceinline__ uint32_t ldu32(const uint8_t* p) {
     return __funnelshift_r(lo, hi, (uint32_t)(a & 3) * 8);
 }
 
+// Byte sources for the decoders: global memory (read-only path) or a block
+// staged in shared memory.  w(i) reads 4 bytes at an arbitrary offset i.
+struct GlobalSrc {
+    const uint8_t* p;
+    __device__ __forceinline__ uint32_t b(uint32_t i) const { return ldb(p + i); }
+    __device__ __forceinline__ uint32_t w(uint32_t i) const { return ldu32(p + i); }
+};
+struct SharedSrc {
+    const uint8_t* p;  // 16-byte aligned, >= 4 readable bytes past the stream end
+    __device__ __forceinline__ uint32_t b(uint32_t i) const { return p[i]; }
+    __device__ __forceinline__ uint32_t w(uint32_t i) const {
+        const uint32_t* a = (const uint32_t*)(p + (i & ~3u));
+        return __funnelshift_r(a[0], a[1], (i & 3u) * 8);
+    }
+};
+
+// ------------------------------------------------ TMA bulk copy + mbarrier
+// One-dimensional cp.async.bulk (no multicast) from global memory into this
+// CTA's shared memory, completed on an mbarrier.  Source, destination and
+// size must be 16-byte aligned / multiples of 16.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* m, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// Orders this thread's earlier generic-proxy accesses of shared memory
+// before later async-proxy (TMA) writes to it.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* m) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(m))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* m, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(m)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase to complete (never spins forever).
+constexpr uint32_t kMbarWaitCap = 1u << 22;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* m, uint32_t phase) {
+    for (uint32_t i = 0; i < kMbarWaitCap; ++i)
+        if (mbar_try_wait(m, phase)) return true;
+    return false;
+}
+
 // ------------------------------------------------- segmented LZ4, one lane
 // Decodes output bytes [ob, oe) of a segmented LZ4 block (format in
 // gx_internal.h) into `out` (word array whose element 0 is output byte ob).
 // Returns 0 or kErrCorrupt.
-__device__ __forceinline__ int lz4_seg_lane(const uint8_t* __restrict__ in, uint32_t in_size,
-                                            uint32_t comp_pos, uint32_t info, uint32_t ob,
-                                            uint32_t oe, uint32_t* __restrict__ out) {
+template <class Src>
+__device__ __forceinline__ int lz4_seg_lane(const Src in, uint32_t in_size, uint32_t comp_pos, uint32_t info,
+                                            uint32_t ob, uint32_t oe, uint32_t* __restrict__ out) {
     if (comp_pos > in_size) return kErrCorrupt;
     uint32_t pos = comp_pos;
     uint32_t k = 0;
@@ -54,14 +110,14 @@ __device__ __forceinline__ int lz4_seg_lane(const uint8_t* __restrict__ in, uint
     while (k < K) {
         if (!resume) {
             if (pos >= in_size) return kErrCorrupt;
-            uint32_t tok = ldb(in + pos++);
+            uint32_t tok = in.b(pos++);
             lit = tok >> 4;
             mnib = tok & 15u;
             if (lit == 15) {
                 uint32_t b;
                 do {
                     if (pos >= in_size) return kErrCorrupt;
-                    b = ldb(in + pos++);
+                    b = in.b(pos++);
                     lit += b;
                 } while (b == 255);
             }
@@ -72,30 +128,29 @@ __device__ __forceinline__ int lz4_seg_lane(const uint8_t* __restrict__ in, uint
         const uint32_t n = min(litw, K - k);
         if ((uint64_t)pos + (uint64_t)n * 4 > (uint64_t)in_size) return kErrCorrupt;
         {
-            const uint8_t* src = in + pos;
             uint32_t i = 0;
             for (; i + 4 <= n; i += 4) {
-                uint32_t a0 = ldu32(src + 4 * i), a1 = ldu32(src + 4 * i + 4);
-                uint32_t a2 = ldu32(src + 4 * i + 8), a3 = ldu32(src + 4 * i + 12);
+                uint32_t a0 = in.w(pos + 4 * i), a1 = in.w(pos + 4 * i + 4);
+                uint32_t a2 = in.w(pos + 4 * i + 8), a3 = in.w(pos + 4 * i + 12);
                 out[k + i] = a0;
                 out[k + i + 1] = a1;
                 out[k + i + 2] = a2;
                 out[k + i + 3] = a3;
             }
-            for (; i < n; ++i) out[k + i] = ldu32(src + 4 * i);
+            for (; i < n; ++i) out[k + i] = in.w(pos + 4 * i);
         }
         k += n;
         pos += n * 4;
         if (k >= K) break;                 // segment ends inside / at the end of this literal run
         if ((uint64_t)pos + 2 > (uint64_t)in_size) return kErrCorrupt;  // block ended before the segment did
-        uint32_t off = ldb(in + pos) | (ldb(in + pos + 1) << 8);
+        uint32_t off = in.b(pos) | (in.b(pos + 1) << 8);
         pos += 2;
         uint32_t ml = mnib + 4;
         if (mnib == 15) {
             uint32_t b;
             do {
                 if (pos >= in_size) return kErrCorrupt;
-                b = ldb(in + pos++);
+                b = in.b(pos++);
                 ml += b;
             } while (b == 255);
         }
@@ -132,38 +187,38 @@ __device__ __forceinline__ int lz4_seg_lane(const uint8_t* __restrict__ in, uint
 // Decodes a complete LZ4 block (any conforming encoder, byte granular) into
 // `out` (out_size bytes expected).  All 32 lanes call it; every lane sees the
 // same control flow.  Returns 0 or kErrCorrupt (uniform across the warp).
-__device__ __forceinline__ int lz4_warp_block(const uint8_t* __restrict__ in, uint32_t in_size,
-                                              uint8_t* __restrict__ out, uint32_t out_size,
-                                              uint32_t lane) {
+template <class Src>
+__device__ __forceinline__ int lz4_warp_block(const Src in, uint32_t in_size, uint8_t* __restrict__ out,
+                                              uint32_t out_size, uint32_t lane) {
     uint32_t pos = 0, o = 0;
     int err = 0;
     while (true) {
         if (pos >= in_size) { err = kErrCorrupt; break; }
-        uint32_t tok = ldb(in + pos++);
+        uint32_t tok = in.b(pos++);
         uint32_t lit = tok >> 4;
         if (lit == 15) {
             uint32_t b;
             do {
                 if (pos >= in_size) { err = kErrCorrupt; break; }
-                b = ldb(in + pos++);
+                b = in.b(pos++);
                 lit += b;
             } while (b == 255);
             if (err) break;
         }
         if ((uint64_t)pos + lit > in_size || (uint64_t)o + lit > out_size) { err = kErrCorrupt; break; }
-        for (uint32_t i = lane; i < lit; i += 32) out[o + i] = (uint8_t)ldb(in + pos + i);
+        for (uint32_t i = lane; i < lit; i += 32) out[o + i] = (uint8_t)in.b(pos + i);
         o += lit;
         pos += lit;
         if (pos == in_size) break;  // last sequence: literals only
         if (pos + 2 > in_size) { err = kErrCorrupt; break; }
-        uint32_t off = ldb(in + pos) | (ldb(in + pos + 1) << 8);
+        uint32_t off = in.b(pos) | (in.b(pos + 1) << 8);
         pos += 2;
         uint32_t ml = (tok & 15u) + 4;
         if ((tok & 15u) == 15) {
             uint32_t b;
             do {
                 if (pos >= in_size) { err = kErrCorrupt; break; }
-                b = ldb(in + pos++);
+                b = in.b(pos++);
                 ml += b;
             } while (b == 255);
             if (err) break;

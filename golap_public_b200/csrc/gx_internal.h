@@ -55,6 +55,7 @@ namespace gx {
 constexpr uint32_t kMaxRowsPerBlock = 16384;   // 64 KiB of int32: one decode buffer
 constexpr uint32_t kMaxSegments = 128;
 constexpr uint32_t kCascMaxRuns = 2048;        // RLE only when runs <= this
+constexpr uint32_t kStageBytes = 66048;        // shared staging buffer for one compressed block
 constexpr uint32_t kPayloadAlign = 16;
 constexpr uint32_t kPayloadSlack = 64;
 constexpr int32_t kEmptyKey = INT32_MIN;        // hash-table empty marker (reserved key)
@@ -102,6 +103,8 @@ struct gx_dcol {
     uint32_t n_chunks;
     uint32_t n_slots;           // n_chunks * blocks_per_chunk
     uint64_t payload_bytes;     // size of the payload allocation
+    uint32_t host_mapped;       // payload lives in pinned host memory (no TMA staging)
+    uint32_t pad_;
 };
 
 // Bit-packed stream reader: element i of width w (0..32).
@@ -169,6 +172,7 @@ struct gx_column {
         v.n_chunks = n_chunks;
         v.n_slots = n_slots;
         v.payload_bytes = payload.size();
+        v.host_mapped = residency == 2 ? 1u : 0u;
         return v;
     }
 };

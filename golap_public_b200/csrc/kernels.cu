@@ -93,11 +93,42 @@ struct ItemsParams {
     uint32_t* work_counter;
 };
 
-// Decode block `slot` of column `c` into shared memory.  Returns the
-// layout flag (1 = padded segment layout) or a negative error.
+// Shared-memory staging of one compressed block.  With HBM-resident columns
+// thread 0 issues a single cp.async.bulk into `stage` and every thread waits
+// on the mbarrier (bounded); host-mapped columns are copied cooperatively
+// with 16-byte loads.  The caller guarantees that no thread still reads
+// `stage`.  Returns 0 or kErrTimeout.
+template <int NT>
+__device__ __forceinline__ int stage_block(const gx_dcol& c, const uint8_t* blk, uint32_t bytes16, uint8_t* stage,
+                                           uint64_t* mbar, uint32_t& phase) {
+    const uint32_t tid = threadIdx.x;
+    int rc = 0;
+    if (!c.host_mapped) {
+        // earlier generic-proxy reads of `stage` by any thread are ordered
+        // before the bulk copy that overwrites it
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) tma_load_1d(stage, blk, bytes16, mbar);
+        if (!mbar_wait_bounded(mbar, phase)) {
+            // give the copy one more bounded chance to land before the buffer is abandoned
+            mbar_wait_bounded(mbar, phase);
+            rc = kErrTimeout;
+        }
+        phase ^= 1u;
+    } else {
+        const uint4* src = (const uint4*)blk;
+        uint4* dst = (uint4*)stage;
+        for (uint32_t i = tid; i < bytes16 / 16; i += NT) dst[i] = src[i];
+    }
+    return rc;
+}
+
+// Decode block `slot` of column `c` into shared memory (`buf`).  Returns the
+// layout (1 = padded segment layout: row r at r + (r >> seg_shift)) or -1;
+// errors are left in *s_err.  All NT threads call it.
 template <int NT>
 __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint32_t rows, uint32_t* buf,
-                                           int32_t* run_val, uint32_t* run_start, uint32_t* tmp,
+                                           uint8_t* stage, uint64_t* mbar, uint32_t& phase, uint32_t* tmp,
                                            int* s_err) {
     const uint32_t tid = threadIdx.x;
     const gx_dblock d = c.blocks[slot];
@@ -105,7 +136,8 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
     // directory sanity: the tile fits the decode buffer and the stream lies
     // inside the payload (its slack covers the decoders' word over-read)
     if (d.n_rows != rows || rows > kMaxRowsPerBlock || d.offset > c.payload_bytes ||
-        (uint64_t)d.comp_bytes + 16 > c.payload_bytes - d.offset) {
+        (uint64_t)d.comp_bytes + 16 > c.payload_bytes - d.offset ||
+        (c.codec == GX_CODEC_LZ4 && d.comp_bytes + 16 > kStageBytes)) {
         if (tid == 0) *s_err = kErrCorrupt;
         __syncthreads();
         return -1;
@@ -123,30 +155,36 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
         __syncthreads();
         return 0;
     }
-    if (c.codec == GX_CODEC_LZ4 && c.S > 1) {
-        const uint32_t seg_rows = 1u << c.seg_shift;
-        if (tid < c.S) {
-            const uint32_t j = tid;
-            const uint32_t ob = min(j * seg_rows, rows) * 4, oe = min((j + 1) * seg_rows, rows) * 4;
-            const uint32_t* e = c.seg + (size_t)2 * c.S * slot + 2 * j;
-            const uint32_t comp_pos = __ldg(e), info = __ldg(e + 1);
-            if (ob < oe) {
-                int rc = lz4_seg_lane(blk, d.comp_bytes, comp_pos, info, ob, oe, buf + j * (seg_rows + 1));
-                if (rc) *s_err = rc;
-            }
-        }
-        __syncthreads();
-        return 1;
-    }
     if (c.codec == GX_CODEC_LZ4) {
-        if (tid < 32) {
-            int rc = lz4_warp_block(blk, d.comp_bytes, (uint8_t*)buf, rows * 4, tid);
-            if (rc && tid == 0) *s_err = rc;
+        const uint32_t bytes16 = (d.comp_bytes + 15u) & ~15u;
+        int rc = stage_block<NT>(c, blk, bytes16, stage, mbar, phase);
+        if (rc && tid == 0) *s_err = rc;
+        __syncthreads();
+        if (rc) return -1;
+        const SharedSrc src{stage};
+        int layout = 0;
+        if (c.S > 1) {
+            const uint32_t seg_rows = 1u << c.seg_shift;
+            for (uint32_t j = tid; j < c.S; j += NT) {
+                const uint32_t ob = min(j * seg_rows, rows) * 4, oe = min((j + 1) * seg_rows, rows) * 4;
+                const uint32_t* e = c.seg + (size_t)2 * c.S * slot + 2 * j;
+                const uint32_t comp_pos = __ldg(e), info = __ldg(e + 1);
+                if (ob < oe) {
+                    int r2 = lz4_seg_lane(src, d.comp_bytes, comp_pos, info, ob, oe, buf + j * (seg_rows + 1));
+                    if (r2) *s_err = r2;
+                }
+            }
+            layout = 1;
+        } else if (tid < 32) {
+            int r2 = lz4_warp_block(src, d.comp_bytes, (uint8_t*)buf, rows * 4, tid);
+            if (r2 && tid == 0) *s_err = r2;
         }
         __syncthreads();
-        return 0;
+        return layout;
     }
-    // cascaded
+    // cascaded: run tables live in the (idle) staging area
+    int32_t* run_val = (int32_t*)stage;
+    uint32_t* run_start = (uint32_t*)(stage + 4 * kCascMaxRuns);
     int rc = casc_decode_block<NT>(blk, d.comp_bytes, rows, (int32_t*)buf, run_val, run_start, tmp);
     if (rc && tid == 0) *s_err = rc;
     __syncthreads();
@@ -160,13 +198,14 @@ __global__ void __launch_bounds__(kScanThreads, 1) scan_kernel(const __grid_cons
     uint32_t* buf = (uint32_t*)smem;
     uint32_t* aux = buf + kBufWords;
     uint32_t* mask = aux + (P.need_aux ? kMaxRowsPerBlock : 0);
-    int32_t* run_val = (int32_t*)(mask + kMaskWords);
-    uint32_t* run_start = (uint32_t*)(run_val + kCascMaxRuns);
-    uint32_t* gkeys = run_start + kCascMaxRuns + 4;
+    uint8_t* stage = (uint8_t*)(mask + kMaskWords);
+    uint32_t* gkeys = (uint32_t*)(stage + kStageBytes);
     unsigned long long* gsums = (unsigned long long*)(gkeys + (P.grouped ? (1u << kSmemGroupLog2) : 0));
 
+    __shared__ __align__(8) uint64_t s_mbar;
     __shared__ uint32_t s_item;
     __shared__ int s_err;
+    __shared__ int s_fatal;
     __shared__ uint32_t s_alive;
     __shared__ uint32_t s_tmp[NW + 1];
     __shared__ unsigned long long s_red[NW];
@@ -178,7 +217,12 @@ __global__ void __launch_bounds__(kScanThreads, 1) scan_kernel(const __grid_cons
             gsums[i] = 0;
         }
     }
-    if (tid == 0) s_err = 0;
+    if (tid == 0) {
+        s_err = 0;
+        s_fatal = 0;
+        mbar_init(&s_mbar, 1);
+    }
+    uint32_t phase = 0;
     int64_t local_sum = 0;
     unsigned long long local_rows = 0;
     const uint32_t bpc = P.blocks_per_chunk;
@@ -186,7 +230,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) scan_kernel(const __grid_cons
     __syncthreads();
 
     while (true) {
-        if (tid == 0) s_item = atomicAdd(P.work_counter, 1u);
+        if (tid == 0) s_item = s_fatal ? 0xFFFFFFFFu : atomicAdd(P.work_counter, 1u);
         __syncthreads();
         const uint32_t it = s_item;
         __syncthreads();
@@ -203,13 +247,14 @@ __global__ void __launch_bounds__(kScanThreads, 1) scan_kernel(const __grid_cons
 
         for (uint32_t si = 0; si < P.n_steps; ++si) {
             const ScanStep& st = P.steps[si];
-            const int layout = decode_tile<NT>(st.col, slot, rows, buf, run_val, run_start, s_tmp, &s_err);
+            const int layout = decode_tile<NT>(st.col, slot, rows, buf, stage, &s_mbar, phase, s_tmp, &s_err);
             const int derr = s_err;
             __syncthreads();  // every thread has read s_err before it is reset
             if (derr) {       // corrupt block: drop the tile, remember the error
                 if (tid == 0) {
                     raise_error(derr);
                     s_err = 0;
+                    if (derr == kErrTimeout) s_fatal = 1;  // staging buffer no longer trusted
                 }
                 __syncthreads();
                 break;
@@ -351,16 +396,20 @@ __global__ void __launch_bounds__(kDecThreads) decompress_kernel(const gx_dcol c
     constexpr int NT = kDecThreads;
     extern __shared__ __align__(16) uint8_t smem[];
     uint32_t* buf = (uint32_t*)smem;
-    int32_t* run_val = (int32_t*)(buf + kBufWords);
-    uint32_t* run_start = (uint32_t*)(run_val + kCascMaxRuns);
+    uint8_t* stage = (uint8_t*)(buf + kBufWords);
+    __shared__ __align__(8) uint64_t s_mbar;
     __shared__ int s_err;
     __shared__ uint32_t s_tmp[NT / 32 + 1];
     const uint32_t slot = slot0 + blockIdx.x;
     const gx_dblock d = c.blocks[slot];
     if (d.n_rows == 0) return;
-    if (threadIdx.x == 0) s_err = 0;
+    if (threadIdx.x == 0) {
+        s_err = 0;
+        mbar_init(&s_mbar, 1);
+    }
     __syncthreads();
-    const int layout = decode_tile<NT>(c, slot, d.n_rows, buf, run_val, run_start, s_tmp, &s_err);
+    uint32_t phase = 0;
+    const int layout = decode_tile<NT>(c, slot, d.n_rows, buf, stage, &s_mbar, phase, s_tmp, &s_err);
     if (s_err) {
         if (threadIdx.x == 0) raise_error(s_err);
         return;
@@ -379,7 +428,8 @@ __global__ void raw_lz4_kernel(const uint8_t* comp, const uint64_t* coff, uint8_
     const uint64_t c0 = coff[b], c1 = coff[b + 1], o0 = ooff[b], o1 = ooff[b + 1];
     int rc = kErrCorrupt;
     if (c1 >= c0 && o1 >= o0 && c1 - c0 < (1ull << 31) && o1 - o0 < (1ull << 31))
-        rc = lz4_warp_block(comp + c0, (uint32_t)(c1 - c0), out + o0, (uint32_t)(o1 - o0), threadIdx.x & 31);
+        rc = lz4_warp_block(GlobalSrc{comp + c0}, (uint32_t)(c1 - c0), out + o0, (uint32_t)(o1 - o0),
+                            threadIdx.x & 31);
     if ((threadIdx.x & 31) == 0) status[b] = rc;
 }
 
@@ -505,12 +555,14 @@ size_t scan_smem_bytes(bool need_aux, bool grouped) {
     size_t b = 4ull * kBufWords;
     if (need_aux) b += 4ull * kMaxRowsPerBlock;
     b += 4ull * kMaskWords;
-    b += 4ull * kCascMaxRuns + 4ull * (kCascMaxRuns + 4);
+    b += kStageBytes;  // also holds the cascaded run tables
     if (grouped) b += (4ull + 8ull) * (1u << kSmemGroupLog2);
     return b;
 }
 
-size_t dec_smem_bytes() { return 4ull * kBufWords + 4ull * kCascMaxRuns + 4ull * (kCascMaxRuns + 4); }
+size_t dec_smem_bytes() { return 4ull * kBufWords + kStageBytes; }
+
+static_assert(4 * kCascMaxRuns + 4 * (kCascMaxRuns + 4) <= kStageBytes, "run tables fit the staging area");
 
 gx_status wait_stream(cudaStream_t s, double timeout_s) {
     auto t0 = std::chrono::steady_clock::now();

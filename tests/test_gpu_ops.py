@@ -46,8 +46,9 @@ def test_metachecker_known_answers(cuda):
                          (7, 1993, [1, 1, 1])]:
         api.MetaChecker(3).add_minmax(col, lo, hi).run(keep)
         assert keep.cpu().tolist() == want
+    # AND of two predicates: [0,100] keeps chunks 0,1; [8,2000] keeps chunks 1,2
     api.MetaChecker(3).add_minmax(col, 0, 100).add_minmax(col, 8, 2000).run(keep)
-    assert keep.cpu().tolist() == [0, 1, 1]
+    assert keep.cpu().tolist() == [0, 1, 0]
 
 
 def test_join_count_1to1(cuda):
