@@ -58,9 +58,14 @@ class ScanStep(C.Structure):
                 ("digit_base", C.c_int32), ("digit_card", C.c_uint32)]
 
 
+class ScanPrune(C.Structure):
+    _fields_ = [("col", P), ("lo", C.c_int32), ("hi", C.c_int32)]
+
+
 class ScanPlan(C.Structure):
     _fields_ = [("n_steps", C.c_uint32), ("steps", ScanStep * GX_MAX_STEPS), ("agg", C.c_uint32),
-                ("keep_chunks_dev", P), ("groupby", P), ("result_dev", P)]
+                ("keep_chunks_dev", P), ("groupby", P), ("result_dev", P), ("n_prune", C.c_uint32),
+                ("prune", ScanPrune * GX_MAX_STEPS), ("keep_out_dev", P)]
 
 
 # name -> (restype, argtypes)
@@ -90,6 +95,8 @@ _SIGS = {
     "gx_hashtable_build": (C.c_int32, [P, P, P, C.c_uint64, P, C.c_uint32, P]),
     "gx_hashtable_count": (C.c_int32, [P, C.POINTER(C.c_uint64), P]),
     "gx_hashtable_probe": (C.c_int32, [P, P, C.c_uint64, P, P, P]),
+    "gx_hashtable_view": (C.c_int32, [P, C.POINTER(P), C.POINTER(C.c_uint32)]),
+    "gx_groupby_view": (C.c_int32, [P, C.POINTER(P), C.POINTER(P), C.POINTER(C.c_uint32)]),
     "gx_groupby_create": (C.c_int32, [C.c_uint64, C.POINTER(P)]),
     "gx_groupby_free": (C.c_int32, [P]),
     "gx_groupby_reset": (C.c_int32, [P, P]),

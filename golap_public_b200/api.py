@@ -45,7 +45,7 @@ class Column:
     """One compressed int32 column: chunks of rows_per_chunk rows, blocks of rows_per_block rows."""
 
     def __init__(self, values: np.ndarray, codec: str = "lz4", rows_per_chunk: int = 1_000_000,
-                 rows_per_block: int = 16384, lz4_segments: int = 32, lz4_min_match: int = 4,
+                 rows_per_block: int = 16384, lz4_segments: int = 128, lz4_min_match: int = 4,
                  lz4_search_depth: int = 16, threads: int = 0, name: str = ""):
         values = np.ascontiguousarray(values, dtype=np.int32)
         o = L.EncodeOpts()
@@ -247,6 +247,12 @@ class ScanPlan:
     keep_chunks: object = None      # device uint16 tensor or None
     groupby: HashAggregate | None = None
     result: object = None           # device int64 tensor (1 element)
+    prune: list = field(default_factory=list)  # (Column, lo, hi) min/max predicates
+    keep_out: object = None         # device uint16 tensor receiving the chunk flags
+
+    def prune_minmax(self, col, lo, hi):
+        self.prune.append((col, lo, hi))
+        return self
 
     def filter(self, col, lo, hi, carry=False):
         self.steps.append(Step(col, L.GX_STEP_FILTER | (L.GX_STEP_CARRY if carry else 0), lo, hi))
@@ -283,6 +289,12 @@ class ScanPlan:
         p.keep_chunks_dev = self.keep_chunks.data_ptr() if self.keep_chunks is not None else None
         p.groupby = self.groupby.handle.value if self.groupby is not None else None
         p.result_dev = self.result.data_ptr() if self.result is not None else None
+        p.n_prune = len(self.prune)
+        for i, (col, lo, hi) in enumerate(self.prune):
+            p.prune[i].col = col.handle.value
+            p.prune[i].lo = lo
+            p.prune[i].hi = hi
+        p.keep_out_dev = self.keep_out.data_ptr() if self.keep_out is not None else None
         self._c = p  # keep alive
         return p
 

@@ -66,7 +66,7 @@ gx_status gx_encode_opts_default(gx_encode_opts* o) {
     o->codec = GX_CODEC_LZ4;
     o->rows_per_chunk = 1000000;
     o->rows_per_block = 16384;
-    o->lz4_segments = 32;
+    o->lz4_segments = 128;
     o->lz4_min_match = 4;
     o->lz4_search_depth = 16;
     o->casc_rle = 1;

@@ -1,12 +1,13 @@
 // gx_device.cuh -- sm_100a device building blocks: block decoders (segmented
-// LZ4, generic LZ4, cascaded, raw), join-table probing and group-table
-// updates.  Included by kernels.cu only.
+// LZ4, generic LZ4, cascaded), TMA bulk staging, join-table probing and
+// group-table updates.  Included by kernels.cu only.
 //
 // Reference counterparts: the nvCOMP decompressors behind
 // ChunkDecompressor::step (core/comp.cuh:186), HashMap::probe
 // (core/dev_structs.cuh:105-113) and HashAggregate::add
 // (core/dev_structs.cuh:210-244).  Unlike HashAggregate::add, no wait here
-// is unbounded: every probe loop is capped by the table size.
+// is unbounded: every probe loop is capped by the table size and every
+// mbarrier wait by an iteration count.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -25,30 +26,15 @@ constexpr uint32_t kEmptyGKey = 0xFFFFFFFFu;                    // shared-memory
 // ---------------------------------------------------------- byte access
 __device__ __forceinline__ uint32_t ldb(const uint8_t* p) { return (uint32_t)__ldg(p); }
 
-// 32-bit load from an arbitrary byte address in global memory (two aligned
-// loads + funnel shift).  The payload carries >= 16 bytes of slack so the
-// second word is always inside the allocation.
-__device__ __forceinline__ uint32_t ldu32(const uint8_t* p) {
-    uintptr_t a = (uintptr_t)p;
-    const uint32_t* w = (const uint32_t*)(a & ~(uintptr_t)3);
-    uint32_t lo = __ldg(w), hi = __ldg(w + 1);
-    return __funnelshift_r(lo, hi, (uint32_t)(a & 3) * 8);
-}
-
-// Byte sources for the decoders: global memory (read-only path) or a block
-// staged in shared memory.  w(i) reads 4 bytes at an arbitrary offset i.
+// Global-memory byte source (read-only path) for the generic LZ4 decoder.
 struct GlobalSrc {
     const uint8_t* p;
     __device__ __forceinline__ uint32_t b(uint32_t i) const { return ldb(p + i); }
-    __device__ __forceinline__ uint32_t w(uint32_t i) const { return ldu32(p + i); }
 };
+// Byte source over a block staged in shared memory.
 struct SharedSrc {
-    const uint8_t* p;  // 16-byte aligned, >= 4 readable bytes past the stream end
+    const uint8_t* p;
     __device__ __forceinline__ uint32_t b(uint32_t i) const { return p[i]; }
-    __device__ __forceinline__ uint32_t w(uint32_t i) const {
-        const uint32_t* a = (const uint32_t*)(p + (i & ~3u));
-        return __funnelshift_r(a[0], a[1], (i & 3u) * 8);
-    }
 };
 
 // ------------------------------------------------ TMA bulk copy + mbarrier
@@ -91,94 +77,99 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* m, uint32_t phase) {
 }
 
 // ------------------------------------------------- segmented LZ4, one lane
-// Decodes output bytes [ob, oe) of a segmented LZ4 block (format in
-// gx_internal.h) into `out` (word array whose element 0 is output byte ob).
-// Returns 0 or kErrCorrupt.
-template <class Src>
-__device__ __forceinline__ int lz4_seg_lane(const Src in, uint32_t in_size, uint32_t comp_pos, uint32_t info,
-                                            uint32_t ob, uint32_t oe, uint32_t* __restrict__ out) {
-    if (comp_pos > in_size) return kErrCorrupt;
+// Decodes the K output words of one segment of a segmented LZ4 block (format
+// in gx_internal.h) into out[0..K).  The block's compressed bytes from
+// stream position wbase on are staged in shared memory as the word array A;
+// the lane may read stream positions [lo, hi) only (its tile's window), and
+// the block's stream ends at block_end.
+//
+// One output word per loop iteration: a literal word (rolling funnel shift
+// over the staged words, one shared load per word) or a match word
+// out[k - offw] (LZ4 overlap semantics follow from the word order).  Token
+// and offset parsing happens between words only when a lane needs it, so
+// the 32 lanes of a warp stay in lockstep.  Returns 0 or kErrCorrupt.
+__device__ __forceinline__ int lz4_seg_lane(const uint32_t* __restrict__ A, uint32_t wbase, uint32_t lo,
+                                            uint32_t hi, uint32_t block_end, uint32_t comp_pos, uint32_t info,
+                                            uint32_t K, uint32_t* __restrict__ out) {
+    if (comp_pos < lo || comp_pos > hi) return kErrCorrupt;
     uint32_t pos = comp_pos;
-    uint32_t k = 0;
-    const uint32_t K = (oe - ob) >> 2;
-    uint32_t lit = 0, mnib = 0;
-    bool resume = (info & 16u) != 0;
-    if (resume) {
-        lit = info >> 5;
-        mnib = info & 15u;
-    }
-    while (k < K) {
-        if (!resume) {
-            if (pos >= in_size) return kErrCorrupt;
-            uint32_t tok = in.b(pos++);
-            lit = tok >> 4;
-            mnib = tok & 15u;
-            if (lit == 15) {
-                uint32_t b;
-                do {
-                    if (pos >= in_size) return kErrCorrupt;
-                    b = in.b(pos++);
-                    lit += b;
-                } while (b == 255);
-            }
-        }
-        resume = false;
+    uint32_t litw = 0, mw = 0, offw = 0, mnib = 0;
+    uint32_t phase = 0;  // 0: next is a token, 1: next is a match offset
+    uint32_t lwprev = 0, lsh = 0;
+    auto byte = [&](uint32_t i) -> uint32_t {
+        const uint32_t r = i - wbase;
+        return (A[r >> 2] >> ((r & 3u) * 8)) & 255u;
+    };
+    if (info & 16u) {
+        const uint32_t lit = info >> 5;
         if (lit & 3u) return kErrCorrupt;
-        const uint32_t litw = lit >> 2;
-        const uint32_t n = min(litw, K - k);
-        if ((uint64_t)pos + (uint64_t)n * 4 > (uint64_t)in_size) return kErrCorrupt;
-        {
-            uint32_t i = 0;
-            for (; i + 4 <= n; i += 4) {
-                uint32_t a0 = in.w(pos + 4 * i), a1 = in.w(pos + 4 * i + 4);
-                uint32_t a2 = in.w(pos + 4 * i + 8), a3 = in.w(pos + 4 * i + 12);
-                out[k + i] = a0;
-                out[k + i + 1] = a1;
-                out[k + i + 2] = a2;
-                out[k + i + 3] = a3;
-            }
-            for (; i < n; ++i) out[k + i] = in.w(pos + 4 * i);
+        litw = lit >> 2;
+        mnib = info & 15u;
+        phase = 1;
+        if ((uint64_t)pos + 4ull * min(litw, K) > hi) return kErrCorrupt;
+        if (litw) {
+            const uint32_t r = pos - wbase;
+            lsh = (r & 3u) * 8;
+            lwprev = A[r >> 2];
         }
-        k += n;
-        pos += n * 4;
-        if (k >= K) break;                 // segment ends inside / at the end of this literal run
-        if ((uint64_t)pos + 2 > (uint64_t)in_size) return kErrCorrupt;  // block ended before the segment did
-        uint32_t off = in.b(pos) | (in.b(pos + 1) << 8);
-        pos += 2;
-        uint32_t ml = mnib + 4;
-        if (mnib == 15) {
-            uint32_t b;
-            do {
-                if (pos >= in_size) return kErrCorrupt;
-                b = in.b(pos++);
-                ml += b;
-            } while (b == 255);
-        }
-        if ((off & 3u) || (ml & 3u) || off == 0) return kErrCorrupt;
-        const uint32_t offw = off >> 2, mlw = ml >> 2;
-        if (offw > k || mlw > K - k) return kErrCorrupt;
-        uint32_t* dst = out + k;
-        const uint32_t* s = out + (k - offw);
-        if (offw >= mlw) {
-            uint32_t i = 0;
-            for (; i + 4 <= mlw; i += 4) {
-                uint32_t a0 = s[i], a1 = s[i + 1], a2 = s[i + 2], a3 = s[i + 3];
-                dst[i] = a0;
-                dst[i + 1] = a1;
-                dst[i + 2] = a2;
-                dst[i + 3] = a3;
+    }
+    for (uint32_t k = 0; k < K; ++k) {
+        while (litw == 0 && mw == 0) {
+            if (phase == 0) {
+                if (pos >= hi) return kErrCorrupt;
+                const uint32_t tok = byte(pos++);
+                uint32_t lit = tok >> 4;
+                mnib = tok & 15u;
+                if (lit == 15) {
+                    uint32_t b;
+                    do {
+                        if (pos >= hi) return kErrCorrupt;
+                        b = byte(pos++);
+                        lit += b;
+                    } while (b == 255);
+                }
+                if (lit & 3u) return kErrCorrupt;
+                litw = lit >> 2;
+                if ((uint64_t)pos + 4ull * min(litw, K - k) > hi) return kErrCorrupt;
+                if (litw) {
+                    const uint32_t r = pos - wbase;
+                    lsh = (r & 3u) * 8;
+                    lwprev = A[r >> 2];
+                }
+                phase = 1;
+            } else {
+                // literals done: the block may end here (then the segment is short)
+                if (pos == block_end || (uint64_t)pos + 2 > hi) return kErrCorrupt;
+                const uint32_t off = byte(pos) | (byte(pos + 1) << 8);
+                pos += 2;
+                uint32_t ml = mnib + 4;
+                if (mnib == 15) {
+                    uint32_t b;
+                    do {
+                        if (pos >= hi) return kErrCorrupt;
+                        b = byte(pos++);
+                        ml += b;
+                    } while (b == 255);
+                }
+                if ((off & 3u) || (ml & 3u) || off == 0) return kErrCorrupt;
+                offw = off >> 2;
+                mw = ml >> 2;
+                if (offw > k || mw > K - k) return kErrCorrupt;
+                phase = 0;
             }
-            for (; i < mlw; ++i) dst[i] = s[i];
+        }
+        uint32_t w;
+        if (litw) {
+            const uint32_t nxt = A[((pos - wbase) >> 2) + 1];
+            w = __funnelshift_r(lwprev, nxt, lsh);
+            lwprev = nxt;
+            pos += 4;
+            --litw;
         } else {
-            // overlapping match: output word i repeats source word i mod offw,
-            // and all source words precede k, so the copies are independent
-            uint32_t j = 0;
-            for (uint32_t i = 0; i < mlw; ++i) {
-                dst[i] = s[j];
-                if (++j == offw) j = 0;
-            }
+            w = out[k - offw];
+            --mw;
         }
-        k += mlw;
+        out[k] = w;
     }
     return 0;
 }
@@ -241,8 +232,8 @@ __device__ __forceinline__ int lz4_warp_block(const Src in, uint32_t in_size, ui
 
 // ------------------------------------------------------ block-wide scans
 // Inclusive scan (wrapping uint32 addition) of a[0..n) in shared memory by
-// NT threads; each thread owns a contiguous range.  `tmp` has >= NT/32 + 1
-// words.  Must be called by all NT threads.
+// NT threads; thread t owns the contiguous range [t*per, (t+1)*per).  `tmp`
+// has >= NT/32 words.  Must be called by all NT threads.
 template <int NT>
 __device__ __forceinline__ void block_inclusive_scan(uint32_t* a, uint32_t n, uint32_t* tmp) {
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -276,75 +267,141 @@ __device__ __forceinline__ void block_inclusive_scan(uint32_t* a, uint32_t n, ui
     __syncthreads();
 }
 
-// ------------------------------------------------------- cascaded block
-// Decodes one cascaded block (format in gx_internal.h) into out[0..rows)
-// (shared memory).  run_val/run_start are shared scratch of kCascMaxRuns
-// (+1) entries.  All NT threads call it.  Returns 0 or kErrCorrupt (uniform).
+// Block-wide sum (wrapping uint32) of one value per thread.
 template <int NT>
-__device__ __forceinline__ int casc_decode_block(const uint8_t* __restrict__ blk, uint32_t blk_bytes,
-                                                 uint32_t rows, int32_t* out, int32_t* run_val,
-                                                 uint32_t* run_start, uint32_t* tmp) {
-    const uint32_t tid = threadIdx.x;
-    casc_hdr h;
-    {
-        const uint32_t* hw = (const uint32_t*)blk;
-        uint32_t w[8];
+__device__ __forceinline__ uint32_t block_sum_u32(uint32_t v, uint32_t* tmp) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) w[i] = __ldg(hw + i);
-        memcpy(&h, w, sizeof(h));
-    }
-    const bool rle = (h.flags & CASC_RLE) != 0, delta = (h.flags & CASC_DELTA) != 0;
-    if (blk_bytes < 32 || h.n_rows != rows || h.val_bits > 32 || h.len_bits > 32 ||
-        (rle ? (h.n_runs == 0 || h.n_runs > kCascMaxRuns) : h.n_runs != rows) ||
-        h.vals_off < 32 || (h.vals_off & 3) ||
-        (uint64_t)h.vals_off + 4ull * (((uint64_t)h.n_runs * h.val_bits + 31) / 32 + 1) > blk_bytes ||
-        (rle && ((h.lens_off & 3) || h.lens_off < 32 ||
-                 (uint64_t)h.lens_off + 4ull * (((uint64_t)h.n_runs * h.len_bits + 31) / 32 + 1) > blk_bytes)))
-        return kErrCorrupt;
-    const uint32_t* vw = (const uint32_t*)(blk + h.vals_off);
-    uint32_t* dst = rle ? (uint32_t*)run_val : (uint32_t*)out;
-    const uint32_t n = h.n_runs;
-    for (uint32_t i = tid; i < n; i += NT) dst[i] = unpack_bits(vw, i, h.val_bits) + (uint32_t)h.val_base;
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, d);
+    if (lane == 0) tmp[warp] = v;
     __syncthreads();
-    if (delta) {
-        block_inclusive_scan<NT>(dst, n, tmp);
-        for (uint32_t i = tid; i < n; i += NT) dst[i] += (uint32_t)h.first;
+    uint32_t t = 0;
+    for (uint32_t w = 0; w < NT / 32; ++w) t += tmp[w];
+    __syncthreads();
+    return t;
+}
+
+// ------------------------------------------------------- cascaded blocks
+// Result of decoding one tile [r0, r0+n) of a cascaded block.
+struct CascTile {
+    uint32_t rle;     // 1: values are given as runs (run_val/run_start)
+    uint32_t ra, rb;  // runs intersecting the tile: [ra, rb)
+};
+
+__device__ __forceinline__ bool casc_header_ok(const casc_hdr& h, uint32_t blk_bytes, uint32_t rows) {
+    const bool rle = (h.flags & CASC_RLE) != 0;
+    if (blk_bytes < 32 || h.n_rows != rows || h.val_bits > 32 || h.len_bits > 32) return false;
+    if (rle ? (h.n_runs == 0 || h.n_runs > kCascMaxRuns) : h.n_runs != rows) return false;
+    if (h.vals_off < 32 || (h.vals_off & 3) ||
+        (uint64_t)h.vals_off + 4ull * (((uint64_t)h.n_runs * h.val_bits + 31) / 32 + 1) > blk_bytes)
+        return false;
+    if (rle && ((h.lens_off & 3) || h.lens_off < 32 ||
+                (uint64_t)h.lens_off + 4ull * (((uint64_t)h.n_runs * h.len_bits + 31) / 32 + 1) > blk_bytes))
+        return false;
+    return true;
+}
+
+__device__ __forceinline__ casc_hdr casc_load_header(const uint8_t* blk) {
+    casc_hdr h;
+    const uint32_t* hw = (const uint32_t*)blk;
+    uint32_t w[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) w[i] = __ldg(hw + i);
+    memcpy(&h, w, sizeof(h));
+    return h;
+}
+
+// Decodes tile [r0, r0+n) of a cascaded block of `rows` rows.  RLE blocks
+// leave their runs in run_val/run_start (block-wide, shared) and report the
+// tile's run range; other blocks write the tile's values to out[0..n).
+// All NT threads call it.  Returns 0 or kErrCorrupt (uniform).
+template <int NT>
+__device__ __forceinline__ int casc_decode_tile(const uint8_t* __restrict__ blk, uint32_t blk_bytes, uint32_t rows,
+                                                uint32_t r0, uint32_t n, int32_t* out, int32_t* run_val,
+                                                uint32_t* run_start, uint32_t* tmp, CascTile* t) {
+    const uint32_t tid = threadIdx.x;
+    const casc_hdr h = casc_load_header(blk);
+    if (!casc_header_ok(h, blk_bytes, rows)) return kErrCorrupt;
+    const bool rle = (h.flags & CASC_RLE) != 0, delta = (h.flags & CASC_DELTA) != 0;
+    const uint32_t* vw = (const uint32_t*)(blk + h.vals_off);
+    if (!rle) {
+        // values of the tile only; with delta, add the sum of the entries before it
+        uint32_t before = 0;
+        if (delta) {
+            uint32_t part = 0;
+            for (uint32_t i = 1 + tid; i < r0 && i < rows; i += NT)  // entries 1..r0-1
+                part += unpack_bits(vw, i, h.val_bits) + (uint32_t)h.val_base;
+            before = block_sum_u32<NT>(part, tmp);
+        }
+        for (uint32_t i = tid; i < n; i += NT) {
+            const uint32_t e = r0 + i;
+            out[i] = (int32_t)((e == 0 && delta) ? 0u : unpack_bits(vw, e, h.val_bits) + (uint32_t)h.val_base);
+        }
         __syncthreads();
+        if (delta) {
+            block_inclusive_scan<NT>((uint32_t*)out, n, tmp);
+            const uint32_t add = before + (uint32_t)h.first;
+            for (uint32_t i = tid; i < n; i += NT) out[i] = (int32_t)((uint32_t)out[i] + add);
+            __syncthreads();
+        }
+        if (tid == 0) *t = CascTile{0, 0, 0};
+        __syncthreads();
+        return 0;
     }
-    if (!rle) return 0;
+    const uint32_t nr = h.n_runs;
     const uint32_t* lw = (const uint32_t*)(blk + h.lens_off);
-    for (uint32_t i = tid; i < n; i += NT) run_start[i + 1] = unpack_bits(lw, i, h.len_bits) + h.len_base;
+    for (uint32_t i = tid; i < nr; i += NT) {
+        run_val[i] = (int32_t)((i == 0 && delta) ? 0u : unpack_bits(vw, i, h.val_bits) + (uint32_t)h.val_base);
+        run_start[i + 1] = unpack_bits(lw, i, h.len_bits) + h.len_base;
+    }
     if (tid == 0) run_start[0] = 0;
     __syncthreads();
-    block_inclusive_scan<NT>(run_start + 1, n, tmp);
-    if (run_start[n] != rows) return kErrCorrupt;  // uniform: all threads read the same word
-    // fill: each thread owns a contiguous row range; binary search its first run
-    const uint32_t per = (rows + NT - 1) / NT;
-    const uint32_t r0 = min(rows, tid * per), r1 = min(rows, r0 + per);
-    if (r0 < r1) {
-        uint32_t lo = 0, hi = n;  // find last run with start <= r0
-        while (hi - lo > 1) {
-            uint32_t mid = (lo + hi) >> 1;
-            if (run_start[mid] <= r0) lo = mid; else hi = mid;
+    if (delta) {
+        block_inclusive_scan<NT>((uint32_t*)run_val, nr, tmp);
+        for (uint32_t i = tid; i < nr; i += NT) run_val[i] = (int32_t)((uint32_t)run_val[i] + (uint32_t)h.first);
+    }
+    block_inclusive_scan<NT>(run_start + 1, nr, tmp);
+    if (run_start[nr] != rows) return kErrCorrupt;  // uniform: all threads read the same word
+    if (tid == 0) {
+        // runs intersecting [r0, r0+n): first run ending after r0 .. first run starting at/after r0+n
+        uint32_t lo = 0, hi = nr;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (run_start[mid + 1] <= r0) lo = mid + 1; else hi = mid;
         }
-        uint32_t run = lo, end = run_start[run + 1];
-        int32_t v = run_val[run];
-        for (uint32_t r = r0; r < r1; ++r) {
-            while (r >= end) {
-                ++run;
-                end = run_start[run + 1];
-                v = run_val[run];
-            }
-            out[r] = v;
+        const uint32_t a = lo;
+        hi = nr;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (run_start[mid] < r0 + n) lo = mid + 1; else hi = mid;
         }
+        *t = CascTile{1, a, lo};
     }
     __syncthreads();
     return 0;
 }
 
+// Writes the tile's rows from runs into out[0..n): thread-interleaved rows
+// (bank-conflict free), each thread locating its run by binary search over
+// the tile's run range.
+template <int NT>
+__device__ __forceinline__ void casc_runs_to_rows(const CascTile& t, const int32_t* run_val,
+                                                  const uint32_t* run_start, uint32_t r0, uint32_t n, int32_t* out) {
+    for (uint32_t i = threadIdx.x; i < n; i += NT) {
+        const uint32_t r = r0 + i;
+        uint32_t lo = t.ra, hi = t.rb;  // last run with start <= r
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (run_start[mid] <= r) lo = mid; else hi = mid;
+        }
+        out[i] = run_val[lo];
+    }
+    __syncthreads();
+}
+
 // --------------------------------------------------------- join tables
-__device__ __forceinline__ bool ht_probe(const uint64_t* __restrict__ slots, uint32_t log2cap,
-                                         int32_t key, int32_t* payload) {
+__device__ __forceinline__ bool ht_probe(const uint64_t* __restrict__ slots, uint32_t log2cap, int32_t key,
+                                         int32_t* payload) {
     if (key == kEmptyKey) return false;
     const uint32_t mask = (1u << log2cap) - 1;
     uint32_t s = hash_key32(key, log2cap);
@@ -363,8 +420,8 @@ __device__ __forceinline__ bool ht_probe(const uint64_t* __restrict__ slots, uin
 
 // --------------------------------------------------------- group tables
 // Global open-addressing group table: keys int64 (kEmptyGroup = free), sums int64.
-__device__ __forceinline__ bool group_add_global(int64_t* keys, int64_t* sums, uint32_t log2cap,
-                                                 int64_t key, int64_t v) {
+__device__ __forceinline__ bool group_add_global(int64_t* keys, int64_t* sums, uint32_t log2cap, int64_t key,
+                                                 int64_t v) {
     const uint32_t mask = (1u << log2cap) - 1;
     uint32_t s = hash_key64(key, log2cap);
     for (uint32_t i = 0; i <= mask; ++i) {
@@ -395,8 +452,8 @@ __device__ __forceinline__ bool group_add_smem(uint32_t* keys, unsigned long lon
     return false;
 }
 
-// Sum of a 64-bit value over the lanes in `peers` (all 32 lanes call it,
-// non-members contribute 0).  Exact: four 16-bit limbs reduced separately.
+// Sum of a 64-bit value over all 32 lanes (non-members pass 0).  Exact:
+// four 16-bit limbs are reduced separately and recombined modulo 2^64.
 __device__ __forceinline__ uint64_t warp_sum_u64(uint64_t u) {
     uint32_t p0 = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)(u & 0xFFFF));
     uint32_t p1 = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)((u >> 16) & 0xFFFF));

@@ -42,6 +42,8 @@
 #pragma once
 #include <stdint.h>
 
+#include "../../include/gx_hash.h"
+
 #ifndef GX_HOSTDEV
 #if defined(__CUDACC__)
 #define GX_HOSTDEV __host__ __device__
@@ -117,15 +119,9 @@ GX_HOSTDEV inline uint32_t unpack_bits(const uint32_t* words, uint32_t i, uint32
     return (uint32_t)((two >> sh) & mask);
 }
 
-// Multiplicative hash used by the join tables (Fibonacci hashing).
-GX_HOSTDEV inline uint32_t hash_key32(int32_t key, uint32_t log2cap) {
-    uint32_t h = (uint32_t)key * 0x9E3779B1u;
-    return log2cap ? (h >> (32 - log2cap)) : 0;
-}
-GX_HOSTDEV inline uint32_t hash_key64(int64_t key, uint32_t log2cap) {
-    uint64_t h = (uint64_t)key * 0x9E3779B97F4A7C15ull;
-    return log2cap ? (uint32_t)(h >> (64 - log2cap)) : 0;
-}
+// Join/group table hashing: the public definitions in include/gx_hash.h.
+GX_HOSTDEV inline uint32_t hash_key32(int32_t key, uint32_t log2cap) { return gx_hash32(key, log2cap); }
+GX_HOSTDEV inline uint32_t hash_key64(int64_t key, uint32_t log2cap) { return gx_hash64(key, log2cap); }
 
 }  // namespace gx
 

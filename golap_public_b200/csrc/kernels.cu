@@ -13,12 +13,17 @@
 //                      (hash_map_build_pred_other core/join.cuh:107-135,
 //                       hash_join_count core/join.cuh:46-59)
 //   groupby_add_kernel (group_by_agg_2col core/group.cuh:15-24 with SumAgg)
+//
+// A work unit is a row tile: one (chunk, block, tile) triple covering up to
+// kTileRows rows of every column of the table.  Segmented LZ4 blocks are
+// decoded tile by tile (a tile holds whole segments), so four CTAs fit on
+// an SM; plans with plain LZ4 or segments longer than a tile fall back to
+// whole-block tiles.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
 #include <cstring>
-#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -42,11 +47,19 @@ __device__ __forceinline__ void raise_error(int code) { atomicCAS(&g_gx_error, 0
 
 namespace {
 
-constexpr int kScanThreads = 256;
-constexpr int kDecThreads = 256;
-constexpr uint32_t kBufWords = kMaxRowsPerBlock + kMaxSegments;  // padded segment layout
-constexpr uint32_t kMaskWords = kMaxRowsPerBlock / 32;
-constexpr uint32_t kSmemGroupLog2 = 11;                          // 2048-slot partial table
+constexpr uint32_t kTileRows = 4096;      // tile of the small configuration
+constexpr uint32_t kSmemGroupLog2 = 10;   // 1024-slot shared partial group table
+
+// Shared-memory budget of one CTA for tiles of up to MAXT rows.
+template <int MAXT>
+struct Cfg {
+    static constexpr uint32_t kBufWords = MAXT + kMaxSegments;                // one pad word per segment
+    static constexpr uint32_t kMaskWords = MAXT / 32;
+    static constexpr uint32_t kStage = MAXT * 4 + MAXT * 4 / 128 + 256;      // compressed window + slack
+    static_assert(4 * kCascMaxRuns + 4 * (kCascMaxRuns + 4) <= kStage, "run tables fit the stage");
+    static_assert(MAXT * 4 <= kStage, "raw tile fits the stage");
+};
+static_assert(Cfg<kMaxRowsPerBlock>::kStage >= kStageBytes, "a whole block fits the large stage");
 
 struct ScanStep {
     gx_dcol col;
@@ -72,6 +85,8 @@ struct ScanParams {
     uint32_t grouped;       // sums per group key
     uint32_t need_aux;      // aux array (carry or group key) in shared memory
     uint32_t blocks_per_chunk;
+    uint32_t tile_rows;
+    uint32_t tiles_per_block;
     const uint32_t* items;  // surviving chunk ids
     const uint32_t* n_items;
     uint32_t* work_counter;
@@ -93,13 +108,16 @@ struct ItemsParams {
     uint32_t* work_counter;
 };
 
-// Shared-memory staging of one compressed block.  With HBM-resident columns
-// thread 0 issues a single cp.async.bulk into `stage` and every thread waits
-// on the mbarrier (bounded); host-mapped columns are copied cooperatively
-// with 16-byte loads.  The caller guarantees that no thread still reads
-// `stage`.  Returns 0 or kErrTimeout.
+// Layout of a decoded tile in shared memory.
+enum : int { kRows = 0, kSegRows = 1, kRuns = 2 };
+
+// Stage `bytes` bytes from `src` (16-byte aligned, bytes a multiple of 16
+// and within the stage) into shared memory.  HBM-resident columns: thread 0
+// issues one cp.async.bulk and every thread waits on the mbarrier (bounded);
+// host-mapped columns: cooperative 16-byte loads.  All NT threads call it.
+// Returns 0 or kErrTimeout.
 template <int NT>
-__device__ __forceinline__ int stage_block(const gx_dcol& c, const uint8_t* blk, uint32_t bytes16, uint8_t* stage,
+__device__ __forceinline__ int stage_bytes(const gx_dcol& c, const uint8_t* src, uint32_t bytes, uint8_t* stage,
                                            uint64_t* mbar, uint32_t& phase) {
     const uint32_t tid = threadIdx.x;
     int rc = 0;
@@ -108,7 +126,7 @@ __device__ __forceinline__ int stage_block(const gx_dcol& c, const uint8_t* blk,
         // before the bulk copy that overwrites it
         fence_proxy_async_smem();
         __syncthreads();
-        if (tid == 0) tma_load_1d(stage, blk, bytes16, mbar);
+        if (tid == 0) tma_load_1d(stage, src, bytes, mbar);
         if (!mbar_wait_bounded(mbar, phase)) {
             // give the copy one more bounded chance to land before the buffer is abandoned
             mbar_wait_bounded(mbar, phase);
@@ -116,28 +134,30 @@ __device__ __forceinline__ int stage_block(const gx_dcol& c, const uint8_t* blk,
         }
         phase ^= 1u;
     } else {
-        const uint4* src = (const uint4*)blk;
-        uint4* dst = (uint4*)stage;
-        for (uint32_t i = tid; i < bytes16 / 16; i += NT) dst[i] = src[i];
+        __syncthreads();
+        const uint4* s = (const uint4*)src;
+        uint4* d = (uint4*)stage;
+        for (uint32_t i = tid; i < bytes / 16; i += NT) d[i] = s[i];
     }
     return rc;
 }
 
-// Decode block `slot` of column `c` into shared memory (`buf`).  Returns the
-// layout (1 = padded segment layout: row r at r + (r >> seg_shift)) or -1;
-// errors are left in *s_err.  All NT threads call it.
-template <int NT>
-__device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint32_t rows, uint32_t* buf,
-                                           uint8_t* stage, uint64_t* mbar, uint32_t& phase, uint32_t* tmp,
-                                           int* s_err) {
+// Decode rows [r0, r0+n) of block `slot` of column `c` into shared memory.
+// Returns the layout (kRows: buf[r]; kSegRows: buf[r + (r >> seg_shift)];
+// kRuns: runs in the stage area, described by *ct) or -1 with *s_err set.
+// All NT threads call it.
+template <int NT, int MAXT>
+__device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint32_t rows, uint32_t r0, uint32_t n,
+                                           uint32_t* buf, uint8_t* stage, uint64_t* mbar, uint32_t& phase,
+                                           uint32_t* tmp, CascTile* ct, int* s_err) {
+    using C = Cfg<MAXT>;
     const uint32_t tid = threadIdx.x;
     const gx_dblock d = c.blocks[slot];
     const uint8_t* blk = c.payload + d.offset;
-    // directory sanity: the tile fits the decode buffer and the stream lies
-    // inside the payload (its slack covers the decoders' word over-read)
-    if (d.n_rows != rows || rows > kMaxRowsPerBlock || d.offset > c.payload_bytes ||
-        (uint64_t)d.comp_bytes + 16 > c.payload_bytes - d.offset ||
-        (c.codec == GX_CODEC_LZ4 && d.comp_bytes + 16 > kStageBytes)) {
+    // directory sanity: the stream lies inside the payload (whose slack
+    // covers the decoders' over-read) and the tile fits the buffers
+    if (d.n_rows != rows || rows > kMaxRowsPerBlock || n > MAXT || d.offset > c.payload_bytes ||
+        (uint64_t)d.comp_bytes + 32 > c.payload_bytes - d.offset) {
         if (tid == 0) *s_err = kErrCorrupt;
         __syncthreads();
         return -1;
@@ -146,61 +166,92 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
         if (d.comp_bytes != rows * 4) {
             if (tid == 0) *s_err = kErrCorrupt;
         } else {
-            const uint4* src = (const uint4*)blk;
-            uint4* dst = (uint4*)buf;
-            const uint32_t nv = rows / 4;
-            for (uint32_t i = tid; i < nv; i += NT) dst[i] = __ldg(src + i);
-            for (uint32_t i = nv * 4 + tid; i < rows; i += NT) buf[i] = __ldg((const uint32_t*)blk + i);
+            const uint32_t* src = (const uint32_t*)blk + r0;
+            if ((r0 & 3u) == 0) {
+                const uint32_t nv = n / 4;
+                for (uint32_t i = tid; i < nv; i += NT) ((uint4*)buf)[i] = __ldg((const uint4*)src + i);
+                for (uint32_t i = nv * 4 + tid; i < n; i += NT) buf[i] = __ldg(src + i);
+            } else {
+                for (uint32_t i = tid; i < n; i += NT) buf[i] = __ldg(src + i);
+            }
         }
         __syncthreads();
-        return 0;
+        return kRows;
     }
     if (c.codec == GX_CODEC_LZ4) {
-        const uint32_t bytes16 = (d.comp_bytes + 15u) & ~15u;
-        int rc = stage_block<NT>(c, blk, bytes16, stage, mbar, phase);
+        uint32_t lo = 0, hi = d.comp_bytes, j0 = 0, nseg = 0, seg_rows = 0;
+        if (c.S > 1) {
+            seg_rows = 1u << c.seg_shift;
+            j0 = r0 >> c.seg_shift;
+            nseg = (n + seg_rows - 1) >> c.seg_shift;
+            const uint32_t tile_span = (uint32_t)MAXT < c.rows_per_block ? (uint32_t)MAXT : c.rows_per_block;
+            const uint32_t jn = j0 + (tile_span >> c.seg_shift);
+            const uint32_t* e = c.seg + (size_t)2 * c.S * slot;
+            lo = __ldg(e + 2 * j0);
+            hi = jn < c.S ? __ldg(e + 2 * jn) : d.comp_bytes;
+            if ((r0 & (seg_rows - 1)) || j0 + nseg > c.S || lo > hi || hi > d.comp_bytes) {
+                if (tid == 0) *s_err = kErrCorrupt;
+                __syncthreads();
+                return -1;
+            }
+        } else if (r0 != 0 || n != rows) {  // plain LZ4 decodes whole blocks only
+            if (tid == 0) *s_err = kErrInvalid;
+            __syncthreads();
+            return -1;
+        }
+        const uint32_t wbase = lo & ~15u;
+        const uint32_t bytes = ((hi + 15u) & ~15u) - wbase + 16u;
+        if (bytes > C::kStage) {
+            if (tid == 0) *s_err = kErrCorrupt;
+            __syncthreads();
+            return -1;
+        }
+        const int rc = stage_bytes<NT>(c, blk + wbase, bytes, stage, mbar, phase);
         if (rc && tid == 0) *s_err = rc;
         __syncthreads();
         if (rc) return -1;
-        const SharedSrc src{stage};
-        int layout = 0;
         if (c.S > 1) {
-            const uint32_t seg_rows = 1u << c.seg_shift;
-            for (uint32_t j = tid; j < c.S; j += NT) {
-                const uint32_t ob = min(j * seg_rows, rows) * 4, oe = min((j + 1) * seg_rows, rows) * 4;
-                const uint32_t* e = c.seg + (size_t)2 * c.S * slot + 2 * j;
-                const uint32_t comp_pos = __ldg(e), info = __ldg(e + 1);
-                if (ob < oe) {
-                    int r2 = lz4_seg_lane(src, d.comp_bytes, comp_pos, info, ob, oe, buf + j * (seg_rows + 1));
-                    if (r2) *s_err = r2;
-                }
+            const uint32_t* e = c.seg + (size_t)2 * c.S * slot;
+            for (uint32_t t = tid; t < nseg; t += NT) {
+                const uint32_t j = j0 + t;
+                const uint32_t K = min(seg_rows, rows - j * seg_rows);
+                const int r2 = lz4_seg_lane((const uint32_t*)stage, wbase, lo, hi, d.comp_bytes, __ldg(e + 2 * j),
+                                            __ldg(e + 2 * j + 1), K, buf + t * (seg_rows + 1));
+                if (r2) *s_err = r2;
             }
-            layout = 1;
-        } else if (tid < 32) {
-            int r2 = lz4_warp_block(src, d.comp_bytes, (uint8_t*)buf, rows * 4, tid);
+            __syncthreads();
+            return kSegRows;
+        }
+        if (tid < 32) {
+            const int r2 = lz4_warp_block(SharedSrc{stage}, d.comp_bytes, (uint8_t*)buf, rows * 4, tid);
             if (r2 && tid == 0) *s_err = r2;
         }
         __syncthreads();
-        return layout;
+        return kRows;
     }
-    // cascaded: run tables live in the (idle) staging area
+    // cascaded: run tables live in the (idle) stage area
     int32_t* run_val = (int32_t*)stage;
     uint32_t* run_start = (uint32_t*)(stage + 4 * kCascMaxRuns);
-    int rc = casc_decode_block<NT>(blk, d.comp_bytes, rows, (int32_t*)buf, run_val, run_start, tmp);
+    const int rc = casc_decode_tile<NT>(blk, d.comp_bytes, rows, r0, n, (int32_t*)buf, run_val, run_start, tmp, ct);
     if (rc && tid == 0) *s_err = rc;
     __syncthreads();
-    return 0;
+    if (rc) return -1;
+    return ct->rle ? kRuns : kRows;
 }
 
-__global__ void __launch_bounds__(kScanThreads, 1) scan_kernel(const __grid_constant__ ScanParams P) {
-    constexpr int NT = kScanThreads;
+template <int NT, int MAXT>
+__global__ void __launch_bounds__(NT) scan_kernel(const __grid_constant__ ScanParams P) {
+    using C = Cfg<MAXT>;
     constexpr int NW = NT / 32;
     extern __shared__ __align__(16) uint8_t smem[];
     uint32_t* buf = (uint32_t*)smem;
-    uint32_t* aux = buf + kBufWords;
-    uint32_t* mask = aux + (P.need_aux ? kMaxRowsPerBlock : 0);
-    uint8_t* stage = (uint8_t*)(mask + kMaskWords);
-    uint32_t* gkeys = (uint32_t*)(stage + kStageBytes);
+    uint32_t* aux = buf + C::kBufWords;
+    uint32_t* mask = aux + (P.need_aux ? MAXT : 0);
+    uint8_t* stage = (uint8_t*)(mask + C::kMaskWords);
+    uint32_t* gkeys = (uint32_t*)(stage + C::kStage);
     unsigned long long* gsums = (unsigned long long*)(gkeys + (P.grouped ? (1u << kSmemGroupLog2) : 0));
+    const int32_t* run_val = (const int32_t*)stage;
+    const uint32_t* run_start = (const uint32_t*)(stage + 4 * kCascMaxRuns);
 
     __shared__ __align__(8) uint64_t s_mbar;
     __shared__ uint32_t s_item;
@@ -209,6 +260,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) scan_kernel(const __grid_cons
     __shared__ uint32_t s_alive;
     __shared__ uint32_t s_tmp[NW + 1];
     __shared__ unsigned long long s_red[NW];
+    __shared__ CascTile s_ct;
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (P.grouped) {
@@ -225,8 +277,9 @@ __global__ void __launch_bounds__(kScanThreads, 1) scan_kernel(const __grid_cons
     uint32_t phase = 0;
     int64_t local_sum = 0;
     unsigned long long local_rows = 0;
-    const uint32_t bpc = P.blocks_per_chunk;
-    const uint32_t total = *P.n_items * bpc;
+    const uint32_t tpb = P.tiles_per_block, tile_rows = P.tile_rows;
+    const uint32_t per_chunk = P.blocks_per_chunk * tpb;
+    const uint32_t total = *P.n_items * per_chunk;
     __syncthreads();
 
     while (true) {
@@ -235,86 +288,121 @@ __global__ void __launch_bounds__(kScanThreads, 1) scan_kernel(const __grid_cons
         const uint32_t it = s_item;
         __syncthreads();
         if (it >= total) break;
-        const uint32_t chunk = P.items[it / bpc];
-        const uint32_t slot = chunk * bpc + it % bpc;
+        const uint32_t rem = it % per_chunk;
+        const uint32_t slot = P.items[it / per_chunk] * P.blocks_per_chunk + rem / tpb;
+        const uint32_t r0 = (rem % tpb) * tile_rows;
         const uint32_t rows = P.steps[0].col.blocks[slot].n_rows;
-        if (rows == 0) continue;
-        const uint32_t ngroups = (rows + 31) / 32;
+        if (r0 >= rows) continue;
+        const uint32_t n = min(tile_rows, rows - r0);
+        const uint32_t ngroups = (n + 31) / 32;
         for (uint32_t g = tid; g < ngroups; g += NT)
-            mask[g] = (g + 1) * 32 <= rows ? 0xFFFFFFFFu : ((1u << (rows & 31)) - 1u);
-        if (tid == 0) local_rows += rows;
+            mask[g] = (g + 1) * 32 <= n ? 0xFFFFFFFFu : ((1u << (n & 31)) - 1u);
+        if (tid == 0) local_rows += n;
         __syncthreads();
 
         for (uint32_t si = 0; si < P.n_steps; ++si) {
             const ScanStep& st = P.steps[si];
-            const int layout = decode_tile<NT>(st.col, slot, rows, buf, stage, &s_mbar, phase, s_tmp, &s_err);
+            int layout = decode_tile<NT, MAXT>(st.col, slot, rows, r0, n, buf, stage, &s_mbar, phase, s_tmp, &s_ct,
+                                               &s_err);
             const int derr = s_err;
             __syncthreads();  // every thread has read s_err before it is reset
             if (derr) {       // corrupt block: drop the tile, remember the error
                 if (tid == 0) {
                     raise_error(derr);
                     s_err = 0;
-                    if (derr == kErrTimeout) s_fatal = 1;  // staging buffer no longer trusted
+                    if (derr == kErrTimeout) s_fatal = 1;  // the stage may still be written: stop this CTA
                 }
                 __syncthreads();
                 break;
             }
-            const uint32_t shift = st.col.seg_shift;
+            const bool per_row = (st.flags & (GX_STEP_CARRY | GX_STEP_VALUE)) || st.digit_card;
+            if (layout == kRuns && per_row) {
+                casc_runs_to_rows<NT>(s_ct, run_val, run_start, r0, n, (int32_t*)buf);
+                layout = kRows;
+            }
             if (tid == 0) s_alive = 0;
             __syncthreads();
             uint32_t alive_w = 0;
-            for (uint32_t g = warp; g < ngroups; g += NW) {
-                const uint32_t m = mask[g];
-                if (m == 0) continue;
-                const uint32_t r = g * 32 + lane;
-                bool keep = (m >> lane) & 1u;
-                int32_t v = 0;
-                if (keep) v = (int32_t)buf[layout == 1 ? r + (r >> shift) : r];
-                if ((st.flags & GX_STEP_FILTER) && keep) keep = v >= st.lo && v <= st.hi;
-                if ((st.flags & GX_STEP_PROBE) && keep) {
-                    int32_t p = 0;
-                    keep = ht_probe(st.ht, st.ht_log2, v, &p);
-                    if (keep && st.digit_card) {
-                        uint32_t dgt = (uint32_t)(p - st.digit_base);
-                        if (dgt >= st.digit_card) {
-                            raise_error(kErrInvalid);
-                            keep = false;
-                        } else {
-                            aux[r] = st.first_digit ? dgt : aux[r] * st.digit_card + dgt;
+            if (layout == kRuns) {
+                // predicate per run: rows of failing runs leave the mask
+                const CascTile ct = s_ct;
+                for (uint32_t i = ct.ra + tid; i < ct.rb; i += NT) {
+                    const int32_t v = run_val[i];
+                    bool pass = true;
+                    if (st.flags & GX_STEP_FILTER) pass = v >= st.lo && v <= st.hi;
+                    if ((st.flags & GX_STEP_PROBE) && pass) {
+                        int32_t p;
+                        pass = ht_probe(st.ht, st.ht_log2, v, &p);
+                    }
+                    if (!pass) {
+                        const uint32_t a = max(run_start[i], r0) - r0, b = min(run_start[i + 1], r0 + n) - r0;
+                        for (uint32_t r = a; r < b;) {
+                            const uint32_t w = r >> 5, hb = min(b, (w + 1) * 32);
+                            const uint32_t bits = (hb - r == 32) ? 0xFFFFFFFFu : (((1u << (hb - r)) - 1u) << (r & 31));
+                            atomicAnd(&mask[w], ~bits);
+                            r = hb;
                         }
                     }
                 }
-                if ((st.flags & GX_STEP_CARRY) && keep) aux[r] = (uint32_t)v;
-                if (st.flags & GX_STEP_VALUE) {
-                    int64_t val = 0;
-                    if (keep) {
-                        if (P.agg == GX_AGG_SUM_PRODUCT) val = (int64_t)v * (int64_t)(int32_t)aux[r];
-                        else if (P.agg == GX_AGG_COUNT) val = 1;
-                        else val = v;
-                    }
-                    if (!P.grouped) {
-                        local_sum += val;
-                    } else {
-                        const uint32_t gk = keep ? aux[r] : 0;
-                        uint32_t active = __ballot_sync(0xFFFFFFFFu, keep);
-                        while (active) {
-                            const int leader = __ffs(active) - 1;
-                            const uint32_t lk = __shfl_sync(0xFFFFFFFFu, gk, leader);
-                            const bool peer = keep && gk == lk && ((active >> lane) & 1u);
-                            const uint32_t peers = __ballot_sync(0xFFFFFFFFu, peer);
-                            const uint64_t tot = warp_sum_u64(peer ? (uint64_t)val : 0ull);
-                            if ((int)lane == leader) {
-                                if (!group_add_smem(gkeys, gsums, kSmemGroupLog2, lk, tot))
-                                    if (!group_add_global(P.g_keys, P.g_sums, P.g_log2, (int64_t)lk, (int64_t)tot))
-                                        raise_error(kErrCapacity);
+                __syncthreads();
+                for (uint32_t g = warp; g < ngroups; g += NW)
+                    if (lane == 0) alive_w += __popc(mask[g]);
+            } else {
+                const uint32_t shift = st.col.seg_shift;
+                for (uint32_t g = warp; g < ngroups; g += NW) {
+                    const uint32_t m = mask[g];
+                    if (m == 0) continue;
+                    const uint32_t r = g * 32 + lane;
+                    bool keep = (m >> lane) & 1u;
+                    int32_t v = 0;
+                    if (keep) v = (int32_t)buf[layout == kSegRows ? r + (r >> shift) : r];
+                    if ((st.flags & GX_STEP_FILTER) && keep) keep = v >= st.lo && v <= st.hi;
+                    if ((st.flags & GX_STEP_PROBE) && keep) {
+                        int32_t p = 0;
+                        keep = ht_probe(st.ht, st.ht_log2, v, &p);
+                        if (keep && st.digit_card) {
+                            const uint32_t dgt = (uint32_t)(p - st.digit_base);
+                            if (dgt >= st.digit_card) {
+                                raise_error(kErrInvalid);
+                                keep = false;
+                            } else {
+                                aux[r] = st.first_digit ? dgt : aux[r] * st.digit_card + dgt;
                             }
-                            active &= ~peers;
                         }
                     }
+                    if ((st.flags & GX_STEP_CARRY) && keep) aux[r] = (uint32_t)v;
+                    if (st.flags & GX_STEP_VALUE) {
+                        int64_t val = 0;
+                        if (keep) {
+                            if (P.agg == GX_AGG_SUM_PRODUCT) val = (int64_t)v * (int64_t)(int32_t)aux[r];
+                            else if (P.agg == GX_AGG_COUNT) val = 1;
+                            else val = v;
+                        }
+                        if (!P.grouped) {
+                            local_sum += val;
+                        } else {
+                            // warp-aggregated update of the shared partial group table
+                            const uint32_t gk = keep ? aux[r] : 0;
+                            uint32_t active = __ballot_sync(0xFFFFFFFFu, keep);
+                            while (active) {
+                                const int leader = __ffs(active) - 1;
+                                const uint32_t lk = __shfl_sync(0xFFFFFFFFu, gk, leader);
+                                const bool peer = keep && gk == lk && ((active >> lane) & 1u);
+                                const uint32_t peers = __ballot_sync(0xFFFFFFFFu, peer);
+                                const uint64_t tot = warp_sum_u64(peer ? (uint64_t)val : 0ull);
+                                if ((int)lane == leader) {
+                                    if (!group_add_smem(gkeys, gsums, kSmemGroupLog2, lk, tot))
+                                        if (!group_add_global(P.g_keys, P.g_sums, P.g_log2, (int64_t)lk, (int64_t)tot))
+                                            raise_error(kErrCapacity);
+                                }
+                                active &= ~peers;
+                            }
+                        }
+                    }
+                    const uint32_t nm = __ballot_sync(0xFFFFFFFFu, keep);
+                    if (lane == 0) mask[g] = nm;
+                    alive_w += __popc(nm);
                 }
-                const uint32_t nm = __ballot_sync(0xFFFFFFFFu, keep);
-                if (lane == 0) mask[g] = nm;
-                alive_w += __popc(nm);
             }
             if (lane == 0 && alive_w) atomicAdd(&s_alive, alive_w);
             __syncthreads();
@@ -347,10 +435,12 @@ __global__ void __launch_bounds__(kScanThreads, 1) scan_kernel(const __grid_cons
     }
 }
 
-// One CTA: per-chunk keep flags (AND over min/max predicates), compaction
-// of the surviving chunk ids, reset of the work counter.
+// One CTA: per-chunk keep flags (AND over min/max predicates and the
+// optional input flags), order-preserving compaction of the surviving chunk
+// ids, reset of the work counter.
 __global__ void __launch_bounds__(1024) items_kernel(const __grid_constant__ ItemsParams P) {
     __shared__ uint32_t s_count;
+    __shared__ uint32_t s_warp[32];
     if (threadIdx.x == 0) s_count = 0;
     __syncthreads();
     for (uint32_t base = 0; base < P.n_chunks; base += blockDim.x) {
@@ -364,16 +454,14 @@ __global__ void __launch_bounds__(1024) items_kernel(const __grid_constant__ Ite
             }
             if (P.keep_out) P.keep_out[c] = keep ? 1 : 0;
         }
-        // order-preserving compaction within this round
         const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const uint32_t b = __ballot_sync(0xFFFFFFFFu, keep);
-        __shared__ uint32_t s_warp[32];
         if (lane == 0) s_warp[warp] = __popc(b);
         __syncthreads();
         if (threadIdx.x == 0) {
             uint32_t run = s_count;
             for (uint32_t w = 0; w < blockDim.x / 32; ++w) {
-                uint32_t x = s_warp[w];
+                const uint32_t x = s_warp[w];
                 s_warp[w] = run;
                 run += x;
             }
@@ -389,36 +477,45 @@ __global__ void __launch_bounds__(1024) items_kernel(const __grid_constant__ Ite
     }
 }
 
-// Decompress slots [slot0, slot0 + gridDim.x) of a column into dst (rows
-// laid out contiguously from the first row of slot0).
-__global__ void __launch_bounds__(kDecThreads) decompress_kernel(const gx_dcol c, uint32_t slot0,
-                                                                 uint64_t row0, int32_t* dst) {
-    constexpr int NT = kDecThreads;
+// Decompress tiles of slots [slot0, slot0 + gridDim.x / tpb) into dst, rows
+// laid out contiguously from the first row of chunk row0.  One CTA per tile.
+template <int NT, int MAXT>
+__global__ void __launch_bounds__(NT) decompress_kernel(const gx_dcol c, uint32_t slot0, uint32_t tile_rows,
+                                                        uint32_t tpb, uint64_t row0, int32_t* dst) {
+    using C = Cfg<MAXT>;
     extern __shared__ __align__(16) uint8_t smem[];
     uint32_t* buf = (uint32_t*)smem;
-    uint8_t* stage = (uint8_t*)(buf + kBufWords);
+    uint8_t* stage = (uint8_t*)(buf + C::kBufWords);
     __shared__ __align__(8) uint64_t s_mbar;
     __shared__ int s_err;
     __shared__ uint32_t s_tmp[NT / 32 + 1];
-    const uint32_t slot = slot0 + blockIdx.x;
+    __shared__ CascTile s_ct;
+    const uint32_t slot = slot0 + blockIdx.x / tpb;
+    const uint32_t r0 = (blockIdx.x % tpb) * tile_rows;
     const gx_dblock d = c.blocks[slot];
-    if (d.n_rows == 0) return;
+    if (r0 >= d.n_rows) return;
+    const uint32_t n = min(tile_rows, d.n_rows - r0);
     if (threadIdx.x == 0) {
         s_err = 0;
         mbar_init(&s_mbar, 1);
     }
     __syncthreads();
     uint32_t phase = 0;
-    const int layout = decode_tile<NT>(c, slot, d.n_rows, buf, stage, &s_mbar, phase, s_tmp, &s_err);
+    int layout = decode_tile<NT, MAXT>(c, slot, d.n_rows, r0, n, buf, stage, &s_mbar, phase, s_tmp, &s_ct, &s_err);
     if (s_err) {
         if (threadIdx.x == 0) raise_error(s_err);
         return;
     }
+    if (layout == kRuns) {
+        casc_runs_to_rows<NT>(s_ct, (const int32_t*)stage, (const uint32_t*)(stage + 4 * kCascMaxRuns), r0, n,
+                              (int32_t*)buf);
+        layout = kRows;
+    }
     const uint32_t chunk = slot / c.blocks_per_chunk, j = slot % c.blocks_per_chunk;
-    const uint64_t first = (uint64_t)chunk * c.rows_per_chunk + (uint64_t)j * c.rows_per_block - row0;
+    const uint64_t first = (uint64_t)chunk * c.rows_per_chunk + (uint64_t)j * c.rows_per_block + r0 - row0;
     int32_t* out = dst + first;
-    for (uint32_t r = threadIdx.x; r < d.n_rows; r += NT)
-        out[r] = (int32_t)buf[layout == 1 ? r + (r >> c.seg_shift) : r];
+    for (uint32_t r = threadIdx.x; r < n; r += NT)
+        out[r] = (int32_t)buf[layout == kSegRows ? r + (r >> c.seg_shift) : r];
 }
 
 __global__ void raw_lz4_kernel(const uint8_t* comp, const uint64_t* coff, uint8_t* out, const uint64_t* ooff,
@@ -551,18 +648,21 @@ uint32_t log2_ceil(uint64_t x) {
     return l;
 }
 
+template <int MAXT>
 size_t scan_smem_bytes(bool need_aux, bool grouped) {
-    size_t b = 4ull * kBufWords;
-    if (need_aux) b += 4ull * kMaxRowsPerBlock;
-    b += 4ull * kMaskWords;
-    b += kStageBytes;  // also holds the cascaded run tables
+    using C = Cfg<MAXT>;
+    size_t b = 4ull * C::kBufWords;
+    if (need_aux) b += 4ull * MAXT;
+    b += 4ull * C::kMaskWords;
+    b += C::kStage;  // also holds the cascaded run tables
     if (grouped) b += (4ull + 8ull) * (1u << kSmemGroupLog2);
     return b;
 }
 
-size_t dec_smem_bytes() { return 4ull * kBufWords + kStageBytes; }
-
-static_assert(4 * kCascMaxRuns + 4 * (kCascMaxRuns + 4) <= kStageBytes, "run tables fit the staging area");
+template <int MAXT>
+size_t dec_smem_bytes() {
+    return 4ull * Cfg<MAXT>::kBufWords + Cfg<MAXT>::kStage;
+}
 
 gx_status wait_stream(cudaStream_t s, double timeout_s) {
     auto t0 = std::chrono::steady_clock::now();
@@ -574,6 +674,26 @@ gx_status wait_stream(cudaStream_t s, double timeout_s) {
         if (el > timeout_s) return set_error(GX_ERR_TIMEOUT, "stream did not finish within %.0f s", timeout_s);
         std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 5 : 200));
     }
+}
+
+// Tile size usable for a set of columns: kTileRows when every LZ4 column is
+// segmented with segments no longer than a tile, else whole blocks.
+uint32_t pick_tile_rows(const gx_column* const* cols, uint32_t n) {
+    const uint32_t rb = cols[0]->rows_per_block;
+    if (rb <= kTileRows) return rb;
+    for (uint32_t i = 0; i < n; ++i) {
+        const gx_column* c = cols[i];
+        if (c->codec == GX_CODEC_LZ4 && (c->S <= 1 || (1u << c->seg_shift) > kTileRows)) return rb;
+    }
+    return kTileRows;
+}
+
+// Per-device setup of a kernel's dynamic shared-memory limit.
+template <class K>
+gx_status allow_smem(K kernel, size_t bytes) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+    return GX_OK;
 }
 
 }  // namespace
@@ -653,15 +773,23 @@ gx_status gx_decompress_chunks(const gx_column* col, uint64_t first_chunk, uint6
     int dev = 0;
     cudaGetDevice(&dev);
     if (!attr_set[dev & 63]) {
-        GX_CK(cudaFuncSetAttribute(decompress_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)dec_smem_bytes()));
+        gx_status st = allow_smem(decompress_kernel<128, kTileRows>, dec_smem_bytes<kTileRows>());
+        if (!st) st = allow_smem(decompress_kernel<256, kMaxRowsPerBlock>, dec_smem_bytes<kMaxRowsPerBlock>());
+        if (st) return st;
         attr_set[dev & 63] = true;
     }
     const uint32_t slot0 = (uint32_t)(first_chunk * col->blocks_per_chunk);
     const uint32_t nslots = (uint32_t)(n_chunks * col->blocks_per_chunk);
     const uint64_t row0 = first_chunk * (uint64_t)col->rows_per_chunk;
-    decompress_kernel<<<nslots, kDecThreads, dec_smem_bytes(), (cudaStream_t)stream>>>(col->view(), slot0, row0,
-                                                                                        (int32_t*)dst_dev);
+    const uint32_t tile = pick_tile_rows(&col, 1);
+    const uint32_t tpb = (col->rows_per_block + tile - 1) / tile;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (tile <= kTileRows)
+        decompress_kernel<128, kTileRows><<<nslots * tpb, 128, dec_smem_bytes<kTileRows>(), s>>>(
+            col->view(), slot0, tile, tpb, row0, (int32_t*)dst_dev);
+    else
+        decompress_kernel<256, kMaxRowsPerBlock><<<nslots * tpb, 256, dec_smem_bytes<kMaxRowsPerBlock>(), s>>>(
+            col->view(), slot0, tile, tpb, row0, (int32_t*)dst_dev);
     GX_CK(cudaGetLastError());
     return GX_OK;
 }
@@ -701,25 +829,16 @@ gx_status gx_combine_and(uint16_t* out_dev, const uint16_t* a_dev, const uint16_
     return GX_OK;
 }
 
-static gx_status launch_items(const gx_column* const* cols, const int32_t* lo, const int32_t* hi, uint32_t n_preds,
-                              uint32_t n_chunks, const uint16_t* keep_in, uint16_t* keep_out, uint32_t* items,
-                              uint32_t* n_items, uint32_t* counter, cudaStream_t s) {
-    ItemsParams ip{};
+static gx_status fill_prune(ItemsParams* ip, const gx_column* const* cols, const int32_t* lo, const int32_t* hi,
+                            uint32_t n_preds, uint32_t n_chunks) {
     if (n_preds > GX_MAX_STEPS) return set_error(GX_ERR_INVALID, "too many prune predicates");
     for (uint32_t p = 0; p < n_preds; ++p) {
         if (!cols[p] || !cols[p]->residency) return set_error(GX_ERR_INVALID, "prune column %u not on device", p);
         if (cols[p]->n_chunks != n_chunks) return set_error(GX_ERR_INVALID, "prune columns disagree on chunk count");
-        ip.preds[p] = PrunePred{cols[p]->d_mins, cols[p]->d_maxs, lo[p], hi[p]};
+        ip->preds[p] = PrunePred{cols[p]->d_mins, cols[p]->d_maxs, lo[p], hi[p]};
     }
-    ip.n_preds = n_preds;
-    ip.n_chunks = n_chunks;
-    ip.keep_in = keep_in;
-    ip.keep_out = keep_out;
-    ip.items = items;
-    ip.n_items = n_items;
-    ip.work_counter = counter;
-    items_kernel<<<1, 1024, 0, s>>>(ip);
-    GX_CK(cudaGetLastError());
+    ip->n_preds = n_preds;
+    ip->n_chunks = n_chunks;
     return GX_OK;
 }
 
@@ -728,11 +847,20 @@ gx_status gx_prune_minmax(const gx_column* const* cols, const int32_t* lo, const
     if (!cols || !lo || !hi || !keep_dev || n_preds == 0) return set_error(GX_ERR_INVALID, "gx_prune_minmax: bad args");
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t n_chunks = cols[0]->n_chunks;
+    ItemsParams ip{};
+    gx_status st = fill_prune(&ip, cols, lo, hi, n_preds, n_chunks);
+    if (st) return st;
     uint32_t* scratch = nullptr;
     GX_CK(cudaMallocAsync(&scratch, 4ull * (n_chunks + 2), s));
-    gx_status st = launch_items(cols, lo, hi, n_preds, n_chunks, nullptr, keep_dev, scratch + 2, scratch, scratch + 1, s);
+    ip.keep_out = keep_dev;
+    ip.items = scratch + 2;
+    ip.n_items = scratch;
+    ip.work_counter = scratch + 1;
+    items_kernel<<<1, 1024, 0, s>>>(ip);
+    cudaError_t e = cudaGetLastError();
     cudaFreeAsync(scratch, s);
-    return st;
+    if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "items_kernel: %s", cudaGetErrorString(e));
+    return GX_OK;
 }
 
 // ------------------------------------------------------------ hash tables
@@ -791,6 +919,21 @@ gx_status gx_hashtable_count(const gx_hashtable* ht, uint64_t* n_entries, void* 
     return GX_OK;
 }
 
+gx_status gx_hashtable_view(const gx_hashtable* ht, const uint64_t** slots_dev, uint32_t* log2cap) {
+    if (!ht || !slots_dev || !log2cap) return set_error(GX_ERR_INVALID, "gx_hashtable_view: null argument");
+    *slots_dev = ht->slots;
+    *log2cap = ht->log2cap;
+    return GX_OK;
+}
+
+gx_status gx_groupby_view(gx_groupby* gb, int64_t** keys_dev, int64_t** sums_dev, uint32_t* log2cap) {
+    if (!gb || !keys_dev || !sums_dev || !log2cap) return set_error(GX_ERR_INVALID, "gx_groupby_view: null argument");
+    *keys_dev = gb->keys;
+    *sums_dev = gb->sums;
+    *log2cap = gb->log2cap;
+    return GX_OK;
+}
+
 gx_status gx_hashtable_probe(const gx_hashtable* ht, const int32_t* keys_dev, uint64_t n, int32_t* payload_out_dev,
                              uint64_t* hits_dev, void* stream) {
     if (!ht || (!keys_dev && n)) return set_error(GX_ERR_INVALID, "gx_hashtable_probe: bad args");
@@ -816,8 +959,10 @@ gx_status gx_groupby_create(uint64_t max_groups, gx_groupby** out) {
         return set_error(GX_ERR_NOMEM, "gx_groupby_create: %s", cudaGetErrorString(e));
     }
     *out = g;
-    return gx_groupby_reset(g, nullptr) == GX_OK ? (cudaDeviceSynchronize() == cudaSuccess ? GX_OK : GX_ERR_CUDA)
-                                                  : GX_ERR_CUDA;
+    gx_status st = gx_groupby_reset(g, nullptr);
+    if (st) return st;
+    GX_CK(cudaDeviceSynchronize());
+    return GX_OK;
 }
 
 gx_status gx_groupby_free(gx_groupby* gb) {
@@ -883,14 +1028,16 @@ gx_status gx_groupby_read(gx_groupby* gb, int64_t* keys_host, int64_t* sums_host
 
 // ------------------------------------------------------------------- scan
 
-static gx_status build_scan_params(const gx_scan_plan* plan, ScanParams* P, const gx_column** ref_col) {
+static gx_status build_scan_params(const gx_scan_plan* plan, ScanParams* P, ItemsParams* ip, const gx_column** ref_col) {
     if (!plan || plan->n_steps == 0 || plan->n_steps > GX_MAX_STEPS)
         return set_error(GX_ERR_INVALID, "scan plan needs 1..%d steps", GX_MAX_STEPS);
     std::memset(P, 0, sizeof(*P));
+    std::memset(ip, 0, sizeof(*ip));
     const gx_column* c0 = plan->steps[0].col;
     if (!c0 || !c0->residency) return set_error(GX_ERR_INVALID, "step 0 column is not on the device");
     bool any_value = false, any_digit = false, any_carry = false;
     uint64_t card_prod = 1;
+    const gx_column* cols[GX_MAX_STEPS];
     for (uint32_t i = 0; i < plan->n_steps; ++i) {
         const gx_scan_step& s = plan->steps[i];
         const gx_column* c = s.col;
@@ -900,6 +1047,7 @@ static gx_status build_scan_params(const gx_scan_plan* plan, ScanParams* P, cons
             return set_error(GX_ERR_INVALID, "step %u column layout differs from step 0", i);
         if (s.flags == 0 || (s.flags & ~(uint32_t)(GX_STEP_FILTER | GX_STEP_PROBE | GX_STEP_CARRY | GX_STEP_VALUE)))
             return set_error(GX_ERR_INVALID, "step %u has invalid flags", i);
+        cols[i] = c;
         ScanStep& d = P->steps[i];
         d.col = c->view();
         d.flags = s.flags;
@@ -932,54 +1080,72 @@ static gx_status build_scan_params(const gx_scan_plan* plan, ScanParams* P, cons
     P->grouped = plan->groupby ? 1 : 0;
     P->need_aux = (any_carry || any_digit) ? 1 : 0;
     P->blocks_per_chunk = c0->blocks_per_chunk;
+    P->tile_rows = pick_tile_rows(cols, plan->n_steps);
+    P->tiles_per_block = (c0->rows_per_block + P->tile_rows - 1) / P->tile_rows;
     P->result = plan->result_dev;
     if (plan->groupby) {
         P->g_keys = plan->groupby->keys;
         P->g_sums = plan->groupby->sums;
         P->g_log2 = plan->groupby->log2cap;
     }
+    // pruning predicates of the plan
+    if (plan->n_prune > GX_MAX_STEPS) return set_error(GX_ERR_INVALID, "too many prune predicates");
+    const gx_column* pc[GX_MAX_STEPS];
+    int32_t plo[GX_MAX_STEPS], phi[GX_MAX_STEPS];
+    for (uint32_t i = 0; i < plan->n_prune; ++i) {
+        pc[i] = plan->prune[i].col;
+        plo[i] = plan->prune[i].lo;
+        phi[i] = plan->prune[i].hi;
+    }
+    gx_status st = fill_prune(ip, pc, plo, phi, plan->n_prune, c0->n_chunks);
+    if (st) return st;
+    ip->keep_in = plan->keep_chunks_dev;
+    ip->keep_out = plan->keep_out_dev;
     *ref_col = c0;
     return GX_OK;
 }
 
 static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned long long* rows_dev) {
     ScanParams P;
+    ItemsParams ip;
     const gx_column* c0 = nullptr;
-    gx_status st = build_scan_params(plan, &P, &c0);
+    gx_status st = build_scan_params(plan, &P, &ip, &c0);
     if (st) return st;
-    const uint32_t n_chunks = c0->n_chunks;
-    uint32_t* scratch = nullptr;
-    GX_CK(cudaMallocAsync(&scratch, 4ull * (n_chunks + 4), s));
-    uint32_t* n_items = scratch;
-    uint32_t* counter = scratch + 1;
-    uint32_t* items = scratch + 4;
-    st = launch_items(nullptr, nullptr, nullptr, 0, n_chunks, plan->keep_chunks_dev, nullptr, items, n_items, counter, s);
-    if (st) {
-        cudaFreeAsync(scratch, s);
-        return st;
-    }
-    P.items = items;
-    P.n_items = n_items;
-    P.work_counter = counter;
-    P.rows_scanned = rows_dev;
-    const size_t smem = scan_smem_bytes(P.need_aux, P.grouped);
     static bool attr_set[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (!attr_set[dev & 63]) {
-        cudaError_t e = cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)scan_smem_bytes(true, true));
-        if (e != cudaSuccess) {
-            cudaFreeAsync(scratch, s);
-            return set_error(GX_ERR_CUDA, "cudaFuncSetAttribute(scan_kernel): %s", cudaGetErrorString(e));
-        }
+        st = allow_smem(scan_kernel<128, kTileRows>, scan_smem_bytes<kTileRows>(true, true));
+        if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
+        if (st) return st;
         attr_set[dev & 63] = true;
     }
-    const uint32_t grid = std::min<uint32_t>((uint32_t)sm_count(), n_chunks * c0->blocks_per_chunk);
-    scan_kernel<<<std::max(1u, grid), kScanThreads, smem, s>>>(P);
+    const uint32_t n_chunks = c0->n_chunks;
+    uint32_t* scratch = nullptr;
+    GX_CK(cudaMallocAsync(&scratch, 4ull * (n_chunks + 4), s));
+    ip.n_items = scratch;
+    ip.work_counter = scratch + 1;
+    ip.items = scratch + 4;
+    items_kernel<<<1, 1024, 0, s>>>(ip);
+    P.items = ip.items;
+    P.n_items = ip.n_items;
+    P.work_counter = ip.work_counter;
+    P.rows_scanned = rows_dev;
+    const uint64_t tiles = (uint64_t)n_chunks * c0->blocks_per_chunk * P.tiles_per_block;
+    if (P.tile_rows <= kTileRows) {
+        const size_t smem = scan_smem_bytes<kTileRows>(P.need_aux, P.grouped);
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_kernel<128, kTileRows>, 128, smem);
+        const uint64_t grid = std::min<uint64_t>((uint64_t)sm_count() * std::max(1, per_sm), tiles);
+        scan_kernel<128, kTileRows><<<(unsigned)std::max<uint64_t>(1, grid), 128, smem, s>>>(P);
+    } else {
+        const size_t smem = scan_smem_bytes<kMaxRowsPerBlock>(P.need_aux, P.grouped);
+        const uint64_t grid = std::min<uint64_t>(sm_count(), tiles);
+        scan_kernel<256, kMaxRowsPerBlock><<<(unsigned)std::max<uint64_t>(1, grid), 256, smem, s>>>(P);
+    }
     cudaError_t e = cudaGetLastError();
     cudaFreeAsync(scratch, s);
-    if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "scan_kernel launch: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "scan launch: %s", cudaGetErrorString(e));
     return GX_OK;
 }
 

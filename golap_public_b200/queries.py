@@ -20,7 +20,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib as L
-from .api import Column, HashAggregate, HashMap, MetaChecker, ScanPlan, _stream_handle
+from .api import Column, HashAggregate, HashMap, ScanPlan
 
 
 def _dev(a):
@@ -35,7 +35,7 @@ class FactTable:
     n_rows: int
 
 
-def encode_fact(data: dict, codecs: dict, rows_per_chunk=1_000_000, rows_per_block=16384, lz4_segments=32,
+def encode_fact(data: dict, codecs: dict, rows_per_chunk=1_000_000, rows_per_block=16384, lz4_segments=128,
                 residency="hbm", threads=0, **kw) -> FactTable:
     cols = {}
     for name, v in data.items():
@@ -62,10 +62,11 @@ class Q1Query:
         self.prune = prune
         n_chunks = fact.cols["date_key"].info.n_chunks
         self.keep = torch.zeros(n_chunks, dtype=torch.uint16, device="cuda") if prune else None
-        self.checker = MetaChecker(n_chunks).add_minmax(fact.cols["date_key"], date_lo, date_hi)
         self.result = torch.zeros(1, dtype=torch.int64, device="cuda")
         c = fact.cols
-        self.plan = ScanPlan(agg=L.GX_AGG_SUM_PRODUCT, keep_chunks=self.keep, result=self.result)
+        self.plan = ScanPlan(agg=L.GX_AGG_SUM_PRODUCT, result=self.result, keep_out=self.keep)
+        if prune:  # MetaChecker::add_minmax on the date column, evaluated by the scan launch
+            self.plan.prune_minmax(c["date_key"], date_lo, date_hi)
         self.plan.probe(c["date_key"], self.ht)
         self.plan.filter(c["discount"], dlo, dhi, carry=True)
         self.plan.filter(c["quantity"], qlo, qhi)
@@ -73,10 +74,8 @@ class Q1Query:
         self.plan.to_c()
 
     def launch(self, stream=None):
-        """Enqueue: clear result, prune, fused scan (no host synchronisation)."""
+        """Enqueue: clear result, prune + fused scan (no host synchronisation)."""
         self.result.zero_()
-        if self.prune:
-            self.checker.run(self.keep, stream)
         self.plan.launch(stream)
 
     def run(self, stream=None) -> int:
@@ -111,11 +110,12 @@ class Q3Query:
         n_chunks = fact.cols["date_key"].info.n_chunks
         self.prune = prune
         self.keep = torch.zeros(n_chunks, dtype=torch.uint16, device="cuda") if prune else None
-        self.checker = MetaChecker(n_chunks).add_minmax(fact.cols["date_key"], ylo * 10000 + 101, yhi * 10000 + 1231)
         self.ycard = yhi - ylo + 1
         self.agg = HashAggregate(n_nations * n_nations * self.ycard)
         c = fact.cols
-        self.plan = ScanPlan(agg=L.GX_AGG_SUM, keep_chunks=self.keep, groupby=self.agg)
+        self.plan = ScanPlan(agg=L.GX_AGG_SUM, groupby=self.agg, keep_out=self.keep)
+        if prune:
+            self.plan.prune_minmax(c["date_key"], ylo * 10000 + 101, yhi * 10000 + 1231)
         self.plan.probe(c["cust_key"], self.hc, 0, n_nations)
         self.plan.probe(c["supp_key"], self.hs, 0, n_nations)
         self.plan.probe(c["date_key"], self.hd, ylo, self.ycard)
@@ -124,8 +124,6 @@ class Q3Query:
 
     def launch(self, stream=None):
         self.agg.reset(stream)
-        if self.prune:
-            self.checker.run(self.keep, stream)
         self.plan.launch(stream)
 
     def decode_key(self, k: int):

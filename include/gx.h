@@ -182,6 +182,11 @@ gx_status gx_hashtable_count(const gx_hashtable* ht, uint64_t* n_entries, void* 
 gx_status gx_hashtable_probe(const gx_hashtable* ht, const int32_t* keys_dev, uint64_t n,
                              int32_t* payload_out_dev, uint64_t* hits_dev, void* stream);
 
+/* Device view of the table for probing from other kernels (slot format and
+ * hash in include/gx_hash.h): *slots_dev = 2^log2cap 64-bit slots.  Replaces
+ * passing HashMap by value to a kernel (core/dev_structs.cuh:71-82). */
+gx_status gx_hashtable_view(const gx_hashtable* ht, const uint64_t** slots_dev, uint32_t* log2cap);
+
 /* ---------------------------------------------------------- hash aggregate
  * Replaces: HashAggregate (core/dev_structs.cuh:158-253) with SumAgg
  * (usecases/ssb/queries/query_common.cuh:24-29) and the group_by_agg kernels
@@ -194,6 +199,10 @@ gx_status gx_groupby_reset(gx_groupby* gb, void* stream);
 /* sums[key] += vals[i] for i < n (device arrays). */
 gx_status gx_groupby_add(gx_groupby* gb, const int64_t* keys_dev, const int64_t* vals_dev,
                          uint64_t n, void* stream);
+/* Device view for aggregating from other kernels (format in include/gx_hash.h):
+ * 2^log2cap int64 keys and sums.  Replaces passing HashAggregate by value
+ * (core/dev_structs.cuh:196-207). */
+gx_status gx_groupby_view(gx_groupby* gb, int64_t** keys_dev, int64_t** sums_dev, uint32_t* log2cap);
 /* Copy the non-empty groups to host arrays (unordered); *n_groups = count.
  * Fails with GX_ERR_CAPACITY if cap is too small or the table overflowed. */
 gx_status gx_groupby_read(gx_groupby* gb, int64_t* keys_host, int64_t* sums_host, uint64_t cap,
@@ -234,6 +243,13 @@ typedef struct gx_scan_step {
     uint32_t digit_card;         /* PROBE: payload cardinality (0 = no digit)  */
 } gx_scan_step;
 
+/* Min/max pruning predicate evaluated by the scan itself (the MetaChecker
+ * pass of usecases/ssb/queries/01.hpp:263-281 folded into the launch). */
+typedef struct gx_scan_prune {
+    const gx_column* col;
+    int32_t lo, hi;
+} gx_scan_prune;
+
 typedef struct gx_scan_plan {
     uint32_t n_steps;
     gx_scan_step steps[GX_MAX_STEPS];
@@ -241,6 +257,9 @@ typedef struct gx_scan_plan {
     const uint16_t* keep_chunks_dev;  /* per-chunk keep flags or NULL (scan all) */
     gx_groupby* groupby;              /* NULL = scalar result                    */
     int64_t* result_dev;              /* scalar result (int64, device)           */
+    uint32_t n_prune;                 /* min/max predicates ANDed with keep_chunks */
+    gx_scan_prune prune[GX_MAX_STEPS];
+    uint16_t* keep_out_dev;           /* optional: resulting per-chunk flags     */
 } gx_scan_plan;
 
 /* Run the plan on `stream`.  Does not clear result_dev or the group table

@@ -16,7 +16,8 @@ def declared_functions():
     names = set()
     for h in (ROOT / "include").glob("*.h"):
         text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
-        names |= set(re.findall(r"\b(gx_[a-z0-9_]+)\s*\(", text))
+        # prototypes only (declarations ending in ';'), not inline helpers
+        names |= set(re.findall(r"\b(gx_[a-z0-9_]+)\s*\([^;{}]*\)\s*;", text))
     return names
 
 
@@ -41,7 +42,7 @@ def test_status_strings_and_errors():
     assert lib.gx_version().startswith(b"gx")
     o = L.EncodeOpts()
     assert lib.gx_encode_opts_default(C.byref(o)) == 0
-    assert o.rows_per_block == 16384 and o.lz4_segments == 32
+    assert o.rows_per_block == 16384 and o.lz4_segments == 128
     h = C.c_void_p()
     assert lib.gx_column_encode(None, 10, C.byref(o), C.byref(h)) == L.GX_ERR_INVALID
     assert "null" in L.last_error()

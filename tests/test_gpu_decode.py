@@ -30,7 +30,9 @@ def test_decompress_distributions(cuda, codec, S):
     f = datagen.fact_q1(2_500_000, True)
     rng = np.random.default_rng(1)
     cols = dict(f, random=rng.integers(-2**31, 2**31 - 1, 2_500_000, dtype=np.int64).astype(np.int32),
-                const=np.full(2_500_000, -3, np.int32))
+                const=np.full(2_500_000, -3, np.int32),
+                # strictly increasing: cascaded picks delta without RLE (tile prefix sums)
+                ramp=(np.arange(2_500_000, dtype=np.int64) * 3 + rng.integers(0, 3, 2_500_000) - 7).astype(np.int32))
     for name, v in cols.items():
         col = api.Column(v, codec, lz4_segments=S).to_device()
         got = _decode_all(col, cuda)
