@@ -16,7 +16,7 @@ u8p = C.POINTER(C.c_uint8)
 
 GX_OK, GX_ERR_CUDA, GX_ERR_CORRUPT, GX_ERR_CAPACITY, GX_ERR_TIMEOUT, GX_ERR_NOMEM, GX_ERR_INVALID = range(7)
 GX_CODEC_NONE, GX_CODEC_LZ4, GX_CODEC_CASCADED = 0, 1, 2
-GX_STEP_FILTER, GX_STEP_PROBE, GX_STEP_CARRY, GX_STEP_VALUE = 1, 2, 4, 8
+GX_STEP_FILTER, GX_STEP_PROBE, GX_STEP_CARRY, GX_STEP_VALUE, GX_STEP_GROUP = 1, 2, 4, 8, 16
 GX_AGG_SUM, GX_AGG_SUM_PRODUCT, GX_AGG_COUNT = 0, 1, 2
 GX_MAX_STEPS = 8
 
@@ -68,6 +68,10 @@ class ScanPlan(C.Structure):
                 ("prune", ScanPrune * GX_MAX_STEPS), ("keep_out_dev", P)]
 
 
+class Query(C.Structure):
+    _fields_ = [("plan", ScanPlan), ("row_lo", C.c_uint64), ("row_hi", C.c_uint64)]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "gx_status_str": (C.c_char_p, [C.c_int32]),
@@ -105,6 +109,11 @@ _SIGS = {
     "gx_scan": (C.c_int32, [C.POINTER(ScanPlan), P]),
     "gx_scan_sync": (C.c_int32, [C.POINTER(ScanPlan), P, C.POINTER(C.c_uint64)]),
     "gx_scan_check": (C.c_int32, [P]),
+    "gx_batch_create": (C.c_int32, [C.POINTER(Query), C.c_uint32, C.POINTER(P)]),
+    "gx_batch_free": (C.c_int32, [P]),
+    "gx_batch_run": (C.c_int32, [P, P]),
+    "gx_batch_graph": (C.c_int32, [P, P]),
+    "gx_batch_rows": (C.c_int32, [P, C.POINTER(C.c_uint64), P]),
 }
 
 _lib = None

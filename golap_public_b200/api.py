@@ -262,6 +262,11 @@ class ScanPlan:
         self.steps.append(Step(col, L.GX_STEP_PROBE, ht=ht, digit_base=digit_base, digit_card=digit_card))
         return self
 
+    def group(self, col, digit_base, digit_card):
+        """GROUP BY the column's value (one digit of the group key)."""
+        self.steps.append(Step(col, L.GX_STEP_GROUP, digit_base=digit_base, digit_card=digit_card))
+        return self
+
     def carry(self, col):
         self.steps.append(Step(col, L.GX_STEP_CARRY))
         return self
@@ -309,3 +314,42 @@ class ScanPlan:
 
 def scan_check(stream=None):
     check(L.lib().gx_scan_check(_stream_handle(stream)))
+
+
+class Batch:
+    """Many scan plans over one table, each on a row slice, in one persistent launch."""
+
+    def __init__(self, queries):
+        """queries: iterable of (ScanPlan, row_lo, row_hi)."""
+        queries = list(queries)
+        arr = (L.Query * len(queries))()
+        for i, (plan, lo, hi) in enumerate(queries):
+            arr[i].plan = plan.to_c()
+            arr[i].row_lo = lo
+            arr[i].row_hi = hi
+        self.plans = [q[0] for q in queries]
+        h = C.c_void_p()
+        check(L.lib().gx_batch_create(arr, len(queries), C.byref(h)))
+        self.handle = h
+
+    def run(self, stream=None):
+        check(L.lib().gx_batch_run(self.handle, _stream_handle(stream)))
+
+    def graph(self, stream=None):
+        check(L.lib().gx_batch_graph(self.handle, _stream_handle(stream)))
+
+    def rows(self, stream=None) -> int:
+        n = C.c_uint64()
+        check(L.lib().gx_batch_rows(self.handle, C.byref(n), _stream_handle(stream)))
+        return n.value
+
+    def free(self):
+        if self.handle:
+            L.lib().gx_batch_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -96,10 +96,7 @@ __device__ __forceinline__ int lz4_seg_lane(const uint32_t* __restrict__ A, uint
     uint32_t litw = 0, mw = 0, offw = 0, mnib = 0;
     uint32_t phase = 0;  // 0: next is a token, 1: next is a match offset
     uint32_t lwprev = 0, lsh = 0;
-    auto byte = [&](uint32_t i) -> uint32_t {
-        const uint32_t r = i - wbase;
-        return (A[r >> 2] >> ((r & 3u) * 8)) & 255u;
-    };
+#define GX_BYTE(i) ((A[((i) - wbase) >> 2] >> ((((i) - wbase) & 3u) * 8)) & 255u)
     if (info & 16u) {
         const uint32_t lit = info >> 5;
         if (lit & 3u) return kErrCorrupt;
@@ -117,14 +114,16 @@ __device__ __forceinline__ int lz4_seg_lane(const uint32_t* __restrict__ A, uint
         while (litw == 0 && mw == 0) {
             if (phase == 0) {
                 if (pos >= hi) return kErrCorrupt;
-                const uint32_t tok = byte(pos++);
+                const uint32_t tok = GX_BYTE(pos);
+                ++pos;
                 uint32_t lit = tok >> 4;
                 mnib = tok & 15u;
                 if (lit == 15) {
                     uint32_t b;
                     do {
                         if (pos >= hi) return kErrCorrupt;
-                        b = byte(pos++);
+                        b = GX_BYTE(pos);
+                        ++pos;
                         lit += b;
                     } while (b == 255);
                 }
@@ -140,14 +139,15 @@ __device__ __forceinline__ int lz4_seg_lane(const uint32_t* __restrict__ A, uint
             } else {
                 // literals done: the block may end here (then the segment is short)
                 if (pos == block_end || (uint64_t)pos + 2 > hi) return kErrCorrupt;
-                const uint32_t off = byte(pos) | (byte(pos + 1) << 8);
+                const uint32_t off = GX_BYTE(pos) | (GX_BYTE(pos + 1) << 8);
                 pos += 2;
                 uint32_t ml = mnib + 4;
                 if (mnib == 15) {
                     uint32_t b;
                     do {
                         if (pos >= hi) return kErrCorrupt;
-                        b = byte(pos++);
+                        b = GX_BYTE(pos);
+                        ++pos;
                         ml += b;
                     } while (b == 255);
                 }
@@ -172,6 +172,7 @@ __device__ __forceinline__ int lz4_seg_lane(const uint32_t* __restrict__ A, uint
         out[k] = w;
     }
     return 0;
+#undef GX_BYTE
 }
 
 // ------------------------------------------------ generic LZ4, one warp
@@ -302,12 +303,20 @@ __device__ __forceinline__ bool casc_header_ok(const casc_hdr& h, uint32_t blk_b
 }
 
 __device__ __forceinline__ casc_hdr casc_load_header(const uint8_t* blk) {
+    const uint4* hw = (const uint4*)blk;  // blocks are 16-byte aligned
+    const uint4 a = __ldg(hw), b = __ldg(hw + 1);
     casc_hdr h;
-    const uint32_t* hw = (const uint32_t*)blk;
-    uint32_t w[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) w[i] = __ldg(hw + i);
-    memcpy(&h, w, sizeof(h));
+    h.n_rows = a.x;
+    h.n_runs = a.y;
+    h.flags = (uint8_t)(a.z & 255u);
+    h.val_bits = (uint8_t)((a.z >> 8) & 255u);
+    h.len_bits = (uint8_t)((a.z >> 16) & 255u);
+    h.pad = (uint8_t)(a.z >> 24);
+    h.first = (int32_t)a.w;
+    h.val_base = (int32_t)b.x;
+    h.len_base = b.y;
+    h.vals_off = b.z;
+    h.lens_off = b.w;
     return h;
 }
 

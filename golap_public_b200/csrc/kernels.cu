@@ -78,22 +78,36 @@ struct PrunePred {
     int32_t lo, hi;
 };
 
-struct ScanParams {
-    uint32_t n_steps;
+// One query: its steps, the row slice it covers, where its aggregate goes.
+struct QueryDesc {
     ScanStep steps[GX_MAX_STEPS];
+    uint32_t n_steps;
     uint32_t agg;
     uint32_t grouped;       // sums per group key
     uint32_t need_aux;      // aux array (carry or group key) in shared memory
-    uint32_t blocks_per_chunk;
-    uint32_t tile_rows;
-    uint32_t tiles_per_block;
-    const uint32_t* items;  // surviving chunk ids
-    const uint32_t* n_items;
-    uint32_t* work_counter;
+    uint64_t row_lo, row_hi;
     int64_t* result;
     int64_t* g_keys;
     int64_t* g_sums;
     uint32_t g_log2;
+    uint32_t n_prune;
+    PrunePred prune[GX_MAX_STEPS];
+};
+
+struct ScanParams {
+    QueryDesc q;             // the query (single mode)
+    const QueryDesc* qs;     // the queries (batch mode)
+    const uint32_t* item_q;  // batch mode: query of each work item
+    uint32_t blocks_per_chunk;
+    uint32_t rows_per_chunk;
+    uint32_t rows_per_block;
+    uint32_t tile_rows;
+    uint32_t tiles_per_block;
+    uint32_t smem_aux;       // shared-memory layout: aux array present
+    uint32_t smem_groups;    // shared-memory layout: partial group table present
+    const uint32_t* items;   // surviving chunk ids
+    const uint32_t* n_items;
+    uint32_t* work_counter;
     unsigned long long* rows_scanned;
 };
 
@@ -239,17 +253,57 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
     return ct->rle ? kRuns : kRows;
 }
 
-template <int NT, int MAXT>
-__global__ void __launch_bounds__(NT) scan_kernel(const __grid_constant__ ScanParams P) {
+// Flush a CTA's partial aggregate of query Q: the scalar sum (one global
+// atomic) or the shared partial group table (merged into Q's global table,
+// then cleared).  All NT threads call it.
+template <int NT>
+__device__ __forceinline__ void flush_query(const QueryDesc& Q, int64_t& local_sum, uint32_t* gkeys,
+                                            unsigned long long* gsums, unsigned long long* s_red) {
+    constexpr int NW = NT / 32;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (!Q.grouped) {
+        unsigned long long u = (unsigned long long)local_sum;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) u += __shfl_down_sync(0xFFFFFFFFu, u, d);
+        if (lane == 0) s_red[warp] = u;
+        __syncthreads();
+        if (tid == 0 && Q.result) {
+            unsigned long long t = 0;
+            for (int w = 0; w < NW; ++w) t += s_red[w];
+            if (t) atomicAdd((unsigned long long*)Q.result, t);
+        }
+        local_sum = 0;
+        __syncthreads();
+    } else {
+        __syncthreads();
+        for (uint32_t i = tid; i < (1u << kSmemGroupLog2); i += NT) {
+            if (gkeys[i] != kEmptyGKey) {
+                if (!group_add_global(Q.g_keys, Q.g_sums, Q.g_log2, (int64_t)gkeys[i], (int64_t)gsums[i]))
+                    raise_error(kErrCapacity);
+                gkeys[i] = kEmptyGKey;
+                gsums[i] = 0;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// The fused scan.  Persistent CTAs take row tiles from a work list (one
+// entry per surviving chunk of a query); per tile, every step of the query
+// decodes its column into shared memory and updates the selection mask;
+// the VALUE step aggregates.  BATCH: the tile's query comes from the work
+// list and query descriptors live in global memory.
+template <int NT, int MAXT, bool BATCH>
+__global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const __grid_constant__ ScanParams P) {
     using C = Cfg<MAXT>;
     constexpr int NW = NT / 32;
     extern __shared__ __align__(16) uint8_t smem[];
     uint32_t* buf = (uint32_t*)smem;
     uint32_t* aux = buf + C::kBufWords;
-    uint32_t* mask = aux + (P.need_aux ? MAXT : 0);
+    uint32_t* mask = aux + (P.smem_aux ? MAXT : 0);
     uint8_t* stage = (uint8_t*)(mask + C::kMaskWords);
     uint32_t* gkeys = (uint32_t*)(stage + C::kStage);
-    unsigned long long* gsums = (unsigned long long*)(gkeys + (P.grouped ? (1u << kSmemGroupLog2) : 0));
+    unsigned long long* gsums = (unsigned long long*)(gkeys + (P.smem_groups ? (1u << kSmemGroupLog2) : 0));
     const int32_t* run_val = (const int32_t*)stage;
     const uint32_t* run_start = (const uint32_t*)(stage + 4 * kCascMaxRuns);
 
@@ -263,7 +317,7 @@ __global__ void __launch_bounds__(NT) scan_kernel(const __grid_constant__ ScanPa
     __shared__ CascTile s_ct;
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (P.grouped) {
+    if (P.smem_groups) {
         for (uint32_t i = tid; i < (1u << kSmemGroupLog2); i += NT) {
             gkeys[i] = kEmptyGKey;
             gsums[i] = 0;
@@ -280,6 +334,7 @@ __global__ void __launch_bounds__(NT) scan_kernel(const __grid_constant__ ScanPa
     const uint32_t tpb = P.tiles_per_block, tile_rows = P.tile_rows;
     const uint32_t per_chunk = P.blocks_per_chunk * tpb;
     const uint32_t total = *P.n_items * per_chunk;
+    int cur_q = -1;
     __syncthreads();
 
     while (true) {
@@ -288,20 +343,35 @@ __global__ void __launch_bounds__(NT) scan_kernel(const __grid_constant__ ScanPa
         const uint32_t it = s_item;
         __syncthreads();
         if (it >= total) break;
-        const uint32_t rem = it % per_chunk;
-        const uint32_t slot = P.items[it / per_chunk] * P.blocks_per_chunk + rem / tpb;
+        const uint32_t k = it / per_chunk, rem = it % per_chunk;
+        const int q = BATCH ? (int)P.item_q[k] : 0;
+        if (q != cur_q) {  // uniform across the CTA
+            if (cur_q >= 0) flush_query<NT>(BATCH ? P.qs[cur_q] : P.q, local_sum, gkeys, gsums, s_red);
+            cur_q = q;
+        }
+        const QueryDesc& Q = BATCH ? P.qs[q] : P.q;
+        const uint32_t chunk = P.items[k];
+        const uint32_t j = rem / tpb;
+        const uint32_t slot = chunk * P.blocks_per_chunk + j;
         const uint32_t r0 = (rem % tpb) * tile_rows;
-        const uint32_t rows = P.steps[0].col.blocks[slot].n_rows;
+        const uint32_t rows = Q.steps[0].col.blocks[slot].n_rows;
         if (r0 >= rows) continue;
         const uint32_t n = min(tile_rows, rows - r0);
+        // rows of the tile inside the query's slice [row_lo, row_hi)
+        const uint64_t g0 = (uint64_t)chunk * P.rows_per_chunk + (uint64_t)j * P.rows_per_block + r0;
+        const uint32_t a = Q.row_lo > g0 ? (Q.row_lo - g0 < n ? (uint32_t)(Q.row_lo - g0) : n) : 0u;
+        const uint32_t b = Q.row_hi > g0 ? (Q.row_hi - g0 < n ? (uint32_t)(Q.row_hi - g0) : n) : 0u;
+        if (a >= b) continue;
         const uint32_t ngroups = (n + 31) / 32;
-        for (uint32_t g = tid; g < ngroups; g += NT)
-            mask[g] = (g + 1) * 32 <= n ? 0xFFFFFFFFu : ((1u << (n & 31)) - 1u);
-        if (tid == 0) local_rows += n;
+        for (uint32_t g = tid; g < ngroups; g += NT) {
+            const uint32_t lo = max(a, g * 32), hi = min(b, g * 32 + 32);
+            mask[g] = lo >= hi ? 0u : ((hi - lo == 32) ? 0xFFFFFFFFu : (((1u << (hi - lo)) - 1u) << (lo & 31)));
+        }
+        if (tid == 0) local_rows += b - a;
         __syncthreads();
 
-        for (uint32_t si = 0; si < P.n_steps; ++si) {
-            const ScanStep& st = P.steps[si];
+        for (uint32_t si = 0; si < Q.n_steps; ++si) {
+            const ScanStep& st = Q.steps[si];
             int layout = decode_tile<NT, MAXT>(st.col, slot, rows, r0, n, buf, stage, &s_mbar, phase, s_tmp, &s_ct,
                                                &s_err);
             const int derr = s_err;
@@ -315,7 +385,9 @@ __global__ void __launch_bounds__(NT) scan_kernel(const __grid_constant__ ScanPa
                 __syncthreads();
                 break;
             }
-            const bool per_row = (st.flags & (GX_STEP_CARRY | GX_STEP_VALUE)) || st.digit_card;
+            const uint32_t flags = st.flags;
+            const uint32_t dcard = st.digit_card;
+            const bool per_row = (flags & (GX_STEP_CARRY | GX_STEP_VALUE | GX_STEP_GROUP)) || dcard;
             if (layout == kRuns && per_row) {
                 casc_runs_to_rows<NT>(s_ct, run_val, run_start, r0, n, (int32_t*)buf);
                 layout = kRows;
@@ -329,15 +401,15 @@ __global__ void __launch_bounds__(NT) scan_kernel(const __grid_constant__ ScanPa
                 for (uint32_t i = ct.ra + tid; i < ct.rb; i += NT) {
                     const int32_t v = run_val[i];
                     bool pass = true;
-                    if (st.flags & GX_STEP_FILTER) pass = v >= st.lo && v <= st.hi;
-                    if ((st.flags & GX_STEP_PROBE) && pass) {
+                    if (flags & GX_STEP_FILTER) pass = v >= st.lo && v <= st.hi;
+                    if ((flags & GX_STEP_PROBE) && pass) {
                         int32_t p;
                         pass = ht_probe(st.ht, st.ht_log2, v, &p);
                     }
                     if (!pass) {
-                        const uint32_t a = max(run_start[i], r0) - r0, b = min(run_start[i + 1], r0 + n) - r0;
-                        for (uint32_t r = a; r < b;) {
-                            const uint32_t w = r >> 5, hb = min(b, (w + 1) * 32);
+                        const uint32_t ra = max(run_start[i], r0) - r0, rb = min(run_start[i + 1], r0 + n) - r0;
+                        for (uint32_t r = ra; r < rb;) {
+                            const uint32_t w = r >> 5, hb = min(rb, (w + 1) * 32);
                             const uint32_t bits = (hb - r == 32) ? 0xFFFFFFFFu : (((1u << (hb - r)) - 1u) << (r & 31));
                             atomicAnd(&mask[w], ~bits);
                             r = hb;
@@ -356,29 +428,27 @@ __global__ void __launch_bounds__(NT) scan_kernel(const __grid_constant__ ScanPa
                     bool keep = (m >> lane) & 1u;
                     int32_t v = 0;
                     if (keep) v = (int32_t)buf[layout == kSegRows ? r + (r >> shift) : r];
-                    if ((st.flags & GX_STEP_FILTER) && keep) keep = v >= st.lo && v <= st.hi;
-                    if ((st.flags & GX_STEP_PROBE) && keep) {
-                        int32_t p = 0;
-                        keep = ht_probe(st.ht, st.ht_log2, v, &p);
-                        if (keep && st.digit_card) {
-                            const uint32_t dgt = (uint32_t)(p - st.digit_base);
-                            if (dgt >= st.digit_card) {
-                                raise_error(kErrInvalid);
-                                keep = false;
-                            } else {
-                                aux[r] = st.first_digit ? dgt : aux[r] * st.digit_card + dgt;
-                            }
+                    if ((flags & GX_STEP_FILTER) && keep) keep = v >= st.lo && v <= st.hi;
+                    int32_t p = v;
+                    if ((flags & GX_STEP_PROBE) && keep) keep = ht_probe(st.ht, st.ht_log2, v, &p);
+                    if (dcard && keep) {
+                        const uint32_t dgt = (uint32_t)(p - st.digit_base);
+                        if (dgt >= dcard) {
+                            raise_error(kErrInvalid);
+                            keep = false;
+                        } else {
+                            aux[r] = st.first_digit ? dgt : aux[r] * dcard + dgt;
                         }
                     }
-                    if ((st.flags & GX_STEP_CARRY) && keep) aux[r] = (uint32_t)v;
-                    if (st.flags & GX_STEP_VALUE) {
+                    if ((flags & GX_STEP_CARRY) && keep) aux[r] = (uint32_t)v;
+                    if (flags & GX_STEP_VALUE) {
                         int64_t val = 0;
                         if (keep) {
-                            if (P.agg == GX_AGG_SUM_PRODUCT) val = (int64_t)v * (int64_t)(int32_t)aux[r];
-                            else if (P.agg == GX_AGG_COUNT) val = 1;
+                            if (Q.agg == GX_AGG_SUM_PRODUCT) val = (int64_t)v * (int64_t)(int32_t)aux[r];
+                            else if (Q.agg == GX_AGG_COUNT) val = 1;
                             else val = v;
                         }
-                        if (!P.grouped) {
+                        if (!Q.grouped) {
                             local_sum += val;
                         } else {
                             // warp-aggregated update of the shared partial group table
@@ -392,7 +462,7 @@ __global__ void __launch_bounds__(NT) scan_kernel(const __grid_constant__ ScanPa
                                 const uint64_t tot = warp_sum_u64(peer ? (uint64_t)val : 0ull);
                                 if ((int)lane == leader) {
                                     if (!group_add_smem(gkeys, gsums, kSmemGroupLog2, lk, tot))
-                                        if (!group_add_global(P.g_keys, P.g_sums, P.g_log2, (int64_t)lk, (int64_t)tot))
+                                        if (!group_add_global(Q.g_keys, Q.g_sums, Q.g_log2, (int64_t)lk, (int64_t)tot))
                                             raise_error(kErrCapacity);
                                 }
                                 active &= ~peers;
@@ -410,29 +480,8 @@ __global__ void __launch_bounds__(NT) scan_kernel(const __grid_constant__ ScanPa
         }
         __syncthreads();
     }
-
-    // scalar result: one atomic per CTA
-    if (!P.grouped && P.result) {
-        unsigned long long u = (unsigned long long)local_sum;
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) u += __shfl_down_sync(0xFFFFFFFFu, u, d);
-        if (lane == 0) s_red[warp] = u;
-        __syncthreads();
-        if (tid == 0) {
-            unsigned long long t = 0;
-            for (int w = 0; w < NW; ++w) t += s_red[w];
-            if (t) atomicAdd((unsigned long long*)P.result, t);
-        }
-    }
+    if (cur_q >= 0) flush_query<NT>(BATCH ? P.qs[cur_q] : P.q, local_sum, gkeys, gsums, s_red);
     if (tid == 0 && P.rows_scanned && local_rows) atomicAdd(P.rows_scanned, local_rows);
-    if (P.grouped) {
-        __syncthreads();
-        for (uint32_t i = tid; i < (1u << kSmemGroupLog2); i += NT) {
-            if (gkeys[i] != kEmptyGKey)
-                if (!group_add_global(P.g_keys, P.g_sums, P.g_log2, (int64_t)gkeys[i], (int64_t)gsums[i]))
-                    raise_error(kErrCapacity);
-        }
-    }
 }
 
 // One CTA: per-chunk keep flags (AND over min/max predicates and the
@@ -477,10 +526,80 @@ __global__ void __launch_bounds__(1024) items_kernel(const __grid_constant__ Ite
     }
 }
 
+// Batch: per-query reset of the aggregate targets (scalar result = 0, group
+// table emptied).  blockIdx.y = query; blocks along x stride the table.
+__global__ void batch_reset_kernel(const QueryDesc* __restrict__ qs, unsigned long long* rows) {
+    const QueryDesc& Q = qs[blockIdx.y];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (Q.result) *Q.result = 0;
+        if (blockIdx.y == 0 && rows) *rows = 0;
+    }
+    if (Q.grouped) {
+        const uint64_t cap = 1ull << Q.g_log2;
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cap; i += (uint64_t)gridDim.x * blockDim.x) {
+            Q.g_keys[i] = kEmptyGroup;
+            Q.g_sums[i] = 0;
+        }
+    }
+}
+
+// Batch: min/max pruning of every (query, chunk) candidate (the chunks that
+// overlap the query's slice) and order-preserving compaction of the
+// survivors into the work list; resets the work counter.  One CTA.
+__global__ void __launch_bounds__(1024) batch_items_kernel(const QueryDesc* __restrict__ qs,
+                                                           const uint32_t* __restrict__ cand_q,
+                                                           const uint32_t* __restrict__ cand_chunk, uint32_t n_cand,
+                                                           uint32_t* items_q, uint32_t* items_chunk, uint32_t* n_items,
+                                                           uint32_t* work_counter) {
+    __shared__ uint32_t s_count;
+    __shared__ uint32_t s_warp[32];
+    if (threadIdx.x == 0) s_count = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < n_cand; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        bool keep = false;
+        uint32_t q = 0, c = 0;
+        if (i < n_cand) {
+            q = cand_q[i];
+            c = cand_chunk[i];
+            const QueryDesc& Q = qs[q];
+            keep = true;
+            for (uint32_t p = 0; p < Q.n_prune; ++p) {
+                const PrunePred& pr = Q.prune[p];
+                keep = keep && (pr.lo <= pr.maxs[c]) && (pr.hi >= pr.mins[c]);
+            }
+        }
+        const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const uint32_t b = __ballot_sync(0xFFFFFFFFu, keep);
+        if (lane == 0) s_warp[warp] = __popc(b);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t run = s_count;
+            for (uint32_t w = 0; w < blockDim.x / 32; ++w) {
+                const uint32_t x = s_warp[w];
+                s_warp[w] = run;
+                run += x;
+            }
+            s_count = run;
+        }
+        __syncthreads();
+        if (keep) {
+            const uint32_t o = s_warp[warp] + __popc(b & ((1u << lane) - 1u));
+            items_q[o] = q;
+            items_chunk[o] = c;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        *n_items = s_count;
+        *work_counter = 0;
+    }
+}
+
 // Decompress tiles of slots [slot0, slot0 + gridDim.x / tpb) into dst, rows
 // laid out contiguously from the first row of chunk row0.  One CTA per tile.
 template <int NT, int MAXT>
-__global__ void __launch_bounds__(NT) decompress_kernel(const gx_dcol c, uint32_t slot0, uint32_t tile_rows,
+__global__ void __launch_bounds__(NT) decompress_kernel(const __grid_constant__ gx_dcol c, uint32_t slot0, uint32_t tile_rows,
                                                         uint32_t tpb, uint64_t row0, int32_t* dst) {
     using C = Cfg<MAXT>;
     extern __shared__ __align__(16) uint8_t smem[];
@@ -712,6 +831,21 @@ struct gx_groupby {
     int64_t* sums = nullptr;
     uint32_t log2cap = 0;
     uint64_t max_groups = 0;
+};
+
+struct gx_batch {
+    uint32_t n = 0;
+    QueryDesc* d_qs = nullptr;
+    uint32_t* d_buf = nullptr;  // cand_q | cand_chunk | items_q | items_chunk | n_items | counter
+    uint32_t n_cand = 0;
+    unsigned long long* d_rows = nullptr;
+    ScanParams P{};
+    uint32_t grid = 1, threads = 128;
+    size_t smem = 0;
+    uint32_t reset_x = 1;
+    int device = -1;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
 };
 
 extern "C" {
@@ -1028,16 +1162,20 @@ gx_status gx_groupby_read(gx_groupby* gb, int64_t* keys_host, int64_t* sums_host
 
 // ------------------------------------------------------------------- scan
 
-static gx_status build_scan_params(const gx_scan_plan* plan, ScanParams* P, ItemsParams* ip, const gx_column** ref_col) {
+}  // extern "C"
+
+// Validates a plan and fills the query descriptor (steps, aggregate target,
+// prune predicates).  *tile_rows receives the tile size its columns allow.
+static gx_status build_query(const gx_scan_plan* plan, QueryDesc* Q, uint32_t* tile_rows, const gx_column** ref_col) {
     if (!plan || plan->n_steps == 0 || plan->n_steps > GX_MAX_STEPS)
         return set_error(GX_ERR_INVALID, "scan plan needs 1..%d steps", GX_MAX_STEPS);
-    std::memset(P, 0, sizeof(*P));
-    std::memset(ip, 0, sizeof(*ip));
+    std::memset(Q, 0, sizeof(*Q));
     const gx_column* c0 = plan->steps[0].col;
     if (!c0 || !c0->residency) return set_error(GX_ERR_INVALID, "step 0 column is not on the device");
     bool any_value = false, any_digit = false, any_carry = false;
     uint64_t card_prod = 1;
     const gx_column* cols[GX_MAX_STEPS];
+    const uint32_t known = GX_STEP_FILTER | GX_STEP_PROBE | GX_STEP_CARRY | GX_STEP_VALUE | GX_STEP_GROUP;
     for (uint32_t i = 0; i < plan->n_steps; ++i) {
         const gx_scan_step& s = plan->steps[i];
         const gx_column* c = s.col;
@@ -1045,10 +1183,11 @@ static gx_status build_scan_params(const gx_scan_plan* plan, ScanParams* P, Item
         if (c->n_rows != c0->n_rows || c->rows_per_chunk != c0->rows_per_chunk ||
             c->rows_per_block != c0->rows_per_block)
             return set_error(GX_ERR_INVALID, "step %u column layout differs from step 0", i);
-        if (s.flags == 0 || (s.flags & ~(uint32_t)(GX_STEP_FILTER | GX_STEP_PROBE | GX_STEP_CARRY | GX_STEP_VALUE)))
-            return set_error(GX_ERR_INVALID, "step %u has invalid flags", i);
+        if (s.flags == 0 || (s.flags & ~known)) return set_error(GX_ERR_INVALID, "step %u has invalid flags", i);
+        if ((s.flags & GX_STEP_PROBE) && (s.flags & GX_STEP_GROUP))
+            return set_error(GX_ERR_INVALID, "step %u: PROBE and GROUP are exclusive", i);
         cols[i] = c;
-        ScanStep& d = P->steps[i];
+        ScanStep& d = Q->steps[i];
         d.col = c->view();
         d.flags = s.flags;
         d.lo = s.lo;
@@ -1057,14 +1196,16 @@ static gx_status build_scan_params(const gx_scan_plan* plan, ScanParams* P, Item
             if (!s.ht) return set_error(GX_ERR_INVALID, "step %u probes a null hash table", i);
             d.ht = s.ht->slots;
             d.ht_log2 = s.ht->log2cap;
+        }
+        if ((s.flags & GX_STEP_GROUP) && s.digit_card == 0)
+            return set_error(GX_ERR_INVALID, "step %u: GROUP needs digit_card > 0", i);
+        if ((s.flags & (GX_STEP_PROBE | GX_STEP_GROUP)) && s.digit_card) {
             d.digit_base = s.digit_base;
             d.digit_card = s.digit_card;
-            if (s.digit_card) {
-                d.first_digit = any_digit ? 0 : 1;
-                any_digit = true;
-                card_prod *= s.digit_card;
-                if (card_prod >= 0xFFFFFFFFull) return set_error(GX_ERR_INVALID, "group key space exceeds 2^32-1");
-            }
+            d.first_digit = any_digit ? 0 : 1;
+            any_digit = true;
+            card_prod *= s.digit_card;
+            if (card_prod >= 0xFFFFFFFFull) return set_error(GX_ERR_INVALID, "group key space exceeds 2^32-1");
         }
         if (s.flags & GX_STEP_CARRY) any_carry = true;
         if (s.flags & GX_STEP_VALUE) any_value = true;
@@ -1073,53 +1214,88 @@ static gx_status build_scan_params(const gx_scan_plan* plan, ScanParams* P, Item
     if (plan->agg > GX_AGG_COUNT) return set_error(GX_ERR_INVALID, "unknown aggregate");
     if (plan->agg == GX_AGG_SUM_PRODUCT && !any_carry) return set_error(GX_ERR_INVALID, "SUM_PRODUCT needs a CARRY step");
     if (any_carry && any_digit) return set_error(GX_ERR_INVALID, "CARRY and group-key digits cannot be combined");
-    if (plan->groupby && !any_digit) return set_error(GX_ERR_INVALID, "grouped scan needs PROBE steps with digits");
+    if (plan->groupby && !any_digit) return set_error(GX_ERR_INVALID, "grouped scan needs PROBE/GROUP steps with digits");
     if (!plan->groupby && !plan->result_dev) return set_error(GX_ERR_INVALID, "scan plan needs result_dev or groupby");
-    P->n_steps = plan->n_steps;
-    P->agg = plan->agg;
-    P->grouped = plan->groupby ? 1 : 0;
-    P->need_aux = (any_carry || any_digit) ? 1 : 0;
-    P->blocks_per_chunk = c0->blocks_per_chunk;
-    P->tile_rows = pick_tile_rows(cols, plan->n_steps);
-    P->tiles_per_block = (c0->rows_per_block + P->tile_rows - 1) / P->tile_rows;
-    P->result = plan->result_dev;
+    if (!plan->groupby && any_digit) return set_error(GX_ERR_INVALID, "group-key digits need a groupby table");
+    Q->n_steps = plan->n_steps;
+    Q->agg = plan->agg;
+    Q->grouped = plan->groupby ? 1 : 0;
+    Q->need_aux = (any_carry || any_digit) ? 1 : 0;
+    Q->row_lo = 0;
+    Q->row_hi = ~0ull;
+    Q->result = plan->result_dev;
     if (plan->groupby) {
-        P->g_keys = plan->groupby->keys;
-        P->g_sums = plan->groupby->sums;
-        P->g_log2 = plan->groupby->log2cap;
+        Q->g_keys = plan->groupby->keys;
+        Q->g_sums = plan->groupby->sums;
+        Q->g_log2 = plan->groupby->log2cap;
     }
-    // pruning predicates of the plan
     if (plan->n_prune > GX_MAX_STEPS) return set_error(GX_ERR_INVALID, "too many prune predicates");
-    const gx_column* pc[GX_MAX_STEPS];
-    int32_t plo[GX_MAX_STEPS], phi[GX_MAX_STEPS];
     for (uint32_t i = 0; i < plan->n_prune; ++i) {
-        pc[i] = plan->prune[i].col;
-        plo[i] = plan->prune[i].lo;
-        phi[i] = plan->prune[i].hi;
+        const gx_column* pc = plan->prune[i].col;
+        if (!pc || !pc->residency) return set_error(GX_ERR_INVALID, "prune column %u not on device", i);
+        if (pc->n_chunks != c0->n_chunks) return set_error(GX_ERR_INVALID, "prune column %u has another chunking", i);
+        Q->prune[i] = PrunePred{pc->d_mins, pc->d_maxs, plan->prune[i].lo, plan->prune[i].hi};
     }
-    gx_status st = fill_prune(ip, pc, plo, phi, plan->n_prune, c0->n_chunks);
-    if (st) return st;
-    ip->keep_in = plan->keep_chunks_dev;
-    ip->keep_out = plan->keep_out_dev;
+    Q->n_prune = plan->n_prune;
+    *tile_rows = pick_tile_rows(cols, plan->n_steps);
     *ref_col = c0;
     return GX_OK;
 }
 
-static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned long long* rows_dev) {
-    ScanParams P;
-    ItemsParams ip;
-    const gx_column* c0 = nullptr;
-    gx_status st = build_scan_params(plan, &P, &ip, &c0);
-    if (st) return st;
+static gx_status ensure_kernel_attrs() {
     static bool attr_set[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (!attr_set[dev & 63]) {
-        st = allow_smem(scan_kernel<128, kTileRows>, scan_smem_bytes<kTileRows>(true, true));
-        if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
-        if (st) return st;
-        attr_set[dev & 63] = true;
+    if (attr_set[dev & 63]) return GX_OK;
+    gx_status st = allow_smem(scan_kernel<128, kTileRows, false>, scan_smem_bytes<kTileRows>(true, true));
+    if (!st) st = allow_smem(scan_kernel<128, kTileRows, true>, scan_smem_bytes<kTileRows>(true, true));
+    if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock, false>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
+    if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock, true>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
+    if (st) return st;
+    attr_set[dev & 63] = true;
+    return GX_OK;
+}
+
+// Grid and shared memory of a scan launch (persistent: CTAs per SM x SMs).
+template <bool BATCH>
+static void scan_geometry(uint32_t tile_rows, bool aux, bool groups, uint64_t tiles, uint32_t* grid, uint32_t* threads,
+                          size_t* smem) {
+    if (tile_rows <= kTileRows) {
+        *smem = scan_smem_bytes<kTileRows>(aux, groups);
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_kernel<128, kTileRows, BATCH>, 128, *smem);
+        *grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * std::max(1, per_sm), tiles));
+        *threads = 128;
+    } else {
+        *smem = scan_smem_bytes<kMaxRowsPerBlock>(aux, groups);
+        *grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(sm_count(), tiles));
+        *threads = 256;
     }
+}
+
+template <bool BATCH>
+static void launch_scan_kernel(const ScanParams& P, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t s) {
+    if (threads == 128)
+        scan_kernel<128, kTileRows, BATCH><<<grid, 128, smem, s>>>(P);
+    else
+        scan_kernel<256, kMaxRowsPerBlock, BATCH><<<grid, 256, smem, s>>>(P);
+}
+
+static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned long long* rows_dev) {
+    ScanParams P;
+    std::memset(&P, 0, sizeof(P));
+    const gx_column* c0 = nullptr;
+    uint32_t tile_rows = 0;
+    gx_status st = build_query(plan, &P.q, &tile_rows, &c0);
+    if (st) return st;
+    st = ensure_kernel_attrs();
+    if (st) return st;
+    ItemsParams ip{};
+    for (uint32_t i = 0; i < P.q.n_prune; ++i) ip.preds[i] = P.q.prune[i];
+    ip.n_preds = P.q.n_prune;
+    ip.n_chunks = c0->n_chunks;
+    ip.keep_in = plan->keep_chunks_dev;
+    ip.keep_out = plan->keep_out_dev;
     const uint32_t n_chunks = c0->n_chunks;
     uint32_t* scratch = nullptr;
     GX_CK(cudaMallocAsync(&scratch, 4ull * (n_chunks + 4), s));
@@ -1127,27 +1303,29 @@ static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned 
     ip.work_counter = scratch + 1;
     ip.items = scratch + 4;
     items_kernel<<<1, 1024, 0, s>>>(ip);
+    P.blocks_per_chunk = c0->blocks_per_chunk;
+    P.rows_per_chunk = c0->rows_per_chunk;
+    P.rows_per_block = c0->rows_per_block;
+    P.tile_rows = tile_rows;
+    P.tiles_per_block = (c0->rows_per_block + tile_rows - 1) / tile_rows;
+    P.smem_aux = P.q.need_aux;
+    P.smem_groups = P.q.grouped;
     P.items = ip.items;
     P.n_items = ip.n_items;
     P.work_counter = ip.work_counter;
     P.rows_scanned = rows_dev;
     const uint64_t tiles = (uint64_t)n_chunks * c0->blocks_per_chunk * P.tiles_per_block;
-    if (P.tile_rows <= kTileRows) {
-        const size_t smem = scan_smem_bytes<kTileRows>(P.need_aux, P.grouped);
-        int per_sm = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_kernel<128, kTileRows>, 128, smem);
-        const uint64_t grid = std::min<uint64_t>((uint64_t)sm_count() * std::max(1, per_sm), tiles);
-        scan_kernel<128, kTileRows><<<(unsigned)std::max<uint64_t>(1, grid), 128, smem, s>>>(P);
-    } else {
-        const size_t smem = scan_smem_bytes<kMaxRowsPerBlock>(P.need_aux, P.grouped);
-        const uint64_t grid = std::min<uint64_t>(sm_count(), tiles);
-        scan_kernel<256, kMaxRowsPerBlock><<<(unsigned)std::max<uint64_t>(1, grid), 256, smem, s>>>(P);
-    }
+    uint32_t grid = 1, threads = 128;
+    size_t smem = 0;
+    scan_geometry<false>(tile_rows, P.smem_aux, P.smem_groups, tiles, &grid, &threads, &smem);
+    launch_scan_kernel<false>(P, grid, threads, smem, s);
     cudaError_t e = cudaGetLastError();
     cudaFreeAsync(scratch, s);
     if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "scan launch: %s", cudaGetErrorString(e));
     return GX_OK;
 }
+
+extern "C" {
 
 gx_status gx_scan(const gx_scan_plan* plan, void* stream) {
     return scan_launch(plan, (cudaStream_t)stream, nullptr);
@@ -1184,6 +1362,132 @@ gx_status gx_scan_sync(const gx_scan_plan* plan, void* stream, uint64_t* rows_sc
     if (rows) cudaFreeAsync(rows, s);
     if (st) return st;
     return gx_scan_check(stream);
+}
+
+
+gx_status gx_batch_create(const gx_query* queries, uint32_t n_queries, gx_batch** out) {
+    if (!queries || !out || n_queries == 0) return set_error(GX_ERR_INVALID, "gx_batch_create: bad args");
+    std::vector<QueryDesc> qs(n_queries);
+    const gx_column* c0 = nullptr;
+    uint32_t tile_rows = ~0u;
+    bool aux = false, groups = false;
+    uint64_t max_table = 0;
+    std::vector<uint32_t> cq, cc;
+    for (uint32_t i = 0; i < n_queries; ++i) {
+        const gx_column* ci = nullptr;
+        uint32_t tr = 0;
+        gx_status st = build_query(&queries[i].plan, &qs[i], &tr, &ci);
+        if (st) return st;
+        if (c0 && (ci->n_rows != c0->n_rows || ci->rows_per_chunk != c0->rows_per_chunk ||
+                   ci->rows_per_block != c0->rows_per_block))
+            return set_error(GX_ERR_INVALID, "query %u scans a table with another layout", i);
+        c0 = c0 ? c0 : ci;
+        tile_rows = std::min(tile_rows, tr);
+        aux = aux || qs[i].need_aux;
+        groups = groups || qs[i].grouped;
+        if (qs[i].grouped) max_table = std::max<uint64_t>(max_table, 1ull << qs[i].g_log2);
+        const uint64_t lo = queries[i].row_lo, hi = std::min<uint64_t>(queries[i].row_hi, c0->n_rows);
+        if (lo > hi) return set_error(GX_ERR_INVALID, "query %u has row_lo > row_hi", i);
+        qs[i].row_lo = lo;
+        qs[i].row_hi = hi;
+        if (lo < hi)
+            for (uint64_t c = lo / c0->rows_per_chunk; c <= (hi - 1) / c0->rows_per_chunk; ++c) {
+                cq.push_back(i);
+                cc.push_back((uint32_t)c);
+            }
+    }
+    gx_status st = ensure_kernel_attrs();
+    if (st) return st;
+    gx_batch* b = new gx_batch();
+    b->n = n_queries;
+    b->n_cand = (uint32_t)cq.size();
+    const size_t nc = std::max<size_t>(1, cq.size());
+    cudaError_t e = cudaMalloc(&b->d_qs, sizeof(QueryDesc) * n_queries);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_buf, 4 * (4 * nc + 4));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_rows, 8);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_qs, qs.data(), sizeof(QueryDesc) * n_queries, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !cq.empty()) e = cudaMemcpy(b->d_buf, cq.data(), 4 * cq.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !cc.empty()) e = cudaMemcpy(b->d_buf + nc, cc.data(), 4 * cc.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        gx_batch_free(b);
+        return set_error(GX_ERR_NOMEM, "gx_batch_create: %s", cudaGetErrorString(e));
+    }
+    ScanParams& P = b->P;
+    std::memset(&P, 0, sizeof(P));
+    P.qs = b->d_qs;
+    P.item_q = b->d_buf + 2 * nc;
+    P.items = b->d_buf + 3 * nc;
+    P.n_items = b->d_buf + 4 * nc;
+    P.work_counter = b->d_buf + 4 * nc + 1;
+    P.rows_scanned = b->d_rows;
+    P.blocks_per_chunk = c0->blocks_per_chunk;
+    P.rows_per_chunk = c0->rows_per_chunk;
+    P.rows_per_block = c0->rows_per_block;
+    P.tile_rows = tile_rows;
+    P.tiles_per_block = (c0->rows_per_block + tile_rows - 1) / tile_rows;
+    P.smem_aux = aux;
+    P.smem_groups = groups;
+    const uint64_t tiles = (uint64_t)nc * c0->blocks_per_chunk * P.tiles_per_block;
+    scan_geometry<true>(tile_rows, aux, groups, tiles, &b->grid, &b->threads, &b->smem);
+    b->reset_x = (uint32_t)std::min<uint64_t>(64, std::max<uint64_t>(1, max_table / 4096));
+    cudaGetDevice(&b->device);
+    *out = b;
+    return GX_OK;
+}
+
+gx_status gx_batch_free(gx_batch* b) {
+    if (!b) return GX_OK;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    cudaFree(b->d_qs);
+    cudaFree(b->d_buf);
+    cudaFree(b->d_rows);
+    delete b;
+    return GX_OK;
+}
+
+gx_status gx_batch_run(gx_batch* b, void* stream) {
+    if (!b) return set_error(GX_ERR_INVALID, "null batch");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t nc = std::max<uint32_t>(1, b->n_cand);
+    batch_reset_kernel<<<dim3(b->reset_x, b->n), 256, 0, s>>>(b->d_qs, b->d_rows);
+    batch_items_kernel<<<1, 1024, 0, s>>>(b->d_qs, b->d_buf, b->d_buf + nc, b->n_cand, b->d_buf + 2 * nc,
+                                          b->d_buf + 3 * nc, b->d_buf + 4 * nc, b->d_buf + 4 * nc + 1);
+    launch_scan_kernel<true>(b->P, b->grid, b->threads, b->smem, s);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+gx_status gx_batch_graph(gx_batch* b, void* stream) {
+    if (!b) return set_error(GX_ERR_INVALID, "null batch");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!b->exec) {
+        cudaStream_t cap;
+        GX_CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            gx_status st = gx_batch_run(b, cap);
+            e = cudaStreamEndCapture(cap, &b->graph);
+            if (st) {
+                cudaStreamDestroy(cap);
+                return st;
+            }
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+        cudaStreamDestroy(cap);
+        if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(e));
+    }
+    GX_CK(cudaGraphLaunch(b->exec, s));
+    return GX_OK;
+}
+
+gx_status gx_batch_rows(gx_batch* b, uint64_t* rows, void* stream) {
+    if (!b || !rows) return set_error(GX_ERR_INVALID, "gx_batch_rows: bad args");
+    unsigned long long r = 0;
+    GX_CK(cudaMemcpyAsync(&r, b->d_rows, 8, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    gx_status st = wait_stream((cudaStream_t)stream, 300.0);
+    *rows = r;
+    return st;
 }
 
 }  // extern "C"

@@ -222,13 +222,16 @@ gx_status gx_groupby_read(gx_groupby* gb, int64_t* keys_host, int64_t* sums_host
  *             payload p extends the group key: g = g*digit_card + (p-digit_base)
  *   CARRY   : remember v for the product aggregate
  *   VALUE   : aggregate v (times the carried value when agg == SUM_PRODUCT)
+ *   GROUP   : the value itself extends the group key like a PROBE payload
+ *             (g = g*digit_card + (v-digit_base)); GROUP BY a fact column
  * Flags may be OR-ed (FILTER|CARRY).  The aggregate is int64:
  * a scalar sum (groupby == NULL) or sums per group key. */
 enum {
     GX_STEP_FILTER = 1,
     GX_STEP_PROBE = 2,
     GX_STEP_CARRY = 4,
-    GX_STEP_VALUE = 8
+    GX_STEP_VALUE = 8,
+    GX_STEP_GROUP = 16
 };
 enum { GX_AGG_SUM = 0, GX_AGG_SUM_PRODUCT = 1, GX_AGG_COUNT = 2 };
 
@@ -270,6 +273,32 @@ gx_status gx_scan(const gx_scan_plan* plan, void* stream);
 gx_status gx_scan_sync(const gx_scan_plan* plan, void* stream, uint64_t* rows_scanned);
 /* Read and clear the device error word of the scan engine. */
 gx_status gx_scan_check(void* stream);
+
+/* ------------------------------------------------------------ batched scan
+ * No reference counterpart (the reference runs one query per pipeline).
+ * Many plans over the same fact table, each restricted to a row slice
+ * [row_lo, row_hi), run as ONE persistent launch: a single work list of
+ * (query, chunk) items is built on the device after per-query min/max
+ * pruning, and every CTA switches between queries as it takes items.  Each
+ * query's result_dev (scalar) or groupby (grouped) receives exactly what
+ * gx_scan of that plan alone over the slice would produce; gx_batch_run
+ * clears them first.  The launch sequence can be captured once into a CUDA
+ * graph and replayed (gx_batch_graph). */
+typedef struct gx_query {
+    gx_scan_plan plan;   /* keep_chunks_dev / keep_out_dev are ignored */
+    uint64_t row_lo, row_hi;
+} gx_query;
+
+typedef struct gx_batch gx_batch;
+
+gx_status gx_batch_create(const gx_query* queries, uint32_t n_queries, gx_batch** out);
+gx_status gx_batch_free(gx_batch* b);
+/* Clear results, build the work list, run all queries (3 launches). */
+gx_status gx_batch_run(gx_batch* b, void* stream);
+/* Capture gx_batch_run into a CUDA graph on first use, then replay it. */
+gx_status gx_batch_graph(gx_batch* b, void* stream);
+/* Rows of surviving tiles counted by the last run (host, synchronises). */
+gx_status gx_batch_rows(gx_batch* b, uint64_t* rows, void* stream);
 
 #ifdef __cplusplus
 }
