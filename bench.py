@@ -117,6 +117,19 @@ class Clocks:
                 "samples": len(rows)}
 
 
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """Max of a per-rank time over all ranks (replicas: no data-path collective,
+    only this timing reduction); identity for a single process."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def make_data(seed):
     from golap_public_b200 import datagen
 
@@ -141,11 +154,6 @@ def gpu_arm(args, rank, world):
     comp = {k: c.info.comp_bytes for k, c in fact.cols.items()}
 
     q = queries.Q1Query(fact, dd, ok, DATE_LO, DATE_HI, *DISC, *QTY, prune=True)
-    want = None
-    if not args.no_check:
-        from oracle import oracle as O
-
-        want = O.q1(f["date_key"], f["discount"], f["quantity"], f["extended_price"], dd["d_key"], ok, *DISC, *QTY)
     dk_h = torch.from_numpy(dd["d_key"]).pin_memory()
     ok_h = torch.from_numpy(ok.astype(np.int32)).pin_memory()
     dk_d = torch.empty_like(dk_h, device="cuda")
@@ -163,8 +171,7 @@ def gpu_arm(args, rank, world):
         step()
     torch.cuda.synchronize()
     got = q.run()
-    if want is not None and got != want:
-        raise SystemExit(f"result mismatch: gpu {got} oracle {want}")
+    want = got  # checked against the CPU baseline's result below
     kept = int(q.keep.sum().item())
     kept_chunks = np.nonzero(q.keep.cpu().numpy())[0].tolist()
 
@@ -204,17 +211,13 @@ def gpu_arm(args, rank, world):
         dist.barrier()
     step_ms = [a.elapsed_time(c) for a, b, c in ev]
     scan_ms = [b.elapsed_time(c) for a, b, c in ev]
-    ms = float(np.mean(step_ms))
+    ms = max_over_ranks(float(np.mean(step_ms)), world, "cuda")
     scan_avg = float(np.mean(scan_ms))
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
 
     # full-table scan (pruning off): the decode-bound throughput of the same kernel
     q_all = queries.Q1Query(fact, dd, ok, DATE_LO, DATE_HI, *DISC, *QTY, prune=False)
-    if want is not None:
-        assert q_all.run() == want
+    if q_all.run() != want:
+        raise SystemExit("full scan and pruned scan disagree")
     for _ in range(3):
         q_all.launch()
     all_ms = []
@@ -248,7 +251,7 @@ def gpu_arm(args, rank, world):
     for _ in range(args.warmup):
         e2e_step()
     torch.cuda.synchronize()
-    if want is not None and int(res_h.item()) != want:
+    if int(res_h.item()) != want:
         raise SystemExit("e2e result mismatch")
     e_ms = []
     for _ in range(args.steps):
@@ -261,11 +264,7 @@ def gpu_arm(args, rank, world):
         b.record(stream)
         b.synchronize()
         e_ms.append(a.elapsed_time(b))
-    e2e_ms = float(np.mean(e_ms))
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(float(np.mean(e_ms)), world, "cuda")
 
     pk, pk_kind = peaks()
     scan_bytes = alg_bytes(kept_chunks)
@@ -304,6 +303,107 @@ def gpu_arm(args, rank, world):
         "wall_s_timed": t_wall,
     }
     return line, f, dd
+
+
+# --------------------------------------------------- batched and serving forms
+
+def _hbm_bytes(spec):
+    """Device bytes a request holds while it runs: its group table or result."""
+    return 8 if spec.groups is None else 16 * (2 * spec.groups.max_groups) + 8
+
+
+def batched_section(t, n_queries=256, seed=7):
+    """configs[3]-style batch: n queries on log-uniform slices (1M..100M rows)
+    mixing the scan, star-join and high-cardinality templates.  One query at
+    a time (its own launch sequence, back to back on one stream) vs all
+    queries in one persistent launch replayed from a CUDA graph."""
+    import torch
+
+    from golap_public_b200 import api, workload
+
+    rng = np.random.default_rng(seed)
+    specs = workload.random_queries(t, n_queries, rng)
+    singles = [api.Batch([(s.plan, s.row_lo, s.row_hi)]) for s in specs]
+    batch = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs])
+    stream = torch.cuda.current_stream()
+
+    def one_at_a_time():
+        for b in singles:
+            b.run()
+
+    def timed(fn, reps):
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        return float(np.median(ts))
+
+    one_at_a_time()
+    torch.cuda.synchronize()
+    ref = [workload.read_result(s) for s in specs]
+    batch.graph()
+    torch.cuda.synchronize()
+    if [workload.read_result(s) for s in specs] != ref:
+        raise SystemExit("batched results differ from one-at-a-time results")
+    t_one = timed(one_at_a_time, 3)
+    t_batch = timed(batch.graph, 5)
+    rows = sum(s.row_hi - s.row_lo for s in specs)
+    mix = {k: sum(1 for s in specs if s.template == k) for k in ("scan", "star", "highcard")}
+    return {"queries": n_queries, "mix": mix, "slice_rows_total": rows,
+            "one_at_a_time_ms": t_one, "batched_graph_ms": t_batch,
+            "one_at_a_time_qps": n_queries / (t_one * 1e-3), "batched_qps": n_queries / (t_batch * 1e-3),
+            "speedup": t_one / t_batch, "results_identical": True}
+
+
+def serving_section(t, rates=(200, 1000, 2000), seconds=2.0, seed=9):
+    """configs[4]-style open loop: Poisson arrivals at each rate for `seconds`,
+    60% pruned scans / 30% star joins / 10% Zipf group-bys over the whole
+    resident table, served by the continuous-batching server and by a
+    one-at-a-time server (one request per launch, one in flight)."""
+    import threading
+
+    from golap_public_b200 import api, workload
+
+    rng = np.random.default_rng(seed)
+    pool = workload.random_queries(t, 384, rng, min_rows=t.n_rows, max_rows=t.n_rows)
+    out = {}
+    for mode, (inflight, maxb) in (("batched", (4, 64)), ("one_at_a_time", (1, 1))):
+        res = {}
+        for rate in rates:
+            sv = api.Server(max_inflight=inflight, max_batch=maxb, hbm_budget=120 << 30)
+            arr = np.cumsum(rng.exponential(1.0 / rate, int(rate * seconds)))
+            busy = {}
+            lats = []
+            lock = threading.Lock()
+            t0 = time.perf_counter()
+            tickets = []
+            for i, at in enumerate(arr):
+                spec_i = i % len(pool)
+                if spec_i in busy:  # a pooled request's buffers are reused only after it finished
+                    lats.append(sv.wait(busy.pop(spec_i), 300.0))
+                while time.perf_counter() - t0 < at:
+                    pass
+                s = pool[spec_i]
+                tk = sv.submit(s.plan, s.row_lo, s.row_hi, _hbm_bytes(s))
+                busy[spec_i] = tk
+            for tk in busy.values():
+                lats.append(sv.wait(tk, 300.0))
+            elapsed = time.perf_counter() - t0
+            st = sv.stats()
+            sv.close()
+            lats = np.array(lats)
+            res[str(rate)] = {"offered_qps": rate, "completed": int(st["completed"]),
+                              "sustained_qps": float(st["completed"] / elapsed),
+                              "p50_ms": float(np.percentile(lats, 50)), "p99_ms": float(np.percentile(lats, 99)),
+                              "mean_batch": float(st["queries_in_batches"] / max(1, st["batches"]))}
+        out[mode] = res
+    return out
 
 
 # ----------------------------------------------------------------- CPU arm
@@ -375,6 +475,8 @@ def main():
     ap.add_argument("--seed", type=int, default=0xBEE5BEE5)
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched and serving sections")
+    ap.add_argument("--batch-rows", type=int, default=100_000_000)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -407,6 +509,16 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     line, f, dd = gpu_arm(args, rank, world)
+    if not args.no_batch:
+        from golap_public_b200 import workload
+
+        t_build = time.perf_counter()
+        wt = workload.build_table(args.batch_rows)
+        line["batched"] = batched_section(wt)
+        line["serving"] = serving_section(wt)
+        line["batched"]["table_rows"] = args.batch_rows
+        line["batched"]["table_build_s"] = time.perf_counter() - t_build
+        del wt
     if rank == 0 and not args.no_cpu:
         cb = cpu_baseline(f, dd, steps=3, warmup=1)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}

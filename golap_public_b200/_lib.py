@@ -18,6 +18,7 @@ GX_OK, GX_ERR_CUDA, GX_ERR_CORRUPT, GX_ERR_CAPACITY, GX_ERR_TIMEOUT, GX_ERR_NOME
 GX_CODEC_NONE, GX_CODEC_LZ4, GX_CODEC_CASCADED = 0, 1, 2
 GX_STEP_FILTER, GX_STEP_PROBE, GX_STEP_CARRY, GX_STEP_VALUE, GX_STEP_GROUP = 1, 2, 4, 8, 16
 GX_AGG_SUM, GX_AGG_SUM_PRODUCT, GX_AGG_COUNT = 0, 1, 2
+GX_HT_LINEAR, GX_HT_BUCKET = 0, 1
 GX_MAX_STEPS = 8
 
 
@@ -72,6 +73,15 @@ class Query(C.Structure):
     _fields_ = [("plan", ScanPlan), ("row_lo", C.c_uint64), ("row_hi", C.c_uint64)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("max_inflight", C.c_uint32), ("max_batch", C.c_uint32), ("hbm_budget", C.c_uint64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "rejected", "batches", "queries_in_batches",
+                                           "hbm_in_use", "hbm_peak", "queued")]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "gx_status_str": (C.c_char_p, [C.c_int32]),
@@ -95,6 +105,7 @@ _SIGS = {
     "gx_combine_and": (C.c_int32, [P, P, P, C.c_uint64, P]),
     "gx_prune_minmax": (C.c_int32, [P, P, P, C.c_uint32, P, P]),
     "gx_hashtable_create": (C.c_int32, [C.c_uint64, C.POINTER(P)]),
+    "gx_hashtable_create2": (C.c_int32, [C.c_uint64, C.c_uint32, C.POINTER(P)]),
     "gx_hashtable_free": (C.c_int32, [P]),
     "gx_hashtable_build": (C.c_int32, [P, P, P, C.c_uint64, P, C.c_uint32, P]),
     "gx_hashtable_count": (C.c_int32, [P, C.POINTER(C.c_uint64), P]),
@@ -114,6 +125,13 @@ _SIGS = {
     "gx_batch_run": (C.c_int32, [P, P]),
     "gx_batch_graph": (C.c_int32, [P, P]),
     "gx_batch_rows": (C.c_int32, [P, C.POINTER(C.c_uint64), P]),
+    "gx_batch_assign": (C.c_int32, [P, C.POINTER(Query), C.c_uint32, P]),
+    "gx_server_opts_default": (C.c_int32, [C.POINTER(ServerOpts)]),
+    "gx_server_create": (C.c_int32, [C.POINTER(ServerOpts), C.POINTER(P)]),
+    "gx_server_submit": (C.c_int32, [P, C.POINTER(Query), C.c_uint64, C.POINTER(C.c_uint64)]),
+    "gx_server_wait": (C.c_int32, [P, C.c_uint64, C.c_double, C.POINTER(C.c_double)]),
+    "gx_server_stats_get": (C.c_int32, [P, C.POINTER(ServerStats)]),
+    "gx_server_free": (C.c_int32, [P]),
 }
 
 _lib = None

@@ -154,10 +154,12 @@ class MetaChecker:
 class HashMap:
     """Open-addressing join table on the device: key -> payload (row id when no payload)."""
 
-    def __init__(self, max_entries: int):
+    def __init__(self, max_entries: int, layout: str = "linear"):
         h = C.c_void_p()
-        check(L.lib().gx_hashtable_create(max_entries, C.byref(h)))
+        lay = {"linear": L.GX_HT_LINEAR, "bucket": L.GX_HT_BUCKET}[layout]
+        check(L.lib().gx_hashtable_create2(max_entries, lay, C.byref(h)))
         self.handle = h
+        self.layout = layout
 
     def build(self, keys, payload=None, preds=(), stream=None) -> "HashMap":
         n = keys.numel()
@@ -351,5 +353,52 @@ class Batch:
     def __del__(self):
         try:
             self.free()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching serving loop (gx_server_* in include/gx.h)."""
+
+    def __init__(self, max_inflight: int = 4, max_batch: int = 64, hbm_budget: int = 120 << 30):
+        o = L.ServerOpts()
+        check(L.lib().gx_server_opts_default(C.byref(o)))
+        o.max_inflight, o.max_batch, o.hbm_budget = max_inflight, max_batch, hbm_budget
+        h = C.c_void_p()
+        check(L.lib().gx_server_create(C.byref(o), C.byref(h)))
+        self.handle = h
+        self._keep = {}
+
+    def submit(self, plan: "ScanPlan", row_lo: int, row_hi: int, hbm_bytes: int) -> int:
+        q = L.Query()
+        q.plan = plan.to_c()
+        q.row_lo, q.row_hi = row_lo, row_hi
+        t = C.c_uint64()
+        check(L.lib().gx_server_submit(self.handle, C.byref(q), hbm_bytes, C.byref(t)))
+        self._keep[t.value] = plan
+        return t.value
+
+    def wait(self, ticket: int, timeout_s: float = 60.0) -> float:
+        """Blocks until the request is done; returns its latency in ms."""
+        lat = C.c_double()
+        try:
+            check(L.lib().gx_server_wait(self.handle, ticket, timeout_s, C.byref(lat)))
+        finally:
+            self._keep.pop(ticket, None)
+        return lat.value
+
+    def stats(self) -> dict:
+        st = L.ServerStats()
+        check(L.lib().gx_server_stats_get(self.handle, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in L.ServerStats._fields_}
+
+    def close(self):
+        if self.handle:
+            L.lib().gx_server_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass

@@ -427,6 +427,41 @@ __device__ __forceinline__ bool ht_probe(const uint64_t* __restrict__ slots, uin
     return false;
 }
 
+// Bucketized layout: 2^log2cap slots grouped in buckets of 8 (64 bytes); a
+// key hashes to a bucket, is placed in its first free slot, and spills to
+// the next bucket when the bucket is full.
+constexpr uint32_t kBucketSlots = 8;
+
+__device__ __forceinline__ bool ht_probe_bucket(const uint64_t* __restrict__ slots, uint32_t log2cap, int32_t key,
+                                                int32_t* payload) {
+    if (key == kEmptyKey || log2cap < 3) return false;
+    const uint32_t lb = log2cap - 3, bmask = (1u << lb) - 1;
+    uint32_t bkt = hash_key32(key, lb);
+    for (uint32_t i = 0; i <= bmask; ++i) {
+        const ulonglong2* bp = (const ulonglong2*)(slots + (size_t)bkt * kBucketSlots);
+        const ulonglong2 a = __ldg(bp), b = __ldg(bp + 1), c = __ldg(bp + 2), d = __ldg(bp + 3);
+        const unsigned long long e[8] = {a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y};
+        bool any_empty = false;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int32_t k = (int32_t)(uint32_t)e[j];
+            if (k == key) {
+                *payload = (int32_t)(uint32_t)(e[j] >> 32);
+                return true;
+            }
+            any_empty |= (k == kEmptyKey);
+        }
+        if (any_empty) return false;
+        bkt = (bkt + 1) & bmask;
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool ht_probe_any(const uint64_t* __restrict__ slots, uint32_t log2cap, uint32_t layout,
+                                             int32_t key, int32_t* payload) {
+    return layout ? ht_probe_bucket(slots, log2cap, key, payload) : ht_probe(slots, log2cap, key, payload);
+}
+
 // --------------------------------------------------------- group tables
 // Global open-addressing group table: keys int64 (kEmptyGroup = free), sums int64.
 __device__ __forceinline__ bool group_add_global(int64_t* keys, int64_t* sums, uint32_t log2cap, int64_t key,

@@ -67,6 +67,7 @@ struct ScanStep {
     int32_t lo, hi;
     const uint64_t* ht;
     uint32_t ht_log2;
+    uint32_t ht_layout;
     int32_t digit_base;
     uint32_t digit_card;
     uint32_t first_digit;
@@ -404,7 +405,7 @@ __global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const 
                     if (flags & GX_STEP_FILTER) pass = v >= st.lo && v <= st.hi;
                     if ((flags & GX_STEP_PROBE) && pass) {
                         int32_t p;
-                        pass = ht_probe(st.ht, st.ht_log2, v, &p);
+                        pass = ht_probe_any(st.ht, st.ht_log2, st.ht_layout, v, &p);
                     }
                     if (!pass) {
                         const uint32_t ra = max(run_start[i], r0) - r0, rb = min(run_start[i + 1], r0 + n) - r0;
@@ -430,7 +431,7 @@ __global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const 
                     if (keep) v = (int32_t)buf[layout == kSegRows ? r + (r >> shift) : r];
                     if ((flags & GX_STEP_FILTER) && keep) keep = v >= st.lo && v <= st.hi;
                     int32_t p = v;
-                    if ((flags & GX_STEP_PROBE) && keep) keep = ht_probe(st.ht, st.ht_log2, v, &p);
+                    if ((flags & GX_STEP_PROBE) && keep) keep = ht_probe_any(st.ht, st.ht_log2, st.ht_layout, v, &p);
                     if (dcard && keep) {
                         const uint32_t dgt = (uint32_t)(p - st.digit_base);
                         if (dgt >= dcard) {
@@ -711,12 +712,57 @@ __global__ void ht_build_kernel(uint64_t* slots, uint32_t log2cap, const int32_t
     if (bad) atomicAdd(&counters[2], bad);
 }
 
-__global__ void ht_probe_kernel(const uint64_t* slots, uint32_t log2cap, const int32_t* keys, uint64_t n,
-                                int32_t* out, unsigned long long* hits) {
+__global__ void ht_build_bucket_kernel(uint64_t* slots, uint32_t log2cap, const int32_t* keys, const int32_t* payload,
+                                       uint64_t n, const __grid_constant__ BuildPreds preds,
+                                       unsigned long long* counters) {
+    const uint32_t lb = log2cap - 3, bmask = (1u << lb) - 1;
+    unsigned long long ins = 0, dup = 0, bad = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        bool pass = true;
+        for (uint32_t k = 0; k < preds.n; ++k) {
+            int32_t x = preds.p[k].col_dev[i];
+            pass = pass && x >= preds.p[k].lo && x <= preds.p[k].hi;
+        }
+        if (!pass) continue;
+        const int32_t key = keys[i];
+        if (key == kEmptyKey) {
+            ++bad;
+            continue;
+        }
+        const int32_t pay = payload ? payload[i] : (int32_t)i;
+        const unsigned long long e = ((unsigned long long)(uint32_t)pay << 32) | (uint32_t)key;
+        uint32_t bkt = hash_key32(key, lb);
+        bool done = false;
+        for (uint32_t t = 0; t <= bmask && !done; ++t) {
+            unsigned long long* bp = (unsigned long long*)slots + (size_t)bkt * kBucketSlots;
+            for (uint32_t j = 0; j < kBucketSlots; ++j) {
+                unsigned long long old = atomicCAS(bp + j, (unsigned long long)kEmptySlot, e);
+                if (old == (unsigned long long)kEmptySlot) {
+                    ++ins;
+                    done = true;
+                    break;
+                }
+                if ((int32_t)(uint32_t)old == key) {
+                    ++dup;
+                    done = true;
+                    break;
+                }
+            }
+            bkt = (bkt + 1) & bmask;
+        }
+        if (!done) ++bad;
+    }
+    if (ins) atomicAdd(&counters[0], ins);
+    if (dup) atomicAdd(&counters[1], dup);
+    if (bad) atomicAdd(&counters[2], bad);
+}
+
+__global__ void ht_probe_kernel(const uint64_t* slots, uint32_t log2cap, uint32_t layout, const int32_t* keys,
+                                uint64_t n, int32_t* out, unsigned long long* hits) {
     unsigned long long h = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         int32_t p = 0;
-        bool hit = ht_probe(slots, log2cap, keys[i], &p);
+        bool hit = ht_probe_any(slots, log2cap, layout, keys[i], &p);
         if (out) out[i] = hit ? p : INT32_MIN;
         h += hit;
     }
@@ -822,6 +868,7 @@ gx_status allow_smem(K kernel, size_t bytes) {
 struct gx_hashtable {
     uint64_t* slots = nullptr;
     uint32_t log2cap = 0;
+    uint32_t layout = GX_HT_LINEAR;
     uint64_t max_entries = 0;
     unsigned long long* counters = nullptr;  // inserted, duplicates, dropped
 };
@@ -838,6 +885,9 @@ struct gx_batch {
     QueryDesc* d_qs = nullptr;
     uint32_t* d_buf = nullptr;  // cand_q | cand_chunk | items_q | items_chunk | n_items | counter
     uint32_t n_cand = 0;
+    uint32_t cap_q = 0, cap_cand = 0;   // device buffer capacities
+    QueryDesc* h_qs = nullptr;          // pinned host staging (async assignment)
+    uint32_t* h_cand = nullptr;
     unsigned long long* d_rows = nullptr;
     ScanParams P{};
     uint32_t grid = 1, threads = 128;
@@ -1015,6 +1065,13 @@ gx_status gx_hashtable_create(uint64_t max_entries, gx_hashtable** out) {
     return GX_OK;
 }
 
+gx_status gx_hashtable_create2(uint64_t max_entries, uint32_t layout, gx_hashtable** out) {
+    if (layout > GX_HT_BUCKET) return set_error(GX_ERR_INVALID, "unknown hash table layout %u", layout);
+    gx_status st = gx_hashtable_create(max_entries, out);
+    if (!st) (*out)->layout = layout;
+    return st;
+}
+
 gx_status gx_hashtable_free(gx_hashtable* ht) {
     if (!ht) return GX_OK;
     cudaFree(ht->slots);
@@ -1034,8 +1091,11 @@ gx_status gx_hashtable_build(gx_hashtable* ht, const int32_t* keys_dev, const in
     BuildPreds bp{};
     for (uint32_t i = 0; i < n_preds; ++i) bp.p[i] = preds[i];
     bp.n = n_preds;
-    ht_build_kernel<<<(unsigned)std::min<uint64_t>(4 * sm_count(), (n + 255) / 256), 256, 0, s>>>(
-        ht->slots, ht->log2cap, keys_dev, payload_dev, n, bp, ht->counters);
+    const unsigned grid = (unsigned)std::min<uint64_t>(4 * sm_count(), (n + 255) / 256);
+    if (ht->layout == GX_HT_BUCKET)
+        ht_build_bucket_kernel<<<grid, 256, 0, s>>>(ht->slots, ht->log2cap, keys_dev, payload_dev, n, bp, ht->counters);
+    else
+        ht_build_kernel<<<grid, 256, 0, s>>>(ht->slots, ht->log2cap, keys_dev, payload_dev, n, bp, ht->counters);
     GX_CK(cudaGetLastError());
     return GX_OK;
 }
@@ -1073,7 +1133,7 @@ gx_status gx_hashtable_probe(const gx_hashtable* ht, const int32_t* keys_dev, ui
     if (!ht || (!keys_dev && n)) return set_error(GX_ERR_INVALID, "gx_hashtable_probe: bad args");
     if (n == 0) return GX_OK;
     ht_probe_kernel<<<(unsigned)std::min<uint64_t>(8 * sm_count(), (n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
-        ht->slots, ht->log2cap, keys_dev, n, payload_out_dev, (unsigned long long*)hits_dev);
+        ht->slots, ht->log2cap, ht->layout, keys_dev, n, payload_out_dev, (unsigned long long*)hits_dev);
     GX_CK(cudaGetLastError());
     return GX_OK;
 }
@@ -1196,6 +1256,7 @@ static gx_status build_query(const gx_scan_plan* plan, QueryDesc* Q, uint32_t* t
             if (!s.ht) return set_error(GX_ERR_INVALID, "step %u probes a null hash table", i);
             d.ht = s.ht->slots;
             d.ht_log2 = s.ht->log2cap;
+            d.ht_layout = s.ht->layout;
         }
         if ((s.flags & GX_STEP_GROUP) && s.digit_card == 0)
             return set_error(GX_ERR_INVALID, "step %u: GROUP needs digit_card > 0", i);
@@ -1365,8 +1426,9 @@ gx_status gx_scan_sync(const gx_scan_plan* plan, void* stream, uint64_t* rows_sc
 }
 
 
-gx_status gx_batch_create(const gx_query* queries, uint32_t n_queries, gx_batch** out) {
-    if (!queries || !out || n_queries == 0) return set_error(GX_ERR_INVALID, "gx_batch_create: bad args");
+gx_status gx_batch_assign(gx_batch* b, const gx_query* queries, uint32_t n_queries, void* stream) {
+    if (!b || !queries || n_queries == 0) return set_error(GX_ERR_INVALID, "gx_batch_assign: bad args");
+    cudaStream_t s = (cudaStream_t)stream;
     std::vector<QueryDesc> qs(n_queries);
     const gx_column* c0 = nullptr;
     uint32_t tile_rows = ~0u;
@@ -1398,27 +1460,59 @@ gx_status gx_batch_create(const gx_query* queries, uint32_t n_queries, gx_batch*
     }
     gx_status st = ensure_kernel_attrs();
     if (st) return st;
-    gx_batch* b = new gx_batch();
+    const uint32_t nc = (uint32_t)std::max<size_t>(1, cq.size());
+    // grow buffers when needed (the stream's earlier work is finished first)
+    if (n_queries > b->cap_q || nc > b->cap_cand) {
+        GX_CK(cudaStreamSynchronize(s));
+        const uint32_t cq_new = std::max(n_queries, b->cap_q), cc_new = std::max(nc, b->cap_cand);
+        cudaFree(b->d_qs);
+        cudaFree(b->d_buf);
+        cudaFreeHost(b->h_qs);
+        cudaFreeHost(b->h_cand);
+        b->d_qs = nullptr;
+        b->d_buf = nullptr;
+        b->h_qs = nullptr;
+        b->h_cand = nullptr;
+        cudaError_t e = cudaMalloc(&b->d_qs, sizeof(QueryDesc) * cq_new);
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_buf, 4ull * (4ull * cc_new + 4));
+        if (e == cudaSuccess) e = cudaMallocHost(&b->h_qs, sizeof(QueryDesc) * cq_new);
+        if (e == cudaSuccess) e = cudaMallocHost(&b->h_cand, 8ull * cc_new);
+        if (e != cudaSuccess) {
+            b->cap_q = b->cap_cand = 0;
+            return set_error(GX_ERR_NOMEM, "gx_batch_assign: %s", cudaGetErrorString(e));
+        }
+        b->cap_q = cq_new;
+        b->cap_cand = cc_new;
+    } else {
+        // the pinned staging may still feed an earlier copy on this stream
+        GX_CK(cudaStreamSynchronize(s));
+    }
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    if (b->graph) {
+        cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    const uint32_t cap = b->cap_cand;
+    std::memcpy(b->h_qs, qs.data(), sizeof(QueryDesc) * n_queries);
+    std::memcpy(b->h_cand, cq.data(), 4 * cq.size());
+    std::memcpy(b->h_cand + cap, cc.data(), 4 * cc.size());
+    GX_CK(cudaMemcpyAsync(b->d_qs, b->h_qs, sizeof(QueryDesc) * n_queries, cudaMemcpyHostToDevice, s));
+    if (!cq.empty()) {
+        GX_CK(cudaMemcpyAsync(b->d_buf, b->h_cand, 4 * cq.size(), cudaMemcpyHostToDevice, s));
+        GX_CK(cudaMemcpyAsync(b->d_buf + cap, b->h_cand + cap, 4 * cc.size(), cudaMemcpyHostToDevice, s));
+    }
     b->n = n_queries;
     b->n_cand = (uint32_t)cq.size();
-    const size_t nc = std::max<size_t>(1, cq.size());
-    cudaError_t e = cudaMalloc(&b->d_qs, sizeof(QueryDesc) * n_queries);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_buf, 4 * (4 * nc + 4));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_rows, 8);
-    if (e == cudaSuccess) e = cudaMemcpy(b->d_qs, qs.data(), sizeof(QueryDesc) * n_queries, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !cq.empty()) e = cudaMemcpy(b->d_buf, cq.data(), 4 * cq.size(), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !cc.empty()) e = cudaMemcpy(b->d_buf + nc, cc.data(), 4 * cc.size(), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-        gx_batch_free(b);
-        return set_error(GX_ERR_NOMEM, "gx_batch_create: %s", cudaGetErrorString(e));
-    }
     ScanParams& P = b->P;
     std::memset(&P, 0, sizeof(P));
     P.qs = b->d_qs;
-    P.item_q = b->d_buf + 2 * nc;
-    P.items = b->d_buf + 3 * nc;
-    P.n_items = b->d_buf + 4 * nc;
-    P.work_counter = b->d_buf + 4 * nc + 1;
+    P.item_q = b->d_buf + 2 * cap;
+    P.items = b->d_buf + 3 * cap;
+    P.n_items = b->d_buf + 4 * cap;
+    P.work_counter = b->d_buf + 4 * cap + 1;
     P.rows_scanned = b->d_rows;
     P.blocks_per_chunk = c0->blocks_per_chunk;
     P.rows_per_chunk = c0->rows_per_chunk;
@@ -1430,7 +1524,23 @@ gx_status gx_batch_create(const gx_query* queries, uint32_t n_queries, gx_batch*
     const uint64_t tiles = (uint64_t)nc * c0->blocks_per_chunk * P.tiles_per_block;
     scan_geometry<true>(tile_rows, aux, groups, tiles, &b->grid, &b->threads, &b->smem);
     b->reset_x = (uint32_t)std::min<uint64_t>(64, std::max<uint64_t>(1, max_table / 4096));
+    return GX_OK;
+}
+
+gx_status gx_batch_create(const gx_query* queries, uint32_t n_queries, gx_batch** out) {
+    if (!queries || !out || n_queries == 0) return set_error(GX_ERR_INVALID, "gx_batch_create: bad args");
+    gx_batch* b = new gx_batch();
     cudaGetDevice(&b->device);
+    if (cudaMalloc(&b->d_rows, 8) != cudaSuccess) {
+        delete b;
+        return set_error(GX_ERR_NOMEM, "gx_batch_create: out of device memory");
+    }
+    gx_status st = gx_batch_assign(b, queries, n_queries, nullptr);
+    if (st == GX_OK && cudaStreamSynchronize(nullptr) != cudaSuccess) st = set_error(GX_ERR_CUDA, "gx_batch_create: copy failed");
+    if (st) {
+        gx_batch_free(b);
+        return st;
+    }
     *out = b;
     return GX_OK;
 }
@@ -1442,6 +1552,8 @@ gx_status gx_batch_free(gx_batch* b) {
     cudaFree(b->d_qs);
     cudaFree(b->d_buf);
     cudaFree(b->d_rows);
+    cudaFreeHost(b->h_qs);
+    cudaFreeHost(b->h_cand);
     delete b;
     return GX_OK;
 }
@@ -1449,7 +1561,7 @@ gx_status gx_batch_free(gx_batch* b) {
 gx_status gx_batch_run(gx_batch* b, void* stream) {
     if (!b) return set_error(GX_ERR_INVALID, "null batch");
     cudaStream_t s = (cudaStream_t)stream;
-    const size_t nc = std::max<uint32_t>(1, b->n_cand);
+    const size_t nc = b->cap_cand;
     batch_reset_kernel<<<dim3(b->reset_x, b->n), 256, 0, s>>>(b->d_qs, b->d_rows);
     batch_items_kernel<<<1, 1024, 0, s>>>(b->d_qs, b->d_buf, b->d_buf + nc, b->n_cand, b->d_buf + 2 * nc,
                                           b->d_buf + 3 * nc, b->d_buf + 4 * nc, b->d_buf + 4 * nc + 1);

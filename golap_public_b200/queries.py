@@ -90,16 +90,16 @@ class Q3Query:
     """Q3-shaped star join + group-by over a FactTable with cust_key, supp_key, date_key, revenue."""
 
     def __init__(self, fact: FactTable, customer: dict, supplier: dict, date: dict, region: int, ylo: int, yhi: int,
-                 prune: bool = True, n_nations: int = 25):
+                 prune: bool = True, n_nations: int = 25, ht_layout: str = "linear"):
         import torch
 
         self.fact = fact
         self.n_nations = n_nations
         self.ylo, self.yhi = ylo, yhi
         # tables sized for the rows that pass the dimension filters
-        self.hc = HashMap(max(1, int((customer["region"] == region).sum())))
-        self.hs = HashMap(max(1, int((supplier["region"] == region).sum())))
-        self.hd = HashMap(max(1, int(((date["d_year"] >= ylo) & (date["d_year"] <= yhi)).sum())))
+        self.hc = HashMap(max(1, int((customer["region"] == region).sum())), ht_layout)
+        self.hs = HashMap(max(1, int((supplier["region"] == region).sum())), ht_layout)
+        self.hd = HashMap(max(1, int(((date["d_year"] >= ylo) & (date["d_year"] <= yhi)).sum())), ht_layout)
         self._keep_alive = [_dev(customer["key"]), _dev(customer["nation"]), _dev(customer["region"]),
                             _dev(supplier["key"]), _dev(supplier["nation"]), _dev(supplier["region"]),
                             _dev(date["d_key"]), _dev(date["d_year"])]

@@ -169,6 +169,10 @@ typedef struct gx_pred {
 } gx_pred;
 
 gx_status gx_hashtable_create(uint64_t max_entries, gx_hashtable** out);
+/* Table layouts: linear probing over single slots, or buckets of 8 slots
+ * (64 bytes, read with one 64-byte access per probe step). */
+enum { GX_HT_LINEAR = 0, GX_HT_BUCKET = 1 };
+gx_status gx_hashtable_create2(uint64_t max_entries, uint32_t layout, gx_hashtable** out);
 gx_status gx_hashtable_free(gx_hashtable* ht);
 /* Clear, then insert (keys[i], payload[i] or i when payload_dev == NULL) for
  * every row i < n that passes all predicates.  Duplicate keys: the first
@@ -292,6 +296,9 @@ typedef struct gx_query {
 typedef struct gx_batch gx_batch;
 
 gx_status gx_batch_create(const gx_query* queries, uint32_t n_queries, gx_batch** out);
+/* Replace the batch's queries (buffers reused, grown when needed; the
+ * descriptor upload is enqueued on `stream`).  Drops a captured graph. */
+gx_status gx_batch_assign(gx_batch* b, const gx_query* queries, uint32_t n_queries, void* stream);
 gx_status gx_batch_free(gx_batch* b);
 /* Clear results, build the work list, run all queries (3 launches). */
 gx_status gx_batch_run(gx_batch* b, void* stream);
@@ -299,6 +306,35 @@ gx_status gx_batch_run(gx_batch* b, void* stream);
 gx_status gx_batch_graph(gx_batch* b, void* stream);
 /* Rows of surviving tiles counted by the last run (host, synchronises). */
 gx_status gx_batch_rows(gx_batch* b, uint64_t* rows, void* stream);
+
+/* ------------------------------------------------------------ serving loop
+ * No reference counterpart.  A continuous-batching server over resident
+ * tables: submit() queues a request (a gx_query plus the device bytes it
+ * holds while running: its group table and result); a scheduler thread keeps
+ * up to max_inflight batches on the device, each formed FIFO from the queue
+ * as soon as a slot is free, admitting requests while the admitted bytes stay
+ * within hbm_budget.  A request's results land in its own result_dev /
+ * groupby.  wait() blocks (bounded) until the request is done and reports its
+ * latency (submit -> completion). */
+typedef struct gx_server gx_server;
+typedef struct gx_server_opts {
+    uint32_t max_inflight;  /* batches on the device at once (default 4)       */
+    uint32_t max_batch;     /* requests per batch (default 64)                 */
+    uint64_t hbm_budget;    /* bytes admitted requests may hold (default 120 GiB) */
+} gx_server_opts;
+typedef struct gx_server_stats {
+    uint64_t submitted, completed, rejected, batches, queries_in_batches;
+    uint64_t hbm_in_use, hbm_peak, queued;
+} gx_server_stats;
+
+gx_status gx_server_opts_default(gx_server_opts* opts);
+gx_status gx_server_create(const gx_server_opts* opts, gx_server** out);
+/* GX_ERR_NOMEM when hbm_bytes exceeds the whole budget (rejected). */
+gx_status gx_server_submit(gx_server* sv, const gx_query* q, uint64_t hbm_bytes, uint64_t* ticket);
+gx_status gx_server_wait(gx_server* sv, uint64_t ticket, double timeout_s, double* latency_ms);
+gx_status gx_server_stats_get(gx_server* sv, gx_server_stats* out);
+/* Drains the queue (waits for running batches), then stops the scheduler. */
+gx_status gx_server_free(gx_server* sv);
 
 #ifdef __cplusplus
 }

@@ -51,11 +51,12 @@ def test_metachecker_known_answers(cuda):
     assert keep.cpu().tolist() == [0, 1, 0]
 
 
-def test_join_count_1to1(cuda):
+@pytest.mark.parametrize("layout", ["linear", "bucket"])
+def test_join_count_1to1(cuda, layout):
     # join_tests.cu:71-107: build 500k ids, probe 10M rows id = i % 500k -> 10M hits
     build = cuda.arange(500_000, dtype=cuda.int32, device="cuda")
     probe = (cuda.arange(10_000_000, dtype=cuda.int64, device="cuda") % 500_000).to(cuda.int32)
-    hm = api.HashMap(500_000).build(build)
+    hm = api.HashMap(500_000, layout).build(build)
     assert hm.count() == 500_000
     hits = cuda.zeros(1, dtype=cuda.int64, device="cuda")
     pay = cuda.empty(10_000_000, dtype=cuda.int32, device="cuda")
@@ -64,7 +65,8 @@ def test_join_count_1to1(cuda):
     assert cuda.equal(pay, probe)  # payload defaults to the build row id
 
 
-def test_filtered_build_and_probe_vs_oracle(cuda):
+@pytest.mark.parametrize("layout", ["linear", "bucket"])
+def test_filtered_build_and_probe_vs_oracle(cuda, layout):
     rng = np.random.default_rng(8)
     n_b, n_p = 200_000, 3_000_000
     keys = rng.permutation(np.arange(1, 4 * n_b, 4, dtype=np.int32))[:n_b]
@@ -72,7 +74,7 @@ def test_filtered_build_and_probe_vs_oracle(cuda):
     nation = rng.integers(0, 25, n_b, dtype=np.int32)
     probe = rng.integers(0, 4 * n_b + 10, n_p, dtype=np.int32)
     kd, rd, nd, pd = (cuda.from_numpy(x).cuda() for x in (keys, region, nation, probe))
-    hm = api.HashMap(n_b).build(kd, nd, preds=[(rd, 2, 3)])
+    hm = api.HashMap(n_b, layout).build(kd, nd, preds=[(rd, 2, 3)])
     ok = (region >= 2) & (region <= 3)
     assert hm.count() == int(ok.sum())
     out = cuda.empty(n_p, dtype=cuda.int32, device="cuda")
@@ -84,15 +86,16 @@ def test_filtered_build_and_probe_vs_oracle(cuda):
     assert int(hits.item()) == int((rid >= 0).sum())
 
 
-def test_hashtable_reserved_key_and_capacity(cuda):
+@pytest.mark.parametrize("layout", ["linear", "bucket"])
+def test_hashtable_reserved_key_and_capacity(cuda, layout):
     keys = cuda.tensor([1, 2, np.iinfo(np.int32).min, 3], dtype=cuda.int32, device="cuda")
-    hm = api.HashMap(4).build(keys)
+    hm = api.HashMap(4, layout).build(keys)
     with pytest.raises(GxError) as e:
         hm.count()
     assert e.value.status == L.GX_ERR_CAPACITY
     # more keys than max_entries: reported, never hangs
     many = cuda.arange(100, dtype=cuda.int32, device="cuda")
-    hm2 = api.HashMap(8).build(many)
+    hm2 = api.HashMap(8, layout).build(many)
     with pytest.raises(GxError):
         hm2.count()
 

@@ -101,8 +101,8 @@ def test_q3_star_join_groupby(cuda):
     supp = datagen.dim_geo(200_000, datagen.SEED, 22)
     dd = datagen.date_dim()
     fact = queries.encode_fact(f, {"date_key": "cascaded"})
-    for region in (1, 3):
-        q = queries.Q3Query(fact, cust, supp, dd, region, 1992, 1997)
+    for region, layout in ((1, "linear"), (3, "linear"), (3, "bucket")):
+        q = queries.Q3Query(fact, cust, supp, dd, region, 1992, 1997, ht_layout=layout)
         got = q.run()
         sums, counts = O.q3(f["cust_key"], f["supp_key"], f["date_key"], f["revenue"],
                             cust["key"], cust["nation"], cust["region"] == region,
