@@ -19,6 +19,7 @@ GX_CODEC_NONE, GX_CODEC_LZ4, GX_CODEC_CASCADED = 0, 1, 2
 GX_STEP_FILTER, GX_STEP_PROBE, GX_STEP_CARRY, GX_STEP_VALUE, GX_STEP_GROUP = 1, 2, 4, 8, 16
 GX_AGG_SUM, GX_AGG_SUM_PRODUCT, GX_AGG_COUNT = 0, 1, 2
 GX_HT_LINEAR, GX_HT_BUCKET = 0, 1
+GX_BATCH_AUTO, GX_BATCH_QUEUE, GX_BATCH_SHARED = 0, 1, 2
 GX_MAX_STEPS = 8
 
 
@@ -121,6 +122,8 @@ _SIGS = {
     "gx_scan_sync": (C.c_int32, [C.POINTER(ScanPlan), P, C.POINTER(C.c_uint64)]),
     "gx_scan_check": (C.c_int32, [P]),
     "gx_batch_create": (C.c_int32, [C.POINTER(Query), C.c_uint32, C.POINTER(P)]),
+    "gx_batch_create2": (C.c_int32, [C.POINTER(Query), C.c_uint32, C.c_uint32, C.POINTER(P)]),
+    "gx_batch_mode": (C.c_int32, [P, C.POINTER(C.c_uint32)]),
     "gx_batch_free": (C.c_int32, [P]),
     "gx_batch_run": (C.c_int32, [P, P]),
     "gx_batch_graph": (C.c_int32, [P, P]),

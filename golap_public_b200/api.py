@@ -321,8 +321,12 @@ def scan_check(stream=None):
 class Batch:
     """Many scan plans over one table, each on a row slice, in one persistent launch."""
 
-    def __init__(self, queries):
-        """queries: iterable of (ScanPlan, row_lo, row_hi)."""
+    MODES = {"auto": L.GX_BATCH_AUTO, "queue": L.GX_BATCH_QUEUE, "shared": L.GX_BATCH_SHARED}
+
+    def __init__(self, queries, mode: str = "auto"):
+        """queries: iterable of (ScanPlan, row_lo, row_hi).  mode: "auto",
+        "queue" (per-query work items) or "shared" (each tile decoded once for
+        all queries that need it)."""
         queries = list(queries)
         arr = (L.Query * len(queries))()
         for i, (plan, lo, hi) in enumerate(queries):
@@ -331,8 +335,14 @@ class Batch:
             arr[i].row_hi = hi
         self.plans = [q[0] for q in queries]
         h = C.c_void_p()
-        check(L.lib().gx_batch_create(arr, len(queries), C.byref(h)))
+        check(L.lib().gx_batch_create2(arr, len(queries), self.MODES[mode], C.byref(h)))
         self.handle = h
+
+    @property
+    def mode(self) -> str:
+        m = C.c_uint32()
+        check(L.lib().gx_batch_mode(self.handle, C.byref(m)))
+        return {L.GX_BATCH_QUEUE: "queue", L.GX_BATCH_SHARED: "shared"}[m.value]
 
     def run(self, stream=None):
         check(L.lib().gx_batch_run(self.handle, _stream_handle(stream)))

@@ -302,6 +302,8 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
     if (S > 1) col->seg.assign((size_t)2 * S * col->n_slots, 0);
     col->mins.assign(col->n_chunks, 0);
     col->maxs.assign(col->n_chunks, 0);
+    col->bmins.assign(col->n_slots, INT32_MAX);  // absent slots keep the empty range
+    col->bmaxs.assign(col->n_slots, INT32_MIN);
 
     // min/max per chunk (inclusive)
     for (uint32_t c = 0; c < col->n_chunks; ++c) {
@@ -333,6 +335,15 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
             uint64_t r0 = chunk_r0 + (uint64_t)j * rows_per_block;
             if (r0 >= chunk_r1) continue;  // absent slot
             uint32_t rows = (uint32_t)std::min<uint64_t>(rows_per_block, chunk_r1 - r0);
+            {
+                int32_t mn = INT32_MAX, mx = INT32_MIN;
+                for (uint32_t r = 0; r < rows; ++r) {
+                    mn = std::min(mn, vals[r0 + r]);
+                    mx = std::max(mx, vals[r0 + r]);
+                }
+                col->bmins[s] = mn;
+                col->bmaxs[s] = mx;
+            }
             size_t start = buf.size();
             size_t used = 0;
             if (codec == GX_CODEC_NONE) {

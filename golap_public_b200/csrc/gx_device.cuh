@@ -175,6 +175,117 @@ __device__ __forceinline__ int lz4_seg_lane(const uint32_t* __restrict__ A, uint
 #undef GX_BYTE
 }
 
+// 4 bytes at byte offset r of a staged window (little endian, any alignment).
+__device__ __forceinline__ uint32_t fetch4(const uint32_t* __restrict__ A, uint32_t r) {
+    const uint32_t w = r >> 2;
+    return __funnelshift_r(A[w], A[w + 1], (r & 3u) * 8);
+}
+
+// LZ4 length extension at stream position pos: adds bytes to len until one
+// below 255 has been added, four bytes per step (per-byte equality with 255
+// by __vcmpeq4).  Consumes no byte at or past hi (returns false then).
+__device__ __forceinline__ bool lz4_len_ext(const uint32_t* __restrict__ A, uint32_t wbase, uint32_t& pos,
+                                            uint32_t hi, uint32_t& len) {
+    while (true) {
+        if (pos >= hi) return false;
+        const uint32_t x = fetch4(A, pos - wbase);
+        const uint32_t ff = __vcmpeq4(x, 0xFFFFFFFFu);
+        if (ff == 0xFFFFFFFFu) {
+            len += 4 * 255;
+            pos += 4;
+            continue;
+        }
+        const uint32_t nfull = (uint32_t)(__ffs(~ff) - 1) >> 3;  // leading bytes equal to 255
+        len += 255 * nfull + ((x >> (8 * nfull)) & 255u);
+        pos += nfull + 1;
+        return pos <= hi;
+    }
+}
+
+// Decodes one segment of a segmented LZ4 block with a group of G lanes
+// (G a power of two <= 32, the group's lanes adjacent in one warp; gmask =
+// the group's lanes, gl = this lane's index in the group).  Every lane of the
+// group parses the same sequence headers (broadcast shared loads), so the
+// group stays converged; literal runs and matches are copied G words per
+// step.  A match's words are all computed from output before the match:
+// out[k + i] = out[k - offw + (i mod offw)] (LZ4 overlap semantics), so one
+// __syncwarp before each match orders it after every earlier write of the
+// group.  Same stream contract as the per-lane decoder: A = staged words
+// from byte wbase, [lo, hi) the tile's compressed range, K output words.
+// Returns 0 or kErrCorrupt (identical on every lane of the group).
+__device__ __forceinline__ int lz4_seg_group(const uint32_t* __restrict__ A, uint32_t wbase, uint32_t lo,
+                                             uint32_t hi, uint32_t block_end, uint32_t comp_pos, uint32_t info,
+                                             uint32_t K, uint32_t* __restrict__ out, uint32_t gl, uint32_t G,
+                                             uint32_t gmask) {
+    if (comp_pos < lo || comp_pos > hi) return kErrCorrupt;
+    uint32_t pos = comp_pos, k = 0, litw = 0, mnib = 0;
+    bool tok_next = true;
+    if (info & 16u) {  // the segment starts inside a sequence
+        const uint32_t lit = info >> 5;
+        if (lit & 3u) return kErrCorrupt;
+        litw = lit >> 2;
+        mnib = info & 15u;
+        tok_next = false;
+    }
+    while (true) {
+        if (tok_next) {
+            if (k >= K) break;
+            if (pos >= hi) return kErrCorrupt;
+            const uint32_t x = fetch4(A, pos - wbase);
+            uint32_t lit = (x >> 4) & 15u;
+            mnib = x & 15u;
+            ++pos;
+            if (lit == 15 && !lz4_len_ext(A, wbase, pos, hi, lit)) return kErrCorrupt;
+            if (lit & 3u) return kErrCorrupt;
+            litw = lit >> 2;
+        }
+        const uint32_t n = min(litw, K - k);
+        if ((uint64_t)pos + 4ull * n > hi) return kErrCorrupt;
+        {
+            const uint32_t r = pos - wbase, w = r >> 2, sh = (r & 3u) * 8;
+            for (uint32_t i = gl; i < n; i += G) out[k + i] = __funnelshift_r(A[w + i], A[w + i + 1], sh);
+        }
+        k += n;
+        pos += 4 * n;
+        if (k >= K) break;  // the segment ends inside or right after the literals
+        // literals done: the block may end here (then the segment is short)
+        if (pos == block_end || (uint64_t)pos + 2 > hi) return kErrCorrupt;
+        const uint32_t off = fetch4(A, pos - wbase) & 0xFFFFu;
+        pos += 2;
+        uint32_t ml = mnib + 4;
+        if (mnib == 15 && !lz4_len_ext(A, wbase, pos, hi, ml)) return kErrCorrupt;
+        if ((off & 3u) || (ml & 3u) || off == 0) return kErrCorrupt;
+        const uint32_t offw = off >> 2, mw = ml >> 2;
+        if (offw > k || mw > K - k) return kErrCorrupt;
+        __syncwarp(gmask);
+        const uint32_t* src = out + (k - offw);
+        if (offw >= mw) {
+            for (uint32_t i = gl; i < mw; i += G) out[k + i] = src[i];
+        } else if (offw == 1) {
+            const uint32_t v = src[0];
+            for (uint32_t i = gl; i < mw; i += G) out[k + i] = v;
+        } else {
+            uint32_t r = gl % offw;
+            const uint32_t step = G % offw;
+            for (uint32_t i = gl; i < mw; i += G) {
+                out[k + i] = src[r];
+                r += step;
+                if (r >= offw) r -= offw;
+            }
+        }
+        k += mw;
+        tok_next = true;
+    }
+    return 0;
+}
+
+// log2 of the lanes per segment for `nseg` segments on NT threads: the
+// largest power of two G <= 32 with nseg * G <= NT (at least 1).
+__device__ __forceinline__ uint32_t seg_group_log2(uint32_t nseg, uint32_t NT) {
+    const uint32_t q = nseg ? NT / nseg : NT;
+    return q <= 1 ? 0u : min(5u, 31u - (uint32_t)__clz(q));
+}
+
 // ------------------------------------------------ generic LZ4, one warp
 // Decodes a complete LZ4 block (any conforming encoder, byte granular) into
 // `out` (out_size bytes expected).  All 32 lanes call it; every lane sees the

@@ -141,6 +141,7 @@ struct gx_column {
     std::vector<gx::gx_dblock> blocks;   // n_slots entries
     std::vector<uint32_t> seg;           // 2*S*n_slots words (S > 1)
     std::vector<int32_t> mins, maxs;     // n_chunks
+    std::vector<int32_t> bmins, bmaxs;   // n_slots: per-block zone map (absent slots: empty range)
     // device copy
     int residency = 0;                   // 0 none, 1 HBM, 2 pinned host (mapped)
     void* d_payload = nullptr;           // device address (HBM or mapped)
@@ -149,6 +150,8 @@ struct gx_column {
     uint32_t* d_seg = nullptr;
     int32_t* d_mins = nullptr;
     int32_t* d_maxs = nullptr;
+    int32_t* d_bmins = nullptr;
+    int32_t* d_bmaxs = nullptr;
     int device = -1;
 
     gx::gx_dcol view() const {

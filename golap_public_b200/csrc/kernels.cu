@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -53,7 +54,7 @@ constexpr uint32_t kSmemGroupLog2 = 10;   // 1024-slot shared partial group tabl
 // Shared-memory budget of one CTA for tiles of up to MAXT rows.
 template <int MAXT>
 struct Cfg {
-    static constexpr uint32_t kBufWords = MAXT + kMaxSegments;                // one pad word per segment
+    static constexpr uint32_t kBufWords = MAXT + 256;  // segment padding: nseg * lanes per segment <= 256
     static constexpr uint32_t kMaskWords = MAXT / 32;
     static constexpr uint32_t kStage = MAXT * 4 + MAXT * 4 / 128 + 256;      // compressed window + slack
     static_assert(4 * kCascMaxRuns + 4 * (kCascMaxRuns + 4) <= kStage, "run tables fit the stage");
@@ -74,9 +75,11 @@ struct ScanStep {
 };
 
 struct PrunePred {
-    const int32_t* mins;
+    const int32_t* mins;   // per chunk (the reference's MinMaxMeta granularity)
     const int32_t* maxs;
     int32_t lo, hi;
+    const int32_t* bmins;  // per block slot (zone map), or null
+    const int32_t* bmaxs;
 };
 
 // One query: its steps, the row slice it covers, where its aggregate goes.
@@ -158,13 +161,14 @@ __device__ __forceinline__ int stage_bytes(const gx_dcol& c, const uint8_t* src,
 }
 
 // Decode rows [r0, r0+n) of block `slot` of column `c` into shared memory.
-// Returns the layout (kRows: buf[r]; kSegRows: buf[r + (r >> seg_shift)];
-// kRuns: runs in the stage area, described by *ct) or -1 with *s_err set.
-// All NT threads call it.
+// Returns the layout (kRows: buf[r]; kSegRows: buf[r + ((r >> seg_shift) <<
+// pad_log2)], each segment followed by 2^pad_log2 pad words; kRuns: runs in
+// the stage area, described by *ct) or -1 with *s_err set.  All NT threads
+// call it.
 template <int NT, int MAXT>
 __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint32_t rows, uint32_t r0, uint32_t n,
                                            uint32_t* buf, uint8_t* stage, uint64_t* mbar, uint32_t& phase,
-                                           uint32_t* tmp, CascTile* ct, int* s_err) {
+                                           uint32_t* tmp, CascTile* ct, int* s_err, uint32_t& pad_log2) {
     using C = Cfg<MAXT>;
     const uint32_t tid = threadIdx.x;
     const gx_dblock d = c.blocks[slot];
@@ -199,8 +203,7 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
             seg_rows = 1u << c.seg_shift;
             j0 = r0 >> c.seg_shift;
             nseg = (n + seg_rows - 1) >> c.seg_shift;
-            const uint32_t tile_span = (uint32_t)MAXT < c.rows_per_block ? (uint32_t)MAXT : c.rows_per_block;
-            const uint32_t jn = j0 + (tile_span >> c.seg_shift);
+            const uint32_t jn = j0 + nseg;
             const uint32_t* e = c.seg + (size_t)2 * c.S * slot;
             lo = __ldg(e + 2 * j0);
             hi = jn < c.S ? __ldg(e + 2 * jn) : d.comp_bytes;
@@ -226,14 +229,26 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
         __syncthreads();
         if (rc) return -1;
         if (c.S > 1) {
+            // a group of G adjacent lanes per segment; segment t at buf + t * (seg_rows + G)
             const uint32_t* e = c.seg + (size_t)2 * c.S * slot;
-            for (uint32_t t = tid; t < nseg; t += NT) {
+            // lanes per segment: a whole warp when the tile is mostly literals
+            // (few sequences; conflict-free 32-word copies), else spread the
+            // segments over all NT threads
+            const bool literal_tile = (uint64_t)(hi - lo) * 8 >= (uint64_t)n * 4 * 7;
+            const uint32_t glog = literal_tile ? 5u : seg_group_log2(nseg, NT), G = 1u << glog;
+            // pad words after each segment: G (groups of a warp on distinct
+            // banks), 1 for a whole-warp group (its stores are contiguous)
+            const uint32_t pl = glog == 5 ? 0u : glog;
+            const uint32_t gl = tid & (G - 1u), lane = tid & 31u;
+            const uint32_t gmask = G >= 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (lane & ~(G - 1u)));
+            for (uint32_t t = tid >> glog; t < nseg; t += (NT >> glog)) {
                 const uint32_t j = j0 + t;
                 const uint32_t K = min(seg_rows, rows - j * seg_rows);
-                const int r2 = lz4_seg_lane((const uint32_t*)stage, wbase, lo, hi, d.comp_bytes, __ldg(e + 2 * j),
-                                            __ldg(e + 2 * j + 1), K, buf + t * (seg_rows + 1));
-                if (r2) *s_err = r2;
+                const int r2 = lz4_seg_group((const uint32_t*)stage, wbase, lo, hi, d.comp_bytes, __ldg(e + 2 * j),
+                                             __ldg(e + 2 * j + 1), K, buf + t * (seg_rows + (1u << pl)), gl, G, gmask);
+                if (r2 && gl == 0) *s_err = r2;
             }
+            pad_log2 = pl;
             __syncthreads();
             return kSegRows;
         }
@@ -363,6 +378,14 @@ __global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const 
         const uint32_t a = Q.row_lo > g0 ? (Q.row_lo - g0 < n ? (uint32_t)(Q.row_lo - g0) : n) : 0u;
         const uint32_t b = Q.row_hi > g0 ? (Q.row_hi - g0 < n ? (uint32_t)(Q.row_hi - g0) : n) : 0u;
         if (a >= b) continue;
+        // block zone maps: a block outside a prune predicate's range holds no
+        // row the plan keeps (prune predicates are implied by its filters)
+        bool zone_out = false;
+        for (uint32_t p = 0; p < Q.n_prune; ++p) {
+            const PrunePred& pr = Q.prune[p];
+            if (pr.bmins && (pr.lo > __ldg(pr.bmaxs + slot) || pr.hi < __ldg(pr.bmins + slot))) zone_out = true;
+        }
+        if (zone_out) continue;
         const uint32_t ngroups = (n + 31) / 32;
         for (uint32_t g = tid; g < ngroups; g += NT) {
             const uint32_t lo = max(a, g * 32), hi = min(b, g * 32 + 32);
@@ -373,8 +396,9 @@ __global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const 
 
         for (uint32_t si = 0; si < Q.n_steps; ++si) {
             const ScanStep& st = Q.steps[si];
+            uint32_t pad_log2 = 0;
             int layout = decode_tile<NT, MAXT>(st.col, slot, rows, r0, n, buf, stage, &s_mbar, phase, s_tmp, &s_ct,
-                                               &s_err);
+                                               &s_err, pad_log2);
             const int derr = s_err;
             __syncthreads();  // every thread has read s_err before it is reset
             if (derr) {       // corrupt block: drop the tile, remember the error
@@ -428,7 +452,7 @@ __global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const 
                     const uint32_t r = g * 32 + lane;
                     bool keep = (m >> lane) & 1u;
                     int32_t v = 0;
-                    if (keep) v = (int32_t)buf[layout == kSegRows ? r + (r >> shift) : r];
+                    if (keep) v = (int32_t)buf[layout == kSegRows ? r + ((r >> shift) << pad_log2) : r];
                     if ((flags & GX_STEP_FILTER) && keep) keep = v >= st.lo && v <= st.hi;
                     int32_t p = v;
                     if ((flags & GX_STEP_PROBE) && keep) keep = ht_probe_any(st.ht, st.ht_log2, st.ht_layout, v, &p);
@@ -620,8 +644,9 @@ __global__ void __launch_bounds__(NT) decompress_kernel(const __grid_constant__ 
         mbar_init(&s_mbar, 1);
     }
     __syncthreads();
-    uint32_t phase = 0;
-    int layout = decode_tile<NT, MAXT>(c, slot, d.n_rows, r0, n, buf, stage, &s_mbar, phase, s_tmp, &s_ct, &s_err);
+    uint32_t phase = 0, pad_log2 = 0;
+    int layout = decode_tile<NT, MAXT>(c, slot, d.n_rows, r0, n, buf, stage, &s_mbar, phase, s_tmp, &s_ct, &s_err,
+                                       pad_log2);
     if (s_err) {
         if (threadIdx.x == 0) raise_error(s_err);
         return;
@@ -635,7 +660,7 @@ __global__ void __launch_bounds__(NT) decompress_kernel(const __grid_constant__ 
     const uint64_t first = (uint64_t)chunk * c.rows_per_chunk + (uint64_t)j * c.rows_per_block + r0 - row0;
     int32_t* out = dst + first;
     for (uint32_t r = threadIdx.x; r < n; r += NT)
-        out[r] = (int32_t)buf[layout == kSegRows ? r + (r >> c.seg_shift) : r];
+        out[r] = (int32_t)buf[layout == kSegRows ? r + ((r >> c.seg_shift) << pad_log2) : r];
 }
 
 __global__ void raw_lz4_kernel(const uint8_t* comp, const uint64_t* coff, uint8_t* out, const uint64_t* ooff,
@@ -861,6 +886,8 @@ gx_status allow_smem(K kernel, size_t bytes) {
     return GX_OK;
 }
 
+#include "shared_scan.cuh"
+
 }  // namespace
 
 // ---------------------------------------------------------------- objects
@@ -896,6 +923,24 @@ struct gx_batch {
     int device = -1;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // execution form
+    uint32_t mode_pref = GX_BATCH_AUTO;
+    uint32_t mode = GX_BATCH_QUEUE;
+    // shared form
+    ShQuery* d_sq = nullptr;
+    ShQuery* h_sq = nullptr;      // pinned staging
+    uint32_t cap_sq = 0;
+    gx_dcol* d_cols = nullptr;
+    gx_dcol* h_cols = nullptr;    // pinned staging (kShMaxCols entries)
+    uint32_t* d_slot_mask = nullptr;
+    size_t cap_mask = 0;          // words
+    uint32_t* d_sh_items = nullptr;  // n_items | work_counter | items[n_slots]
+    uint32_t cap_slots = 0;
+    ShParams SP{};
+    uint32_t n_slots = 0;
+    const gx_dblock* dir0 = nullptr;
+    uint32_t sh_grid = 1, sh_items_grid = 1;
+    size_t sh_smem = 0;
 };
 
 extern "C" {
@@ -924,6 +969,12 @@ gx_status gx_column_to_device(gx_column* col, int residency, void* stream) {
     GX_CK(cudaMalloc(&col->d_maxs, 4 * col->n_chunks));
     GX_CK(cudaMemcpyAsync(col->d_mins, col->mins.data(), 4 * col->n_chunks, cudaMemcpyHostToDevice, s));
     GX_CK(cudaMemcpyAsync(col->d_maxs, col->maxs.data(), 4 * col->n_chunks, cudaMemcpyHostToDevice, s));
+    if (col->bmins.size() == col->n_slots && col->n_slots) {
+        GX_CK(cudaMalloc(&col->d_bmins, 4ull * col->n_slots));
+        GX_CK(cudaMalloc(&col->d_bmaxs, 4ull * col->n_slots));
+        GX_CK(cudaMemcpyAsync(col->d_bmins, col->bmins.data(), 4ull * col->n_slots, cudaMemcpyHostToDevice, s));
+        GX_CK(cudaMemcpyAsync(col->d_bmaxs, col->bmaxs.data(), 4ull * col->n_slots, cudaMemcpyHostToDevice, s));
+    }
     GX_CK(cudaStreamSynchronize(s));
     cudaGetDevice(&col->device);
     col->residency = residency;
@@ -938,6 +989,9 @@ gx_status gx_column_release_device(gx_column* col) {
     if (col->d_seg) cudaFree(col->d_seg);
     if (col->d_mins) cudaFree(col->d_mins);
     if (col->d_maxs) cudaFree(col->d_maxs);
+    if (col->d_bmins) cudaFree(col->d_bmins);
+    if (col->d_bmaxs) cudaFree(col->d_bmaxs);
+    col->d_bmins = col->d_bmaxs = nullptr;
     col->d_payload = nullptr;
     col->h_pinned = nullptr;
     col->d_blocks = nullptr;
@@ -1019,7 +1073,7 @@ static gx_status fill_prune(ItemsParams* ip, const gx_column* const* cols, const
     for (uint32_t p = 0; p < n_preds; ++p) {
         if (!cols[p] || !cols[p]->residency) return set_error(GX_ERR_INVALID, "prune column %u not on device", p);
         if (cols[p]->n_chunks != n_chunks) return set_error(GX_ERR_INVALID, "prune columns disagree on chunk count");
-        ip->preds[p] = PrunePred{cols[p]->d_mins, cols[p]->d_maxs, lo[p], hi[p]};
+        ip->preds[p] = PrunePred{cols[p]->d_mins, cols[p]->d_maxs, lo[p], hi[p], nullptr, nullptr};
     }
     ip->n_preds = n_preds;
     ip->n_chunks = n_chunks;
@@ -1295,7 +1349,7 @@ static gx_status build_query(const gx_scan_plan* plan, QueryDesc* Q, uint32_t* t
         const gx_column* pc = plan->prune[i].col;
         if (!pc || !pc->residency) return set_error(GX_ERR_INVALID, "prune column %u not on device", i);
         if (pc->n_chunks != c0->n_chunks) return set_error(GX_ERR_INVALID, "prune column %u has another chunking", i);
-        Q->prune[i] = PrunePred{pc->d_mins, pc->d_maxs, plan->prune[i].lo, plan->prune[i].hi};
+        Q->prune[i] = PrunePred{pc->d_mins, pc->d_maxs, plan->prune[i].lo, plan->prune[i].hi, pc->d_bmins, pc->d_bmaxs};
     }
     Q->n_prune = plan->n_prune;
     *tile_rows = pick_tile_rows(cols, plan->n_steps);
@@ -1312,6 +1366,9 @@ static gx_status ensure_kernel_attrs() {
     if (!st) st = allow_smem(scan_kernel<128, kTileRows, true>, scan_smem_bytes<kTileRows>(true, true));
     if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock, false>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
     if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock, true>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
+    if (!st)
+        st = allow_smem(shared_scan_kernel, 4ull * kShColWords * kShMaxCols + Cfg<kTileRows>::kStage +
+                                                8ull * kShMaxQueries + 4ull * (kShMaxQueries / 32));
     if (st) return st;
     attr_set[dev & 63] = true;
     return GX_OK;
@@ -1426,6 +1483,135 @@ gx_status gx_scan_sync(const gx_scan_plan* plan, void* stream, uint64_t* rows_sc
 }
 
 
+}  // extern "C"
+
+// Shared form: checks that the batch qualifies (why = the first reason it
+// does not) and fills the shared descriptors; uploads on stream s.
+static gx_status shared_prepare(gx_batch* b, const gx_query* queries, uint32_t n, const std::vector<QueryDesc>& qs,
+                                const gx_column* c0, cudaStream_t s, bool* ok, std::string* why) {
+    *ok = false;
+    if (n > kShMaxQueries) {
+        *why = "more than 1024 queries";
+        return GX_OK;
+    }
+    std::vector<const gx_column*> cols;
+    std::vector<ShQuery> sq(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const gx_scan_plan& pl = queries[i].plan;
+        std::memset(&sq[i], 0, sizeof(ShQuery));
+        for (uint32_t k = 0; k < pl.n_steps; ++k) {
+            const bool is_value = (pl.steps[k].flags & GX_STEP_VALUE) != 0;
+            if (is_value != (k + 1 == pl.n_steps)) {
+                *why = "a plan whose only VALUE step is not its last step";
+                return GX_OK;
+            }
+            const gx_column* c = pl.steps[k].col;
+            if (c->codec == GX_CODEC_LZ4 && (c->S <= 1 || (1u << c->seg_shift) > kShTile)) {
+                *why = "an LZ4 column without segments of at most 2048 rows";
+                return GX_OK;
+            }
+            uint32_t ci = 0;
+            while (ci < cols.size() && cols[ci] != c) ++ci;
+            if (ci == cols.size()) {
+                if (cols.size() == kShMaxCols) {
+                    *why = "more than 16 distinct columns";
+                    return GX_OK;
+                }
+                cols.push_back(c);
+            }
+            const ScanStep& d = qs[i].steps[k];
+            ShStep& e = sq[i].steps[k];
+            e.flags = d.flags;
+            e.lo = d.lo;
+            e.hi = d.hi;
+            e.col = ci;
+            e.ht = d.ht;
+            e.ht_log2 = d.ht_log2;
+            e.ht_layout = d.ht_layout;
+            e.digit_base = d.digit_base;
+            e.digit_card = d.digit_card;
+            sq[i].col_mask |= 1u << ci;
+        }
+        ShQuery& Q = sq[i];
+        Q.n_steps = pl.n_steps;
+        Q.agg = qs[i].agg;
+        Q.grouped = qs[i].grouped;
+        Q.row_lo = qs[i].row_lo;
+        Q.row_hi = qs[i].row_hi;
+        Q.result = qs[i].result;
+        Q.g_keys = qs[i].g_keys;
+        Q.g_sums = qs[i].g_sums;
+        Q.g_log2 = qs[i].g_log2;
+        Q.n_prune = qs[i].n_prune;
+        for (uint32_t p = 0; p < Q.n_prune; ++p) Q.prune[p] = qs[i].prune[p];
+        Q.keep_in = nullptr;
+    }
+    const uint32_t mw = (n + 31) / 32;
+    const uint32_t n_slots = c0->n_slots;
+    // grow buffers (the stream's earlier work is finished by the caller)
+    if (n > b->cap_sq) {
+        cudaFree(b->d_sq);
+        cudaFreeHost(b->h_sq);
+        b->d_sq = nullptr;
+        b->h_sq = nullptr;
+        b->cap_sq = 0;
+        GX_CK(cudaMalloc(&b->d_sq, sizeof(ShQuery) * n));
+        GX_CK(cudaMallocHost(&b->h_sq, sizeof(ShQuery) * n));
+        b->cap_sq = n;
+    }
+    if (!b->d_cols) {
+        GX_CK(cudaMalloc(&b->d_cols, sizeof(gx_dcol) * kShMaxCols));
+        GX_CK(cudaMallocHost(&b->h_cols, sizeof(gx_dcol) * kShMaxCols));
+    }
+    if ((size_t)n_slots * mw > b->cap_mask) {
+        cudaFree(b->d_slot_mask);
+        b->d_slot_mask = nullptr;
+        b->cap_mask = 0;
+        GX_CK(cudaMalloc(&b->d_slot_mask, 4ull * n_slots * mw));
+        b->cap_mask = (size_t)n_slots * mw;
+    }
+    if (n_slots > b->cap_slots) {
+        cudaFree(b->d_sh_items);
+        b->d_sh_items = nullptr;
+        b->cap_slots = 0;
+        GX_CK(cudaMalloc(&b->d_sh_items, 4ull * (n_slots + 2)));
+        b->cap_slots = n_slots;
+    }
+    std::memcpy(b->h_sq, sq.data(), sizeof(ShQuery) * n);
+    for (size_t i = 0; i < cols.size(); ++i) b->h_cols[i] = cols[i]->view();
+    GX_CK(cudaMemcpyAsync(b->d_sq, b->h_sq, sizeof(ShQuery) * n, cudaMemcpyHostToDevice, s));
+    GX_CK(cudaMemcpyAsync(b->d_cols, b->h_cols, sizeof(gx_dcol) * cols.size(), cudaMemcpyHostToDevice, s));
+    ShParams& P = b->SP;
+    std::memset(&P, 0, sizeof(P));
+    P.cols = b->d_cols;
+    P.n_cols = (uint32_t)cols.size();
+    P.qs = b->d_sq;
+    P.n_queries = n;
+    P.mask_words = mw;
+    P.slot_mask = b->d_slot_mask;
+    P.n_items = b->d_sh_items;
+    P.work_counter = b->d_sh_items + 1;
+    P.items = b->d_sh_items + 2;
+    P.blocks_per_chunk = c0->blocks_per_chunk;
+    P.rows_per_chunk = c0->rows_per_chunk;
+    P.rows_per_block = c0->rows_per_block;
+    P.tile_rows = std::min<uint32_t>(kShTile, c0->rows_per_block);
+    P.tiles_per_block = (c0->rows_per_block + P.tile_rows - 1) / P.tile_rows;
+    P.rows_scanned = b->d_rows;
+    b->n_slots = n_slots;
+    b->dir0 = c0->d_blocks;
+    b->sh_smem = 4ull * kShColWords * P.n_cols + Cfg<kTileRows>::kStage + 8ull * n + 4ull * mw;
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shared_scan_kernel, kShNT, b->sh_smem);
+    const uint64_t tiles = (uint64_t)n_slots * P.tiles_per_block;
+    b->sh_grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * std::max(1, per_sm), tiles));
+    b->sh_items_grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(8ull * sm_count(), (n_slots + 7) / 8));
+    *ok = true;
+    return GX_OK;
+}
+
+extern "C" {
+
 gx_status gx_batch_assign(gx_batch* b, const gx_query* queries, uint32_t n_queries, void* stream) {
     if (!b || !queries || n_queries == 0) return set_error(GX_ERR_INVALID, "gx_batch_assign: bad args");
     cudaStream_t s = (cudaStream_t)stream;
@@ -1524,12 +1710,34 @@ gx_status gx_batch_assign(gx_batch* b, const gx_query* queries, uint32_t n_queri
     const uint64_t tiles = (uint64_t)nc * c0->blocks_per_chunk * P.tiles_per_block;
     scan_geometry<true>(tile_rows, aux, groups, tiles, &b->grid, &b->threads, &b->smem);
     b->reset_x = (uint32_t)std::min<uint64_t>(64, std::max<uint64_t>(1, max_table / 4096));
+    b->mode = GX_BATCH_QUEUE;
+    if (b->mode_pref != GX_BATCH_QUEUE) {
+        bool ok = false;
+        std::string why;
+        st = shared_prepare(b, queries, n_queries, qs, c0, s, &ok, &why);
+        if (st) return st;
+        if (ok) b->mode = GX_BATCH_SHARED;
+        else if (b->mode_pref == GX_BATCH_SHARED)
+            return set_error(GX_ERR_INVALID, "batch cannot run in the shared form: %s", why.c_str());
+    }
     return GX_OK;
 }
 
 gx_status gx_batch_create(const gx_query* queries, uint32_t n_queries, gx_batch** out) {
-    if (!queries || !out || n_queries == 0) return set_error(GX_ERR_INVALID, "gx_batch_create: bad args");
+    return gx_batch_create2(queries, n_queries, GX_BATCH_AUTO, out);
+}
+
+gx_status gx_batch_mode(const gx_batch* b, uint32_t* mode) {
+    if (!b || !mode) return set_error(GX_ERR_INVALID, "gx_batch_mode: bad args");
+    *mode = b->mode;
+    return GX_OK;
+}
+
+gx_status gx_batch_create2(const gx_query* queries, uint32_t n_queries, uint32_t mode, gx_batch** out) {
+    if (!queries || !out || n_queries == 0 || mode > GX_BATCH_SHARED)
+        return set_error(GX_ERR_INVALID, "gx_batch_create: bad args");
     gx_batch* b = new gx_batch();
+    b->mode_pref = mode;
     cudaGetDevice(&b->device);
     if (cudaMalloc(&b->d_rows, 8) != cudaSuccess) {
         delete b;
@@ -1554,6 +1762,12 @@ gx_status gx_batch_free(gx_batch* b) {
     cudaFree(b->d_rows);
     cudaFreeHost(b->h_qs);
     cudaFreeHost(b->h_cand);
+    cudaFree(b->d_sq);
+    cudaFreeHost(b->h_sq);
+    cudaFree(b->d_cols);
+    cudaFreeHost(b->h_cols);
+    cudaFree(b->d_slot_mask);
+    cudaFree(b->d_sh_items);
     delete b;
     return GX_OK;
 }
@@ -1563,6 +1777,16 @@ gx_status gx_batch_run(gx_batch* b, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     const size_t nc = b->cap_cand;
     batch_reset_kernel<<<dim3(b->reset_x, b->n), 256, 0, s>>>(b->d_qs, b->d_rows);
+    if (b->mode == GX_BATCH_SHARED) {
+        GX_CK(cudaMemsetAsync(b->d_sh_items, 0, 8, s));
+        shared_items_kernel<<<b->sh_items_grid, 256, 0, s>>>(b->dir0, b->n_slots, b->d_sq, b->n, b->SP.mask_words,
+                                                               b->SP.blocks_per_chunk, b->SP.rows_per_chunk,
+                                                               b->SP.rows_per_block, b->d_slot_mask,
+                                                               b->d_sh_items + 2, b->d_sh_items);
+        shared_scan_kernel<<<b->sh_grid, kShNT, b->sh_smem, s>>>(b->SP);
+        GX_CK(cudaGetLastError());
+        return GX_OK;
+    }
     batch_items_kernel<<<1, 1024, 0, s>>>(b->d_qs, b->d_buf, b->d_buf + nc, b->n_cand, b->d_buf + 2 * nc,
                                           b->d_buf + 3 * nc, b->d_buf + 4 * nc, b->d_buf + 4 * nc + 1);
     launch_scan_kernel<true>(b->P, b->grid, b->threads, b->smem, s);

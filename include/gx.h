@@ -296,11 +296,23 @@ typedef struct gx_query {
 typedef struct gx_batch gx_batch;
 
 gx_status gx_batch_create(const gx_query* queries, uint32_t n_queries, gx_batch** out);
+/* Execution form.  QUEUE: the work list above, every query decoding its own
+ * columns.  SHARED: every (block, tile) that any query needs is decoded once
+ * -- each column its active queries read, into shared memory -- and all of
+ * those queries are evaluated on it; needs every plan to end with its only
+ * VALUE step, LZ4 columns with segments of at most 2048 rows, at most 16
+ * distinct columns and 1024 queries.  AUTO (gx_batch_create): SHARED when
+ * the batch qualifies, else QUEUE; asking for SHARED when it does not
+ * qualifies fails with GX_ERR_INVALID and the reason. */
+enum { GX_BATCH_AUTO = 0, GX_BATCH_QUEUE = 1, GX_BATCH_SHARED = 2 };
+gx_status gx_batch_create2(const gx_query* queries, uint32_t n_queries, uint32_t mode, gx_batch** out);
+/* The form the batch currently runs in (GX_BATCH_QUEUE or GX_BATCH_SHARED). */
+gx_status gx_batch_mode(const gx_batch* b, uint32_t* mode);
 /* Replace the batch's queries (buffers reused, grown when needed; the
  * descriptor upload is enqueued on `stream`).  Drops a captured graph. */
 gx_status gx_batch_assign(gx_batch* b, const gx_query* queries, uint32_t n_queries, void* stream);
 gx_status gx_batch_free(gx_batch* b);
-/* Clear results, build the work list, run all queries (3 launches). */
+/* Clear results, build the work list, run all queries (3 or 4 launches). */
 gx_status gx_batch_run(gx_batch* b, void* stream);
 /* Capture gx_batch_run into a CUDA graph on first use, then replay it. */
 gx_status gx_batch_graph(gx_batch* b, void* stream);

@@ -1,10 +1,14 @@
 """Batched form: many plans on row slices of one resident table in one
-persistent launch (and as a replayed CUDA graph).  Every query's result must
-equal the oracle on its slice, alone and in the mix."""
+persistent launch (and as a replayed CUDA graph), in both execution forms
+(per-query work items, and the shared scan that decodes each tile once for
+all queries).  Every query's result must equal the oracle on its slice,
+alone and in the mix."""
 import numpy as np
 import pytest
 
+from golap_public_b200 import _lib as L
 from golap_public_b200 import api, workload
+from golap_public_b200._lib import GxError
 from oracle import workload_oracle as WO
 
 pytestmark = pytest.mark.gpu
@@ -20,11 +24,16 @@ def _check(t, specs):
         assert workload.read_result(s) == WO.expected(t, s), (s.template, s.row_lo, s.row_hi, s.params)
 
 
-def test_batch_mixed_queries(table):
+MODES = ["queue", "shared"]
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_batch_mixed_queries(table, mode):
     rng = np.random.default_rng(5)
     specs = workload.random_queries(table, 48, rng, min_rows=100_000, max_rows=6_000_000)
     assert {s.template for s in specs} >= {"scan", "star"}
-    b = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs])
+    b = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs], mode)
+    assert b.mode == mode
     b.run()
     api.scan_check()
     _check(table, specs)
@@ -35,25 +44,27 @@ def test_batch_mixed_queries(table):
     _check(table, specs)
 
 
-def test_each_query_alone_equals_in_mix(table):
+@pytest.mark.parametrize("mode", MODES)
+def test_each_query_alone_equals_in_mix(table, mode):
     rng = np.random.default_rng(11)
     specs = workload.random_queries(table, 12, rng, min_rows=50_000, max_rows=3_000_000,
                                     mix=(("scan", 0.4), ("star", 0.4), ("highcard", 0.2)))
-    mixed = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs])
+    mixed = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs], mode)
     mixed.run()
     api.scan_check()
     in_mix = [workload.read_result(s) for s in specs]
     for s, want in zip(specs, in_mix):
-        alone = api.Batch([(s.plan, s.row_lo, s.row_hi)])
+        alone = api.Batch([(s.plan, s.row_lo, s.row_hi)], mode)
         alone.run()
         api.scan_check()
         assert workload.read_result(s) == want == WO.expected(table, s)
 
 
-def test_highcard_group_by_part_key(table):
+@pytest.mark.parametrize("mode", MODES)
+def test_highcard_group_by_part_key(table, mode):
     rng = np.random.default_rng(2)
     s = workload.make_query(table, "highcard", rng, 0, table.n_rows)
-    b = api.Batch([(s.plan, 0, table.n_rows)])
+    b = api.Batch([(s.plan, 0, table.n_rows)], mode)
     b.run()
     api.scan_check()
     got = workload.read_result(s)
@@ -61,12 +72,40 @@ def test_highcard_group_by_part_key(table):
     assert got == WO.expected(table, s)
 
 
-def test_empty_and_edge_slices(table):
+@pytest.mark.parametrize("mode", MODES)
+def test_empty_and_edge_slices(table, mode):
     rng = np.random.default_rng(3)
     specs = [workload.make_query(table, "scan", rng, 0, 0), workload.make_query(table, "scan", rng, 5, 6),
              workload.make_query(table, "star", rng, table.n_rows - 1, table.n_rows),
              workload.make_query(table, "scan", rng, 999_999, 1_000_001)]
-    b = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs])
+    b = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs], mode)
     b.run()
     api.scan_check()
     _check(table, specs)
+
+
+def test_shared_rows_equal_queue_rows(table):
+    # both forms count, per query, the slice rows of every tile they evaluate
+    rng = np.random.default_rng(8)
+    specs = workload.random_queries(table, 16, rng, min_rows=100_000, max_rows=6_000_000,
+                                    mix=(("star", 0.5), ("highcard", 0.5)))
+    got = {}
+    for mode in MODES:
+        b = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs], mode)
+        b.run()
+        api.scan_check()
+        got[mode] = (b.rows(), [workload.read_result(s) for s in specs])
+    assert got["queue"] == got["shared"]
+
+
+def test_shared_form_eligibility(table, cuda):
+    rng = np.random.default_rng(4)
+    s = workload.make_query(table, "scan", rng, 0, table.n_rows)
+    assert api.Batch([(s.plan, 0, table.n_rows)]).mode == "shared"  # auto picks the shared form
+    # a plan with a VALUE step before its last step does not qualify
+    res = cuda.zeros(1, dtype=cuda.int64, device="cuda")
+    p = api.ScanPlan(agg=L.GX_AGG_SUM, result=res).value(table.cols["quantity"]).filter(table.cols["discount"], 0, 5)
+    assert api.Batch([(p, 0, 1000)]).mode == "queue"
+    with pytest.raises(GxError) as e:
+        api.Batch([(p, 0, 1000)], "shared")
+    assert e.value.status == L.GX_ERR_INVALID and "VALUE" in str(e.value)
