@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -1443,7 +1444,87 @@ static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned 
     return GX_OK;
 }
 
+// Work-list scratch of gx_scan_static, one per device: word 0 = surviving
+// chunk count, word 1 = work counter, words 4.. = surviving chunk ids.
+// items_kernel writes both counters before scan_kernel reads them (same
+// stream), so no word needs to be zero beforehand.
+constexpr uint32_t kStaticMaxChunks = GX_SCAN_STATIC_MAX_CHUNKS;
+static __device__ __align__(256) uint32_t g_scan_static_scratch[4 + kStaticMaxChunks];
+
+// Device address of g_scan_static_scratch on the current device, looked up
+// once per device (with that device current) and cached.
+static gx_status static_scratch(uint32_t** out) {
+    static std::mutex mu;
+    static uint32_t* addr[64] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "gx_scan_static: cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= 64) return set_error(GX_ERR_INVALID, "gx_scan_static: device %d out of range", dev);
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_scan_static_scratch);
+        if (e != cudaSuccess || !p)
+            return set_error(GX_ERR_CUDA, "gx_scan_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        addr[dev] = (uint32_t*)p;
+    }
+    *out = addr[dev];
+    return GX_OK;
+}
+
+// scan_launch with the work list in g_scan_static_scratch: no allocation.
+static gx_status scan_launch_static(const gx_scan_plan* plan, cudaStream_t s) {
+    ScanParams P;
+    std::memset(&P, 0, sizeof(P));
+    const gx_column* c0 = nullptr;
+    uint32_t tile_rows = 0;
+    gx_status st = build_query(plan, &P.q, &tile_rows, &c0);
+    if (st) return st;
+    const uint32_t n_chunks = c0->n_chunks;
+    if (n_chunks > kStaticMaxChunks)
+        return set_error(GX_ERR_INVALID, "gx_scan_static: %u chunks exceed the static work list of %u chunks", n_chunks,
+                         kStaticMaxChunks);
+    st = ensure_kernel_attrs();
+    if (st) return st;
+    uint32_t* scratch = nullptr;
+    st = static_scratch(&scratch);
+    if (st) return st;
+    ItemsParams ip{};
+    for (uint32_t i = 0; i < P.q.n_prune; ++i) ip.preds[i] = P.q.prune[i];
+    ip.n_preds = P.q.n_prune;
+    ip.n_chunks = n_chunks;
+    ip.keep_in = plan->keep_chunks_dev;
+    ip.keep_out = plan->keep_out_dev;
+    ip.n_items = scratch;
+    ip.work_counter = scratch + 1;
+    ip.items = scratch + 4;
+    items_kernel<<<1, 1024, 0, s>>>(ip);
+    P.blocks_per_chunk = c0->blocks_per_chunk;
+    P.rows_per_chunk = c0->rows_per_chunk;
+    P.rows_per_block = c0->rows_per_block;
+    P.tile_rows = tile_rows;
+    P.tiles_per_block = (c0->rows_per_block + tile_rows - 1) / tile_rows;
+    P.smem_aux = P.q.need_aux;
+    P.smem_groups = P.q.grouped;
+    P.items = ip.items;
+    P.n_items = ip.n_items;
+    P.work_counter = ip.work_counter;
+    P.rows_scanned = nullptr;
+    const uint64_t tiles = (uint64_t)n_chunks * c0->blocks_per_chunk * P.tiles_per_block;
+    uint32_t grid = 1, threads = 128;
+    size_t smem = 0;
+    scan_geometry<false>(tile_rows, P.smem_aux, P.smem_groups, tiles, &grid, &threads, &smem);
+    launch_scan_kernel<false>(P, grid, threads, smem, s);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "gx_scan_static launch: %s", cudaGetErrorString(e));
+    return GX_OK;
+}
+
 extern "C" {
+
+gx_status gx_scan_static(const gx_scan_plan* plan, void* stream) {
+    return scan_launch_static(plan, (cudaStream_t)stream);
+}
 
 gx_status gx_scan(const gx_scan_plan* plan, void* stream) {
     return scan_launch(plan, (cudaStream_t)stream, nullptr);

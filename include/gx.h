@@ -278,6 +278,25 @@ gx_status gx_scan_sync(const gx_scan_plan* plan, void* stream, uint64_t* rows_sc
 /* Read and clear the device error word of the scan engine. */
 gx_status gx_scan_check(void* stream);
 
+/* Allocation-free form of gx_scan.  No reference counterpart: the reference
+ * has no scan entry point whose scratch avoids the allocator.
+ * Identical results to gx_scan, but the chunk work list lives in one
+ * file-scope device array per device (GX_SCAN_STATIC_MAX_CHUNKS chunk ids,
+ * 64 KiB) instead of stream-ordered pool memory, so the call never allocates
+ * or frees device memory.  It is for callers that own every byte of device
+ * memory through their own budget (tables carved out of HBM up front, with
+ * the driver's pool kept empty) and for callers that cannot afford a pool
+ * allocation that may fail or map new memory in the middle of a query.
+ * Plans over more than GX_SCAN_STATIC_MAX_CHUNKS chunks are rejected with
+ * GX_ERR_INVALID.  Nothing in the array has to start at zero: the launch
+ * writes the chunk count and resets the work counter before the scan reads
+ * them, in stream order.  The array is shared by all callers on a device, so
+ * two calls that can overlap in time (different streams, or different host
+ * threads without ordering between their streams) race and give wrong
+ * results: serialise them on one stream. */
+#define GX_SCAN_STATIC_MAX_CHUNKS 16384u
+gx_status gx_scan_static(const gx_scan_plan* plan, void* stream);
+
 /* ------------------------------------------------------------ batched scan
  * No reference counterpart (the reference runs one query per pipeline).
  * Many plans over the same fact table, each restricted to a row slice
