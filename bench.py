@@ -346,19 +346,24 @@ def _hbm_bytes(spec):
     return 8 if spec.groups is None else 16 * (2 * spec.groups.max_groups) + 8
 
 
-def batched_section(t, n_queries=256, seed=7):
+def batched_section(t, n_queries=256, seed=7, choices=None):
     """configs[3]-style batch: n queries on log-uniform slices (1M..100M rows)
     mixing the scan, star-join and high-cardinality templates.  One query at
     a time (its own launch sequence, back to back on one stream) vs all
     queries in one persistent launch replayed from a CUDA graph."""
     import torch
 
-    from golap_public_b200 import api, workload
+    from golap_public_b200 import api, autotune, workload
 
+    choices = choices or {}
     rng = np.random.default_rng(seed)
-    specs = workload.random_queries(t, n_queries, rng)
+    specs = workload.random_queries(t, n_queries, rng, ht_layout=autotune.layouts(choices))
     singles = {m: [api.Batch([(s.plan, s.row_lo, s.row_hi)], m) for s in specs] for m in ("queue", "shared")}
+    for s, b in zip(specs, singles["shared"]):
+        b.set_launch(**autotune.choose(choices, [s.template]))
     batch = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs])
+    launch = autotune.choose(choices, [s.template for s in specs])
+    batch.set_launch(**launch)
     stream = torch.cuda.current_stream()
     single_mode = "queue"
 
@@ -400,13 +405,14 @@ def batched_section(t, n_queries=256, seed=7):
     rows = sum(s.row_hi - s.row_lo for s in specs)
     mix = {k: sum(1 for s in specs if s.template == k) for k in ("scan", "star", "highcard")}
     return {"queries": n_queries, "mix": mix, "slice_rows_total": rows, "batch_form": batch.mode,
+            "batch_launch": launch,
             "one_at_a_time_ms": t_one, "one_at_a_time_form": single_mode,
             "one_at_a_time_ms_by_form": t_single, "batched_graph_ms": t_batch,
             "one_at_a_time_qps": n_queries / (t_one * 1e-3), "batched_qps": n_queries / (t_batch * 1e-3),
             "speedup": t_one / t_batch, "results_identical": True}
 
 
-def serving_section(t, rates=(200, 1000, 2000), seconds=2.0, seed=9, max_backlog=300):
+def serving_section(t, rates=(200, 1000, 2000), seconds=2.0, seed=9, max_backlog=300, choices=None):
     """configs[4]-style open loop: Poisson arrivals at each rate for `seconds`,
     60% pruned scans / 30% star joins / 10% Zipf group-bys over the whole
     resident table, served by the continuous-batching server and by a
@@ -415,15 +421,18 @@ def serving_section(t, rates=(200, 1000, 2000), seconds=2.0, seed=9, max_backlog
     arrivals stop there (counted as `shed`) so that the drain stays bounded."""
     import threading
 
-    from golap_public_b200 import api, workload
+    from golap_public_b200 import api, autotune, workload
 
+    choices = choices or {}
     rng = np.random.default_rng(seed)
-    pool = workload.random_queries(t, 384, rng, min_rows=t.n_rows, max_rows=t.n_rows)
-    out = {}
+    pool = workload.random_queries(t, 384, rng, min_rows=t.n_rows, max_rows=t.n_rows,
+                                   ht_layout=autotune.layouts(choices))
+    threads = autotune.choose(choices, [s.template for s in pool])["threads"]
+    out = {"batch_threads": threads}
     for mode, (inflight, maxb) in (("batched", (4, 64)), ("one_at_a_time", (1, 1))):
         res = {}
         for rate in rates:
-            sv = api.Server(max_inflight=inflight, max_batch=maxb, hbm_budget=120 << 30)
+            sv = api.Server(max_inflight=inflight, max_batch=maxb, hbm_budget=120 << 30, batch_threads=threads)
             arr = np.cumsum(rng.exponential(1.0 / rate, int(rate * seconds)))
             busy = {}
             lats = []
@@ -527,6 +536,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched and serving sections")
     ap.add_argument("--batch-rows", type=int, default=100_000_000)
+    ap.add_argument("--no-tune", action="store_true", help="batched/serving with the default launch shape")
+    ap.add_argument("--tune-rows", type=int, default=20_000_000)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -560,14 +571,25 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     line, f, dd = gpu_arm(args, rank, world)
     if not args.no_batch:
-        from golap_public_b200 import workload
+        from golap_public_b200 import autotune, workload
 
+        choices = {}
+        if not args.no_tune:
+            tr = autotune.tune(n_rows=args.tune_rows, queries_per_template=16, reps=3)
+            choices = {t: v["best"] for t, v in tr["templates"].items()}
+            line["autotune"] = {"sample_rows": args.tune_rows, "queries_per_template": 16, "tune_s": tr["tune_s"],
+                                "grid": {k: list(v) for k, v in autotune.SPACE.items()}, "best": choices,
+                                "default_ms": {t: next(p["ms"] for p in v["points"]
+                                                       if all(p[k] == autotune.DEFAULT[k] for k in autotune.DEFAULT))
+                                               for t, v in tr["templates"].items()}}
+        cfg = autotune.table_config(choices)
         t_build = time.perf_counter()
-        wt = workload.build_table(args.batch_rows)
+        wt = workload.build_table(args.batch_rows, rows_per_chunk=cfg["rows_per_chunk"], ht_layouts=cfg["ht_layouts"])
         build_s = time.perf_counter() - t_build
-        line["batched"] = batched_section(wt)
-        line["serving"] = serving_section(wt)
+        line["batched"] = batched_section(wt, choices=choices)
+        line["serving"] = serving_section(wt, choices=choices)
         line["batched"]["table_rows"] = args.batch_rows
+        line["batched"]["table_rows_per_chunk"] = cfg["rows_per_chunk"]
         line["batched"]["table_build_s"] = build_s
         del wt
     if rank == 0 and not args.no_cpu:

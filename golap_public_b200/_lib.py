@@ -75,7 +75,8 @@ class Query(C.Structure):
 
 
 class ServerOpts(C.Structure):
-    _fields_ = [("max_inflight", C.c_uint32), ("max_batch", C.c_uint32), ("hbm_budget", C.c_uint64)]
+    _fields_ = [("max_inflight", C.c_uint32), ("max_batch", C.c_uint32), ("hbm_budget", C.c_uint64),
+                ("batch_threads", C.c_uint32), ("batch_mode", C.c_uint32)]
 
 
 class ServerStats(C.Structure):
@@ -125,6 +126,7 @@ _SIGS = {
     "gx_batch_create": (C.c_int32, [C.POINTER(Query), C.c_uint32, C.POINTER(P)]),
     "gx_batch_create2": (C.c_int32, [C.POINTER(Query), C.c_uint32, C.c_uint32, C.POINTER(P)]),
     "gx_batch_mode": (C.c_int32, [P, C.POINTER(C.c_uint32)]),
+    "gx_batch_set_launch": (C.c_int32, [P, C.c_uint32, C.c_uint32]),
     "gx_batch_free": (C.c_int32, [P]),
     "gx_batch_run": (C.c_int32, [P, P]),
     "gx_batch_graph": (C.c_int32, [P, P]),

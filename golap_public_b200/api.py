@@ -45,7 +45,7 @@ class Column:
     """One compressed int32 column: chunks of rows_per_chunk rows, blocks of rows_per_block rows."""
 
     def __init__(self, values: np.ndarray, codec: str = "lz4", rows_per_chunk: int = 1_000_000,
-                 rows_per_block: int = 16384, lz4_segments: int = 128, lz4_min_match: int = 4,
+                 rows_per_block: int = 16384, lz4_segments: int = 128, lz4_min_match: int = 0,
                  lz4_search_depth: int = 16, threads: int = 0, name: str = ""):
         values = np.ascontiguousarray(values, dtype=np.int32)
         o = L.EncodeOpts()
@@ -338,6 +338,10 @@ class Batch:
         check(L.lib().gx_batch_create2(arr, len(queries), self.MODES[mode], C.byref(h)))
         self.handle = h
 
+    def set_launch(self, threads: int = 256, ctas_per_sm: int = 0) -> "Batch":
+        check(L.lib().gx_batch_set_launch(self.handle, threads, ctas_per_sm))
+        return self
+
     @property
     def mode(self) -> str:
         m = C.c_uint32()
@@ -370,10 +374,12 @@ class Batch:
 class Server:
     """Continuous-batching serving loop (gx_server_* in include/gx.h)."""
 
-    def __init__(self, max_inflight: int = 4, max_batch: int = 64, hbm_budget: int = 120 << 30):
+    def __init__(self, max_inflight: int = 4, max_batch: int = 64, hbm_budget: int = 120 << 30,
+                 batch_threads: int = 0, batch_mode: str = "auto"):
         o = L.ServerOpts()
         check(L.lib().gx_server_opts_default(C.byref(o)))
         o.max_inflight, o.max_batch, o.hbm_budget = max_inflight, max_batch, hbm_budget
+        o.batch_threads, o.batch_mode = batch_threads, Batch.MODES[batch_mode]
         h = C.c_void_p()
         check(L.lib().gx_server_create(C.byref(o), C.byref(h)))
         self.handle = h

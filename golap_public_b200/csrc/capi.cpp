@@ -67,7 +67,7 @@ gx_status gx_encode_opts_default(gx_encode_opts* o) {
     o->rows_per_chunk = 1000000;
     o->rows_per_block = 16384;
     o->lz4_segments = 128;
-    o->lz4_min_match = 4;
+    o->lz4_min_match = 0;  // decode-cost-aware
     o->lz4_search_depth = 16;
     o->casc_rle = 1;
     o->casc_delta = 1;

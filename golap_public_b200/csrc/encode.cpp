@@ -39,6 +39,7 @@ inline uint32_t ext_bytes(uint32_t len) {  // extension bytes for a 4-bit field 
 
 struct SeqEmitter {
     std::vector<uint8_t>& out;
+    uint32_t n_seq = 0;     // sequences emitted
     size_t base;            // offset of the block start in out
     const uint8_t* bytes;   // input block as bytes
     uint32_t* seg;          // 2*S entries
@@ -50,6 +51,7 @@ struct SeqEmitter {
     // offset off words.  Resolves segment entries whose boundary lies in
     // [anchor, m] (or [anchor, end) for the final literal-only sequence).
     void emit(uint32_t anchor, uint32_t m, bool has_match, uint32_t off_w, uint32_t mlen_w) {
+        ++n_seq;
         const uint32_t tp = (uint32_t)(out.size() - base);
         const uint32_t Lb = (m - anchor) * 4;
         const uint32_t Mb = mlen_w * 4;
@@ -97,7 +99,7 @@ struct SeqEmitter {
 // current segment.
 size_t lz4_encode_block(const int32_t* vals, uint32_t W, uint32_t S, uint32_t seg_rows,
                         uint32_t min_match, uint32_t depth, std::vector<uint8_t>& out,
-                        uint32_t* seg) {
+                        uint32_t* seg, uint32_t* n_seq) {
     constexpr uint32_t HB = 14;
     const size_t base = out.size();
     std::vector<int32_t> head(1u << HB, -1);
@@ -106,7 +108,7 @@ size_t lz4_encode_block(const int32_t* vals, uint32_t W, uint32_t S, uint32_t se
     for (uint32_t j = 0; j <= S; ++j) bound[j] = std::min<uint64_t>((uint64_t)j * seg_rows, W);
     seg[0] = 0;
     seg[1] = 0;
-    SeqEmitter em{out, base, (const uint8_t*)vals, seg, bound.data(), S};
+    SeqEmitter em{out, 0, base, (const uint8_t*)vals, seg, bound.data(), S};
     const uint32_t min_w = std::max<uint32_t>(1, (min_match + 3) / 4);
     const uint32_t* v = (const uint32_t*)vals;
     auto h = [&](uint32_t x) { return (x * 2654435761u) >> (32 - HB); };
@@ -152,7 +154,37 @@ size_t lz4_encode_block(const int32_t* vals, uint32_t W, uint32_t S, uint32_t se
     }
     em.emit(anchor, W, false, 0, 0);
     em.finish(W);
+    if (n_seq) *n_seq = em.n_seq;
     return out.size() - base;
+}
+
+// Decode-cost-aware policy (lz4_min_match = 0): the block is encoded with
+// minimum matches of 1, 2 and 4 words and the encoding with the lowest
+// bytes + kSeqCost * sequences is kept.  A sequence costs the GPU decoder a
+// serial header parse, worth about kSeqCost bytes of streaming: short
+// matches that save a byte or two each are not worth their parse, long
+// matches (runs, repeated stretches) are.
+size_t lz4_encode_block_auto(const int32_t* vals, uint32_t W, uint32_t S, uint32_t seg_rows, uint32_t depth,
+                             std::vector<uint8_t>& out, uint32_t* seg) {
+    constexpr uint64_t kSeqCost = 24;
+    const uint32_t cands[3] = {4, 8, 16};
+    std::vector<uint8_t> best_buf, tmp;
+    std::vector<uint32_t> best_seg(2 * (size_t)S), tmp_seg(2 * (size_t)S);
+    uint64_t best_cost = UINT64_MAX;
+    for (uint32_t mm : cands) {
+        tmp.clear();
+        uint32_t ns = 0;
+        const size_t used = lz4_encode_block(vals, W, S, seg_rows, mm, depth, tmp, tmp_seg.data(), &ns);
+        const uint64_t cost = used + kSeqCost * ns;
+        if (cost < best_cost) {
+            best_cost = cost;
+            best_buf.swap(tmp);
+            best_seg.swap(tmp_seg);
+        }
+    }
+    out.insert(out.end(), best_buf.begin(), best_buf.end());
+    std::memcpy(seg, best_seg.data(), 8ull * S);
+    return best_buf.size();
 }
 
 size_t casc_encode_block(const int32_t* vals, uint32_t rows, bool allow_rle, bool allow_delta,
@@ -280,8 +312,8 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
             return set_error(GX_ERR_INVALID, "lz4_segments must be a power of two in 1..%u", kMaxSegments);
         if (S > 1 && ((rows_per_block & (rows_per_block - 1)) != 0 || rows_per_block < S))
             return set_error(GX_ERR_INVALID, "segmented LZ4 needs a power-of-two rows_per_block >= segments");
-        if (min_match < 4 || (min_match & 3))
-            return set_error(GX_ERR_INVALID, "lz4_min_match must be a multiple of 4 >= 4");
+        if (min_match != 0 && (min_match < 4 || (min_match & 3)))
+            return set_error(GX_ERR_INVALID, "lz4_min_match must be 0 (decode-cost-aware) or a multiple of 4 >= 4");
     } else {
         S = 1;
     }
@@ -351,8 +383,9 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
                 used = (size_t)rows * 4;
             } else if (codec == GX_CODEC_LZ4) {
                 uint32_t tmp_seg[2 * kMaxSegments];
-                used = lz4_encode_block(vals + r0, rows, S, rows_per_block / S, min_match, depth, buf,
-                                        tmp_seg);
+                used = min_match ? lz4_encode_block(vals + r0, rows, S, rows_per_block / S, min_match, depth, buf,
+                                                    tmp_seg, nullptr)
+                                 : lz4_encode_block_auto(vals + r0, rows, S, rows_per_block / S, depth, buf, tmp_seg);
                 if (used + 16 > kStageBytes) overflow = true;  // cannot happen for <= 16384 int32 rows
                 if (S > 1) std::memcpy(&col->seg[(size_t)2 * S * s], tmp_seg, 8 * S);
             } else {

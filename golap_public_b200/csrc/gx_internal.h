@@ -185,7 +185,9 @@ int set_error(int status, const char* fmt, ...);
 // block; returns the compressed size, appends S {comp_pos, info} pairs to seg.
 size_t lz4_encode_block(const int32_t* vals, uint32_t rows, uint32_t S, uint32_t seg_rows,
                         uint32_t min_match, uint32_t depth, std::vector<uint8_t>& out,
-                        uint32_t* seg_entries);
+                        uint32_t* seg_entries, uint32_t* n_seq);
+size_t lz4_encode_block_auto(const int32_t* vals, uint32_t rows, uint32_t S, uint32_t seg_rows, uint32_t depth,
+                             std::vector<uint8_t>& out, uint32_t* seg_entries);
 size_t casc_encode_block(const int32_t* vals, uint32_t rows, bool allow_rle, bool allow_delta,
                          bool allow_bp, std::vector<uint8_t>& out);
 // Column encoder (encode.cpp): fills layout, payload, directory, min/max.

@@ -942,7 +942,33 @@ struct gx_batch {
     const gx_dblock* dir0 = nullptr;
     uint32_t sh_grid = 1, sh_items_grid = 1;
     size_t sh_smem = 0;
+    uint32_t sh_threads = kShNT;   // launch shape of the shared form (tunable)
+    uint32_t sh_ctas_per_sm = 0;   // 0 = as many as fit
 };
+
+// Persistent grid of the shared form for the batch's thread count.
+static void shared_geometry(gx_batch* b) {
+    int per_sm = 1;
+    switch (b->sh_threads) {
+        case 128: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shared_scan_kernel<128, 4>, 128, b->sh_smem); break;
+        case 512: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shared_scan_kernel<512, 1>, 512, b->sh_smem); break;
+        case 1024: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shared_scan_kernel<1024, 1>, 1024, b->sh_smem); break;
+        default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shared_scan_kernel<256, 2>, 256, b->sh_smem); break;
+    }
+    per_sm = std::max(1, per_sm);
+    if (b->sh_ctas_per_sm) per_sm = std::min<int>(per_sm, (int)b->sh_ctas_per_sm);
+    const uint64_t tiles = (uint64_t)b->n_slots * b->SP.tiles_per_block;
+    b->sh_grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm, tiles));
+}
+
+static void launch_shared_kernel(const gx_batch* b, cudaStream_t s) {
+    switch (b->sh_threads) {
+        case 128: shared_scan_kernel<128, 4><<<b->sh_grid, 128, b->sh_smem, s>>>(b->SP); break;
+        case 512: shared_scan_kernel<512, 1><<<b->sh_grid, 512, b->sh_smem, s>>>(b->SP); break;
+        case 1024: shared_scan_kernel<1024, 1><<<b->sh_grid, 1024, b->sh_smem, s>>>(b->SP); break;
+        default: shared_scan_kernel<256, 2><<<b->sh_grid, 256, b->sh_smem, s>>>(b->SP); break;
+    }
+}
 
 extern "C" {
 
@@ -1367,9 +1393,12 @@ static gx_status ensure_kernel_attrs() {
     if (!st) st = allow_smem(scan_kernel<128, kTileRows, true>, scan_smem_bytes<kTileRows>(true, true));
     if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock, false>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
     if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock, true>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
-    if (!st)
-        st = allow_smem(shared_scan_kernel, 4ull * kShColWords * kShMaxCols + Cfg<kTileRows>::kStage +
-                                                8ull * kShMaxQueries + 4ull * (kShMaxQueries / 32));
+    const size_t sh_max = 4ull * kShColWords * kShMaxCols + Cfg<kTileRows>::kStage + 8ull * kShMaxQueries +
+                          4ull * (kShMaxQueries / 32);
+    if (!st) st = allow_smem(shared_scan_kernel<128, 4>, sh_max);
+    if (!st) st = allow_smem(shared_scan_kernel<256, 2>, sh_max);
+    if (!st) st = allow_smem(shared_scan_kernel<512, 1>, sh_max);
+    if (!st) st = allow_smem(shared_scan_kernel<1024, 1>, sh_max);
     if (st) return st;
     attr_set[dev & 63] = true;
     return GX_OK;
@@ -1381,9 +1410,17 @@ static void scan_geometry(uint32_t tile_rows, bool aux, bool groups, uint64_t ti
                           size_t* smem) {
     if (tile_rows <= kTileRows) {
         *smem = scan_smem_bytes<kTileRows>(aux, groups);
-        int per_sm = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_kernel<128, kTileRows, BATCH>, 128, *smem);
-        *grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * std::max(1, per_sm), tiles));
+        // resident CTAs per SM, per device and shared-memory layout (queried once)
+        static int occ[64][2][2] = {};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        int& per_sm = occ[dev & 63][aux][groups];
+        if (per_sm == 0) {
+            int v = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, scan_kernel<128, kTileRows, BATCH>, 128, *smem);
+            per_sm = std::max(1, v);
+        }
+        *grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm, tiles));
         *threads = 128;
     } else {
         *smem = scan_smem_bytes<kMaxRowsPerBlock>(aux, groups);
@@ -1400,6 +1437,126 @@ static void launch_scan_kernel(const ScanParams& P, uint32_t grid, uint32_t thre
         scan_kernel<256, kMaxRowsPerBlock, BATCH><<<grid, 256, smem, s>>>(P);
 }
 
+// One query of the shared form: fills `out` from the plan and its validated
+// descriptor, adding the plan's columns to `cols`.  Returns false (why = the
+// reason) when the plan does not qualify.
+static bool shared_query(const gx_scan_plan& pl, const QueryDesc& qd, std::vector<const gx_column*>& cols,
+                         ShQuery& out, std::string* why) {
+    std::memset(&out, 0, sizeof(ShQuery));
+    for (uint32_t k = 0; k < pl.n_steps; ++k) {
+        const bool is_value = (pl.steps[k].flags & GX_STEP_VALUE) != 0;
+        if (is_value != (k + 1 == pl.n_steps)) {
+            *why = "a plan whose only VALUE step is not its last step";
+            return false;
+        }
+        const gx_column* c = pl.steps[k].col;
+        if (c->codec == GX_CODEC_LZ4 && (c->S <= 1 || (1u << c->seg_shift) > kShTile)) {
+            *why = "an LZ4 column without segments of at most 2048 rows";
+            return false;
+        }
+        uint32_t ci = 0;
+        while (ci < cols.size() && cols[ci] != c) ++ci;
+        if (ci == cols.size()) {
+            if (cols.size() == kShMaxCols) {
+                *why = "more than 16 distinct columns";
+                return false;
+            }
+            cols.push_back(c);
+        }
+        const ScanStep& d = qd.steps[k];
+        ShStep& e = out.steps[k];
+        e.flags = d.flags;
+        e.lo = d.lo;
+        e.hi = d.hi;
+        e.col = ci;
+        e.ht = d.ht;
+        e.ht_log2 = d.ht_log2;
+        e.ht_layout = d.ht_layout;
+        e.digit_base = d.digit_base;
+        e.digit_card = d.digit_card;
+        out.col_mask |= 1u << ci;
+    }
+    out.n_steps = pl.n_steps;
+    out.agg = qd.agg;
+    out.grouped = qd.grouped;
+    out.row_lo = qd.row_lo;
+    out.row_hi = qd.row_hi;
+    out.result = qd.result;
+    out.g_keys = qd.g_keys;
+    out.g_sums = qd.g_sums;
+    out.g_log2 = qd.g_log2;
+    out.n_prune = qd.n_prune;
+    for (uint32_t p = 0; p < out.n_prune; ++p) out.prune[p] = qd.prune[p];
+    return true;
+}
+
+// Layout fields of the shared-form parameters for a table whose first column is c0.
+static void shared_layout(ShParams& P, const gx_column* c0) {
+    P.blocks_per_chunk = c0->blocks_per_chunk;
+    P.rows_per_chunk = c0->rows_per_chunk;
+    P.rows_per_block = c0->rows_per_block;
+    P.tile_rows = std::min<uint32_t>(kShTile, c0->rows_per_block);
+    P.tiles_per_block = (c0->rows_per_block + P.tile_rows - 1) / P.tile_rows;
+    P.dir = c0->d_blocks;
+    P.n_slots = c0->n_slots;
+}
+
+static size_t shared_smem_bytes(uint32_t n_cols, uint32_t n_queries) {
+    return 4ull * kShColWords * n_cols + Cfg<kTileRows>::kStage + 8ull * n_queries + 4ull * ((n_queries + 31) / 32);
+}
+
+// A plan that qualifies for the shared form (its only VALUE step last, LZ4
+// columns segmented) runs as a one-query shared scan: the query rides in the
+// kernel parameters, columns are decoded per 2048-row tile only when a step
+// needs them.  *done = false when the plan does not qualify.
+static gx_status scan_launch_shared(const gx_scan_plan* plan, const QueryDesc& qd, const gx_column* c0,
+                                    cudaStream_t s, unsigned long long* rows_dev, bool* done) {
+    *done = false;
+    std::vector<const gx_column*> cols;
+    std::string why;
+    ShParams P;
+    std::memset(&P, 0, sizeof(P));
+    if (!shared_query(*plan, qd, cols, P.q1, &why)) return GX_OK;
+    P.q1.keep_in = plan->keep_chunks_dev;
+    P.q1.keep_out = plan->keep_out_dev;
+    for (size_t i = 0; i < cols.size(); ++i) P.cols1[i] = cols[i]->view();
+    P.n_cols = (uint32_t)cols.size();
+    P.n_queries = 1;
+    P.mask_words = 1;
+    shared_layout(P, c0);
+    P.rows_scanned = rows_dev;
+    const uint32_t n_slots = c0->n_slots;
+    uint32_t* scratch = nullptr;
+    GX_CK(cudaMallocAsync(&scratch, 4ull * (2ull * n_slots + 2), s));
+    P.n_items = scratch;
+    P.work_counter = scratch + 1;
+    P.items = scratch + 2;
+    P.slot_mask = scratch + 2 + n_slots;
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 8, s);
+    if (e == cudaSuccess) {
+        const unsigned ig = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(8ull * sm_count(), (n_slots + 7) / 8));
+        shared_items_kernel<<<ig, 256, 0, s>>>(P, scratch + 2 + n_slots, scratch + 2, scratch);
+        const size_t smem = shared_smem_bytes(P.n_cols, 1);
+        static int occ[64][kShMaxCols + 1] = {};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        int& per_sm = occ[dev & 63][P.n_cols];
+        if (per_sm == 0) {
+            int v = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, shared_scan_kernel<kShNT, 2>, kShNT, smem);
+            per_sm = std::max(1, v);
+        }
+        const uint64_t tiles = (uint64_t)n_slots * P.tiles_per_block;
+        const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm, tiles));
+        shared_scan_kernel<kShNT, 2><<<grid, kShNT, smem, s>>>(P);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(scratch, s);
+    if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "shared scan launch: %s", cudaGetErrorString(e));
+    *done = true;
+    return GX_OK;
+}
+
 static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned long long* rows_dev) {
     ScanParams P;
     std::memset(&P, 0, sizeof(P));
@@ -1409,6 +1566,9 @@ static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned 
     if (st) return st;
     st = ensure_kernel_attrs();
     if (st) return st;
+    bool done = false;
+    st = scan_launch_shared(plan, P.q, c0, s, rows_dev, &done);
+    if (st || done) return st;
     ItemsParams ip{};
     for (uint32_t i = 0; i < P.q.n_prune; ++i) ip.preds[i] = P.q.prune[i];
     ip.n_preds = P.q.n_prune;
@@ -1577,56 +1737,8 @@ static gx_status shared_prepare(gx_batch* b, const gx_query* queries, uint32_t n
     }
     std::vector<const gx_column*> cols;
     std::vector<ShQuery> sq(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        const gx_scan_plan& pl = queries[i].plan;
-        std::memset(&sq[i], 0, sizeof(ShQuery));
-        for (uint32_t k = 0; k < pl.n_steps; ++k) {
-            const bool is_value = (pl.steps[k].flags & GX_STEP_VALUE) != 0;
-            if (is_value != (k + 1 == pl.n_steps)) {
-                *why = "a plan whose only VALUE step is not its last step";
-                return GX_OK;
-            }
-            const gx_column* c = pl.steps[k].col;
-            if (c->codec == GX_CODEC_LZ4 && (c->S <= 1 || (1u << c->seg_shift) > kShTile)) {
-                *why = "an LZ4 column without segments of at most 2048 rows";
-                return GX_OK;
-            }
-            uint32_t ci = 0;
-            while (ci < cols.size() && cols[ci] != c) ++ci;
-            if (ci == cols.size()) {
-                if (cols.size() == kShMaxCols) {
-                    *why = "more than 16 distinct columns";
-                    return GX_OK;
-                }
-                cols.push_back(c);
-            }
-            const ScanStep& d = qs[i].steps[k];
-            ShStep& e = sq[i].steps[k];
-            e.flags = d.flags;
-            e.lo = d.lo;
-            e.hi = d.hi;
-            e.col = ci;
-            e.ht = d.ht;
-            e.ht_log2 = d.ht_log2;
-            e.ht_layout = d.ht_layout;
-            e.digit_base = d.digit_base;
-            e.digit_card = d.digit_card;
-            sq[i].col_mask |= 1u << ci;
-        }
-        ShQuery& Q = sq[i];
-        Q.n_steps = pl.n_steps;
-        Q.agg = qs[i].agg;
-        Q.grouped = qs[i].grouped;
-        Q.row_lo = qs[i].row_lo;
-        Q.row_hi = qs[i].row_hi;
-        Q.result = qs[i].result;
-        Q.g_keys = qs[i].g_keys;
-        Q.g_sums = qs[i].g_sums;
-        Q.g_log2 = qs[i].g_log2;
-        Q.n_prune = qs[i].n_prune;
-        for (uint32_t p = 0; p < Q.n_prune; ++p) Q.prune[p] = qs[i].prune[p];
-        Q.keep_in = nullptr;
-    }
+    for (uint32_t i = 0; i < n; ++i)
+        if (!shared_query(queries[i].plan, qs[i], cols, sq[i], why)) return GX_OK;
     const uint32_t mw = (n + 31) / 32;
     const uint32_t n_slots = c0->n_slots;
     // grow buffers (the stream's earlier work is finished by the caller)
@@ -1673,19 +1785,12 @@ static gx_status shared_prepare(gx_batch* b, const gx_query* queries, uint32_t n
     P.n_items = b->d_sh_items;
     P.work_counter = b->d_sh_items + 1;
     P.items = b->d_sh_items + 2;
-    P.blocks_per_chunk = c0->blocks_per_chunk;
-    P.rows_per_chunk = c0->rows_per_chunk;
-    P.rows_per_block = c0->rows_per_block;
-    P.tile_rows = std::min<uint32_t>(kShTile, c0->rows_per_block);
-    P.tiles_per_block = (c0->rows_per_block + P.tile_rows - 1) / P.tile_rows;
+    shared_layout(P, c0);
     P.rows_scanned = b->d_rows;
     b->n_slots = n_slots;
     b->dir0 = c0->d_blocks;
-    b->sh_smem = 4ull * kShColWords * P.n_cols + Cfg<kTileRows>::kStage + 8ull * n + 4ull * mw;
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shared_scan_kernel, kShNT, b->sh_smem);
-    const uint64_t tiles = (uint64_t)n_slots * P.tiles_per_block;
-    b->sh_grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * std::max(1, per_sm), tiles));
+    b->sh_smem = shared_smem_bytes(P.n_cols, n);
+    shared_geometry(b);
     b->sh_items_grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(8ull * sm_count(), (n_slots + 7) / 8));
     *ok = true;
     return GX_OK;
@@ -1808,6 +1913,23 @@ gx_status gx_batch_create(const gx_query* queries, uint32_t n_queries, gx_batch*
     return gx_batch_create2(queries, n_queries, GX_BATCH_AUTO, out);
 }
 
+gx_status gx_batch_set_launch(gx_batch* b, uint32_t threads, uint32_t ctas_per_sm) {
+    if (!b || (threads != 128 && threads != 256 && threads != 512 && threads != 1024))
+        return set_error(GX_ERR_INVALID, "gx_batch_set_launch: threads must be 128, 256, 512 or 1024");
+    b->sh_threads = threads;
+    b->sh_ctas_per_sm = ctas_per_sm;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    if (b->graph) {
+        cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    if (b->mode == GX_BATCH_SHARED) shared_geometry(b);
+    return GX_OK;
+}
+
 gx_status gx_batch_mode(const gx_batch* b, uint32_t* mode) {
     if (!b || !mode) return set_error(GX_ERR_INVALID, "gx_batch_mode: bad args");
     *mode = b->mode;
@@ -1860,11 +1982,9 @@ gx_status gx_batch_run(gx_batch* b, void* stream) {
     batch_reset_kernel<<<dim3(b->reset_x, b->n), 256, 0, s>>>(b->d_qs, b->d_rows);
     if (b->mode == GX_BATCH_SHARED) {
         GX_CK(cudaMemsetAsync(b->d_sh_items, 0, 8, s));
-        shared_items_kernel<<<b->sh_items_grid, 256, 0, s>>>(b->dir0, b->n_slots, b->d_sq, b->n, b->SP.mask_words,
-                                                               b->SP.blocks_per_chunk, b->SP.rows_per_chunk,
-                                                               b->SP.rows_per_block, b->d_slot_mask,
-                                                               b->d_sh_items + 2, b->d_sh_items);
-        shared_scan_kernel<<<b->sh_grid, kShNT, b->sh_smem, s>>>(b->SP);
+        shared_items_kernel<<<b->sh_items_grid, 256, 0, s>>>(b->SP, b->d_slot_mask, b->d_sh_items + 2,
+                                                               b->d_sh_items);
+        launch_shared_kernel(b, s);
         GX_CK(cudaGetLastError());
         return GX_OK;
     }

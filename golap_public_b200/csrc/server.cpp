@@ -114,8 +114,12 @@ void gx_server::run() {
             stats.queries_in_batches += qs.size();
             lk.unlock();
             gx_status st = GX_OK;
-            if (!sl.b) st = gx_batch_create(qs.data(), (uint32_t)qs.size(), &sl.b);
-            else st = gx_batch_assign(sl.b, qs.data(), (uint32_t)qs.size(), sl.s);
+            if (!sl.b) {
+                st = gx_batch_create2(qs.data(), (uint32_t)qs.size(), opts.batch_mode, &sl.b);
+                if (!st && opts.batch_threads) st = gx_batch_set_launch(sl.b, opts.batch_threads, 0);
+            } else {
+                st = gx_batch_assign(sl.b, qs.data(), (uint32_t)qs.size(), sl.s);
+            }
             if (!st) st = gx_batch_run(sl.b, sl.s);
             if (!st && cudaEventRecord(sl.ev, sl.s) != cudaSuccess) st = GX_ERR_CUDA;
             lk.lock();
@@ -152,11 +156,16 @@ gx_status gx_server_opts_default(gx_server_opts* o) {
     o->max_inflight = 4;
     o->max_batch = 64;
     o->hbm_budget = 120ull << 30;
+    o->batch_threads = 0;
+    o->batch_mode = GX_BATCH_AUTO;
     return GX_OK;
 }
 
 gx_status gx_server_create(const gx_server_opts* opts, gx_server** out) {
-    if (!opts || !out || opts->max_inflight == 0 || opts->max_batch == 0 || opts->max_inflight > 64)
+    if (!opts || !out || opts->max_inflight == 0 || opts->max_batch == 0 || opts->max_inflight > 64 ||
+        opts->batch_mode > GX_BATCH_SHARED ||
+        (opts->batch_threads && opts->batch_threads != 128 && opts->batch_threads != 256 &&
+         opts->batch_threads != 512 && opts->batch_threads != 1024))
         return gx::set_error(GX_ERR_INVALID, "gx_server_create: bad options");
     gx_server* sv = new gx_server();
     sv->opts = *opts;

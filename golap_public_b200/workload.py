@@ -45,40 +45,67 @@ class WideTable:
     data: dict                      # host columns (kept for checking)
     cols: dict                      # name -> Column (device)
     dims: dict                      # customer / supplier / date dicts
-    ht_date: HashMap = None
-    ht_cust: list = field(default_factory=list)  # per region
-    ht_supp: list = field(default_factory=list)
+    rows_per_chunk: int = 1_000_000
+    ht: dict = field(default_factory=dict)  # layout -> {"date": HashMap, "cust": [5], "supp": [5]}
     _keep: list = field(default_factory=list)
 
+    @property
+    def ht_date(self) -> HashMap:
+        return self.ht["linear"]["date"]
 
-def build_table(n_rows: int, seed: int = datagen.SEED, n_customer: int = 3_000_000, n_supplier: int = 200_000,
-                lz4_segments: int = 128, residency: str = "hbm", threads: int = 0) -> WideTable:
+    @property
+    def ht_cust(self) -> list:
+        return self.ht["linear"]["cust"]
+
+    @property
+    def ht_supp(self) -> list:
+        return self.ht["linear"]["supp"]
+
+
+def generate(n_rows: int, seed: int = datagen.SEED, n_customer: int = 3_000_000, n_supplier: int = 200_000) -> dict:
+    """Host columns of the wide fact table (seeded)."""
     f1 = datagen.fact_q1(n_rows, True, seed=seed)
     f3 = datagen.fact_q3(n_rows, True, seed=seed, n_customer=n_customer, n_supplier=n_supplier)
-    data = {"date_key": f1["date_key"], "discount": f1["discount"], "quantity": f1["quantity"],
+    return {"date_key": f1["date_key"], "discount": f1["discount"], "quantity": f1["quantity"],
             "extended_price": f1["extended_price"], "cust_key": f3["cust_key"], "supp_key": f3["supp_key"],
             "revenue": f3["revenue"],
             "part_key": datagen.zipf_keys(n_rows, PART_KEYS, 1.1, seed=seed)}
+
+
+def build_table(n_rows: int, seed: int = datagen.SEED, n_customer: int = 3_000_000, n_supplier: int = 200_000,
+                lz4_segments: int = 128, residency: str = "hbm", threads: int = 0, rows_per_chunk: int = 1_000_000,
+                ht_layouts=("linear",), data: dict | None = None) -> WideTable:
+    """Encode and load the wide table; join tables are built once per layout
+    in ht_layouts ("linear" is always built).  `data` reuses host columns
+    from generate() (same n_rows, seed and dimension sizes)."""
+    if data is None:
+        data = generate(n_rows, seed, n_customer, n_supplier)
     cols = {}
     for name, v in data.items():
-        c = Column(v, "cascaded" if name == "date_key" else "lz4", lz4_segments=lz4_segments, threads=threads,
-                   name=name)
+        c = Column(v, "cascaded" if name == "date_key" else "lz4", rows_per_chunk, lz4_segments=lz4_segments,
+                   threads=threads, name=name)
         if residency:
             c.to_device(residency)
         cols[name] = c
     dims = {"customer": datagen.dim_geo(n_customer, seed, 21), "supplier": datagen.dim_geo(n_supplier, seed, 22),
             "date": datagen.date_dim()}
-    t = WideTable(n_rows, data, cols, dims)
+    t = WideTable(n_rows, data, cols, dims, rows_per_chunk)
     dd = dims["date"]
     dk, dy = _dev(dd["d_key"]), _dev(dd["d_year"])
-    t.ht_date = HashMap(len(dd["d_key"])).build(dk, dy)
     t._keep += [dk, dy]
-    for name, lst in (("customer", t.ht_cust), ("supplier", t.ht_supp)):
+    dev = {}
+    for name in ("customer", "supplier"):
         d = dims[name]
-        k, nat, reg = _dev(d["key"]), _dev(d["nation"]), _dev(d["region"])
-        t._keep += [k, nat, reg]
-        for r in range(5):
-            lst.append(HashMap(max(1, int((d["region"] == r).sum()))).build(k, nat, preds=[(reg, r, r)]))
+        dev[name] = (_dev(d["key"]), _dev(d["nation"]), _dev(d["region"]))
+        t._keep += list(dev[name])
+    for layout in dict.fromkeys(("linear",) + tuple(ht_layouts)):
+        hts = {"date": HashMap(len(dd["d_key"]), layout).build(dk, dy), "cust": [], "supp": []}
+        for name, key in (("customer", "cust"), ("supplier", "supp")):
+            k, nat, reg = dev[name]
+            for r in range(5):
+                n_r = max(1, int((dims[name]["region"] == r).sum()))
+                hts[key].append(HashMap(n_r, layout).build(k, nat, preds=[(reg, r, r)]))
+        t.ht[layout] = hts
     return t
 
 
@@ -99,10 +126,11 @@ def _month_range(rng):
     return y * 10000 + m * 100 + 1, y * 10000 + m * 100 + 31
 
 
-def make_query(t: WideTable, template: str, rng, row_lo: int, row_hi: int) -> QuerySpec:
+def make_query(t: WideTable, template: str, rng, row_lo: int, row_hi: int, ht_layout: str = "linear") -> QuerySpec:
     import torch
 
     c = t.cols
+    hts = t.ht[ht_layout]
     if template == "scan":
         if rng.random() < 0.5:
             dlo, dhi = _month_range(rng)
@@ -115,7 +143,7 @@ def make_query(t: WideTable, template: str, rng, row_lo: int, row_hi: int) -> Qu
         spec.result = torch.zeros(1, dtype=torch.int64, device="cuda")
         p = ScanPlan(agg=L.GX_AGG_SUM_PRODUCT, result=spec.result)
         p.prune_minmax(c["date_key"], dlo, dhi)
-        p.steps.append(_step(c["date_key"], L.GX_STEP_FILTER | L.GX_STEP_PROBE, dlo, dhi, t.ht_date))
+        p.steps.append(_step(c["date_key"], L.GX_STEP_FILTER | L.GX_STEP_PROBE, dlo, dhi, hts["date"]))
         p.filter(c["discount"], d0, d0 + 2, carry=True).filter(c["quantity"], q0, q0 + 9).value(c["extended_price"])
     elif template == "star":
         r = int(rng.integers(0, 5))
@@ -125,9 +153,9 @@ def make_query(t: WideTable, template: str, rng, row_lo: int, row_hi: int) -> Qu
         spec.groups = HashAggregate(N_NATIONS * N_NATIONS * (y2 - y1 + 1))
         p = ScanPlan(agg=L.GX_AGG_SUM, groupby=spec.groups)
         p.prune_minmax(c["date_key"], y1 * 10000 + 101, y2 * 10000 + 1231)
-        p.probe(c["cust_key"], t.ht_cust[r], 0, N_NATIONS).probe(c["supp_key"], t.ht_supp[r], 0, N_NATIONS)
+        p.probe(c["cust_key"], hts["cust"][r], 0, N_NATIONS).probe(c["supp_key"], hts["supp"][r], 0, N_NATIONS)
         p.steps.append(_step(c["date_key"], L.GX_STEP_FILTER | L.GX_STEP_PROBE, y1 * 10000 + 101, y2 * 10000 + 1231,
-                             t.ht_date, y1, y2 - y1 + 1))
+                             hts["date"], y1, y2 - y1 + 1))
         p.value(c["revenue"])
     elif template == "highcard":
         y1 = int(rng.integers(YEARS[0], YEARS[1] + 1))
@@ -151,7 +179,8 @@ def _step(col, flags, lo, hi, ht, digit_base=0, digit_card=0):
 
 
 def random_queries(t: WideTable, n: int, rng, min_rows: int = 1_000_000, max_rows: int = 100_000_000,
-                   mix=(("scan", 0.6), ("star", 0.3), ("highcard", 0.1))) -> list:
+                   mix=(("scan", 0.6), ("star", 0.3), ("highcard", 0.1)), ht_layout=None) -> list:
+    """ht_layout: None (linear), a layout name, or {template: layout}."""
     """n queries; slice sizes log-uniform in [min_rows, max_rows] (clamped to the table)."""
     names = [m[0] for m in mix]
     probs = np.array([m[1] for m in mix], dtype=np.float64)
@@ -162,7 +191,9 @@ def random_queries(t: WideTable, n: int, rng, min_rows: int = 1_000_000, max_row
     for _ in range(n):
         size = int(round(math.exp(rng.uniform(math.log(lo_cap), math.log(hi_cap)))))
         start = int(rng.integers(0, t.n_rows - size + 1))
-        out.append(make_query(t, str(rng.choice(names, p=probs)), rng, start, start + size))
+        tpl = str(rng.choice(names, p=probs))
+        lay = (ht_layout.get(tpl, "linear") if isinstance(ht_layout, dict) else ht_layout) or "linear"
+        out.append(make_query(t, tpl, rng, start, start + size, lay))
     return out
 
 

@@ -68,7 +68,8 @@ typedef struct gx_encode_opts {
     uint32_t rows_per_block;   /* default 16,384 (64 KiB of int32)                       */
     uint32_t lz4_segments;     /* independent decode segments per LZ4 block (1..128);
                                   1 = plain LZ4 (one serial stream per block)             */
-    uint32_t lz4_min_match;    /* minimum match length in bytes (multiple of 4, >= 4)    */
+    uint32_t lz4_min_match;    /* minimum match bytes (multiple of 4, >= 4), or 0: per
+                                  block the cheapest of 4/8/16 by bytes + 24 x sequences */
     uint32_t lz4_search_depth; /* hash-chain candidates examined per position            */
     uint32_t casc_rle;         /* cascaded: allow run-length encoding                    */
     uint32_t casc_delta;       /* cascaded: allow delta encoding                         */
@@ -327,6 +328,10 @@ enum { GX_BATCH_AUTO = 0, GX_BATCH_QUEUE = 1, GX_BATCH_SHARED = 2 };
 gx_status gx_batch_create2(const gx_query* queries, uint32_t n_queries, uint32_t mode, gx_batch** out);
 /* The form the batch currently runs in (GX_BATCH_QUEUE or GX_BATCH_SHARED). */
 gx_status gx_batch_mode(const gx_batch* b, uint32_t* mode);
+/* Launch shape of the shared form: threads per CTA (128, 256, 512 or 1024;
+ * default 256) and a cap on CTAs per SM (0 = as many as fit).  Kept across
+ * gx_batch_assign; drops a captured graph.  The autotuner sets it. */
+gx_status gx_batch_set_launch(gx_batch* b, uint32_t threads, uint32_t ctas_per_sm);
 /* Replace the batch's queries (buffers reused, grown when needed; the
  * descriptor upload is enqueued on `stream`).  Drops a captured graph. */
 gx_status gx_batch_assign(gx_batch* b, const gx_query* queries, uint32_t n_queries, void* stream);
@@ -352,6 +357,8 @@ typedef struct gx_server_opts {
     uint32_t max_inflight;  /* batches on the device at once (default 4)       */
     uint32_t max_batch;     /* requests per batch (default 64)                 */
     uint64_t hbm_budget;    /* bytes admitted requests may hold (default 120 GiB) */
+    uint32_t batch_threads; /* launch shape of shared-form batches (0 = default) */
+    uint32_t batch_mode;    /* GX_BATCH_AUTO / QUEUE / SHARED (default AUTO)   */
 } gx_server_opts;
 typedef struct gx_server_stats {
     uint64_t submitted, completed, rejected, batches, queries_in_batches;
