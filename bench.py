@@ -316,7 +316,7 @@ def gpu_arm(args, rank, world):
         "vs_baseline": None,
         "dtype": "int32",
         "data": "synthetic (seeded, configs[1] shapes and distributions)",
-        "config": {"workload": WORKLOAD, "rows": N_ROWS, "chunks": 60, "chunks_scanned": kept,
+        "config": {"workload": WORKLOAD, "rows": N_ROWS, "chunks": N_ROWS // ROWS_PER_CHUNK, "chunks_scanned": kept,
                    "lz4_segments": args.segments, "residency": "hbm", "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas x{world}", "comp_bytes": comp},
         "result": got,
@@ -525,6 +525,7 @@ def cpu_baseline(f, dd, steps=3, warmup=1, threads=None):
 
 
 def main():
+    global N_ROWS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -537,9 +538,13 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched and serving sections")
     ap.add_argument("--batch-rows", type=int, default=100_000_000)
     ap.add_argument("--no-tune", action="store_true", help="batched/serving with the default launch shape")
+    ap.add_argument("--rows", type=int, default=N_ROWS,
+                    help="fact rows of the Q1 workload (default: the measured 60M-row configuration; smaller "
+                         "values are for profiler captures)")
     ap.add_argument("--tune-rows", type=int, default=20_000_000)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    N_ROWS = args.rows
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
 
@@ -554,7 +559,7 @@ def main():
             "value": cb["value"], "unit": "rows/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": cb["ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded, configs[1] shapes and distributions)",
-            "config": {"workload": WORKLOAD, "rows": N_ROWS, "chunks": 60},
+            "config": {"workload": WORKLOAD, "rows": N_ROWS, "chunks": N_ROWS // ROWS_PER_CHUNK},
             "result": cb["result"],
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -169,7 +169,8 @@ __device__ __forceinline__ int stage_bytes(const gx_dcol& c, const uint8_t* src,
 template <int NT, int MAXT>
 __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint32_t rows, uint32_t r0, uint32_t n,
                                            uint32_t* buf, uint8_t* stage, uint64_t* mbar, uint32_t& phase,
-                                           uint32_t* tmp, CascTile* ct, int* s_err, uint32_t& pad_log2) {
+                                           uint32_t* tmp, CascTile* ct, int* s_err, uint32_t& pad_log2,
+                                           uint32_t* seg_smem) {
     using C = Cfg<MAXT>;
     const uint32_t tid = threadIdx.x;
     const gx_dblock d = c.blocks[slot];
@@ -204,11 +205,17 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
             seg_rows = 1u << c.seg_shift;
             j0 = r0 >> c.seg_shift;
             nseg = (n + seg_rows - 1) >> c.seg_shift;
-            const uint32_t jn = j0 + nseg;
+            // the tile's nseg + 1 segment entries into shared memory (one parallel load)
             const uint32_t* e = c.seg + (size_t)2 * c.S * slot;
-            lo = __ldg(e + 2 * j0);
-            hi = jn < c.S ? __ldg(e + 2 * jn) : d.comp_bytes;
-            if ((r0 & (seg_rows - 1)) || j0 + nseg > c.S || lo > hi || hi > d.comp_bytes) {
+            for (uint32_t t = tid; t <= nseg && t <= kMaxSegments; t += NT) {
+                const uint32_t j = j0 + t;
+                seg_smem[2 * t] = j < c.S ? __ldg(e + 2 * j) : d.comp_bytes;
+                seg_smem[2 * t + 1] = j < c.S ? __ldg(e + 2 * j + 1) : 0u;
+            }
+            __syncthreads();
+            lo = seg_smem[0];
+            hi = nseg <= kMaxSegments ? seg_smem[2 * nseg] : 0u;
+            if ((r0 & (seg_rows - 1)) || j0 + nseg > c.S || nseg > kMaxSegments || lo > hi || hi > d.comp_bytes) {
                 if (tid == 0) *s_err = kErrCorrupt;
                 __syncthreads();
                 return -1;
@@ -231,7 +238,6 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
         if (rc) return -1;
         if (c.S > 1) {
             // a group of G adjacent lanes per segment; segment t at buf + t * (seg_rows + G)
-            const uint32_t* e = c.seg + (size_t)2 * c.S * slot;
             // lanes per segment: a whole warp when the tile is mostly literals
             // (few sequences; conflict-free 32-word copies), else spread the
             // segments over all NT threads
@@ -245,8 +251,8 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
             for (uint32_t t = tid >> glog; t < nseg; t += (NT >> glog)) {
                 const uint32_t j = j0 + t;
                 const uint32_t K = min(seg_rows, rows - j * seg_rows);
-                const int r2 = lz4_seg_group((const uint32_t*)stage, wbase, lo, hi, d.comp_bytes, __ldg(e + 2 * j),
-                                             __ldg(e + 2 * j + 1), K, buf + t * (seg_rows + (1u << pl)), gl, G, gmask);
+                const int r2 = lz4_seg_group((const uint32_t*)stage, wbase, lo, hi, d.comp_bytes, seg_smem[2 * t],
+                                             seg_smem[2 * t + 1], K, buf + t * (seg_rows + (1u << pl)), gl, G, gmask);
                 if (r2 && gl == 0) *s_err = r2;
             }
             pad_log2 = pl;
@@ -332,6 +338,7 @@ __global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const 
     __shared__ uint32_t s_tmp[NW + 1];
     __shared__ unsigned long long s_red[NW];
     __shared__ CascTile s_ct;
+    __shared__ uint32_t s_seg[2 * (kMaxSegments + 1)];
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (P.smem_groups) {
@@ -399,7 +406,7 @@ __global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const 
             const ScanStep& st = Q.steps[si];
             uint32_t pad_log2 = 0;
             int layout = decode_tile<NT, MAXT>(st.col, slot, rows, r0, n, buf, stage, &s_mbar, phase, s_tmp, &s_ct,
-                                               &s_err, pad_log2);
+                                               &s_err, pad_log2, s_seg);
             const int derr = s_err;
             __syncthreads();  // every thread has read s_err before it is reset
             if (derr) {       // corrupt block: drop the tile, remember the error
@@ -635,6 +642,7 @@ __global__ void __launch_bounds__(NT) decompress_kernel(const __grid_constant__ 
     __shared__ int s_err;
     __shared__ uint32_t s_tmp[NT / 32 + 1];
     __shared__ CascTile s_ct;
+    __shared__ uint32_t s_seg[2 * (kMaxSegments + 1)];
     const uint32_t slot = slot0 + blockIdx.x / tpb;
     const uint32_t r0 = (blockIdx.x % tpb) * tile_rows;
     const gx_dblock d = c.blocks[slot];
@@ -647,7 +655,7 @@ __global__ void __launch_bounds__(NT) decompress_kernel(const __grid_constant__ 
     __syncthreads();
     uint32_t phase = 0, pad_log2 = 0;
     int layout = decode_tile<NT, MAXT>(c, slot, d.n_rows, r0, n, buf, stage, &s_mbar, phase, s_tmp, &s_ct, &s_err,
-                                       pad_log2);
+                                       pad_log2, s_seg);
     if (s_err) {
         if (threadIdx.x == 0) raise_error(s_err);
         return;
@@ -1399,6 +1407,7 @@ static gx_status ensure_kernel_attrs() {
     if (!st) st = allow_smem(shared_scan_kernel<256, 2>, sh_max);
     if (!st) st = allow_smem(shared_scan_kernel<512, 1>, sh_max);
     if (!st) st = allow_smem(shared_scan_kernel<1024, 1>, sh_max);
+    if (!st) st = allow_smem(shared_scan_kernel<kShNT, 2, true>, sh_max);
     if (st) return st;
     attr_set[dev & 63] = true;
     return GX_OK;
@@ -1543,12 +1552,12 @@ static gx_status scan_launch_shared(const gx_scan_plan* plan, const QueryDesc& q
         int& per_sm = occ[dev & 63][P.n_cols];
         if (per_sm == 0) {
             int v = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, shared_scan_kernel<kShNT, 2>, kShNT, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, shared_scan_kernel<kShNT, 2, true>, kShNT, smem);
             per_sm = std::max(1, v);
         }
         const uint64_t tiles = (uint64_t)n_slots * P.tiles_per_block;
         const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm, tiles));
-        shared_scan_kernel<kShNT, 2><<<grid, kShNT, smem, s>>>(P);
+        shared_scan_kernel<kShNT, 2, true><<<grid, kShNT, smem, s>>>(P);
         e = cudaGetLastError();
     }
     cudaFreeAsync(scratch, s);

@@ -68,7 +68,19 @@ struct ShParams {
 };
 
 __device__ __forceinline__ const ShQuery* sh_queries(const ShParams& P) { return P.qs ? P.qs : &P.q1; }
-__device__ __forceinline__ const gx_dcol* sh_cols(const ShParams& P) { return P.cols ? P.cols : P.cols1; }
+
+// Query q and column c: in the parameters themselves for a one-query launch
+// (SINGLE: constant-bank reads), else in global memory.
+template <bool SINGLE>
+__device__ __forceinline__ const ShQuery& sh_q(const ShParams& P, uint32_t q) {
+    if constexpr (SINGLE) return P.q1;
+    else return P.qs[q];
+}
+template <bool SINGLE>
+__device__ __forceinline__ const gx_dcol& sh_c(const ShParams& P, uint32_t c) {
+    if constexpr (SINGLE) return P.cols1[c];
+    else return P.cols[c];
+}
 
 // One warp per block slot: lane l tests query 32*w + l of mask word w; the
 // word is the warp ballot.  Slots with any query set are appended to items.
@@ -121,11 +133,12 @@ template <int NT>
 __device__ __forceinline__ int shared_decode(const gx_dcol& col, uint32_t c, uint32_t slot, uint32_t rows,
                                              uint32_t r0, uint32_t n, uint32_t* colbuf, uint8_t* stage,
                                              uint64_t* mbar, uint32_t& phase, uint32_t* s_tmp, CascTile* s_ct,
-                                             int* s_err, int* s_fatal, uint32_t* s_sh, uint32_t* s_pd) {
+                                             int* s_err, int* s_fatal, uint32_t* s_sh, uint32_t* s_pd,
+                                             uint32_t* s_seg) {
     uint32_t* buf = colbuf + c * kShColWords;
     uint32_t pad_log2 = 0;
     int layout = decode_tile<NT, kTileRows>(col, slot, rows, r0, n, buf, stage, mbar, phase, s_tmp, s_ct, s_err,
-                                            pad_log2);
+                                            pad_log2, s_seg);
     const int derr = *s_err;
     __syncthreads();
     if (derr) {
@@ -159,7 +172,7 @@ __device__ __forceinline__ int shared_decode(const gx_dcol& col, uint32_t c, uin
 // only the columns their first steps read.
 // Dynamic shared memory: n_cols column buffers | stage | per-query partial
 // sums | per-tile active-query mask.
-template <int NT, int MINB>
+template <int NT, int MINB, bool SINGLE = false>
 __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_constant__ ShParams P) {
     constexpr int NW = NT / 32;
     constexpr int RPT = (kShTile + NT - 1) / NT;  // row groups per warp
@@ -169,8 +182,6 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
     uint8_t* stage = (uint8_t*)(colbuf + (size_t)P.n_cols * kShColWords);
     unsigned long long* s_part = (unsigned long long*)(stage + C::kStage);
     uint32_t* s_qmask = (uint32_t*)(s_part + P.n_queries);
-    const ShQuery* qs = sh_queries(P);
-    const gx_dcol* cols = sh_cols(P);
 
     __shared__ __align__(8) uint64_t s_mbar;
     __shared__ uint32_t s_item;
@@ -179,6 +190,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
     __shared__ uint32_t s_sh[kShMaxCols], s_pd[kShMaxCols];
     __shared__ uint32_t s_tmp[NW + 1];
     __shared__ CascTile s_ct;
+    __shared__ uint32_t s_seg[2 * (kMaxSegments + 1)];
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (uint32_t i = tid; i < P.n_queries; i += NT) s_part[i] = 0;
@@ -192,20 +204,19 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
     const uint32_t tpb = P.tiles_per_block, tile_rows = P.tile_rows;
     const uint32_t total = *P.n_items * tpb;
     const uint32_t MW = P.mask_words;
+    if (tid == 0) s_item = atomicAdd(P.work_counter, 1u);
     __syncthreads();
 
     while (true) {
-        if (tid == 0) s_item = s_fatal ? 0xFFFFFFFFu : atomicAdd(P.work_counter, 1u);
-        __syncthreads();
         const uint32_t it = s_item;
         if (it >= total) break;
+        // thread 0 takes the next work item now; its result is needed only at the tile's end
+        uint32_t next_it = 0xFFFFFFFFu;
+        if (tid == 0) next_it = atomicAdd(P.work_counter, 1u);
         const uint32_t slot = P.items[it / tpb];
         const uint32_t r0 = (it % tpb) * tile_rows;
         const uint32_t rows = P.dir[slot].n_rows;
-        if (r0 >= rows) {
-            __syncthreads();
-            continue;
-        }
+        if (r0 < rows) {
         const uint32_t n = min(tile_rows, rows - r0);
         const uint32_t chunk = slot / P.blocks_per_chunk, j = slot % P.blocks_per_chunk;
         const uint64_t g0 = (uint64_t)chunk * P.rows_per_chunk + (uint64_t)j * P.rows_per_block + r0;
@@ -215,7 +226,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
             while (m) {
                 const uint32_t bit = __ffs(m) - 1;
                 m &= m - 1;
-                const ShQuery& Q = qs[w * 32 + bit];
+                const ShQuery& Q = sh_q<SINGLE>(P, w * 32 + bit);
                 if (!(Q.row_lo < g0 + n && Q.row_hi > g0)) keepm &= ~(1u << bit);
             }
             s_qmask[w] = keepm;
@@ -228,7 +239,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
             while (m && !dropped) {
                 const uint32_t q = w * 32 + (__ffs(m) - 1);
                 m &= m - 1;
-                const ShQuery& Q = qs[q];
+                const ShQuery& Q = sh_q<SINGLE>(P, q);
                 const uint32_t a = Q.row_lo > g0 ? (uint32_t)(Q.row_lo - g0) : 0u;
                 const uint32_t b = Q.row_hi < g0 + n ? (uint32_t)(Q.row_hi - g0) : n;
                 if (tid == 0) local_rows += b - a;
@@ -251,8 +262,8 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                     if (!((decoded >> c) & 1u)) {
                         // the query's rows are all dead: skip its remaining steps (and this decode)
                         if (s > 0 && !__syncthreads_or(keep != 0)) break;
-                        if (shared_decode<NT>(cols[c], c, slot, rows, r0, n, colbuf, stage, &s_mbar, phase, s_tmp,
-                                              &s_ct, &s_err, &s_fatal, s_sh, s_pd)) {
+                        if (shared_decode<NT>(sh_c<SINGLE>(P, c), c, slot, rows, r0, n, colbuf, stage, &s_mbar,
+                                              phase, s_tmp, &s_ct, &s_err, &s_fatal, s_sh, s_pd, s_seg)) {
                             dropped = true;
                             break;
                         }
@@ -264,6 +275,10 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                     const uint32_t* const col = colbuf + c * kShColWords;
                     const uint32_t sh = s_sh[c], pd = s_pd[c];
                     const bool last = s + 1 == ns;
+                    // one-entry probe memo: a thread's rows are NT apart, so on sorted
+                    // or run-length columns they mostly repeat the previous key
+                    int32_t mv = kEmptyKey, mp = 0;
+                    bool mk = false;
 #pragma unroll
                     for (int i = 0; i < RPT; ++i) {
                         const uint32_t r = (i * NW + warp) * 32 + lane;
@@ -273,7 +288,15 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                             v = (int32_t)col[sh_col_index(r, sh, pd)];
                             if (flags & GX_STEP_FILTER) k = v >= lo && v <= hi;
                             int32_t p = v;
-                            if ((flags & GX_STEP_PROBE) && k) k = ht_probe_any(ht, htlog, htlay, v, &p);
+                            if ((flags & GX_STEP_PROBE) && k) {
+                                if (v != mv) {
+                                    mp = v;
+                                    mk = ht_probe_any(ht, htlog, htlay, v, &mp);
+                                    mv = v;
+                                }
+                                k = mk;
+                                p = mp;
+                            }
                             if (dcard && k) {
                                 const uint32_t dgt = (uint32_t)(p - dbase);
                                 if (dgt >= dcard) {
@@ -318,12 +341,16 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                 }
             }
         }
+        }  // r0 < rows
+        __syncthreads();
+        if (tid == 0) s_item = s_fatal ? 0xFFFFFFFFu : next_it;
         __syncthreads();
     }
     __syncthreads();
     for (uint32_t q = tid; q < P.n_queries; q += NT) {
         const unsigned long long v = s_part[q];
-        if (v && qs[q].result) atomicAdd((unsigned long long*)qs[q].result, v);
+        const ShQuery& Q = sh_q<SINGLE>(P, q);
+        if (v && Q.result) atomicAdd((unsigned long long*)Q.result, v);
     }
     if (tid == 0 && P.rows_scanned && local_rows) atomicAdd(P.rows_scanned, local_rows);
 }
