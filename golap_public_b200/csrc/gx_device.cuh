@@ -68,11 +68,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* m, uint32_t phase) {
     return ok != 0;
 }
 
-// Bounded wait for the phase to complete (never spins forever).
-constexpr uint32_t kMbarWaitCap = 1u << 22;
+// try_wait that may suspend the thread until the phase completes or about
+// `ns` nanoseconds pass: waiting threads sleep instead of spinning through
+// issue slots while a bulk copy is in flight.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* m, uint32_t phase, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(m)), "r"(phase), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase to complete (never waits forever: at most
+// kMbarWaitCap tries of at most 1 us each).
+constexpr uint32_t kMbarWaitCap = 1u << 21;
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* m, uint32_t phase) {
     for (uint32_t i = 0; i < kMbarWaitCap; ++i)
-        if (mbar_try_wait(m, phase)) return true;
+        if (mbar_try_wait_sleep(m, phase, 1000u)) return true;
     return false;
 }
 
@@ -291,8 +305,8 @@ __device__ __forceinline__ uint32_t seg_group_log2(uint32_t nseg, uint32_t NT) {
 // `out` (out_size bytes expected).  All 32 lanes call it; every lane sees the
 // same control flow.  Returns 0 or kErrCorrupt (uniform across the warp).
 template <class Src>
-__device__ __forceinline__ int lz4_warp_block(const Src in, uint32_t in_size, uint8_t* __restrict__ out,
-                                              uint32_t out_size, uint32_t lane) {
+__device__ __noinline__ int lz4_warp_block(const Src in, uint32_t in_size, uint8_t* __restrict__ out,
+                                           uint32_t out_size, uint32_t lane) {
     uint32_t pos = 0, o = 0;
     int err = 0;
     while (true) {

@@ -47,6 +47,34 @@ __device__ __forceinline__ void raise_error(int code) { atomicCAS(&g_gx_error, 0
             return gx::set_error(GX_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
+// Scratch memory of the library's launches comes from a per-device memory
+// pool that keeps up to 256 MiB cached across synchronisations: the default
+// pool returns its memory at every synchronisation, so every call after one
+// would map fresh memory (hundreds of microseconds).
+static cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!pools[dev & 63]) {
+            cudaMemPoolProps props{};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            e = cudaMemPoolCreate(&pools[dev & 63], &props);
+            if (e != cudaSuccess) return e;
+            uint64_t keep = 256ull << 20;
+            cudaMemPoolSetAttribute(pools[dev & 63], cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        pool = pools[dev & 63];
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
+
 namespace {
 
 constexpr uint32_t kTileRows = 4096;      // tile of the small configuration
@@ -1124,7 +1152,7 @@ gx_status gx_prune_minmax(const gx_column* const* cols, const int32_t* lo, const
     gx_status st = fill_prune(&ip, cols, lo, hi, n_preds, n_chunks);
     if (st) return st;
     uint32_t* scratch = nullptr;
-    GX_CK(cudaMallocAsync(&scratch, 4ull * (n_chunks + 2), s));
+    GX_CK(scratch_alloc((void**)&scratch, 4ull * (n_chunks + 2), s));
     ip.keep_out = keep_dev;
     ip.items = scratch + 2;
     ip.n_items = scratch;
@@ -1282,7 +1310,7 @@ gx_status gx_groupby_read(gx_groupby* gb, int64_t* keys_host, int64_t* sums_host
     const uint64_t tcap = 1ull << gb->log2cap;
     const uint64_t ocap = std::max<uint64_t>(cap, 1);
     char* scratch = nullptr;
-    GX_CK(cudaMallocAsync(&scratch, 16 * ocap + 16, s));
+    GX_CK(scratch_alloc((void**)&scratch, 16 * ocap + 16, s));
     int64_t* ok = (int64_t*)scratch;
     int64_t* os = ok + ocap;
     unsigned long long* cnt = (unsigned long long*)(os + ocap);
@@ -1407,7 +1435,7 @@ static gx_status ensure_kernel_attrs() {
     if (!st) st = allow_smem(shared_scan_kernel<256, 2>, sh_max);
     if (!st) st = allow_smem(shared_scan_kernel<512, 1>, sh_max);
     if (!st) st = allow_smem(shared_scan_kernel<1024, 1>, sh_max);
-    if (!st) st = allow_smem(shared_scan_kernel<kShNT, 2, true>, sh_max);
+    if (!st) st = allow_smem(shared_scan_kernel<kShSingleNT, 4, true>, sh_max);
     if (st) return st;
     attr_set[dev & 63] = true;
     return GX_OK;
@@ -1536,7 +1564,7 @@ static gx_status scan_launch_shared(const gx_scan_plan* plan, const QueryDesc& q
     P.rows_scanned = rows_dev;
     const uint32_t n_slots = c0->n_slots;
     uint32_t* scratch = nullptr;
-    GX_CK(cudaMallocAsync(&scratch, 4ull * (2ull * n_slots + 2), s));
+    GX_CK(scratch_alloc((void**)&scratch, 4ull * (2ull * n_slots + 2), s));
     P.n_items = scratch;
     P.work_counter = scratch + 1;
     P.items = scratch + 2;
@@ -1552,12 +1580,13 @@ static gx_status scan_launch_shared(const gx_scan_plan* plan, const QueryDesc& q
         int& per_sm = occ[dev & 63][P.n_cols];
         if (per_sm == 0) {
             int v = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, shared_scan_kernel<kShNT, 2, true>, kShNT, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, shared_scan_kernel<kShSingleNT, 4, true>, kShSingleNT,
+                                                          smem);
             per_sm = std::max(1, v);
         }
         const uint64_t tiles = (uint64_t)n_slots * P.tiles_per_block;
         const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm, tiles));
-        shared_scan_kernel<kShNT, 2, true><<<grid, kShNT, smem, s>>>(P);
+        shared_scan_kernel<kShSingleNT, 4, true><<<grid, kShSingleNT, smem, s>>>(P);
         e = cudaGetLastError();
     }
     cudaFreeAsync(scratch, s);
@@ -1586,7 +1615,7 @@ static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned 
     ip.keep_out = plan->keep_out_dev;
     const uint32_t n_chunks = c0->n_chunks;
     uint32_t* scratch = nullptr;
-    GX_CK(cudaMallocAsync(&scratch, 4ull * (n_chunks + 4), s));
+    GX_CK(scratch_alloc((void**)&scratch, 4ull * (n_chunks + 4), s));
     ip.n_items = scratch;
     ip.work_counter = scratch + 1;
     ip.items = scratch + 4;
@@ -1717,7 +1746,7 @@ gx_status gx_scan_sync(const gx_scan_plan* plan, void* stream, uint64_t* rows_sc
     cudaStream_t s = (cudaStream_t)stream;
     unsigned long long* rows = nullptr;
     if (rows_scanned) {
-        GX_CK(cudaMallocAsync(&rows, 8, s));
+        GX_CK(scratch_alloc((void**)&rows, 8, s));
         GX_CK(cudaMemsetAsync(rows, 0, 8, s));
     }
     gx_status st = scan_launch(plan, s, rows);

@@ -17,7 +17,8 @@
 constexpr uint32_t kShTile = 2048;        // rows per shared tile
 constexpr uint32_t kShMaxCols = 16;       // distinct columns in one shared batch
 constexpr uint32_t kShMaxQueries = 1024;  // queries in one shared batch
-constexpr uint32_t kShNT = 256;           // default threads per CTA (128, 256, 512, 1024 are built)
+constexpr uint32_t kShNT = 256;           // default threads per CTA of a batch (128, 256, 512, 1024 are built)
+constexpr uint32_t kShSingleNT = 128;     // one-query launches: 4 CTAs (4 tiles in flight) per SM
 constexpr uint32_t kShColWords = kShTile + 256;  // one column buffer (with segment padding)
 
 struct ShStep {
