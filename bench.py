@@ -62,8 +62,8 @@ def peaks():
 
 
 def profile_traffic():
-    """dram bytes per scan_kernel launch from the committed ncu summary (or None)."""
-    p = ROOT / "profiles" / "scan_kernel_q1_config1.md"
+    """dram bytes per launch of the fused scan kernel from the committed ncu summary (or None)."""
+    p = ROOT / "profiles" / "shared_scan_kernel_q1_pruned_60M.md"
     if not p.exists():
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", p.read_text())
@@ -210,18 +210,34 @@ def gpu_arm(args, rank, world):
     kept_chunks = np.nonzero(q.keep.cpu().numpy())[0].tolist()
 
     # algorithmic bytes of the scan per launch: compressed bytes of the
-    # surviving tiles of the 4 columns + their block directory and segment
-    # index entries + the date_key min/max read by pruning
-    def alg_bytes(chunks):
+    # blocks the query needs (surviving chunks, and within them the blocks
+    # whose date_key zone map meets the predicate) in the 4 columns + their
+    # block directory and segment index entries + the date_key chunk min/max
+    # and block zone maps read by pruning
+    bpc = fact.cols["date_key"].info.blocks_per_chunk
+
+    def slots_of(chunks, zone=True):
+        out = []
+        dk = f["date_key"]
+        for ch in chunks:
+            for j in range(bpc):
+                r0 = ch * ROWS_PER_CHUNK + j * ROWS_PER_BLOCK
+                r1 = min(N_ROWS, ch * ROWS_PER_CHUNK + min(ROWS_PER_CHUNK, (j + 1) * ROWS_PER_BLOCK))
+                if r0 >= r1:
+                    continue
+                if zone and (dk[r0:r1].max() < DATE_LO or dk[r0:r1].min() > DATE_HI):
+                    continue
+                out.append(ch * bpc + j)
+        return out
+
+    def alg_bytes(chunks, zone=True):
+        slots = slots_of(chunks, zone)
         tot = 0
         for name, c in fact.cols.items():
             info = c.info
-            b = c.blocks()
-            per_chunk = info.blocks_per_chunk
-            for ch in chunks:
-                sel = b[ch * per_chunk:(ch + 1) * per_chunk]
-                tot += int(sel[:, 2].sum()) + 16 * len(sel) + (8 * info.lz4_segments * len(sel) if info.lz4_segments > 1 else 0)
-        return tot + 8 * fact.cols["date_key"].info.n_chunks
+            sel = c.blocks()[slots]
+            tot += int(sel[:, 2].sum()) + 16 * len(sel) + (8 * info.lz4_segments * len(sel) if info.lz4_segments > 1 else 0)
+        return tot + 8 * fact.cols["date_key"].info.n_chunks + (8 * bpc * len(chunks) if zone else 0)
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -248,10 +264,16 @@ def gpu_arm(args, rank, world):
     ms = max_over_ranks(float(np.mean(step_ms)), world, "cuda")
     scan_avg = float(np.mean(scan_ms))
 
-    # full-table scan (pruning off): the decode-bound throughput of the same kernel
-    q_all = queries.Q1Query(fact, dd, ok, DATE_LO, DATE_HI, *DISC, *QTY, prune=False)
-    if q_all.run() != want:
-        raise SystemExit("full scan and pruned scan disagree")
+    # full-table scan: the same Q1 plan over every date (pruning off), so every
+    # tile needs all four columns -- the decode-bound throughput of the kernel
+    ok_all = np.ones(len(dd["d_key"]), dtype=bool)
+    q_all = queries.Q1Query(fact, dd, ok_all, int(dd["d_key"].min()), int(dd["d_key"].max()), *DISC, *QTY,
+                            prune=False)
+    m_all = (f["discount"] >= DISC[0]) & (f["discount"] <= DISC[1]) & (f["quantity"] >= QTY[0]) & \
+            (f["quantity"] <= QTY[1])
+    want_all = int((f["extended_price"][m_all].astype(np.int64) * f["discount"][m_all].astype(np.int64)).sum())
+    if q_all.run() != want_all:
+        raise SystemExit("full scan result differs from the numpy sum")
     for _ in range(3):
         q_all.launch()
     all_ms = []
@@ -266,14 +288,14 @@ def gpu_arm(args, rank, world):
         torch.cuda.synchronize()
         all_ms.append(a.elapsed_time(b))
     all_ms_avg = float(np.mean(all_ms))
-    all_bytes = alg_bytes(range(fact.cols["date_key"].info.n_chunks))
+    all_bytes = alg_bytes(range(fact.cols["date_key"].info.n_chunks), zone=False)
 
     # e2e: pinned-host residency, date dimension in, result out
     fact_h = queries.encode_fact(f, {"date_key": "cascaded"}, ROWS_PER_CHUNK, ROWS_PER_BLOCK, args.segments,
                                  residency="pinned")
     qh = queries.Q1Query(fact_h, dd, ok, DATE_LO, DATE_HI, *DISC, *QTY, prune=True)
     res_h = torch.zeros(1, dtype=torch.int64).pin_memory()
-    h2d_scan = alg_bytes(kept_chunks) - 8 * fact.cols["date_key"].info.n_chunks
+    h2d_scan = alg_bytes(kept_chunks) - 8 * fact.cols["date_key"].info.n_chunks - 8 * bpc * len(kept_chunks)
 
     def e2e_step():
         dk_d.copy_(dk_h, non_blocking=True)
