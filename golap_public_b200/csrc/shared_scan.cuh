@@ -123,6 +123,31 @@ __global__ void shared_items_kernel(const __grid_constant__ ShParams P, uint32_t
     }
 }
 
+// Out-of-line pieces of the evaluation: the row loop is unrolled RPT times,
+// so large bodies inside it are called rather than inlined to keep the hot
+// code small (instruction-fetch stalls).
+__device__ __noinline__ bool sh_probe(const uint64_t* ht, uint32_t htlog, uint32_t htlay, int32_t v, int32_t* p) {
+    return ht_probe_any(ht, htlog, htlay, v, p);
+}
+
+// Warp-aggregated add of (gk, val) for the lanes with k set into the global
+// group table.  All 32 lanes call it.
+__device__ __noinline__ void sh_group_add(bool k, uint32_t gk, int64_t val, int64_t* keys, int64_t* sums,
+                                          uint32_t log2cap) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t active = __ballot_sync(0xFFFFFFFFu, k);
+    while (active) {
+        const int leader = __ffs(active) - 1;
+        const uint32_t lk = __shfl_sync(0xFFFFFFFFu, gk, leader);
+        const bool peer = k && gk == lk && ((active >> lane) & 1u);
+        const uint32_t peers = __ballot_sync(0xFFFFFFFFu, peer);
+        const uint64_t tot = warp_sum_u64(peer ? (uint64_t)val : 0ull);
+        if ((int)lane == leader && !group_add_global(keys, sums, log2cap, (int64_t)lk, (int64_t)tot))
+            raise_error(kErrCapacity);
+        active &= ~peers;
+    }
+}
+
 __device__ __forceinline__ uint32_t sh_col_index(uint32_t r, uint32_t sh, uint32_t pd) {
     return r + ((r >> sh) << pd);
 }
@@ -292,7 +317,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                             if ((flags & GX_STEP_PROBE) && k) {
                                 if (v != mv) {
                                     mp = v;
-                                    mk = ht_probe_any(ht, htlog, htlay, v, &mp);
+                                    mk = sh_probe(ht, htlog, htlay, v, &mp);
                                     mv = v;
                                 }
                                 k = mk;
@@ -315,22 +340,8 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                                               : agg == GX_AGG_SUM_PRODUCT ? (int64_t)v * carry[i]
                                               : agg == GX_AGG_COUNT        ? 1
                                                                            : (int64_t)v;
-                            if (!grouped) {
-                                local += val;
-                            } else {
-                                uint32_t active = __ballot_sync(0xFFFFFFFFu, k);
-                                while (active) {
-                                    const int leader = __ffs(active) - 1;
-                                    const uint32_t lk = __shfl_sync(0xFFFFFFFFu, gk[i], leader);
-                                    const bool peer = k && gk[i] == lk && ((active >> lane) & 1u);
-                                    const uint32_t peers = __ballot_sync(0xFFFFFFFFu, peer);
-                                    const uint64_t tot = warp_sum_u64(peer ? (uint64_t)val : 0ull);
-                                    if ((int)lane == leader &&
-                                        !group_add_global(Q.g_keys, Q.g_sums, Q.g_log2, (int64_t)lk, (int64_t)tot))
-                                        raise_error(kErrCapacity);
-                                    active &= ~peers;
-                                }
-                            }
+                            if (!grouped) local += val;
+                            else sh_group_add(k, gk[i], val, Q.g_keys, Q.g_sums, Q.g_log2);
                         }
                     }
                 }
