@@ -265,6 +265,22 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
         __syncthreads();
         if (rc) return -1;
         if (c.S > 1) {
+            // one literal run covers the whole tile (the first entry resumes inside a
+            // run long enough, and the tile's bytes are exactly its rows): a flat,
+            // vectorised copy of n words from byte lo, rows in plain order
+            const uint32_t info0 = seg_smem[1];
+            if ((info0 & 16u) && (info0 >> 5) >= 4 * n && hi - lo == 4 * n && (n & 3u) == 0 && lo == seg_smem[0]) {
+                const uint32_t* A = (const uint32_t*)stage;
+                const uint32_t rb = lo - wbase, w0 = rb >> 2, sh = (rb & 3u) * 8;
+                for (uint32_t q4 = tid; q4 < n / 4; q4 += NT) {
+                    const uint32_t w = w0 + 4 * q4;
+                    const uint32_t a0 = A[w], a1 = A[w + 1], a2 = A[w + 2], a3 = A[w + 3], a4 = A[w + 4];
+                    ((uint4*)buf)[q4] = make_uint4(__funnelshift_r(a0, a1, sh), __funnelshift_r(a1, a2, sh),
+                                                   __funnelshift_r(a2, a3, sh), __funnelshift_r(a3, a4, sh));
+                }
+                __syncthreads();
+                return kRows;
+            }
             // a group of G adjacent lanes per segment; segment t at buf + t * (seg_rows + G)
             // lanes per segment: a whole warp when the tile is mostly literals
             // (few sequences; conflict-free 32-word copies), else spread the

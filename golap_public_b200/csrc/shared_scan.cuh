@@ -301,47 +301,75 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                     const uint32_t* const col = colbuf + c * kShColWords;
                     const uint32_t sh = s_sh[c], pd = s_pd[c];
                     const bool last = s + 1 == ns;
-                    // one-entry probe memo: a thread's rows are NT apart, so on sorted
-                    // or run-length columns they mostly repeat the previous key
-                    int32_t mv = kEmptyKey, mp = 0;
-                    bool mk = false;
+                    const bool simple = !(flags & GX_STEP_PROBE) && dcard == 0;  // no probe, no digit
+                    const bool filt = (flags & GX_STEP_FILTER) != 0, carry_step = (flags & GX_STEP_CARRY) != 0;
+                    if (simple && !last) {
+                        // FILTER and/or CARRY: branch-free over the thread's rows (dead
+                        // rows read their in-bounds slot and stay dead)
 #pragma unroll
-                    for (int i = 0; i < RPT; ++i) {
-                        const uint32_t r = (i * NW + warp) * 32 + lane;
-                        bool k = (keep >> i) & 1u;
-                        int32_t v = 0;
-                        if (k) {
-                            v = (int32_t)col[sh_col_index(r, sh, pd)];
-                            if (flags & GX_STEP_FILTER) k = v >= lo && v <= hi;
-                            int32_t p = v;
-                            if ((flags & GX_STEP_PROBE) && k) {
-                                if (v != mv) {
-                                    mp = v;
-                                    mk = sh_probe(ht, htlog, htlay, v, &mp);
-                                    mv = v;
-                                }
-                                k = mk;
-                                p = mp;
-                            }
-                            if (dcard && k) {
-                                const uint32_t dgt = (uint32_t)(p - dbase);
-                                if (dgt >= dcard) {
-                                    raise_error(kErrInvalid);
-                                    k = false;
-                                } else {
-                                    gk[i] = gk[i] * dcard + dgt;
-                                }
-                            }
-                            if ((flags & GX_STEP_CARRY) && k) carry[i] = v;
-                            if (!k) keep &= ~(1u << i);
+                        for (int i = 0; i < RPT; ++i) {
+                            const uint32_t r = (i * NW + warp) * 32 + lane;
+                            const int32_t v = (int32_t)col[sh_col_index(r, sh, pd)];
+                            const bool k = ((keep >> i) & 1u) && (!filt || (v >= lo && v <= hi));
+                            if (carry_step) carry[i] = v;
+                            keep = k ? keep : (keep & ~(1u << i));
                         }
-                        if (last) {  // the VALUE step: aggregate the row
-                            const int64_t val = !k ? 0
-                                              : agg == GX_AGG_SUM_PRODUCT ? (int64_t)v * carry[i]
-                                              : agg == GX_AGG_COUNT        ? 1
-                                                                           : (int64_t)v;
-                            if (!grouped) local += val;
-                            else sh_group_add(k, gk[i], val, Q.g_keys, Q.g_sums, Q.g_log2);
+                    } else if (simple && last && !grouped && agg != GX_AGG_COUNT) {
+                        // the VALUE step of a scalar SUM / SUM_PRODUCT
+                        const bool prod = agg == GX_AGG_SUM_PRODUCT;
+#pragma unroll
+                        for (int i = 0; i < RPT; ++i) {
+                            const uint32_t r = (i * NW + warp) * 32 + lane;
+                            const int32_t v = (int32_t)col[sh_col_index(r, sh, pd)];
+                            const bool k = ((keep >> i) & 1u) && (!filt || (v >= lo && v <= hi));
+                            const int32_t c2 = carry_step ? v : carry[i];
+                            const int64_t val = prod ? (int64_t)v * c2 : (int64_t)v;
+                            local += k ? val : 0;
+                        }
+                    } else {
+                        // general step: probes (one-entry memo: a thread's rows are NT apart,
+                        // so on sorted or run-length columns they mostly repeat the key),
+                        // group-key digits, COUNT, grouped aggregation
+                        int32_t mv = kEmptyKey, mp = 0;
+                        bool mk = false;
+#pragma unroll
+                        for (int i = 0; i < RPT; ++i) {
+                            const uint32_t r = (i * NW + warp) * 32 + lane;
+                            bool k = (keep >> i) & 1u;
+                            int32_t v = 0;
+                            if (k) {
+                                v = (int32_t)col[sh_col_index(r, sh, pd)];
+                                if (filt) k = v >= lo && v <= hi;
+                                int32_t p = v;
+                                if ((flags & GX_STEP_PROBE) && k) {
+                                    if (v != mv) {
+                                        mp = v;
+                                        mk = sh_probe(ht, htlog, htlay, v, &mp);
+                                        mv = v;
+                                    }
+                                    k = mk;
+                                    p = mp;
+                                }
+                                if (dcard && k) {
+                                    const uint32_t dgt = (uint32_t)(p - dbase);
+                                    if (dgt >= dcard) {
+                                        raise_error(kErrInvalid);
+                                        k = false;
+                                    } else {
+                                        gk[i] = gk[i] * dcard + dgt;
+                                    }
+                                }
+                                if (carry_step && k) carry[i] = v;
+                                if (!k) keep &= ~(1u << i);
+                            }
+                            if (last) {  // the VALUE step: aggregate the row
+                                const int64_t val = !k ? 0
+                                                  : agg == GX_AGG_SUM_PRODUCT ? (int64_t)v * carry[i]
+                                                  : agg == GX_AGG_COUNT        ? 1
+                                                                               : (int64_t)v;
+                                if (!grouped) local += val;
+                                else sh_group_add(k, gk[i], val, Q.g_keys, Q.g_sums, Q.g_log2);
+                            }
                         }
                     }
                 }
