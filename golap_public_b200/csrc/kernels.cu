@@ -201,22 +201,6 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
                                            uint32_t* seg_smem) {
     using C = Cfg<MAXT>;
     const uint32_t tid = threadIdx.x;
-    // segmented LZ4: this thread's entry of the tile's segment index, loaded
-    // together with the directory entry (the two reads do not depend on each
-    // other, so their latencies overlap)
-    const bool segd = c.codec == GX_CODEC_LZ4 && c.S > 1;
-    uint32_t se0 = 0, se1 = 0;
-    bool se_in = false;
-    if (segd && tid <= kMaxSegments) {
-        const uint32_t j = (r0 >> c.seg_shift) + tid;
-        const uint32_t nseg_t = (n + (1u << c.seg_shift) - 1) >> c.seg_shift;
-        if (tid <= nseg_t && j < c.S) {
-            const uint32_t* e = c.seg + (size_t)2 * c.S * slot + 2 * j;
-            se0 = __ldg(e);
-            se1 = __ldg(e + 1);
-            se_in = true;
-        }
-    }
     const gx_dblock d = c.blocks[slot];
     const uint8_t* blk = c.payload + d.offset;
     // directory sanity: the stream lies inside the payload (whose slack
@@ -249,15 +233,12 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
             seg_rows = 1u << c.seg_shift;
             j0 = r0 >> c.seg_shift;
             nseg = (n + seg_rows - 1) >> c.seg_shift;
-            // the tile's nseg + 1 segment entries into shared memory (entries past
-            // the block's last segment stand for its end); threads beyond the first
-            // NT entries fetch theirs here
+            // the tile's nseg + 1 segment entries into shared memory (one parallel load)
             const uint32_t* e = c.seg + (size_t)2 * c.S * slot;
             for (uint32_t t = tid; t <= nseg && t <= kMaxSegments; t += NT) {
                 const uint32_t j = j0 + t;
-                const bool mine = t == tid && se_in;
-                seg_smem[2 * t] = mine ? se0 : (j < c.S ? __ldg(e + 2 * j) : d.comp_bytes);
-                seg_smem[2 * t + 1] = mine ? se1 : (j < c.S ? __ldg(e + 2 * j + 1) : 0u);
+                seg_smem[2 * t] = j < c.S ? __ldg(e + 2 * j) : d.comp_bytes;
+                seg_smem[2 * t + 1] = j < c.S ? __ldg(e + 2 * j + 1) : 0u;
             }
             __syncthreads();
             lo = seg_smem[0];
@@ -1465,7 +1446,7 @@ static gx_status ensure_kernel_attrs() {
     if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock, false>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
     if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock, true>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
     const size_t sh_max = 4ull * kShColWords * kShMaxCols + Cfg<kTileRows>::kStage + 8ull * kShMaxQueries +
-                          4ull * (kShMaxQueries / 32) + 4ull * kShCacheWords * kShCacheSlots;
+                          4ull * (kShMaxQueries / 32);
     if (!st) st = allow_smem(shared_scan_kernel<128, 4>, sh_max);
     if (!st) st = allow_smem(shared_scan_kernel<256, 2>, sh_max);
     if (!st) st = allow_smem(shared_scan_kernel<512, 1>, sh_max);
@@ -1573,9 +1554,8 @@ static void shared_layout(ShParams& P, const gx_column* c0) {
     P.n_slots = c0->n_slots;
 }
 
-static size_t shared_smem_bytes(uint32_t n_cols, uint32_t n_queries, uint32_t cache_slots = 0) {
-    return 4ull * kShColWords * n_cols + Cfg<kTileRows>::kStage + 8ull * n_queries + 4ull * ((n_queries + 31) / 32) +
-           4ull * kShCacheWords * cache_slots;
+static size_t shared_smem_bytes(uint32_t n_cols, uint32_t n_queries) {
+    return 4ull * kShColWords * n_cols + Cfg<kTileRows>::kStage + 8ull * n_queries + 4ull * ((n_queries + 31) / 32);
 }
 
 // A plan that qualifies for the shared form (its only VALUE step last, LZ4
@@ -1813,21 +1793,6 @@ static gx_status shared_prepare(gx_batch* b, const gx_query* queries, uint32_t n
     std::vector<ShQuery> sq(n);
     for (uint32_t i = 0; i < n; ++i)
         if (!shared_query(queries[i].plan, qs[i], cols, sq[i], why)) return GX_OK;
-    // queries that probe the same tables with the same columns first become
-    // neighbours, so a tile's probe results can serve the next query too
-    // (results go to each query's own targets: the order is internal)
-    auto probe_key = [](const ShQuery& q, uint32_t st) {
-        const bool pr = st < q.n_steps && (q.steps[st].flags & GX_STEP_PROBE);
-        return std::make_pair(pr ? q.steps[st].col : 0xFFFFFFFFu, pr ? (uintptr_t)q.steps[st].ht : (uintptr_t)0);
-    };
-    std::stable_sort(sq.begin(), sq.end(), [&](const ShQuery& a, const ShQuery& b) {
-        return std::make_pair(probe_key(a, 0), probe_key(a, 1)) < std::make_pair(probe_key(b, 0), probe_key(b, 1));
-    });
-    for (uint32_t i = 0; i + 1 < n; ++i)
-        for (uint32_t st = 0; st < kShCacheSlots; ++st) {
-            const auto ka = probe_key(sq[i], st);
-            if (ka.first != 0xFFFFFFFFu && ka == probe_key(sq[i + 1], st)) sq[i].share_next |= 1u << st;
-        }
     const uint32_t mw = (n + 31) / 32;
     const uint32_t n_slots = c0->n_slots;
     // grow buffers (the stream's earlier work is finished by the caller)
@@ -1876,10 +1841,9 @@ static gx_status shared_prepare(gx_batch* b, const gx_query* queries, uint32_t n
     P.items = b->d_sh_items + 2;
     shared_layout(P, c0);
     P.rows_scanned = b->d_rows;
-    P.cache_slots = kShCacheSlots;
     b->n_slots = n_slots;
     b->dir0 = c0->d_blocks;
-    b->sh_smem = shared_smem_bytes(P.n_cols, n, P.cache_slots);
+    b->sh_smem = shared_smem_bytes(P.n_cols, n);
     shared_geometry(b);
     b->sh_items_grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(8ull * sm_count(), (n_slots + 7) / 8));
     *ok = true;

@@ -20,8 +20,6 @@ constexpr uint32_t kShMaxQueries = 1024;  // queries in one shared batch
 constexpr uint32_t kShNT = 256;           // default threads per CTA of a batch (128, 256, 512, 1024 are built)
 constexpr uint32_t kShSingleNT = 128;     // one-query launches: 4 CTAs (4 tiles in flight) per SM
 constexpr uint32_t kShColWords = kShTile + 256;  // one column buffer (with segment padding)
-constexpr uint32_t kShCacheSlots = 2;             // probe-result cache: steps 0 and 1 of a batch's queries
-constexpr uint32_t kShCacheWords = kShTile + kShTile / 32;  // payload per row + hit bit per row
 
 struct ShStep {
     uint32_t flags;
@@ -48,7 +46,6 @@ struct ShQuery {
     PrunePred prune[GX_MAX_STEPS];
     const uint16_t* keep_in;  // per-chunk keep flags or null
     uint16_t* keep_out;       // per-chunk keep flags written by the work-list pass, or null
-    uint32_t share_next;      // bit s: the next query probes the same table with the same column at step s
 };
 
 struct ShParams {
@@ -64,7 +61,6 @@ struct ShParams {
     uint32_t blocks_per_chunk, rows_per_chunk, rows_per_block;
     uint32_t tile_rows, tiles_per_block;
     unsigned long long* rows_scanned;  // optional: sum over (query, tile) of the query's rows in the tile
-    uint32_t cache_slots;       // probe-result cache slots in shared memory (0 or kShCacheSlots)
     const gx_dblock* dir;       // directory of the table (any of its columns)
     uint32_t n_slots;
     // one query carried in the parameters themselves (qs and cols null)
@@ -212,7 +208,6 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
     uint8_t* stage = (uint8_t*)(colbuf + (size_t)P.n_cols * kShColWords);
     unsigned long long* s_part = (unsigned long long*)(stage + C::kStage);
     uint32_t* s_qmask = (uint32_t*)(s_part + P.n_queries);
-    uint32_t* s_cache = s_qmask + P.mask_words;  // cache_slots x kShCacheWords
 
     __shared__ __align__(8) uint64_t s_mbar;
     __shared__ uint32_t s_item;
@@ -265,12 +260,6 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
         __syncthreads();
         uint32_t decoded = 0;  // columns of this tile already in their buffers
         bool dropped = false;
-        // probe-result cache tags (uniform): slot s holds the results of probing
-        // column ctag_c[s] in table ctag_ht[s] for every row of the tile
-        static_assert(kShCacheSlots == 2, "two cache slots: tags held in scalars");
-        uint32_t ctag_c0 = 0xFFFFFFFFu, ctag_c1 = 0xFFFFFFFFu;
-        const uint64_t* ctag_h0 = nullptr;
-        const uint64_t* ctag_h1 = nullptr;
         for (uint32_t w = 0; w < MW && !dropped; ++w) {
             uint32_t m = s_qmask[w];
             while (m && !dropped) {
@@ -343,45 +332,6 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                         // group-key digits, COUNT, grouped aggregation
                         int32_t mv = kEmptyKey, mp = 0;
                         bool mk = false;
-                        // batches: probe results shared between adjacent queries that probe
-                        // the same table with the same column at step 0 or 1
-                        uint32_t* cslot = nullptr;
-                        if (!SINGLE && (flags & GX_STEP_PROBE) && s < P.cache_slots) {
-                            cslot = s_cache + s * kShCacheWords;
-                            const bool tag_hit = s == 0 ? (ctag_c0 == c && ctag_h0 == ht) : (ctag_c1 == c && ctag_h1 == ht);
-                            if (!tag_hit) {
-                                if ((Q.share_next >> s) & 1u) {
-                                    // fill: probe every row this thread owns (alive or not)
-#pragma unroll
-                                    for (int i = 0; i < RPT; ++i) {
-                                        const uint32_t r = (i * NW + warp) * 32 + lane;
-                                        const int32_t v = (int32_t)col[sh_col_index(r, sh, pd)];
-                                        int32_t p = v;
-                                        bool f = false;
-                                        if (v != mv) {
-                                            mp = v;
-                                            mk = sh_probe(ht, htlog, htlay, v, &mp);
-                                            mv = v;
-                                        }
-                                        f = mk;
-                                        p = mp;
-                                        cslot[r] = (uint32_t)p;
-                                        const uint32_t hb = __ballot_sync(0xFFFFFFFFu, f);
-                                        if (lane == 0) cslot[kShTile + (i * NW + warp)] = hb;
-                                    }
-                                    __syncwarp();
-                                    if (s == 0) {
-                                        ctag_c0 = c;
-                                        ctag_h0 = ht;
-                                    } else {
-                                        ctag_c1 = c;
-                                        ctag_h1 = ht;
-                                    }
-                                } else {
-                                    cslot = nullptr;
-                                }
-                            }
-                        }
 #pragma unroll
                         for (int i = 0; i < RPT; ++i) {
                             const uint32_t r = (i * NW + warp) * 32 + lane;
@@ -392,18 +342,13 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                                 if (filt) k = v >= lo && v <= hi;
                                 int32_t p = v;
                                 if ((flags & GX_STEP_PROBE) && k) {
-                                    if (cslot) {
-                                        k = (cslot[kShTile + (i * NW + warp)] >> lane) & 1u;
-                                        p = (int32_t)cslot[r];
-                                    } else {
-                                        if (v != mv) {
-                                            mp = v;
-                                            mk = sh_probe(ht, htlog, htlay, v, &mp);
-                                            mv = v;
-                                        }
-                                        k = mk;
-                                        p = mp;
+                                    if (v != mv) {
+                                        mp = v;
+                                        mk = sh_probe(ht, htlog, htlay, v, &mp);
+                                        mv = v;
                                     }
+                                    k = mk;
+                                    p = mp;
                                 }
                                 if (dcard && k) {
                                     const uint32_t dgt = (uint32_t)(p - dbase);
