@@ -201,6 +201,22 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
                                            uint32_t* seg_smem) {
     using C = Cfg<MAXT>;
     const uint32_t tid = threadIdx.x;
+    // segmented LZ4: this thread's entry of the tile's segment index, loaded
+    // together with the directory entry (the two reads do not depend on each
+    // other, so their latencies overlap)
+    const bool segd = c.codec == GX_CODEC_LZ4 && c.S > 1;
+    uint32_t se0 = 0, se1 = 0;
+    bool se_in = false;
+    if (segd && tid <= kMaxSegments) {
+        const uint32_t j = (r0 >> c.seg_shift) + tid;
+        const uint32_t nseg_t = (n + (1u << c.seg_shift) - 1) >> c.seg_shift;
+        if (tid <= nseg_t && j < c.S) {
+            const uint32_t* e = c.seg + (size_t)2 * c.S * slot + 2 * j;
+            se0 = __ldg(e);
+            se1 = __ldg(e + 1);
+            se_in = true;
+        }
+    }
     const gx_dblock d = c.blocks[slot];
     const uint8_t* blk = c.payload + d.offset;
     // directory sanity: the stream lies inside the payload (whose slack
@@ -233,12 +249,15 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
             seg_rows = 1u << c.seg_shift;
             j0 = r0 >> c.seg_shift;
             nseg = (n + seg_rows - 1) >> c.seg_shift;
-            // the tile's nseg + 1 segment entries into shared memory (one parallel load)
+            // the tile's nseg + 1 segment entries into shared memory (entries past
+            // the block's last segment stand for its end); threads beyond the first
+            // NT entries fetch theirs here
             const uint32_t* e = c.seg + (size_t)2 * c.S * slot;
             for (uint32_t t = tid; t <= nseg && t <= kMaxSegments; t += NT) {
                 const uint32_t j = j0 + t;
-                seg_smem[2 * t] = j < c.S ? __ldg(e + 2 * j) : d.comp_bytes;
-                seg_smem[2 * t + 1] = j < c.S ? __ldg(e + 2 * j + 1) : 0u;
+                const bool mine = t == tid && se_in;
+                seg_smem[2 * t] = mine ? se0 : (j < c.S ? __ldg(e + 2 * j) : d.comp_bytes);
+                seg_smem[2 * t + 1] = mine ? se1 : (j < c.S ? __ldg(e + 2 * j + 1) : 0u);
             }
             __syncthreads();
             lo = seg_smem[0];
@@ -994,6 +1013,9 @@ struct gx_batch {
     const gx_dblock* dir0 = nullptr;
     uint32_t sh_grid = 1, sh_items_grid = 1;
     size_t sh_smem = 0;
+    uint8_t* d_qc = nullptr;       // compact descriptors (device) and pinned staging
+    uint8_t* h_qc = nullptr;
+    size_t cap_qc = 0;
     uint32_t sh_threads = kShNT;   // launch shape of the shared form (tunable)
     uint32_t sh_ctas_per_sm = 0;   // 0 = as many as fit
 };
@@ -1445,8 +1467,7 @@ static gx_status ensure_kernel_attrs() {
     if (!st) st = allow_smem(scan_kernel<128, kTileRows, true>, scan_smem_bytes<kTileRows>(true, true));
     if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock, false>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
     if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock, true>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
-    const size_t sh_max = 4ull * kShColWords * kShMaxCols + Cfg<kTileRows>::kStage + 8ull * kShMaxQueries +
-                          4ull * (kShMaxQueries / 32);
+    const size_t sh_max = kShMaxDynSmem;
     if (!st) st = allow_smem(shared_scan_kernel<128, 4>, sh_max);
     if (!st) st = allow_smem(shared_scan_kernel<256, 2>, sh_max);
     if (!st) st = allow_smem(shared_scan_kernel<512, 1>, sh_max);
@@ -1554,8 +1575,46 @@ static void shared_layout(ShParams& P, const gx_column* c0) {
     P.n_slots = c0->n_slots;
 }
 
-static size_t shared_smem_bytes(uint32_t n_cols, uint32_t n_queries) {
-    return 4ull * kShColWords * n_cols + Cfg<kTileRows>::kStage + 8ull * n_queries + 4ull * ((n_queries + 31) / 32);
+static size_t shared_smem_bytes(uint32_t n_cols, uint32_t n_queries, uint32_t qc_bytes = 0) {
+    return 4ull * kShColWords * n_cols + Cfg<kTileRows>::kStage + 8ull * n_queries + 4ull * ((n_queries + 31) / 32) +
+           (qc_bytes ? 16ull + qc_bytes : 0ull);
+}
+
+// The compact descriptor image of a batch: ShQueryC per query, then ShStepC
+// per step, padded to 16 bytes.
+static std::vector<uint8_t> shared_compact(const std::vector<ShQuery>& sq) {
+    size_t steps = 0;
+    for (const ShQuery& q : sq) steps += q.n_steps;
+    const size_t bytes = (sizeof(ShQueryC) * sq.size() + sizeof(ShStepC) * steps + 15) & ~(size_t)15;
+    std::vector<uint8_t> img(bytes, 0);
+    ShQueryC* qc = (ShQueryC*)img.data();
+    ShStepC* sc = (ShStepC*)(img.data() + sizeof(ShQueryC) * sq.size());
+    uint32_t k = 0;
+    for (size_t i = 0; i < sq.size(); ++i) {
+        const ShQuery& q = sq[i];
+        qc[i].row_lo = q.row_lo;
+        qc[i].row_hi = q.row_hi;
+        qc[i].g_keys = q.g_keys;
+        qc[i].g_sums = q.g_sums;
+        qc[i].step0 = k;
+        qc[i].n_steps = (uint8_t)q.n_steps;
+        qc[i].agg = (uint8_t)q.agg;
+        qc[i].grouped = (uint8_t)q.grouped;
+        qc[i].g_log2 = (uint8_t)q.g_log2;
+        for (uint32_t t = 0; t < q.n_steps; ++t, ++k) {
+            const ShStep& st = q.steps[t];
+            sc[k].lo = st.lo;
+            sc[k].hi = st.hi;
+            sc[k].ht = st.ht;
+            sc[k].dbase = st.digit_base;
+            sc[k].dcard = st.digit_card;
+            sc[k].col = (uint8_t)st.col;
+            sc[k].flags = (uint8_t)st.flags;
+            sc[k].htlog = (uint8_t)st.ht_log2;
+            sc[k].htlay = (uint8_t)st.ht_layout;
+        }
+    }
+    return img;
 }
 
 // A plan that qualifies for the shared form (its only VALUE step last, LZ4
@@ -1793,6 +1852,27 @@ static gx_status shared_prepare(gx_batch* b, const gx_query* queries, uint32_t n
     std::vector<ShQuery> sq(n);
     for (uint32_t i = 0; i < n; ++i)
         if (!shared_query(queries[i].plan, qs[i], cols, sq[i], why)) return GX_OK;
+    const std::vector<uint8_t> img = shared_compact(sq);
+    if (img.size() > kShMaxQcBytes) {
+        *why = "query descriptors above 96 KiB";
+        return GX_OK;
+    }
+    if (shared_smem_bytes((uint32_t)cols.size(), n, (uint32_t)img.size()) > kShMaxDynSmem) {
+        *why = "columns, queries and descriptors above 220 KiB of shared memory";
+        return GX_OK;
+    }
+    if (img.size() > b->cap_qc) {
+        cudaFree(b->d_qc);
+        cudaFreeHost(b->h_qc);
+        b->d_qc = nullptr;
+        b->h_qc = nullptr;
+        b->cap_qc = 0;
+        GX_CK(cudaMalloc(&b->d_qc, img.size()));
+        GX_CK(cudaMallocHost(&b->h_qc, img.size()));
+        b->cap_qc = img.size();
+    }
+    std::memcpy(b->h_qc, img.data(), img.size());
+    GX_CK(cudaMemcpyAsync(b->d_qc, b->h_qc, img.size(), cudaMemcpyHostToDevice, s));
     const uint32_t mw = (n + 31) / 32;
     const uint32_t n_slots = c0->n_slots;
     // grow buffers (the stream's earlier work is finished by the caller)
@@ -1841,9 +1921,11 @@ static gx_status shared_prepare(gx_batch* b, const gx_query* queries, uint32_t n
     P.items = b->d_sh_items + 2;
     shared_layout(P, c0);
     P.rows_scanned = b->d_rows;
+    P.qc = (const uint4*)b->d_qc;
+    P.qc_bytes = (uint32_t)img.size();
     b->n_slots = n_slots;
     b->dir0 = c0->d_blocks;
-    b->sh_smem = shared_smem_bytes(P.n_cols, n);
+    b->sh_smem = shared_smem_bytes(P.n_cols, n, P.qc_bytes);
     shared_geometry(b);
     b->sh_items_grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(8ull * sm_count(), (n_slots + 7) / 8));
     *ok = true;
@@ -2025,6 +2107,8 @@ gx_status gx_batch_free(gx_batch* b) {
     cudaFreeHost(b->h_cols);
     cudaFree(b->d_slot_mask);
     cudaFree(b->d_sh_items);
+    cudaFree(b->d_qc);
+    cudaFreeHost(b->h_qc);
     delete b;
     return GX_OK;
 }

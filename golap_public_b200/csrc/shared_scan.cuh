@@ -20,6 +20,8 @@ constexpr uint32_t kShMaxQueries = 1024;  // queries in one shared batch
 constexpr uint32_t kShNT = 256;           // default threads per CTA of a batch (128, 256, 512, 1024 are built)
 constexpr uint32_t kShSingleNT = 128;     // one-query launches: 4 CTAs (4 tiles in flight) per SM
 constexpr uint32_t kShColWords = kShTile + 256;  // one column buffer (with segment padding)
+constexpr uint32_t kShMaxQcBytes = 96u << 10;     // compact descriptors of a batch held in shared memory
+constexpr uint32_t kShMaxDynSmem = 220u << 10;    // dynamic shared memory of one CTA (static use is ~1.3 KiB)
 
 struct ShStep {
     uint32_t flags;
@@ -48,6 +50,24 @@ struct ShQuery {
     uint16_t* keep_out;       // per-chunk keep flags written by the work-list pass, or null
 };
 
+// Compact copies of a batch's query descriptors, held in shared memory for
+// the whole launch (the evaluation reads them for every (query, tile, step)).
+struct ShStepC {
+    int32_t lo, hi;
+    const uint64_t* ht;
+    int32_t dbase;
+    uint32_t dcard;
+    uint8_t col, flags, htlog, htlay;
+};
+struct ShQueryC {
+    uint64_t row_lo, row_hi;
+    int64_t* g_keys;
+    int64_t* g_sums;
+    uint32_t step0;  // index of the query's first step in the step array
+    uint8_t n_steps, agg, grouped, g_log2;
+};
+static_assert(sizeof(ShStepC) == 32 && sizeof(ShQueryC) == 40, "compact descriptor sizes");
+
 struct ShParams {
     const gx_dcol* cols;        // the batch's column table (global memory)
     uint32_t n_cols;
@@ -61,6 +81,8 @@ struct ShParams {
     uint32_t blocks_per_chunk, rows_per_chunk, rows_per_block;
     uint32_t tile_rows, tiles_per_block;
     unsigned long long* rows_scanned;  // optional: sum over (query, tile) of the query's rows in the tile
+    const uint4* qc;            // batches: [ShQueryC x n_queries | ShStepC x steps], copied to shared memory
+    uint32_t qc_bytes;          // size of that image (a multiple of 16)
     const gx_dblock* dir;       // directory of the table (any of its columns)
     uint32_t n_slots;
     // one query carried in the parameters themselves (qs and cols null)
@@ -69,6 +91,76 @@ struct ShParams {
 };
 
 __device__ __forceinline__ const ShQuery* sh_queries(const ShParams& P) { return P.qs ? P.qs : &P.q1; }
+
+// The fields the evaluation reads, from the parameters (one-query launch) or
+// from the compact copies in shared memory (batch).
+struct QView {
+    uint64_t row_lo, row_hi;
+    int64_t* g_keys;
+    int64_t* g_sums;
+    uint32_t n_steps, agg, g_log2, step0;
+    bool grouped;
+};
+struct SView {
+    int32_t lo, hi, dbase;
+    const uint64_t* ht;
+    uint32_t dcard, col, flags, htlog, htlay;
+};
+template <bool SINGLE>
+__device__ __forceinline__ QView sh_qv(const ShParams& P, const uint8_t* s_qc, uint32_t q) {
+    QView v;
+    if constexpr (SINGLE) {
+        v.row_lo = P.q1.row_lo;
+        v.row_hi = P.q1.row_hi;
+        v.g_keys = P.q1.g_keys;
+        v.g_sums = P.q1.g_sums;
+        v.n_steps = P.q1.n_steps;
+        v.agg = P.q1.agg;
+        v.g_log2 = P.q1.g_log2;
+        v.step0 = 0;
+        v.grouped = P.q1.grouped != 0;
+    } else {
+        const ShQueryC& c = ((const ShQueryC*)s_qc)[q];
+        v.row_lo = c.row_lo;
+        v.row_hi = c.row_hi;
+        v.g_keys = c.g_keys;
+        v.g_sums = c.g_sums;
+        v.n_steps = c.n_steps;
+        v.agg = c.agg;
+        v.g_log2 = c.g_log2;
+        v.step0 = c.step0;
+        v.grouped = c.grouped != 0;
+    }
+    return v;
+}
+template <bool SINGLE>
+__device__ __forceinline__ SView sh_sv(const ShParams& P, const uint8_t* s_qc, const QView& Q, uint32_t s) {
+    SView v;
+    if constexpr (SINGLE) {
+        const ShStep& t = P.q1.steps[s];
+        v.lo = t.lo;
+        v.hi = t.hi;
+        v.dbase = t.digit_base;
+        v.ht = t.ht;
+        v.dcard = t.digit_card;
+        v.col = t.col;
+        v.flags = t.flags;
+        v.htlog = t.ht_log2;
+        v.htlay = t.ht_layout;
+    } else {
+        const ShStepC& t = ((const ShStepC*)(s_qc + sizeof(ShQueryC) * P.n_queries))[Q.step0 + s];
+        v.lo = t.lo;
+        v.hi = t.hi;
+        v.dbase = t.dbase;
+        v.ht = t.ht;
+        v.dcard = t.dcard;
+        v.col = t.col;
+        v.flags = t.flags;
+        v.htlog = t.htlog;
+        v.htlay = t.htlay;
+    }
+    return v;
+}
 
 // Query q and column c: in the parameters themselves for a one-query launch
 // (SINGLE: constant-bank reads), else in global memory.
@@ -208,6 +300,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
     uint8_t* stage = (uint8_t*)(colbuf + (size_t)P.n_cols * kShColWords);
     unsigned long long* s_part = (unsigned long long*)(stage + C::kStage);
     uint32_t* s_qmask = (uint32_t*)(s_part + P.n_queries);
+    uint8_t* s_qc = (uint8_t*)(((uintptr_t)(s_qmask + P.mask_words) + 15) & ~(uintptr_t)15);
 
     __shared__ __align__(8) uint64_t s_mbar;
     __shared__ uint32_t s_item;
@@ -220,6 +313,8 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (uint32_t i = tid; i < P.n_queries; i += NT) s_part[i] = 0;
+    if (!SINGLE)
+        for (uint32_t i = tid; i < P.qc_bytes / 16; i += NT) ((uint4*)s_qc)[i] = __ldg(P.qc + i);
     if (tid == 0) {
         s_err = 0;
         s_fatal = 0;
@@ -252,7 +347,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
             while (m) {
                 const uint32_t bit = __ffs(m) - 1;
                 m &= m - 1;
-                const ShQuery& Q = sh_q<SINGLE>(P, w * 32 + bit);
+                const QView Q = sh_qv<SINGLE>(P, s_qc, w * 32 + bit);
                 if (!(Q.row_lo < g0 + n && Q.row_hi > g0)) keepm &= ~(1u << bit);
             }
             s_qmask[w] = keepm;
@@ -265,7 +360,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
             while (m && !dropped) {
                 const uint32_t q = w * 32 + (__ffs(m) - 1);
                 m &= m - 1;
-                const ShQuery& Q = sh_q<SINGLE>(P, q);
+                const QView Q = sh_qv<SINGLE>(P, s_qc, q);
                 const uint32_t a = Q.row_lo > g0 ? (uint32_t)(Q.row_lo - g0) : 0u;
                 const uint32_t b = Q.row_hi < g0 + n ? (uint32_t)(Q.row_hi - g0) : n;
                 if (tid == 0) local_rows += b - a;
@@ -283,8 +378,8 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                 }
                 int64_t local = 0;
                 for (uint32_t s = 0; s < ns; ++s) {
-                    const ShStep& st = Q.steps[s];
-                    const uint32_t c = st.col, flags = st.flags, dcard = st.digit_card;
+                    const SView st = sh_sv<SINGLE>(P, s_qc, Q, s);
+                    const uint32_t c = st.col, flags = st.flags, dcard = st.dcard;
                     if (!((decoded >> c) & 1u)) {
                         // the query's rows are all dead: skip its remaining steps (and this decode)
                         if (s > 0 && !__syncthreads_or(keep != 0)) break;
@@ -295,9 +390,9 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                         }
                         decoded |= 1u << c;
                     }
-                    const int32_t lo = st.lo, hi = st.hi, dbase = st.digit_base;
+                    const int32_t lo = st.lo, hi = st.hi, dbase = st.dbase;
                     const uint64_t* const ht = st.ht;
-                    const uint32_t htlog = st.ht_log2, htlay = st.ht_layout;
+                    const uint32_t htlog = st.htlog, htlay = st.htlay;
                     const uint32_t* const col = colbuf + c * kShColWords;
                     const uint32_t sh = s_sh[c], pd = s_pd[c];
                     const bool last = s + 1 == ns;
@@ -368,7 +463,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                                                   : agg == GX_AGG_COUNT        ? 1
                                                                                : (int64_t)v;
                                 if (!grouped) local += val;
-                                else sh_group_add(k, gk[i], val, Q.g_keys, Q.g_sums, Q.g_log2);
+                                else if (__any_sync(0xFFFFFFFFu, k)) sh_group_add(k, gk[i], val, Q.g_keys, Q.g_sums, Q.g_log2);
                             }
                         }
                     }
