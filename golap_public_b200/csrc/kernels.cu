@@ -305,7 +305,11 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
             // (few sequences; conflict-free 32-word copies), else spread the
             // segments over all NT threads
             const bool literal_tile = (uint64_t)(hi - lo) * 8 >= (uint64_t)n * 4 * 7;
-            const uint32_t glog = literal_tile ? 5u : seg_group_log2(nseg, NT), G = 1u << glog;
+            // padding (nseg << glog words, or nseg for whole-warp groups) must fit the
+            // 256 words every decode buffer reserves beyond its rows
+            uint32_t glog = literal_tile ? 5u : seg_group_log2(nseg, NT);
+            while (glog > 0 && glog < 5 && (nseg << glog) > 256u) --glog;
+            const uint32_t G = 1u << glog;
             // pad words after each segment: G (groups of a warp on distinct
             // banks), 1 for a whole-warp group (its stores are contiguous)
             const uint32_t pl = glog == 5 ? 0u : glog;

@@ -109,3 +109,26 @@ def test_shared_form_eligibility(table, cuda):
     with pytest.raises(GxError) as e:
         api.Batch([(p, 0, 1000)], "shared")
     assert e.value.status == L.GX_ERR_INVALID and "VALUE" in str(e.value)
+
+
+@pytest.mark.parametrize("threads", [256, 512, 1024])
+def test_shared_small_blocks_many_segments(cuda, threads):
+    # 4096-row blocks of 128 segments (32 rows each) with fixed 4-byte matches:
+    # many short, match-heavy segments per tile on every CTA size
+    rng = np.random.default_rng(threads)
+    n = 1_000_000
+    a = rng.integers(0, 4, n, dtype=np.int32)
+    v = rng.integers(0, 6, n, dtype=np.int32)
+    ca = api.Column(a, "lz4", rows_per_chunk=65_536, rows_per_block=4096, lz4_segments=128, lz4_min_match=4)
+    cv = api.Column(v, "lz4", rows_per_chunk=65_536, rows_per_block=4096, lz4_segments=128, lz4_min_match=4)
+    for c in (ca, cv):
+        c.to_device("hbm")
+    res = [cuda.zeros(1, dtype=cuda.int64, device="cuda") for _ in range(3)]
+    slices = [(0, n), (12_345, 700_001), (500_000, 500_100)]
+    plans = [api.ScanPlan(agg=L.GX_AGG_SUM, result=r).filter(ca, 1, 2).value(cv) for r in res]
+    b = api.Batch([(p, lo, hi) for p, (lo, hi) in zip(plans, slices)], "shared").set_launch(threads)
+    b.run()
+    api.scan_check()
+    for r, (lo, hi) in zip(res, slices):
+        m = (a[lo:hi] >= 1) & (a[lo:hi] <= 2)
+        assert int(r.item()) == int(v[lo:hi][m].astype(np.int64).sum())
