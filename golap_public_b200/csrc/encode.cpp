@@ -159,15 +159,17 @@ size_t lz4_encode_block(const int32_t* vals, uint32_t W, uint32_t S, uint32_t se
 }
 
 // Decode-cost-aware policy (lz4_min_match = 0): the block is encoded with
-// minimum matches of 1, 2 and 4 words and the encoding with the lowest
-// bytes + kSeqCost * sequences is kept.  A sequence costs the GPU decoder a
-// serial header parse, worth about kSeqCost bytes of streaming: short
-// matches that save a byte or two each are not worth their parse, long
-// matches (runs, repeated stretches) are.
+// minimum matches of 1, 2 and 4 words and with no matches at all, and the
+// encoding with the lowest bytes + kSeqCost * sequences (+ kMatchCost when it
+// has any match) is kept.  A sequence costs the GPU decoder a serial header
+// parse, worth about kSeqCost bytes of streaming, and a block of literals
+// only decodes as a flat copy, several times faster than parsing: short
+// matches that save a byte or two each are not worth it, long matches (runs,
+// repeated stretches) are.
 size_t lz4_encode_block_auto(const int32_t* vals, uint32_t W, uint32_t S, uint32_t seg_rows, uint32_t depth,
                              std::vector<uint8_t>& out, uint32_t* seg) {
-    constexpr uint64_t kSeqCost = 24;
-    const uint32_t cands[3] = {4, 8, 16};
+    constexpr uint64_t kSeqCost = 24, kMatchCost = 2048;
+    const uint32_t cands[4] = {4, 8, 16, 0xFFFFFFF0u};  // the last admits no match
     std::vector<uint8_t> best_buf, tmp;
     std::vector<uint32_t> best_seg(2 * (size_t)S), tmp_seg(2 * (size_t)S);
     uint64_t best_cost = UINT64_MAX;
@@ -175,7 +177,7 @@ size_t lz4_encode_block_auto(const int32_t* vals, uint32_t W, uint32_t S, uint32
         tmp.clear();
         uint32_t ns = 0;
         const size_t used = lz4_encode_block(vals, W, S, seg_rows, mm, depth, tmp, tmp_seg.data(), &ns);
-        const uint64_t cost = used + kSeqCost * ns;
+        const uint64_t cost = used + kSeqCost * ns + (ns > 1 ? kMatchCost : 0);
         if (cost < best_cost) {
             best_cost = cost;
             best_buf.swap(tmp);

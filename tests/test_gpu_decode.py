@@ -107,11 +107,15 @@ def _corrupt_payload(col, offset, value):
 
 @pytest.mark.parametrize("codec,S", [("lz4", 32), ("lz4", 1), ("cascaded", 1)])
 def test_corrupt_blocks_are_reported(cuda, codec, S):
+    # fixed 4-byte matches: a token-heavy LZ4 stream (with the default policy
+    # these values encode as one literal run, whose last token's match nibble
+    # no decoder reads)
+    kw = {"lz4_min_match": 4} if codec == "lz4" else {}
     v = np.random.default_rng(2).integers(0, 11, 300_000, dtype=np.int32)
     rng = np.random.default_rng(9)
     reported = 0
     for trial in range(12):
-        col = api.Column(v, codec, lz4_segments=S)
+        col = api.Column(v, codec, lz4_segments=S, **kw)
         blocks = col.blocks()
         b = blocks[trial % len(blocks)]
         off = int(b[0]) + int(rng.integers(0, int(b[2])))
@@ -128,7 +132,7 @@ def test_corrupt_blocks_are_reported(cuda, codec, S):
             reported += 1
     # a flip inside packed values or literals legitimately decodes to other
     # values; a broken header / token stream must be reported
-    col = api.Column(v, codec, lz4_segments=S)
+    col = api.Column(v, codec, lz4_segments=S, **kw)
     first = int(col.blocks()[0][0])
     _corrupt_payload(col, first + (1 if codec == "cascaded" else 0), 0xFF)  # n_runs / first token
     col.to_device()
