@@ -434,44 +434,14 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                             int32_t v = k ? (int32_t)col[sh_col_index(r, sh, pd)] : 0;
                             if (filt) k = k && v >= lo && v <= hi;
                             int32_t p = v;
-                            if (flags & GX_STEP_PROBE) {
-                                // rows whose key misses the thread's memo need a probe; in a
-                                // one-query launch, when all such lanes of the warp share one key
-                                // (sorted or run-length columns), one lane probes for the warp,
-                                // which keeps a whole wave of CTAs from hammering the same table
-                                // lines at once
-                                const bool need = k && v != mv;
-                                const uint32_t nb = SINGLE ? __ballot_sync(0xFFFFFFFFu, need) : 0u;
-                                if (!SINGLE) {
-                                    if (need) {
-                                        mp = v;
-                                        mk = sh_probe(ht, htlog, htlay, v, &mp);
-                                        mv = v;
-                                    }
-                                } else if (nb) {
-                                    const int src = __ffs(nb) - 1;
-                                    const int32_t v0 = __shfl_sync(0xFFFFFFFFu, v, src);
-                                    if (__all_sync(0xFFFFFFFFu, !need || v == v0)) {
-                                        int32_t p0 = v0;
-                                        bool f0 = false;
-                                        if ((int)lane == src) f0 = sh_probe(ht, htlog, htlay, v0, &p0);
-                                        f0 = __shfl_sync(0xFFFFFFFFu, f0, src);
-                                        p0 = __shfl_sync(0xFFFFFFFFu, p0, src);
-                                        if (need) {
-                                            mv = v;
-                                            mk = f0;
-                                            mp = p0;
-                                        }
-                                    } else if (need) {
-                                        mp = v;
-                                        mk = sh_probe(ht, htlog, htlay, v, &mp);
-                                        mv = v;
-                                    }
+                            if ((flags & GX_STEP_PROBE) && k) {
+                                if (v != mv) {
+                                    mp = v;
+                                    mk = sh_probe(ht, htlog, htlay, v, &mp);
+                                    mv = v;
                                 }
-                                if (k) {
-                                    k = mk;
-                                    p = mp;
-                                }
+                                k = mk;
+                                p = mp;
                             }
                             if ((keep >> i) & 1u) {  // alive on entry: digits, carry, and the new alive bit
                                 if (dcard && k) {
