@@ -384,8 +384,7 @@ def batched_section(t, n_queries=256, seed=7, choices=None):
     for s, b in zip(specs, singles["shared"]):
         b.set_launch(**autotune.choose(choices, [s.template]))
     batch = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs])
-    launch = autotune.choose(choices, [s.template for s in specs])
-    batch.set_launch(**launch)
+    launch = autotune.tune_launch(batch)  # the launch shape measured on this batch
     stream = torch.cuda.current_stream()
     single_mode = "queue"
 
@@ -449,8 +448,8 @@ def serving_section(t, rates=(200, 1000, 2000), seconds=2.0, seed=9, max_backlog
     rng = np.random.default_rng(seed)
     pool = workload.random_queries(t, 384, rng, min_rows=t.n_rows, max_rows=t.n_rows,
                                    ht_layout=autotune.layouts(choices))
-    threads = autotune.choose(choices, [s.template for s in pool])["threads"]
-    out = {"batch_threads": threads}
+    threads = 0  # automatic launch shape per served batch (most resident warps for its footprint)
+    out = {"batch_threads": "automatic"}
     for mode, (inflight, maxb) in (("batched", (4, 64)), ("one_at_a_time", (1, 1))):
         res = {}
         for rate in rates:

@@ -127,6 +127,7 @@ _SIGS = {
     "gx_batch_create2": (C.c_int32, [C.POINTER(Query), C.c_uint32, C.c_uint32, C.POINTER(P)]),
     "gx_batch_mode": (C.c_int32, [P, C.POINTER(C.c_uint32)]),
     "gx_batch_set_launch": (C.c_int32, [P, C.c_uint32, C.c_uint32]),
+    "gx_batch_launch_get": (C.c_int32, [P, C.POINTER(C.c_uint32)]),
     "gx_batch_free": (C.c_int32, [P]),
     "gx_batch_run": (C.c_int32, [P, P]),
     "gx_batch_graph": (C.c_int32, [P, P]),

@@ -338,9 +338,16 @@ class Batch:
         check(L.lib().gx_batch_create2(arr, len(queries), self.MODES[mode], C.byref(h)))
         self.handle = h
 
-    def set_launch(self, threads: int = 256, ctas_per_sm: int = 0) -> "Batch":
+    def set_launch(self, threads: int = 0, ctas_per_sm: int = 0) -> "Batch":
+        """threads 0 = automatic (most resident warps for the batch's shared memory)."""
         check(L.lib().gx_batch_set_launch(self.handle, threads, ctas_per_sm))
         return self
+
+    @property
+    def threads(self) -> int:
+        t = C.c_uint32()
+        check(L.lib().gx_batch_launch_get(self.handle, C.byref(t)))
+        return t.value
 
     @property
     def mode(self) -> str:

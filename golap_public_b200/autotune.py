@@ -163,6 +163,24 @@ def choose(choices: dict, templates) -> dict:
     return {"threads": choices.get(top, DEFAULT)["threads"]}
 
 
+def tune_launch(batch: api.Batch, candidates=(0, 256, 512, 1024), reps: int = 3) -> dict:
+    """Launch shape for one concrete batch: times a graph replay of the batch
+    at each candidate CTA size (0 = the library's automatic choice) and keeps
+    the fastest.  Per-template tuning picks chunk size and table layout; the
+    launch shape of a mixed batch depends on its own shared-memory footprint
+    (columns, queries), so it is measured on the batch itself."""
+    best = None
+    times = {}
+    for nt in candidates:
+        batch.set_launch(nt)
+        ms = _time_graph(batch, reps)
+        times[nt if nt else f"auto({batch.threads})"] = ms
+        if best is None or ms < best[1]:
+            best = (nt, ms)
+    batch.set_launch(best[0])
+    return {"threads": batch.threads, "requested": best[0], "ms": best[1], "times_ms": times}
+
+
 def layouts(choices: dict) -> dict:
     """{template: ht_layout} for workload.random_queries."""
     return {t: c["ht_layout"] for t, c in choices.items()}

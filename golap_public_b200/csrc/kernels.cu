@@ -1020,12 +1020,40 @@ struct gx_batch {
     uint8_t* d_qc = nullptr;       // compact descriptors (device) and pinned staging
     uint8_t* h_qc = nullptr;
     size_t cap_qc = 0;
-    uint32_t sh_threads = kShNT;   // launch shape of the shared form (tunable)
+    uint32_t sh_threads = kShNT;   // launch shape of the shared form in use
+    uint32_t sh_threads_req = 0;   // requested threads per CTA (0 = automatic)
     uint32_t sh_ctas_per_sm = 0;   // 0 = as many as fit
 };
 
-// Persistent grid of the shared form for the batch's thread count.
+static int shared_occupancy(uint32_t threads, size_t smem) {
+    int per_sm = 0;
+    switch (threads) {
+        case 128: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shared_scan_kernel<128, 4>, 128, smem); break;
+        case 512: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shared_scan_kernel<512, 1>, 512, smem); break;
+        case 1024: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shared_scan_kernel<1024, 1>, 1024, smem); break;
+        default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shared_scan_kernel<256, 2>, 256, smem); break;
+    }
+    return per_sm;
+}
+
+// Persistent grid of the shared form for the batch's thread count.  An
+// automatic shape (sh_threads_req 0) takes the CTA size with the most
+// resident warps per SM for the batch's shared memory (larger CTAs on ties).
 static void shared_geometry(gx_batch* b) {
+    if (b->sh_threads_req == 0) {
+        uint32_t best = 1024;
+        int best_warps = -1;
+        for (uint32_t nt : {1024u, 512u, 256u, 128u}) {
+            const int w = shared_occupancy(nt, b->sh_smem) * (int)(nt / 32);
+            if (w > best_warps) {
+                best_warps = w;
+                best = nt;
+            }
+        }
+        b->sh_threads = best;
+    } else {
+        b->sh_threads = b->sh_threads_req;
+    }
     int per_sm = 1;
     switch (b->sh_threads) {
         case 128: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shared_scan_kernel<128, 4>, 128, b->sh_smem); break;
@@ -2054,9 +2082,9 @@ gx_status gx_batch_create(const gx_query* queries, uint32_t n_queries, gx_batch*
 }
 
 gx_status gx_batch_set_launch(gx_batch* b, uint32_t threads, uint32_t ctas_per_sm) {
-    if (!b || (threads != 128 && threads != 256 && threads != 512 && threads != 1024))
-        return set_error(GX_ERR_INVALID, "gx_batch_set_launch: threads must be 128, 256, 512 or 1024");
-    b->sh_threads = threads;
+    if (!b || (threads != 0 && threads != 128 && threads != 256 && threads != 512 && threads != 1024))
+        return set_error(GX_ERR_INVALID, "gx_batch_set_launch: threads must be 0 (automatic), 128, 256, 512 or 1024");
+    b->sh_threads_req = threads;
     b->sh_ctas_per_sm = ctas_per_sm;
     if (b->exec) {
         cudaGraphExecDestroy(b->exec);
@@ -2067,6 +2095,12 @@ gx_status gx_batch_set_launch(gx_batch* b, uint32_t threads, uint32_t ctas_per_s
         b->graph = nullptr;
     }
     if (b->mode == GX_BATCH_SHARED) shared_geometry(b);
+    return GX_OK;
+}
+
+gx_status gx_batch_launch_get(const gx_batch* b, uint32_t* threads) {
+    if (!b || !threads) return set_error(GX_ERR_INVALID, "gx_batch_launch_get: bad args");
+    *threads = b->mode == GX_BATCH_SHARED ? b->sh_threads : 0u;
     return GX_OK;
 }
 

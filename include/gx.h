@@ -328,10 +328,14 @@ enum { GX_BATCH_AUTO = 0, GX_BATCH_QUEUE = 1, GX_BATCH_SHARED = 2 };
 gx_status gx_batch_create2(const gx_query* queries, uint32_t n_queries, uint32_t mode, gx_batch** out);
 /* The form the batch currently runs in (GX_BATCH_QUEUE or GX_BATCH_SHARED). */
 gx_status gx_batch_mode(const gx_batch* b, uint32_t* mode);
-/* Launch shape of the shared form: threads per CTA (128, 256, 512 or 1024;
- * default 256) and a cap on CTAs per SM (0 = as many as fit).  Kept across
- * gx_batch_assign; drops a captured graph.  The autotuner sets it. */
+/* Launch shape of the shared form: threads per CTA (128, 256, 512 or 1024,
+ * or 0 = automatic, the default: the size with the most resident warps for
+ * the batch's shared memory) and a cap on CTAs per SM (0 = as many as fit).
+ * Kept across gx_batch_assign; drops a captured graph.  The autotuner sets
+ * it. */
 gx_status gx_batch_set_launch(gx_batch* b, uint32_t threads, uint32_t ctas_per_sm);
+/* Threads per CTA the shared form currently launches with (0 for QUEUE). */
+gx_status gx_batch_launch_get(const gx_batch* b, uint32_t* threads);
 /* Replace the batch's queries (buffers reused, grown when needed; the
  * descriptor upload is enqueued on `stream`).  Drops a captured graph. */
 gx_status gx_batch_assign(gx_batch* b, const gx_query* queries, uint32_t n_queries, void* stream);

@@ -24,7 +24,7 @@ def test_tune_small_grid(cuda, tmp_path):
     assert set(ch) == set(autotune.TEMPLATES)
 
 
-@pytest.mark.parametrize("threads", [128, 512, 1024])
+@pytest.mark.parametrize("threads", [0, 128, 512, 1024])
 def test_launch_shapes_match_oracle(cuda, threads):
     t = workload.build_table(3_000_000, n_customer=100_000, n_supplier=10_000, rows_per_chunk=262_144,
                              ht_layouts=("bucket",))
@@ -32,10 +32,18 @@ def test_launch_shapes_match_oracle(cuda, threads):
     specs = workload.random_queries(t, 12, rng, min_rows=100_000, max_rows=3_000_000,
                                     ht_layout={"scan": "bucket", "star": "bucket"})
     b = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs], "shared").set_launch(threads)
+    assert b.threads in (128, 256, 512, 1024) and (threads == 0 or b.threads == threads)
     b.graph()
     api.scan_check()
     for s in specs:
         assert workload.read_result(s) == WO.expected(t, s)
+    if threads == 0:  # the per-batch launch tuner keeps results and picks a timed shape
+        got = autotune.tune_launch(b, reps=1)
+        assert got["threads"] == b.threads and got["ms"] == min(got["times_ms"].values())
+        b.graph()
+        api.scan_check()
+        for s in specs:
+            assert workload.read_result(s) == WO.expected(t, s)
     sv = api.Server(max_inflight=2, max_batch=8, batch_threads=threads)
     tickets = [sv.submit(s.plan, s.row_lo, s.row_hi, 64) for s in specs]
     for tk in tickets:
