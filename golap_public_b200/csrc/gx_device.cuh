@@ -594,11 +594,23 @@ __device__ __forceinline__ bool group_add_global(int64_t* keys, int64_t* sums, u
     const uint32_t mask = (1u << log2cap) - 1;
     uint32_t s = hash_key64(key, log2cap);
     for (uint32_t i = 0; i <= mask; ++i) {
-        unsigned long long old = atomicCAS((unsigned long long*)&keys[s], (unsigned long long)kEmptyGroup,
-                                           (unsigned long long)key);
-        if (old == (unsigned long long)kEmptyGroup || old == (unsigned long long)key) {
+        // A slot's key is written once (free -> key) and never changes, so a plain
+        // (possibly cached, possibly stale) read that shows a key is final: the
+        // common case -- the key already there -- costs a read and a fire-and-forget
+        // add, and only a slot that reads free takes the compare-and-swap.
+        long long cur;
+        asm volatile("ld.global.ca.b64 %0, [%1];" : "=l"(cur) : "l"(keys + s));
+        if (cur == (long long)key) {
             atomicAdd((unsigned long long*)&sums[s], (unsigned long long)v);
             return true;
+        }
+        if (cur == (long long)kEmptyGroup) {
+            const unsigned long long old = atomicCAS((unsigned long long*)&keys[s], (unsigned long long)kEmptyGroup,
+                                                     (unsigned long long)key);
+            if (old == (unsigned long long)kEmptyGroup || old == (unsigned long long)key) {
+                atomicAdd((unsigned long long*)&sums[s], (unsigned long long)v);
+                return true;
+            }
         }
         s = (s + 1) & mask;
     }

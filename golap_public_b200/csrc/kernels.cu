@@ -1607,14 +1607,90 @@ static void shared_layout(ShParams& P, const gx_column* c0) {
     P.n_slots = c0->n_slots;
 }
 
-static size_t shared_smem_bytes(uint32_t n_cols, uint32_t n_queries, uint32_t qc_bytes = 0) {
+static size_t shared_smem_bytes(uint32_t n_cols, uint32_t n_queries, uint32_t qc_bytes = 0, uint32_t pst_words = 0,
+                                uint32_t gt_slots = 0) {
+    const bool tail = qc_bytes || pst_words || gt_slots;  // 16-byte aligned region after the query mask
     return 4ull * kShColWords * n_cols + Cfg<kTileRows>::kStage + 8ull * n_queries + 4ull * ((n_queries + 31) / 32) +
-           (qc_bytes ? 16ull + qc_bytes : 0ull);
+           (tail ? 16ull : 0ull) + qc_bytes + 4ull * pst_words + 12ull * gt_slots;
+}
+
+// Prefix groups of a batch.  Queries whose first steps (any but the VALUE
+// step) are identical -- same column, flags, bounds, join table and digits --
+// evaluate those steps once per tile in the shared scan.  shared_group sorts
+// the queries so that equal step sequences sit next to each other (stable:
+// equal ones keep their order; results do not depend on the order, every
+// query carries its own outputs) and marks each run of two or more adjacent
+// queries inside one 32-query mask word; the run shares the shortest common
+// prefix of its neighbours.
+struct ShGroup {
+    uint32_t gbits = 0;
+    uint8_t pfx = 0, psave = 0;
+};
+
+static int sh_step_cmp(const ShStep& x, const ShStep& y) {
+    const uint64_t a[9] = {x.col, x.flags, (uint64_t)(uint32_t)x.lo, (uint64_t)(uint32_t)x.hi, (uint64_t)(uintptr_t)x.ht,
+                           x.ht_log2, x.ht_layout, (uint64_t)(uint32_t)x.digit_base, x.digit_card};
+    const uint64_t b[9] = {y.col, y.flags, (uint64_t)(uint32_t)y.lo, (uint64_t)(uint32_t)y.hi, (uint64_t)(uintptr_t)y.ht,
+                           y.ht_log2, y.ht_layout, (uint64_t)(uint32_t)y.digit_base, y.digit_card};
+    for (int i = 0; i < 9; ++i)
+        if (a[i] != b[i]) return a[i] < b[i] ? -1 : 1;
+    return 0;
+}
+
+static uint32_t sh_common_prefix(const ShQuery& x, const ShQuery& y) {
+    const uint32_t lim = std::min(x.n_steps, y.n_steps) - 1;  // the VALUE step is never shared
+    uint32_t k = 0;
+    while (k < lim && sh_step_cmp(x.steps[k], y.steps[k]) == 0) ++k;
+    return k;
+}
+
+static std::vector<ShGroup> shared_group(std::vector<ShQuery>& sq) {
+    std::stable_sort(sq.begin(), sq.end(), [](const ShQuery& x, const ShQuery& y) {
+        const uint32_t lim = std::min(x.n_steps, y.n_steps) - 1;
+        for (uint32_t k = 0; k < lim; ++k)
+            if (const int c = sh_step_cmp(x.steps[k], y.steps[k])) return c < 0;
+        return x.n_steps < y.n_steps;
+    });
+    std::vector<ShGroup> g(sq.size());
+    size_t i = 0;
+    while (i < sq.size()) {
+        size_t j = i + 1;
+        uint32_t p = ~0u;
+        for (; j < sq.size() && j % 32 != 0; ++j) {
+            const uint32_t l = sh_common_prefix(sq[j - 1], sq[j]);
+            if (l == 0) break;
+            p = std::min(p, l);
+        }
+        if (j - i >= 2) {
+            ShGroup e;
+            e.gbits = (uint32_t)((((1ull << (j - i)) - 1ull) << (i % 32)) & 0xFFFFFFFFull);
+            e.pfx = (uint8_t)p;
+            for (uint32_t k = 0; k < p; ++k) {
+                if (sq[i].steps[k].digit_card) e.psave |= 1;
+                if (sq[i].steps[k].flags & GX_STEP_CARRY) e.psave |= 2;
+            }
+            for (size_t k = i; k < j; ++k) g[k] = e;
+        }
+        i = j;
+    }
+    return g;
+}
+
+// Words of prefix state the batch's groups need (group-key digits, carried
+// values: one word per tile row each) and the offset of the carried values.
+static uint32_t shared_pst_words(const std::vector<ShGroup>& g, uint32_t* carry_off) {
+    bool gk = false, cv = false;
+    for (const ShGroup& e : g) {
+        gk = gk || (e.psave & 1);
+        cv = cv || (e.psave & 2);
+    }
+    *carry_off = gk ? kShTile : 0u;
+    return kShTile * ((gk ? 1u : 0u) + (cv ? 1u : 0u));
 }
 
 // The compact descriptor image of a batch: ShQueryC per query, then ShStepC
 // per step, padded to 16 bytes.
-static std::vector<uint8_t> shared_compact(const std::vector<ShQuery>& sq) {
+static std::vector<uint8_t> shared_compact(const std::vector<ShQuery>& sq, const std::vector<ShGroup>& groups) {
     size_t steps = 0;
     for (const ShQuery& q : sq) steps += q.n_steps;
     const size_t bytes = (sizeof(ShQueryC) * sq.size() + sizeof(ShStepC) * steps + 15) & ~(size_t)15;
@@ -1633,6 +1709,9 @@ static std::vector<uint8_t> shared_compact(const std::vector<ShQuery>& sq) {
         qc[i].agg = (uint8_t)q.agg;
         qc[i].grouped = (uint8_t)q.grouped;
         qc[i].g_log2 = (uint8_t)q.g_log2;
+        qc[i].gbits = groups[i].gbits;
+        qc[i].pfx = groups[i].pfx;
+        qc[i].psave = groups[i].psave;
         for (uint32_t t = 0; t < q.n_steps; ++t, ++k) {
             const ShStep& st = q.steps[t];
             sc[k].lo = st.lo;
@@ -1680,11 +1759,12 @@ static gx_status scan_launch_shared(const gx_scan_plan* plan, const QueryDesc& q
     if (e == cudaSuccess) {
         const unsigned ig = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(8ull * sm_count(), (n_slots + 7) / 8));
         shared_items_kernel<<<ig, 256, 0, s>>>(P, scratch + 2 + n_slots, scratch + 2, scratch);
-        const size_t smem = shared_smem_bytes(P.n_cols, 1);
-        static int occ[64][kShMaxCols + 1] = {};
+        P.gt_slots = P.q1.grouped ? kShGroupSlots : 0u;
+        const size_t smem = shared_smem_bytes(P.n_cols, 1, 0, 0, P.gt_slots);
+        static int occ[64][kShMaxCols + 1][2] = {};
         int dev = 0;
         cudaGetDevice(&dev);
-        int& per_sm = occ[dev & 63][P.n_cols];
+        int& per_sm = occ[dev & 63][P.n_cols][P.gt_slots ? 1 : 0];
         if (per_sm == 0) {
             int v = 1;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, shared_scan_kernel<kShSingleNT, 4, true>, kShSingleNT,
@@ -1884,12 +1964,18 @@ static gx_status shared_prepare(gx_batch* b, const gx_query* queries, uint32_t n
     std::vector<ShQuery> sq(n);
     for (uint32_t i = 0; i < n; ++i)
         if (!shared_query(queries[i].plan, qs[i], cols, sq[i], why)) return GX_OK;
-    const std::vector<uint8_t> img = shared_compact(sq);
+    const std::vector<ShGroup> groups = shared_group(sq);
+    uint32_t pst_carry = 0;
+    const uint32_t pst_words = shared_pst_words(groups, &pst_carry);
+    const std::vector<uint8_t> img = shared_compact(sq, groups);
     if (img.size() > kShMaxQcBytes) {
         *why = "query descriptors above 96 KiB";
         return GX_OK;
     }
-    if (shared_smem_bytes((uint32_t)cols.size(), n, (uint32_t)img.size()) > kShMaxDynSmem) {
+    bool any_grouped = false;
+    for (const ShQuery& q : sq) any_grouped = any_grouped || q.grouped;
+    const uint32_t gt_slots = any_grouped ? kShGroupSlots : 0u;
+    if (shared_smem_bytes((uint32_t)cols.size(), n, (uint32_t)img.size(), pst_words, gt_slots) > kShMaxDynSmem) {
         *why = "columns, queries and descriptors above 220 KiB of shared memory";
         return GX_OK;
     }
@@ -1955,9 +2041,12 @@ static gx_status shared_prepare(gx_batch* b, const gx_query* queries, uint32_t n
     P.rows_scanned = b->d_rows;
     P.qc = (const uint4*)b->d_qc;
     P.qc_bytes = (uint32_t)img.size();
+    P.pst_carry = pst_carry;
+    P.pst_words = pst_words;
+    P.gt_slots = gt_slots;
     b->n_slots = n_slots;
     b->dir0 = c0->d_blocks;
-    b->sh_smem = shared_smem_bytes(P.n_cols, n, P.qc_bytes);
+    b->sh_smem = shared_smem_bytes(P.n_cols, n, P.qc_bytes, pst_words, gt_slots);
     shared_geometry(b);
     b->sh_items_grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(8ull * sm_count(), (n_slots + 7) / 8));
     *ok = true;

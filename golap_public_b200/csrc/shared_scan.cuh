@@ -22,6 +22,9 @@ constexpr uint32_t kShSingleNT = 128;     // one-query launches: 4 CTAs (4 tiles
 constexpr uint32_t kShColWords = kShTile + 256;  // one column buffer (with segment padding)
 constexpr uint32_t kShMaxQcBytes = 96u << 10;     // compact descriptors of a batch held in shared memory
 constexpr uint32_t kShMaxDynSmem = 220u << 10;    // dynamic shared memory of one CTA (static use is ~1.3 KiB)
+constexpr uint32_t kShGroupLog2 = 10;             // CTA group table of grouped queries: 1024 slots (12 KiB)
+constexpr uint32_t kShGroupSlots = 1u << kShGroupLog2;
+constexpr uint32_t kShGroupProbes = 32;
 
 struct ShStep {
     uint32_t flags;
@@ -65,8 +68,12 @@ struct ShQueryC {
     int64_t* g_sums;
     uint32_t step0;  // index of the query's first step in the step array
     uint8_t n_steps, agg, grouped, g_log2;
+    uint32_t gbits;  // mask-word bits of the query's prefix group (0: no group)
+    uint8_t pfx;     // steps the group shares (fewer than any member's step count)
+    uint8_t psave;   // what the shared prefix hands on: bit 0 group-key digits, bit 1 carried value
+    uint8_t pad[2];
 };
-static_assert(sizeof(ShStepC) == 32 && sizeof(ShQueryC) == 40, "compact descriptor sizes");
+static_assert(sizeof(ShStepC) == 32 && sizeof(ShQueryC) == 48, "compact descriptor sizes");
 
 struct ShParams {
     const gx_dcol* cols;        // the batch's column table (global memory)
@@ -85,6 +92,9 @@ struct ShParams {
     uint32_t qc_bytes;          // size of that image (a multiple of 16)
     const gx_dblock* dir;       // directory of the table (any of its columns)
     uint32_t n_slots;
+    uint32_t pst_carry;         // offset of the carried values in the prefix-state buffer (words)
+    uint32_t pst_words;         // size of the prefix-state buffer (words)
+    uint32_t gt_slots;          // CTA group-table slots (kShGroupSlots with grouped queries, else 0)
     // one query carried in the parameters themselves (qs and cols null)
     ShQuery q1;
     gx_dcol cols1[kShMaxCols];
@@ -99,6 +109,7 @@ struct QView {
     int64_t* g_keys;
     int64_t* g_sums;
     uint32_t n_steps, agg, g_log2, step0;
+    uint32_t gbits, pfx, psave;
     bool grouped;
 };
 struct SView {
@@ -118,6 +129,9 @@ __device__ __forceinline__ QView sh_qv(const ShParams& P, const uint8_t* s_qc, u
         v.agg = P.q1.agg;
         v.g_log2 = P.q1.g_log2;
         v.step0 = 0;
+        v.gbits = 0;
+        v.pfx = 0;
+        v.psave = 0;
         v.grouped = P.q1.grouped != 0;
     } else {
         const ShQueryC& c = ((const ShQueryC*)s_qc)[q];
@@ -129,6 +143,9 @@ __device__ __forceinline__ QView sh_qv(const ShParams& P, const uint8_t* s_qc, u
         v.agg = c.agg;
         v.g_log2 = c.g_log2;
         v.step0 = c.step0;
+        v.gbits = c.gbits;
+        v.pfx = c.pfx;
+        v.psave = c.psave;
         v.grouped = c.grouped != 0;
     }
     return v;
@@ -222,22 +239,44 @@ __device__ __noinline__ bool sh_probe(const uint64_t* ht, uint32_t htlog, uint32
     return ht_probe_any(ht, htlog, htlay, v, p);
 }
 
-// Warp-aggregated add of (gk, val) for the lanes with k set into the global
-// group table.  All 32 lanes call it.
-__device__ __noinline__ void sh_group_add(bool k, uint32_t gk, int64_t val, int64_t* keys, int64_t* sums,
-                                          uint32_t log2cap) {
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t active = __ballot_sync(0xFFFFFFFFu, k);
-    while (active) {
-        const int leader = __ffs(active) - 1;
-        const uint32_t lk = __shfl_sync(0xFFFFFFFFu, gk, leader);
-        const bool peer = k && gk == lk && ((active >> lane) & 1u);
-        const uint32_t peers = __ballot_sync(0xFFFFFFFFu, peer);
-        const uint64_t tot = warp_sum_u64(peer ? (uint64_t)val : 0ull);
-        if ((int)lane == leader && !group_add_global(keys, sums, log2cap, (int64_t)lk, (int64_t)tot))
-            raise_error(kErrCapacity);
-        active &= ~peers;
+// Add of (gk, val) to the CTA's group table in shared memory (the partial
+// sums of one query over one tile; flushed to the query's global table when
+// its tile is done), so that keys repeated within a tile -- skewed group-bys
+// -- cost one global update per tile.  A key that finds no slot within
+// kShGroupProbes goes to the global table directly.
+__device__ __noinline__ void sh_group_add(uint32_t gk, int64_t val, unsigned long long* tsum, int64_t* keys,
+                                          int64_t* sums, uint32_t log2cap) {
+    uint32_t* const tkey = (uint32_t*)(tsum + kShGroupSlots);
+    if (gk != kEmptyGKey) {
+        uint32_t s = hash_key32((int32_t)gk, kShGroupLog2);
+        for (uint32_t i = 0; i < kShGroupProbes; ++i) {
+            uint32_t cur = ((volatile uint32_t*)tkey)[s];
+            if (cur == kEmptyGKey) cur = atomicCAS(&tkey[s], kEmptyGKey, gk);
+            if (cur == kEmptyGKey || cur == gk) {
+                atomicAdd(&tsum[s], (unsigned long long)val);
+                return;
+            }
+            s = (s + 1) & (kShGroupSlots - 1);
+        }
     }
+    if (!group_add_global(keys, sums, log2cap, (int64_t)gk, val)) raise_error(kErrCapacity);
+}
+
+// Flush of the CTA's group table into the query's global table (all NT
+// threads, between barriers); leaves the table empty.
+template <int NT>
+__device__ __forceinline__ void sh_group_flush(unsigned long long* tsum, uint32_t* tkey, int64_t* keys, int64_t* sums,
+                                               uint32_t log2cap) {
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < kShGroupSlots; j += NT) {
+        const uint32_t key = tkey[j];
+        if (key != kEmptyGKey) {
+            if (!group_add_global(keys, sums, log2cap, (int64_t)key, (int64_t)tsum[j])) raise_error(kErrCapacity);
+            tkey[j] = kEmptyGKey;
+            tsum[j] = 0;
+        }
+    }
+    __syncthreads();
 }
 
 __device__ __forceinline__ uint32_t sh_col_index(uint32_t r, uint32_t sh, uint32_t pd) {
@@ -288,8 +327,13 @@ __device__ __forceinline__ int shared_decode(const gx_dcol& col, uint32_t c, uin
 // serves every later query of the tile; before decoding for a query whose
 // rows are all dead, the query stops (a block-wide vote), so dead tiles cost
 // only the columns their first steps read.
+// Queries whose first steps are identical (star joins over one dimension
+// selection, say) form prefix groups: per tile, those steps run once over
+// the union of the active members' rows and each member starts after them.
 // Dynamic shared memory: n_cols column buffers | stage | per-query partial
-// sums | per-tile active-query mask.
+// sums | per-tile active-query mask | descriptors | prefix state (group-key
+// digits and carried values of the shared steps, one word per tile row) |
+// CTA group table (sums, then keys).
 template <int NT, int MINB, bool SINGLE = false>
 __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_constant__ ShParams P) {
     constexpr int NW = NT / 32;
@@ -313,6 +357,13 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (uint32_t i = tid; i < P.n_queries; i += NT) s_part[i] = 0;
+    // CTA group table (present when the launch has grouped queries)
+    unsigned long long* const s_gsum = (unsigned long long*)(s_qc + P.qc_bytes + 4ull * P.pst_words);
+    uint32_t* const s_gkey = (uint32_t*)(s_gsum + P.gt_slots);
+    for (uint32_t i = tid; i < P.gt_slots; i += NT) {
+        s_gsum[i] = 0;
+        s_gkey[i] = kEmptyGKey;
+    }
     if (!SINGLE)
         for (uint32_t i = tid; i < P.qc_bytes / 16; i += NT) ((uint4*)s_qc)[i] = __ldg(P.qc + i);
     if (tid == 0) {
@@ -353,6 +404,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
             s_qmask[w] = keepm;
         }
         __syncthreads();
+        uint32_t* const s_pst = (uint32_t*)(s_qc + P.qc_bytes);  // prefix-state buffer (batches)
         uint32_t decoded = 0;  // columns of this tile already in their buffers
         bool dropped = false;
         for (uint32_t w = 0; w < MW && !dropped; ++w) {
@@ -360,11 +412,40 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
             while (m && !dropped) {
                 const uint32_t q = w * 32 + (__ffs(m) - 1);
                 m &= m - 1;
-                const QView Q = sh_qv<SINGLE>(P, s_qc, q);
-                const uint32_t a = Q.row_lo > g0 ? (uint32_t)(Q.row_lo - g0) : 0u;
-                const uint32_t b = Q.row_hi < g0 + n ? (uint32_t)(Q.row_hi - g0) : n;
-                if (tid == 0) local_rows += b - a;
-                const uint32_t ns = Q.n_steps, agg = Q.agg;
+                // The other members of q's prefix group that are active in this tile
+                // (the host orders a batch so that a group sits in one mask word).  With
+                // any, a first pass runs the shared steps once over the union of the
+                // members' rows, and each member then starts from its result.
+                const QView Qg = sh_qv<SINGLE>(P, s_qc, q);
+                const uint32_t gm = m & Qg.gbits, pfx = Qg.pfx, psave = Qg.psave;
+                m &= ~gm;
+                uint32_t ua = Qg.row_lo > g0 ? (uint32_t)(Qg.row_lo - g0) : 0u;
+                uint32_t ub = Qg.row_hi < g0 + n ? (uint32_t)(Qg.row_hi - g0) : n;
+                if (gm) {
+                    uint32_t rows_g = ub - ua;
+                    for (uint32_t r2 = gm; r2; r2 &= r2 - 1) {
+                        const QView Qm = sh_qv<SINGLE>(P, s_qc, w * 32 + (__ffs(r2) - 1));
+                        const uint32_t a2 = Qm.row_lo > g0 ? (uint32_t)(Qm.row_lo - g0) : 0u;
+                        const uint32_t b2 = Qm.row_hi < g0 + n ? (uint32_t)(Qm.row_hi - g0) : n;
+                        rows_g += b2 - a2;
+                        ua = min(ua, a2);
+                        ub = max(ub, b2);
+                    }
+                    if (tid == 0) local_rows += rows_g;
+                }
+                bool pre = gm != 0;      // the pass over the shared steps
+                uint32_t keep_pre = 0;   // its surviving rows
+                uint32_t rest = gm, cq = q;
+                while (true) {
+                const QView Q = sh_qv<SINGLE>(P, s_qc, cq);
+                uint32_t a = ua, b = ub;
+                if (!pre) {
+                    a = Q.row_lo > g0 ? (uint32_t)(Q.row_lo - g0) : 0u;
+                    b = Q.row_hi < g0 + n ? (uint32_t)(Q.row_hi - g0) : n;
+                    if (tid == 0 && !gm) local_rows += b - a;
+                }
+                const uint32_t s_begin = gm && !pre ? pfx : 0u, ns = pre ? pfx : Q.n_steps, agg = Q.agg;
+                const bool from_pre = gm && !pre;
                 const bool grouped = Q.grouped != 0;
                 uint32_t keep = 0;  // bit i: row of group i alive
                 uint32_t gk[RPT];
@@ -372,12 +453,12 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
 #pragma unroll
                 for (int i = 0; i < RPT; ++i) {
                     const uint32_t r = (i * NW + warp) * 32 + lane;
-                    if (r >= a && r < b) keep |= 1u << i;
-                    gk[i] = 0;
-                    carry[i] = 0;
+                    if (r >= a && r < b && (!from_pre || ((keep_pre >> i) & 1u))) keep |= 1u << i;
+                    gk[i] = from_pre && (psave & 1u) ? s_pst[r] : 0u;
+                    carry[i] = from_pre && (psave & 2u) ? (int32_t)s_pst[P.pst_carry + r] : 0;
                 }
                 int64_t local = 0;
-                for (uint32_t s = 0; s < ns; ++s) {
+                for (uint32_t s = s_begin; s < ns; ++s) {
                     const SView st = sh_sv<SINGLE>(P, s_qc, Q, s);
                     const uint32_t c = st.col, flags = st.flags, dcard = st.dcard;
                     if (!((decoded >> c) & 1u)) {
@@ -395,7 +476,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                     const uint32_t htlog = st.htlog, htlay = st.htlay;
                     const uint32_t* const col = colbuf + c * kShColWords;
                     const uint32_t sh = s_sh[c], pd = s_pd[c];
-                    const bool last = s + 1 == ns;
+                    const bool last = s + 1 == Q.n_steps;  // never within the shared steps
                     const bool simple = !(flags & GX_STEP_PROBE) && dcard == 0;  // no probe, no digit
                     const bool filt = (flags & GX_STEP_FILTER) != 0, carry_step = (flags & GX_STEP_CARRY) != 0;
                     if (simple && !last) {
@@ -462,17 +543,41 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                                                   : agg == GX_AGG_COUNT        ? 1
                                                                                : (int64_t)v;
                                 if (!grouped) local += val;
-                                else if (__any_sync(0xFFFFFFFFu, k)) sh_group_add(k, gk[i], val, Q.g_keys, Q.g_sums, Q.g_log2);
+                                else if (k) {
+                                    const QView Qa = sh_qv<SINGLE>(P, s_qc, cq);  // re-read: not kept live
+                                    sh_group_add(gk[i], val, s_gsum, Qa.g_keys, Qa.g_sums, Qa.g_log2);
+                                }
                             }
                         }
                     }
+                }
+                if (pre) {
+                    // hand the shared steps' result to the members (each thread keeps its own rows)
+#pragma unroll
+                    for (int i = 0; i < RPT; ++i) {
+                        const uint32_t r = (i * NW + warp) * 32 + lane;
+                        if (psave & 1u) s_pst[r] = gk[i];
+                        if (psave & 2u) s_pst[P.pst_carry + r] = (uint32_t)carry[i];
+                    }
+                    keep_pre = keep;
+                    if (dropped || !__syncthreads_or(keep != 0)) break;  // no member has a live row
+                    pre = false;
+                    continue;
+                }
+                if (grouped) {
+                    const QView Qa = sh_qv<SINGLE>(P, s_qc, cq);
+                    sh_group_flush<NT>(s_gsum, s_gkey, Qa.g_keys, Qa.g_sums, Qa.g_log2);
                 }
                 if (!grouped && !dropped) {
                     unsigned long long u = (unsigned long long)local;
 #pragma unroll
                     for (int d = 16; d > 0; d >>= 1) u += __shfl_down_sync(0xFFFFFFFFu, u, d);
-                    if (lane == 0 && u) atomicAdd(&s_part[q], u);
+                    if (lane == 0 && u) atomicAdd(&s_part[cq], u);
                 }
+                if (dropped || !rest) break;
+                cq = w * 32 + (__ffs(rest) - 1);
+                rest &= rest - 1;
+                }  // jobs of the group
             }
         }
         }  // r0 < rows

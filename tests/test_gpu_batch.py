@@ -132,3 +132,59 @@ def test_shared_small_blocks_many_segments(cuda, threads):
     for r, (lo, hi) in zip(res, slices):
         m = (a[lo:hi] >= 1) & (a[lo:hi] <= 2)
         assert int(r.item()) == int(v[lo:hi][m].astype(np.int64).sum())
+
+
+class _FixedDraws:
+    """Stands in for the generator of workload.make_query: fixed draws, so
+    that many queries share their first steps."""
+
+    def __init__(self, ints, u=0.9):
+        self.ints = iter(ints)
+        self.u = u
+
+    def random(self):
+        return self.u
+
+    def integers(self, lo, hi=None):
+        return next(self.ints)
+
+
+def test_shared_prefix_groups(table):
+    # 40 scans with one date range and one discount filter (two shared steps,
+    # the second carries the discount), 40 star joins over one region (two
+    # shared probes with group-key digits), then random queries; more than
+    # two mask words of queries, so some groups are split at a word boundary.
+    # Slices include short ones inside one tile with gaps between them.
+    rng = np.random.default_rng(21)
+    n = table.n_rows
+    specs = []
+    for i in range(40):
+        lo = int(rng.integers(0, n - 1))
+        hi = lo + (int(rng.integers(1, 3000)) if i % 3 == 0 else int(rng.integers(1, n - lo + 1)))
+        specs.append(workload.make_query(table, "scan", _FixedDraws([1994, 3, int(rng.integers(1, 42))]), lo, min(hi, n)))
+    for i in range(40):
+        if i % 4 == 1:  # 200-row slices at a few places: several per tile, with gaps
+            lo = 4096 * (10, 500, 1200)[i % 3] + 1000 + 300 * (i % 5)
+            hi = lo + 200
+        else:
+            lo = 4096 * int(rng.integers(0, n // 4096)) + (0 if i % 2 else 1000 + 300 * (i % 5))
+            hi = lo + int(rng.integers(1, n - lo + 1))
+        y1 = int(rng.integers(1992, 1999))
+        specs.append(workload.make_query(table, "star", _FixedDraws([1, y1, int(rng.integers(y1, 1999))]), lo, min(hi, n)))
+    specs += workload.random_queries(table, 20, rng, min_rows=1000, max_rows=n)
+    order = rng.permutation(len(specs))
+    specs = [specs[i] for i in order]
+    got = {}
+    for mode in MODES:
+        b = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs], mode)
+        assert b.mode == mode
+        b.run()
+        api.scan_check()
+        first = [workload.read_result(s) for s in specs]
+        b.graph()
+        b.graph()
+        api.scan_check()
+        got[mode] = (b.rows(), [workload.read_result(s) for s in specs])
+        assert got[mode][1] == first
+    assert got["queue"] == got["shared"]
+    _check(table, specs)
