@@ -1712,6 +1712,7 @@ static std::vector<uint8_t> shared_compact(const std::vector<ShQuery>& sq, const
         qc[i].gbits = groups[i].gbits;
         qc[i].pfx = groups[i].pfx;
         qc[i].psave = groups[i].psave;
+        qc[i].col_mask = (uint16_t)q.col_mask;
         for (uint32_t t = 0; t < q.n_steps; ++t, ++k) {
             const ShStep& st = q.steps[t];
             sc[k].lo = st.lo;

@@ -71,7 +71,7 @@ struct ShQueryC {
     uint32_t gbits;  // mask-word bits of the query's prefix group (0: no group)
     uint8_t pfx;     // steps the group shares (fewer than any member's step count)
     uint8_t psave;   // what the shared prefix hands on: bit 0 group-key digits, bit 1 carried value
-    uint8_t pad[2];
+    uint16_t col_mask;  // columns the query reads
 };
 static_assert(sizeof(ShStepC) == 32 && sizeof(ShQueryC) == 48, "compact descriptor sizes");
 
@@ -318,6 +318,70 @@ __device__ __forceinline__ int shared_decode(const gx_dcol& col, uint32_t c, uin
     return 0;
 }
 
+// Batches: the tile's literal columns, copied at once.  A column of
+// segmented LZ4 whose tile lies inside one literal run (random-valued
+// columns; the encoder stores them as literals) is a plain byte range of the
+// block; the tile's columns in that form are copied straight from global
+// memory into their buffers with all their loads in flight together, instead
+// of one staged decode per column as a step first needs it.  Thread c checks
+// column c (directory entry and the tile's segment entries); returns the
+// columns copied (rows in plain order).
+template <int NT>
+__device__ __forceinline__ uint32_t shared_literal_tiles(const ShParams& P, uint32_t cols, uint32_t slot,
+                                                         uint32_t rows, uint32_t r0, uint32_t n, uint32_t* colbuf,
+                                                         const uint8_t** s_lit, uint32_t* s_sh, uint32_t* s_pd) {
+    const uint32_t tid = threadIdx.x;
+    if (tid < kShMaxCols) {
+        const uint8_t* src = nullptr;
+        if ((cols >> tid) & 1u) {
+            const gx_dcol& c = P.cols[tid];
+            if (c.codec == GX_CODEC_LZ4 && c.S > 1 && !c.host_mapped && (n & 3u) == 0 &&
+                (r0 & ((1u << c.seg_shift) - 1u)) == 0) {
+                const gx_dblock d = c.blocks[slot];
+                const uint32_t j0 = r0 >> c.seg_shift;
+                const uint32_t nseg = (n + (1u << c.seg_shift) - 1) >> c.seg_shift;
+                const uint32_t* e = c.seg + (size_t)2 * c.S * slot;
+                if (d.n_rows == rows && d.offset <= c.payload_bytes &&
+                    (uint64_t)d.comp_bytes + 32 <= c.payload_bytes - d.offset && j0 + nseg <= c.S) {
+                    const uint32_t lo = __ldg(e + 2 * j0), info0 = __ldg(e + 2 * j0 + 1);
+                    const uint32_t hi = j0 + nseg < c.S ? __ldg(e + 2 * (j0 + nseg)) : d.comp_bytes;
+                    if ((info0 & 16u) && (info0 >> 5) >= 4 * n && hi >= lo && hi - lo == 4 * n && hi <= d.comp_bytes)
+                        src = c.payload + d.offset + lo;
+                }
+            }
+        }
+        s_lit[tid] = src;
+        if (src) {
+            s_sh[tid] = 31u;
+            s_pd[tid] = 0u;
+        }
+    }
+    __syncthreads();
+    uint32_t done = 0;
+#pragma unroll 1
+    for (uint32_t c = 0; c < kShMaxCols; ++c)
+        if (s_lit[c]) done |= 1u << c;
+    // items (column, 4-row group): five aligned words give the four rows
+    const uint32_t per = n / 4, nlit = __popc(done);
+    uint32_t cm = done;
+    for (uint32_t k = 0; k < nlit; ++k, cm &= cm - 1) {
+        const uint32_t c = __ffs(cm) - 1;
+        const uint8_t* src = s_lit[c];
+        const uint32_t* A = (const uint32_t*)((uintptr_t)src & ~(uintptr_t)3);
+        const uint32_t sh = ((uint32_t)(uintptr_t)src & 3u) * 8;
+        uint4* dst = (uint4*)(colbuf + c * kShColWords);
+#pragma unroll 4
+        for (uint32_t q4 = tid; q4 < per; q4 += NT) {
+            const uint32_t* w = A + 4 * q4;
+            const uint32_t a0 = __ldg(w), a1 = __ldg(w + 1), a2 = __ldg(w + 2), a3 = __ldg(w + 3), a4 = __ldg(w + 4);
+            dst[q4] = make_uint4(__funnelshift_r(a0, a1, sh), __funnelshift_r(a1, a2, sh),
+                                 __funnelshift_r(a2, a3, sh), __funnelshift_r(a3, a4, sh));
+        }
+    }
+    if (done) __syncthreads();
+    return done;
+}
+
 // Persistent shared-scan kernel: NT threads, tiles of up to kShTile rows.
 // Per tile, the active queries are evaluated one after another, step-major:
 // a step's fields go to registers, then the step runs over the RPT row
@@ -354,6 +418,8 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
     __shared__ uint32_t s_tmp[NW + 1];
     __shared__ CascTile s_ct;
     __shared__ uint32_t s_seg[2 * (kMaxSegments + 1)];
+    __shared__ uint32_t s_cols;                    // batches: columns the tile's active queries read
+    __shared__ const uint8_t* s_lit[kShMaxCols];   // batches: a literal tile's first byte, or null
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (uint32_t i = tid; i < P.n_queries; i += NT) s_part[i] = 0;
@@ -369,6 +435,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
     if (tid == 0) {
         s_err = 0;
         s_fatal = 0;
+        if (!SINGLE) s_cols = 0;
         mbar_init(&s_mbar, 1);
     }
     uint32_t phase = 0;
@@ -402,10 +469,17 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                 if (!(Q.row_lo < g0 + n && Q.row_hi > g0)) keepm &= ~(1u << bit);
             }
             s_qmask[w] = keepm;
+            if constexpr (!SINGLE) {
+                uint32_t cm = 0;
+                for (uint32_t mm = keepm; mm; mm &= mm - 1) cm |= ((const ShQueryC*)s_qc)[w * 32 + __ffs(mm) - 1].col_mask;
+                if (cm) atomicOr(&s_cols, cm);
+            }
         }
         __syncthreads();
+        uint32_t lit = 0;  // batches: literal columns already copied
+        if constexpr (!SINGLE) lit = shared_literal_tiles<NT>(P, s_cols, slot, rows, r0, n, colbuf, s_lit, s_sh, s_pd);
         uint32_t* const s_pst = (uint32_t*)(s_qc + P.qc_bytes);  // prefix-state buffer (batches)
-        uint32_t decoded = 0;  // columns of this tile already in their buffers
+        uint32_t decoded = lit;  // columns of this tile already in their buffers
         bool dropped = false;
         for (uint32_t w = 0; w < MW && !dropped; ++w) {
             uint32_t m = s_qmask[w];
@@ -582,7 +656,10 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
         }
         }  // r0 < rows
         __syncthreads();
-        if (tid == 0) s_item = s_fatal ? 0xFFFFFFFFu : next_it;
+        if (tid == 0) {
+            s_item = s_fatal ? 0xFFFFFFFFu : next_it;
+            if (!SINGLE) s_cols = 0;
+        }
         __syncthreads();
     }
     __syncthreads();
