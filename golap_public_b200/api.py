@@ -152,11 +152,13 @@ class MetaChecker:
 
 
 class HashMap:
-    """Open-addressing join table on the device: key -> payload (row id when no payload)."""
+    """Join table on the device: key -> payload (row id when no payload).
+    layout: "linear" or "bucket" (open addressing), or "dense" (one slot per
+    key of the build keys' range; for keys that fill most of their range)."""
 
     def __init__(self, max_entries: int, layout: str = "linear"):
         h = C.c_void_p()
-        lay = {"linear": L.GX_HT_LINEAR, "bucket": L.GX_HT_BUCKET}[layout]
+        lay = {"linear": L.GX_HT_LINEAR, "bucket": L.GX_HT_BUCKET, "dense": L.GX_HT_DENSE}[layout]
         check(L.lib().gx_hashtable_create2(max_entries, lay, C.byref(h)))
         self.handle = h
         self.layout = layout

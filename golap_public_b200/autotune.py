@@ -7,7 +7,7 @@ template's queries in every point of a grid
 
     rows_per_chunk  256K .. 4M rows   (the table is re-encoded per value)
     threads         128 .. 1024       (CTA size of the shared-scan kernel)
-    ht_layout       linear | bucket   (join-table layout)
+    ht_layout       linear | bucket | dense   (join-table layout)
 
 on a sample table, replays each batch from a CUDA graph, takes the median of
 `reps` device-timed replays, checks that every point gives the same results
@@ -32,7 +32,7 @@ TEMPLATES = ("scan", "star", "highcard")
 SPACE = {
     "rows_per_chunk": (262_144, 1_048_576, 4_194_304),
     "threads": (128, 256, 512, 1024),
-    "ht_layout": ("linear", "bucket"),
+    "ht_layout": ("linear", "bucket", "dense"),
 }
 DEFAULT = {"rows_per_chunk": 1_048_576, "threads": 256, "ht_layout": "linear"}
 

@@ -582,8 +582,20 @@ __device__ __forceinline__ bool ht_probe_bucket(const uint64_t* __restrict__ slo
     return false;
 }
 
+// Dense layout: slot 0 = {base, span}; the key's entry at slot 1 + (key - base).
+__device__ __forceinline__ bool ht_probe_dense(const uint64_t* __restrict__ slots, int32_t key, int32_t* payload) {
+    const uint64_t h = __ldg((const unsigned long long*)slots);
+    const uint32_t u = (uint32_t)key - (uint32_t)h;
+    if (key == kEmptyKey || u >= (uint32_t)(h >> 32)) return false;
+    const uint64_t e = __ldg((const unsigned long long*)slots + 1 + u);
+    if ((int32_t)(uint32_t)e != key) return false;
+    *payload = (int32_t)(uint32_t)(e >> 32);
+    return true;
+}
+
 __device__ __forceinline__ bool ht_probe_any(const uint64_t* __restrict__ slots, uint32_t log2cap, uint32_t layout,
                                              int32_t key, int32_t* payload) {
+    if (layout == GX_HT_DENSE) return ht_probe_dense(slots, key, payload);
     return layout ? ht_probe_bucket(slots, log2cap, key, payload) : ht_probe(slots, log2cap, key, payload);
 }
 

@@ -813,6 +813,63 @@ __global__ void ht_build_kernel(uint64_t* slots, uint32_t log2cap, const int32_t
     if (bad) atomicAdd(&counters[2], bad);
 }
 
+// Smallest and largest key of the rows that pass the predicates (range[0],
+// range[1]; start at INT32_MAX, INT32_MIN).  The reserved empty key is skipped.
+__global__ void ht_range_kernel(const int32_t* keys, uint64_t n, const __grid_constant__ BuildPreds preds,
+                                int32_t* range) {
+    int32_t lo = INT32_MAX, hi = INT32_MIN;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        bool pass = true;
+        for (uint32_t k = 0; k < preds.n; ++k) {
+            int32_t x = preds.p[k].col_dev[i];
+            pass = pass && x >= preds.p[k].lo && x <= preds.p[k].hi;
+        }
+        const int32_t key = keys[i];
+        if (!pass || key == kEmptyKey) continue;
+        lo = min(lo, key);
+        hi = max(hi, key);
+    }
+    lo = __reduce_min_sync(0xFFFFFFFFu, lo);
+    hi = __reduce_max_sync(0xFFFFFFFFu, hi);
+    if ((threadIdx.x & 31) == 0 && lo <= hi) {
+        atomicMin(&range[0], lo);
+        atomicMax(&range[1], hi);
+    }
+}
+
+// Dense build: slots[0] holds {base, span}; row i's entry goes to slot
+// 1 + (key - base); the first insert of a key wins, later ones count as
+// duplicates (as in the hashed layouts).
+__global__ void ht_build_dense_kernel(uint64_t* slots, int32_t base, uint32_t span, const int32_t* keys,
+                                      const int32_t* payload, uint64_t n, const __grid_constant__ BuildPreds preds,
+                                      unsigned long long* counters) {
+    unsigned long long ins = 0, dup = 0, bad = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        bool pass = true;
+        for (uint32_t k = 0; k < preds.n; ++k) {
+            int32_t x = preds.p[k].col_dev[i];
+            pass = pass && x >= preds.p[k].lo && x <= preds.p[k].hi;
+        }
+        if (!pass) continue;
+        const int32_t key = keys[i];
+        const uint32_t u = (uint32_t)key - (uint32_t)base;
+        if (key == kEmptyKey || u >= span) {
+            ++bad;
+            continue;
+        }
+        const int32_t pay = payload ? payload[i] : (int32_t)i;
+        const unsigned long long e = ((unsigned long long)(uint32_t)pay << 32) | (uint32_t)key;
+        const unsigned long long old = atomicCAS((unsigned long long*)slots + 1 + u, (unsigned long long)kEmptySlot, e);
+        if (old == (unsigned long long)kEmptySlot)
+            ++ins;
+        else
+            ++dup;
+    }
+    if (ins) atomicAdd(&counters[0], ins);
+    if (dup) atomicAdd(&counters[1], dup);
+    if (bad) atomicAdd(&counters[2], bad);
+}
+
 __global__ void ht_build_bucket_kernel(uint64_t* slots, uint32_t log2cap, const int32_t* keys, const int32_t* payload,
                                        uint64_t n, const __grid_constant__ BuildPreds preds,
                                        unsigned long long* counters) {
@@ -974,6 +1031,7 @@ struct gx_hashtable {
     uint32_t layout = GX_HT_LINEAR;
     uint64_t max_entries = 0;
     unsigned long long* counters = nullptr;  // inserted, duplicates, dropped
+    int32_t* range = nullptr;                // dense layout: key range of the last build (device)
 };
 
 struct gx_groupby {
@@ -1253,32 +1311,87 @@ gx_status gx_hashtable_create(uint64_t max_entries, gx_hashtable** out) {
 }
 
 gx_status gx_hashtable_create2(uint64_t max_entries, uint32_t layout, gx_hashtable** out) {
-    if (layout > GX_HT_BUCKET) return set_error(GX_ERR_INVALID, "unknown hash table layout %u", layout);
+    if (layout > GX_HT_DENSE) return set_error(GX_ERR_INVALID, "unknown hash table layout %u", layout);
     gx_status st = gx_hashtable_create(max_entries, out);
-    if (!st) (*out)->layout = layout;
-    return st;
+    if (st) return st;
+    (*out)->layout = layout;
+    if (layout == GX_HT_DENSE) {
+        cudaError_t e = cudaMalloc(&(*out)->range, 2 * sizeof(int32_t));
+        if (e != cudaSuccess) {
+            gx_hashtable_free(*out);
+            *out = nullptr;
+            return set_error(GX_ERR_NOMEM, "gx_hashtable_create2: %s", cudaGetErrorString(e));
+        }
+    }
+    return GX_OK;
 }
 
 gx_status gx_hashtable_free(gx_hashtable* ht) {
     if (!ht) return GX_OK;
     cudaFree(ht->slots);
     cudaFree(ht->counters);
+    cudaFree(ht->range);
     delete ht;
     return GX_OK;
 }
+
+}  // extern "C"
+
+// Dense build: the key range of the rows that pass (one device reduction,
+// read back), the table sized to it (reallocated when it grows), slot 0 the
+// {base, span} header, then one slot per key of the range.
+static gx_status hashtable_build_dense(gx_hashtable* ht, const int32_t* keys_dev, const int32_t* payload_dev,
+                                       uint64_t n, const BuildPreds& bp, unsigned grid, cudaStream_t s) {
+    int32_t range[2] = {INT32_MAX, INT32_MIN};
+    if (n) {
+        fill_u64_kernel<<<1, 32, 0, s>>>((uint64_t*)ht->range, 1,
+                                         ((uint64_t)(uint32_t)INT32_MIN << 32) | (uint32_t)INT32_MAX);
+        ht_range_kernel<<<grid, 256, 0, s>>>(keys_dev, n, bp, ht->range);
+        GX_CK(cudaGetLastError());
+        GX_CK(cudaMemcpyAsync(range, ht->range, sizeof(range), cudaMemcpyDeviceToHost, s));
+        gx_status st = wait_stream(s, 120.0);
+        if (st) return st;
+    }
+    const uint64_t span = range[0] <= range[1] ? (uint64_t)((int64_t)range[1] - range[0] + 1) : 0;
+    const uint64_t limit = std::min<uint64_t>(1ull << 30, std::max<uint64_t>(64 * ht->max_entries, 1ull << 20));
+    if (span > limit)
+        return set_error(GX_ERR_INVALID, "dense hash table: keys span %llu values, above the limit %llu",
+                         (unsigned long long)span, (unsigned long long)limit);
+    const uint32_t need = std::max<uint32_t>(4, log2_ceil(span + 1));
+    if (need > ht->log2cap) {
+        GX_CK(cudaStreamSynchronize(s));
+        cudaFree(ht->slots);
+        ht->slots = nullptr;
+        ht->log2cap = 0;
+        GX_CK(cudaMalloc(&ht->slots, 8ull << need));
+        ht->log2cap = need;
+    }
+    const uint64_t cap = 1ull << ht->log2cap;
+    fill_u64_kernel<<<(unsigned)std::min<uint64_t>(1024, (cap + 255) / 256), 256, 0, s>>>(ht->slots, cap, kEmptySlot);
+    fill_u64_kernel<<<1, 32, 0, s>>>(ht->slots, 1, (span << 32) | (uint32_t)(span ? range[0] : 0));
+    GX_CK(cudaMemsetAsync(ht->counters, 0, 4 * sizeof(unsigned long long), s));
+    if (span)
+        ht_build_dense_kernel<<<grid, 256, 0, s>>>(ht->slots, range[0], (uint32_t)span, keys_dev, payload_dev, n, bp,
+                                                   ht->counters);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+extern "C" {
 
 gx_status gx_hashtable_build(gx_hashtable* ht, const int32_t* keys_dev, const int32_t* payload_dev, uint64_t n,
                              const gx_pred* preds, uint32_t n_preds, void* stream) {
     if (!ht || (!keys_dev && n) || n_preds > 4 || (n_preds && !preds)) return set_error(GX_ERR_INVALID, "gx_hashtable_build: bad args");
     cudaStream_t s = (cudaStream_t)stream;
-    const uint64_t cap = 1ull << ht->log2cap;
-    fill_u64_kernel<<<(unsigned)std::min<uint64_t>(1024, (cap + 255) / 256), 256, 0, s>>>(ht->slots, cap, kEmptySlot);
-    GX_CK(cudaMemsetAsync(ht->counters, 0, 4 * sizeof(unsigned long long), s));
-    if (n == 0) return GX_OK;
     BuildPreds bp{};
     for (uint32_t i = 0; i < n_preds; ++i) bp.p[i] = preds[i];
     bp.n = n_preds;
     const unsigned grid = (unsigned)std::min<uint64_t>(4 * sm_count(), (n + 255) / 256);
+    if (ht->layout == GX_HT_DENSE) return hashtable_build_dense(ht, keys_dev, payload_dev, n, bp, grid, s);
+    const uint64_t cap = 1ull << ht->log2cap;
+    fill_u64_kernel<<<(unsigned)std::min<uint64_t>(1024, (cap + 255) / 256), 256, 0, s>>>(ht->slots, cap, kEmptySlot);
+    GX_CK(cudaMemsetAsync(ht->counters, 0, 4 * sizeof(unsigned long long), s));
+    if (n == 0) return GX_OK;
     if (ht->layout == GX_HT_BUCKET)
         ht_build_bucket_kernel<<<grid, 256, 0, s>>>(ht->slots, ht->log2cap, keys_dev, payload_dev, n, bp, ht->counters);
     else

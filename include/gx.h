@@ -171,8 +171,14 @@ typedef struct gx_pred {
 
 gx_status gx_hashtable_create(uint64_t max_entries, gx_hashtable** out);
 /* Table layouts: linear probing over single slots, or buckets of 8 slots
- * (64 bytes, read with one 64-byte access per probe step). */
-enum { GX_HT_LINEAR = 0, GX_HT_BUCKET = 1 };
+ * (64 bytes, read with one 64-byte access per probe step), or a dense table
+ * for build keys that fill most of an integer range (surrogate keys,
+ * yyyymmdd dates): slot 1 + (key - base) holds the key's entry, so a probe
+ * is one read.  A dense table is sized by gx_hashtable_build to the range of
+ * the inserted keys (it synchronises the stream once to read the range); a
+ * range wider than max(64 * max_entries, 2^20) keys fails with
+ * GX_ERR_INVALID.  Formats in include/gx_hash.h. */
+enum { GX_HT_LINEAR = 0, GX_HT_BUCKET = 1, GX_HT_DENSE = 2 };
 gx_status gx_hashtable_create2(uint64_t max_entries, uint32_t layout, gx_hashtable** out);
 gx_status gx_hashtable_free(gx_hashtable* ht);
 /* Clear, then insert (keys[i], payload[i] or i when payload_dev == NULL) for
@@ -188,7 +194,8 @@ gx_status gx_hashtable_probe(const gx_hashtable* ht, const int32_t* keys_dev, ui
                              int32_t* payload_out_dev, uint64_t* hits_dev, void* stream);
 
 /* Device view of the table for probing from other kernels (slot format and
- * hash in include/gx_hash.h): *slots_dev = 2^log2cap 64-bit slots.  Replaces
+ * hash in include/gx_hash.h): *slots_dev = 2^log2cap 64-bit slots (for a
+ * dense table, take the view after gx_hashtable_build, which sizes it).  Replaces
  * passing HashMap by value to a kernel (core/dev_structs.cuh:71-82). */
 gx_status gx_hashtable_view(const gx_hashtable* ht, const uint64_t** slots_dev, uint32_t* log2cap);
 

@@ -8,6 +8,9 @@
  * Group table: two arrays of int64 (keys, sums); an empty key is INT64_MIN.
  * Both tables use linear probing from the hash below over a power-of-two
  * capacity 2^log2cap.
+ * Dense join table (GX_HT_DENSE): slot 0 is a header, low 32 bits = base
+ * (int32, the smallest key), high 32 bits = span (keys base .. base+span-1);
+ * slot 1 + (key - base) holds the key's slot as above, or an empty slot.
  */
 #ifndef GX_HASH_H
 #define GX_HASH_H

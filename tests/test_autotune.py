@@ -40,4 +40,4 @@ def test_table_config_and_choose():
 def test_search_space_covers_the_stated_ranges():
     assert min(AT.SPACE["rows_per_chunk"]) == 256 * 1024 and max(AT.SPACE["rows_per_chunk"]) == 4 * 1024 * 1024
     assert min(AT.SPACE["threads"]) == 128 and max(AT.SPACE["threads"]) == 1024
-    assert set(AT.SPACE["ht_layout"]) == {"linear", "bucket"}
+    assert set(AT.SPACE["ht_layout"]) == {"linear", "bucket", "dense"}

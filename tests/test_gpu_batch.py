@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def table(cuda):
-    return workload.build_table(6_000_000, n_customer=300_000, n_supplier=20_000)
+    return workload.build_table(6_000_000, n_customer=300_000, n_supplier=20_000, ht_layouts=("linear", "dense"))
 
 
 def _check(t, specs):
@@ -41,6 +41,19 @@ def test_batch_mixed_queries(table, mode):
     for _ in range(2):
         b.graph()
         api.scan_check()
+    _check(table, specs)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_batch_dense_join_tables(table, mode):
+    # the same templates probing dense join tables (date, customer and
+    # supplier keys fill their ranges)
+    rng = np.random.default_rng(15)
+    specs = workload.random_queries(table, 40, rng, min_rows=100_000, max_rows=6_000_000, ht_layout="dense")
+    assert {s.template for s in specs} >= {"scan", "star"}
+    b = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs], mode)
+    b.run()
+    api.scan_check()
     _check(table, specs)
 
 

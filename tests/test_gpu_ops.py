@@ -51,7 +51,7 @@ def test_metachecker_known_answers(cuda):
     assert keep.cpu().tolist() == [0, 1, 0]
 
 
-@pytest.mark.parametrize("layout", ["linear", "bucket"])
+@pytest.mark.parametrize("layout", ["linear", "bucket", "dense"])
 def test_join_count_1to1(cuda, layout):
     # join_tests.cu:71-107: build 500k ids, probe 10M rows id = i % 500k -> 10M hits
     build = cuda.arange(500_000, dtype=cuda.int32, device="cuda")
@@ -65,7 +65,7 @@ def test_join_count_1to1(cuda, layout):
     assert cuda.equal(pay, probe)  # payload defaults to the build row id
 
 
-@pytest.mark.parametrize("layout", ["linear", "bucket"])
+@pytest.mark.parametrize("layout", ["linear", "bucket", "dense"])
 def test_filtered_build_and_probe_vs_oracle(cuda, layout):
     rng = np.random.default_rng(8)
     n_b, n_p = 200_000, 3_000_000
@@ -86,7 +86,7 @@ def test_filtered_build_and_probe_vs_oracle(cuda, layout):
     assert int(hits.item()) == int((rid >= 0).sum())
 
 
-@pytest.mark.parametrize("layout", ["linear", "bucket"])
+@pytest.mark.parametrize("layout", ["linear", "bucket", "dense"])
 def test_hashtable_reserved_key_and_capacity(cuda, layout):
     keys = cuda.tensor([1, 2, np.iinfo(np.int32).min, 3], dtype=cuda.int32, device="cuda")
     hm = api.HashMap(4, layout).build(keys)
@@ -98,6 +98,42 @@ def test_hashtable_reserved_key_and_capacity(cuda, layout):
     hm2 = api.HashMap(8, layout).build(many)
     with pytest.raises(GxError):
         hm2.count()
+
+
+def test_dense_table_edges(cuda):
+    # negative keys, duplicates (the first insert wins), probes at and just
+    # outside the range ends, the reserved key, an empty build, sparse keys
+    keys = cuda.tensor([-5, 7, -5, 0, 12, 7], dtype=cuda.int32, device="cuda")
+    pay = cuda.tensor([10, 11, 12, 13, 14, 15], dtype=cuda.int32, device="cuda")
+    hm = api.HashMap(8, "dense").build(keys, pay)
+    assert hm.count() == 4
+    probe = cuda.tensor([-6, -5, 0, 7, 12, 13, 3, np.iinfo(np.int32).min, np.iinfo(np.int32).max],
+                        dtype=cuda.int32, device="cuda")
+    out = cuda.empty(9, dtype=cuda.int32, device="cuda")
+    hits = cuda.zeros(1, dtype=cuda.int64, device="cuda")
+    hm.probe(probe, out, hits)
+    miss = np.iinfo(np.int32).min
+    got = out.cpu().tolist()
+    assert got[0] == miss and got[1] in (10, 12) and got[2] == 13 and got[3] in (11, 15) and got[4] == 14
+    assert got[5:] == [miss] * 4 and int(hits.item()) == 4
+    # predicates that pass no row: every probe misses
+    reg = cuda.zeros(6, dtype=cuda.int32, device="cuda")
+    hm.build(keys, pay, preds=[(reg, 1, 1)])
+    assert hm.count() == 0
+    hits.zero_()
+    hm.probe(probe, out, hits)
+    assert int(hits.item()) == 0 and out.cpu().tolist() == [miss] * 9
+    # rebuilt over a wider range: the table grows
+    wide = cuda.arange(0, 900_000, 3, dtype=cuda.int32, device="cuda")
+    hm.build(wide)
+    hits.zero_()
+    hm.probe(wide[::1000].contiguous(), None, hits)
+    assert int(hits.item()) == wide[::1000].numel()
+    # keys too sparse for a dense table
+    sparse = cuda.tensor([0, 1 << 30], dtype=cuda.int32, device="cuda")
+    with pytest.raises(GxError) as e:
+        api.HashMap(2, "dense").build(sparse)
+    assert e.value.status == L.GX_ERR_INVALID and "span" in str(e.value)
 
 
 def test_groupby_exact_sums(cuda):
