@@ -576,6 +576,64 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                             const int64_t val = prod ? (int64_t)v * c2 : (int64_t)v;
                             local += k ? val : 0;
                         }
+                    } else if (RPT <= 8 && (flags & GX_STEP_PROBE) && htlay != GX_HT_BUCKET && !last) {
+                        // probe of a dense or linear join table: the first slot reads of all
+                        // RPT rows are issued before any is used; a linear probe that the
+                        // first slot does not settle (another key there) walks its chain
+                        // (up to 8 rows per thread, where the registers allow)
+                        const bool dense = htlay == GX_HT_DENSE;
+                        uint32_t hbase = 0, hspan = 0;
+                        if (dense) {
+                            const uint64_t hdr = __ldg((const unsigned long long*)ht);
+                            hbase = (uint32_t)hdr;
+                            hspan = (uint32_t)(hdr >> 32);
+                        }
+                        int32_t vv[RPT];
+                        uint64_t ee[RPT];
+                        uint32_t fk = 0;  // rows whose slot was read
+#pragma unroll
+                        for (int i = 0; i < RPT; ++i) {
+                            const uint32_t r = (i * NW + warp) * 32 + lane;
+                            bool k = (keep >> i) & 1u;
+                            const int32_t v = k ? (int32_t)col[sh_col_index(r, sh, pd)] : 0;
+                            if (filt) k = k && v >= lo && v <= hi;
+                            const uint32_t u = (uint32_t)v - hbase;
+                            const bool rd = k && v != kEmptyKey && (!dense || u < hspan);
+                            const unsigned long long* sp =
+                                (const unsigned long long*)ht + (dense ? 1 + u : hash_key32(v, htlog));
+                            vv[i] = v;
+                            ee[i] = rd ? __ldg(sp) : (unsigned long long)kEmptySlot;
+                            fk |= rd ? 1u << i : 0u;
+                        }
+#pragma unroll
+                        for (int i = 0; i < RPT; ++i) {
+                            if (!((keep >> i) & 1u)) continue;
+                            const int32_t v = vv[i];
+                            bool k = (fk >> i) & 1u;
+                            int32_t p = 0;
+                            if (k) {
+                                const int32_t ek = (int32_t)(uint32_t)ee[i];
+                                if (ek == v) {
+                                    p = (int32_t)(uint32_t)(ee[i] >> 32);
+                                } else if (dense || ek == kEmptyKey) {
+                                    k = false;
+                                } else {
+                                    p = v;
+                                    k = sh_probe(ht, htlog, htlay, v, &p);
+                                }
+                            }
+                            if (dcard && k) {
+                                const uint32_t dgt = (uint32_t)(p - dbase);
+                                if (dgt >= dcard) {
+                                    raise_error(kErrInvalid);
+                                    k = false;
+                                } else {
+                                    gk[i] = gk[i] * dcard + dgt;
+                                }
+                            }
+                            if (carry_step && k) carry[i] = v;
+                            if (!k) keep &= ~(1u << i);
+                        }
                     } else {
                         // general step: probes (one-entry memo: a thread's rows are NT apart,
                         // so on sorted or run-length columns they mostly repeat the key),
