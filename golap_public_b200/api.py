@@ -341,7 +341,8 @@ class Batch:
         self.handle = h
 
     def set_launch(self, threads: int = 0, ctas_per_sm: int = 0) -> "Batch":
-        """threads 0 = automatic (most resident warps for the batch's shared memory)."""
+        """threads 0 = automatic (of 256, 512 and 128 threads, the most resident warps
+        for the batch's shared memory)."""
         check(L.lib().gx_batch_set_launch(self.handle, threads, ctas_per_sm))
         return self
 

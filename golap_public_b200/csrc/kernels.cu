@@ -1095,13 +1095,16 @@ static int shared_occupancy(uint32_t threads, size_t smem) {
 }
 
 // Persistent grid of the shared form for the batch's thread count.  An
-// automatic shape (sh_threads_req 0) takes the CTA size with the most
-// resident warps per SM for the batch's shared memory (larger CTAs on ties).
+// automatic shape (sh_threads_req 0) takes, of 256, 512 and 128 threads, the
+// CTA size with the most resident warps per SM for the batch's shared memory
+// (the earlier one on ties).  1024-thread CTAs are left to explicit
+// requests: with 2 rows per thread per tile, a query's per-tile work is
+// spread too thin and its probes have too few reads in flight per thread.
 static void shared_geometry(gx_batch* b) {
     if (b->sh_threads_req == 0) {
-        uint32_t best = 1024;
+        uint32_t best = 256;
         int best_warps = -1;
-        for (uint32_t nt : {1024u, 512u, 256u, 128u}) {
+        for (uint32_t nt : {256u, 512u, 128u}) {
             const int w = shared_occupancy(nt, b->sh_smem) * (int)(nt / 32);
             if (w > best_warps) {
                 best_warps = w;

@@ -336,8 +336,9 @@ gx_status gx_batch_create2(const gx_query* queries, uint32_t n_queries, uint32_t
 /* The form the batch currently runs in (GX_BATCH_QUEUE or GX_BATCH_SHARED). */
 gx_status gx_batch_mode(const gx_batch* b, uint32_t* mode);
 /* Launch shape of the shared form: threads per CTA (128, 256, 512 or 1024,
- * or 0 = automatic, the default: the size with the most resident warps for
- * the batch's shared memory) and a cap on CTAs per SM (0 = as many as fit).
+ * or 0 = automatic, the default: of 256, 512 and 128, the size with the most
+ * resident warps for the batch's shared memory) and a cap on CTAs per SM
+ * (0 = as many as fit).
  * Kept across gx_batch_assign; drops a captured graph.  The autotuner sets
  * it. */
 gx_status gx_batch_set_launch(gx_batch* b, uint32_t threads, uint32_t ctas_per_sm);
