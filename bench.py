@@ -545,6 +545,28 @@ def cpu_baseline(f, dd, steps=3, warmup=1, threads=None):
             "ms": ms, "result": int(res)}
 
 
+def profile_batch(rows):
+    """The batched section's 256-query batch (same seed and mix) with dense
+    join tables, run three times in the shared form; prints its device time."""
+    import torch
+
+    from golap_public_b200 import api, workload
+
+    t = workload.build_table(rows, ht_layouts=("dense",))
+    specs = workload.random_queries(t, 256, np.random.default_rng(7), ht_layout="dense")
+    batch = api.Batch([(s.plan, s.row_lo, s.row_hi) for s in specs], "shared")
+    stream = torch.cuda.current_stream()
+    for i in range(3):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        batch.run()
+        b.record(stream)
+        b.synchronize()
+        api.scan_check()
+        print(json.dumps({"profile_batch": i, "rows": rows, "threads": batch.threads, "ms": a.elapsed_time(b)}))
+
+
 def main():
     global N_ROWS
     ap = argparse.ArgumentParser()
@@ -563,11 +585,18 @@ def main():
                     help="fact rows of the Q1 workload (default: the measured 60M-row configuration; smaller "
                          "values are for profiler captures)")
     ap.add_argument("--tune-rows", type=int, default=20_000_000)
+    ap.add_argument("--profile-batch", action="store_true",
+                    help="only build the batch table and run the 256-query mixed batch (shared form, dense join "
+                         "tables, automatic launch shape) three times: the command profiler captures use")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     N_ROWS = args.rows
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+
+    if args.profile_batch:
+        profile_batch(args.batch_rows)
+        return
 
     if args.impl == "reference":
         if rank != 0:

@@ -318,15 +318,17 @@ __device__ __forceinline__ int shared_decode(const gx_dcol& col, uint32_t c, uin
     return 0;
 }
 
-// Batches: the tile's literal columns, copied at once.  A column of
-// segmented LZ4 whose tile lies inside one literal run (random-valued
-// columns; the encoder stores them as literals) is a plain byte range of the
-// block; the tile's columns in that form are copied straight from global
-// memory into their buffers with all their loads in flight together, instead
-// of one staged decode per column as a step first needs it.  Thread c checks
-// column c (directory entry and the tile's segment entries); returns the
-// columns copied (rows in plain order).
-template <int NT>
+// Literal columns of a tile, copied at once (a batch: every column its
+// active queries read, before they run; one query: its remaining columns
+// once its first step leaves rows alive).  A column of segmented LZ4 whose
+// tile lies inside one literal run (random-valued columns; the encoder
+// stores them as literals) is a plain byte range of the block; the columns
+// in that form are copied straight from global memory into their buffers
+// with all their loads in flight together, instead of one staged decode per
+// column as a step first needs it.  Thread c checks column c (directory
+// entry and the tile's segment entries); returns the columns copied (rows in
+// plain order).  All NT threads call it.
+template <int NT, bool SINGLE>
 __device__ __forceinline__ uint32_t shared_literal_tiles(const ShParams& P, uint32_t cols, uint32_t slot,
                                                          uint32_t rows, uint32_t r0, uint32_t n, uint32_t* colbuf,
                                                          const uint8_t** s_lit, uint32_t* s_sh, uint32_t* s_pd) {
@@ -334,7 +336,7 @@ __device__ __forceinline__ uint32_t shared_literal_tiles(const ShParams& P, uint
     if (tid < kShMaxCols) {
         const uint8_t* src = nullptr;
         if ((cols >> tid) & 1u) {
-            const gx_dcol& c = P.cols[tid];
+            const gx_dcol& c = sh_c<SINGLE>(P, tid);
             if (c.codec == GX_CODEC_LZ4 && c.S > 1 && !c.host_mapped && (n & 3u) == 0 &&
                 (r0 & ((1u << c.seg_shift) - 1u)) == 0) {
                 const gx_dblock d = c.blocks[slot];
@@ -477,10 +479,12 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
         }
         __syncthreads();
         uint32_t lit = 0;  // batches: literal columns already copied
-        if constexpr (!SINGLE) lit = shared_literal_tiles<NT>(P, s_cols, slot, rows, r0, n, colbuf, s_lit, s_sh, s_pd);
+        if constexpr (!SINGLE)
+            lit = shared_literal_tiles<NT, SINGLE>(P, s_cols, slot, rows, r0, n, colbuf, s_lit, s_sh, s_pd);
         uint32_t* const s_pst = (uint32_t*)(s_qc + P.qc_bytes);  // prefix-state buffer (batches)
         uint32_t decoded = lit;  // columns of this tile already in their buffers
         bool dropped = false;
+        bool lit_tried = false;  // one-query launches: literal columns copied past the first step
         for (uint32_t w = 0; w < MW && !dropped; ++w) {
             uint32_t m = s_qmask[w];
             while (m && !dropped) {
@@ -538,6 +542,17 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                     if (!((decoded >> c) & 1u)) {
                         // the query's rows are all dead: skip its remaining steps (and this decode)
                         if (s > 0 && !__syncthreads_or(keep != 0)) break;
+                        if constexpr (SINGLE) {
+                            // past the first step with rows alive: the query's remaining
+                            // literal columns are copied together (their loads in flight at once)
+                            if (s > 0 && !lit_tried) {
+                                lit_tried = true;
+                                decoded |= shared_literal_tiles<NT, SINGLE>(P, P.q1.col_mask & ~decoded, slot, rows,
+                                                                           r0, n, colbuf, s_lit, s_sh, s_pd);
+                            }
+                        }
+                    }
+                    if (!((decoded >> c) & 1u)) {
                         if (shared_decode<NT>(sh_c<SINGLE>(P, c), c, slot, rows, r0, n, colbuf, stage, &s_mbar,
                                               phase, s_tmp, &s_ct, &s_err, &s_fatal, s_sh, s_pd, s_seg)) {
                             dropped = true;
