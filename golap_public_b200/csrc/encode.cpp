@@ -57,6 +57,12 @@ struct SeqEmitter {
         const uint32_t Mb = mlen_w * 4;
         const uint32_t mnib = has_match ? std::min<uint32_t>(Mb - 4, 15) : 0;
         const uint32_t lit0 = tp + 1 + ext_bytes(Lb);
+        if (n_seq == 1 && Lb > 0) {
+            // entry 0 resumes inside the block's first literal run (not at its token),
+            // so a tile at the block start whose rows are literals is a plain byte range
+            seg[0] = lit0;
+            seg[1] = (Lb << 5) | 16u | mnib;
+        }
         while (next_b < S) {
             uint32_t N = bound[next_b];
             if (N == anchor) {

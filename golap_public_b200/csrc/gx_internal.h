@@ -27,7 +27,8 @@
 //       info bit 4 == 1: comp_pos is the position of the literal byte that
 //       produces N_j (or of the 16-bit match offset when no literal remains);
 //       info >> 5 = literal bytes remaining in that sequence, info & 15 = the
-//       token's match-length nibble.
+//       token's match-length nibble.  Entry 0 resumes inside the block's
+//       first literal run when the block starts with literals.
 //
 // Cascaded block (own format; the reference's nvCOMP Cascaded stream format
 // is not available, so only decoded values are comparable):

@@ -134,7 +134,15 @@ def test_corrupt_blocks_are_reported(cuda, codec, S):
     # values; a broken header / token stream must be reported
     col = api.Column(v, codec, lz4_segments=S, **kw)
     first = int(col.blocks()[0][0])
-    _corrupt_payload(col, first + (1 if codec == "cascaded" else 0), 0xFF)  # n_runs / first token
+    if codec == "lz4" and S > 1:
+        # segment decoders start from the side index (entry 0 resumes inside the
+        # first literal run): break the first match's offset, which they read
+        lit_pos, info = (int(x) for x in col.seg_index()[:2])
+        assert info & 16
+        _corrupt_payload(col, first + lit_pos + (info >> 5), 0xFF)
+        _corrupt_payload(col, first + lit_pos + (info >> 5) + 1, 0xFF)
+    else:
+        _corrupt_payload(col, first + (1 if codec == "cascaded" else 0), 0xFF)  # n_runs / first token
     col.to_device()
     out = cuda.zeros(300_000, dtype=cuda.int32, device="cuda")
     api.ChunkDecompressor(col).chunks(0, col.info.n_chunks, out)
