@@ -325,13 +325,16 @@ __device__ __forceinline__ int shared_decode(const gx_dcol& col, uint32_t c, uin
 // stores them as literals) is a plain byte range of the block; the columns
 // in that form are copied straight from global memory into their buffers
 // with all their loads in flight together, instead of one staged decode per
-// column as a step first needs it.  Thread c checks column c (directory
-// entry and the tile's segment entries); returns the columns copied (rows in
-// plain order).  All NT threads call it.
+// column as a step first needs it.  shared_literal_locate: thread c checks
+// column c (directory entry and the tile's segment entries) and records the
+// tile's first byte, or null, in s_lit[c]; a one-query launch locates its
+// later columns at the tile's start and prefetches their bytes into L2, so
+// that the copy after the first step reads L2.  All NT threads call both
+// functions (rows land in plain order).
 template <int NT, bool SINGLE>
-__device__ __forceinline__ uint32_t shared_literal_tiles(const ShParams& P, uint32_t cols, uint32_t slot,
-                                                         uint32_t rows, uint32_t r0, uint32_t n, uint32_t* colbuf,
-                                                         const uint8_t** s_lit, uint32_t* s_sh, uint32_t* s_pd) {
+__device__ __forceinline__ void shared_literal_locate(const ShParams& P, uint32_t cols, uint32_t slot, uint32_t rows,
+                                                      uint32_t r0, uint32_t n, const uint8_t** s_lit, uint32_t* s_sh,
+                                                      uint32_t* s_pd, bool prefetch) {
     const uint32_t tid = threadIdx.x;
     if (tid < kShMaxCols) {
         const uint8_t* src = nullptr;
@@ -347,8 +350,17 @@ __device__ __forceinline__ uint32_t shared_literal_tiles(const ShParams& P, uint
                     (uint64_t)d.comp_bytes + 32 <= c.payload_bytes - d.offset && j0 + nseg <= c.S) {
                     const uint32_t lo = __ldg(e + 2 * j0), info0 = __ldg(e + 2 * j0 + 1);
                     const uint32_t hi = j0 + nseg < c.S ? __ldg(e + 2 * (j0 + nseg)) : d.comp_bytes;
-                    if ((info0 & 16u) && (info0 >> 5) >= 4 * n && hi >= lo && hi - lo == 4 * n && hi <= d.comp_bytes)
+                    if ((info0 & 16u) && (info0 >> 5) >= 4 * n && hi >= lo && hi - lo == 4 * n &&
+                        hi <= d.comp_bytes) {
                         src = c.payload + d.offset + lo;
+                        if (prefetch) {
+                            // the bytes (16-byte aligned cover, inside the payload's slack) into L2
+                            const uint8_t* a = c.payload + d.offset + (lo & ~15u);
+                            const uint32_t bytes = ((hi + 15u) & ~15u) - (lo & ~15u);
+                            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes)
+                                         : "memory");
+                        }
+                    }
                 }
             }
         }
@@ -358,11 +370,17 @@ __device__ __forceinline__ uint32_t shared_literal_tiles(const ShParams& P, uint
             s_pd[tid] = 0u;
         }
     }
-    __syncthreads();
+}
+
+// Copy of the located literal columns in `cols` (after a barrier that made
+// shared_literal_locate's results visible); returns the columns copied.
+template <int NT>
+__device__ __forceinline__ uint32_t shared_literal_copy(uint32_t cols, uint32_t n, uint32_t* colbuf,
+                                                        const uint8_t* const* s_lit) {
+    const uint32_t tid = threadIdx.x;
     uint32_t done = 0;
-#pragma unroll 1
-    for (uint32_t c = 0; c < kShMaxCols; ++c)
-        if (s_lit[c]) done |= 1u << c;
+    for (uint32_t cm = cols; cm; cm &= cm - 1)
+        if (s_lit[__ffs(cm) - 1]) done |= 1u << (__ffs(cm) - 1);
     // items (column, 4-row group): five aligned words give the four rows
     const uint32_t per = n / 4, nlit = __popc(done);
     uint32_t cm = done;
@@ -479,8 +497,16 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
         }
         __syncthreads();
         uint32_t lit = 0;  // batches: literal columns already copied
-        if constexpr (!SINGLE)
-            lit = shared_literal_tiles<NT, SINGLE>(P, s_cols, slot, rows, r0, n, colbuf, s_lit, s_sh, s_pd);
+        if constexpr (!SINGLE) {
+            shared_literal_locate<NT, SINGLE>(P, s_cols, slot, rows, r0, n, s_lit, s_sh, s_pd, false);
+            __syncthreads();
+            lit = shared_literal_copy<NT>(s_cols, n, colbuf, s_lit);
+        } else {
+            // one query: its columns after the first step's, located and prefetched now
+            const uint32_t first = P.q1.steps[0].col;
+            shared_literal_locate<NT, SINGLE>(P, P.q1.col_mask & ~(1u << first), slot, rows, r0, n, s_lit, s_sh,
+                                              s_pd, true);
+        }
         uint32_t* const s_pst = (uint32_t*)(s_qc + P.qc_bytes);  // prefix-state buffer (batches)
         uint32_t decoded = lit;  // columns of this tile already in their buffers
         bool dropped = false;
@@ -547,8 +573,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                             // literal columns are copied together (their loads in flight at once)
                             if (s > 0 && !lit_tried) {
                                 lit_tried = true;
-                                decoded |= shared_literal_tiles<NT, SINGLE>(P, P.q1.col_mask & ~decoded, slot, rows,
-                                                                           r0, n, colbuf, s_lit, s_sh, s_pd);
+                                decoded |= shared_literal_copy<NT>(P.q1.col_mask & ~decoded, n, colbuf, s_lit);
                             }
                         }
                     }
