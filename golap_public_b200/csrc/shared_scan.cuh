@@ -674,6 +674,28 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                             if (carry_step && k) carry[i] = v;
                             if (!k) keep &= ~(1u << i);
                         }
+                    } else if ((flags & GX_STEP_PROBE) && dcard == 0 && !carry_step && !last) {
+                        // a probe that only filters (a date or dimension membership test): a
+                        // rolled loop with a one-entry memo -- small code, which matters on the
+                        // first tiles of a launch, when every CTA runs it cold
+                        int32_t mv = kEmptyKey;
+                        bool mk = false;
+#pragma unroll 1
+                        for (int i = 0; i < RPT; ++i) {
+                            if (!((keep >> i) & 1u)) continue;
+                            const uint32_t r = (i * NW + warp) * 32 + lane;
+                            const int32_t v = (int32_t)col[sh_col_index(r, sh, pd)];
+                            bool k = !filt || (v >= lo && v <= hi);
+                            if (k) {
+                                if (v != mv) {
+                                    int32_t pp = v;
+                                    mk = sh_probe(ht, htlog, htlay, v, &pp);
+                                    mv = v;
+                                }
+                                k = mk;
+                            }
+                            if (!k) keep &= ~(1u << i);
+                        }
                     } else {
                         // general step: probes (one-entry memo: a thread's rows are NT apart,
                         // so on sorted or run-length columns they mostly repeat the key),
