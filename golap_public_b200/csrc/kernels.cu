@@ -772,11 +772,14 @@ struct BuildPreds {
     uint32_t n;
 };
 
-__global__ void ht_build_kernel(uint64_t* slots, uint32_t log2cap, const int32_t* keys, const int32_t* payload,
-                                uint64_t n, const __grid_constant__ BuildPreds preds, unsigned long long* counters) {
+// Linear-probing inserts of rows i0, i0 + stride, ... (< n) that pass the
+// predicates; counts inserted / duplicate / dropped rows into counters.
+__device__ __forceinline__ void ht_insert_rows(uint64_t* slots, uint32_t log2cap, const int32_t* keys,
+                                               const int32_t* payload, uint64_t i0, uint64_t stride, uint64_t n,
+                                               const BuildPreds& preds, unsigned long long* counters) {
     const uint32_t mask = (1u << log2cap) - 1;
     unsigned long long ins = 0, dup = 0, bad = 0;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t i = i0; i < n; i += stride) {
         bool pass = true;
         for (uint32_t k = 0; k < preds.n; ++k) {
             int32_t x = preds.p[k].col_dev[i];
@@ -811,6 +814,25 @@ __global__ void ht_build_kernel(uint64_t* slots, uint32_t log2cap, const int32_t
     if (ins) atomicAdd(&counters[0], ins);
     if (dup) atomicAdd(&counters[1], dup);
     if (bad) atomicAdd(&counters[2], bad);
+}
+
+__global__ void ht_build_kernel(uint64_t* slots, uint32_t log2cap, const int32_t* keys, const int32_t* payload,
+                                uint64_t n, const __grid_constant__ BuildPreds preds, unsigned long long* counters) {
+    ht_insert_rows(slots, log2cap, keys, payload, blockIdx.x * (uint64_t)blockDim.x + threadIdx.x,
+                   (uint64_t)gridDim.x * blockDim.x, n, preds, counters);
+}
+
+// A small linear table in one launch: one CTA clears the slots and the
+// counters, then inserts (dimension tables such as the date table).
+constexpr uint64_t kSmallHtSlots = 1u << 16, kSmallHtRows = 1u << 16;
+__global__ void ht_build_small_kernel(uint64_t* slots, uint32_t log2cap, const int32_t* keys, const int32_t* payload,
+                                      uint64_t n, const __grid_constant__ BuildPreds preds,
+                                      unsigned long long* counters) {
+    const uint64_t cap = 1ull << log2cap;
+    for (uint64_t i = threadIdx.x; i < cap; i += blockDim.x) slots[i] = kEmptySlot;
+    if (threadIdx.x < 4) counters[threadIdx.x] = 0;
+    __syncthreads();
+    ht_insert_rows(slots, log2cap, keys, payload, threadIdx.x, blockDim.x, n, preds, counters);
 }
 
 // Smallest and largest key of the rows that pass the predicates (range[0],
@@ -1392,6 +1414,11 @@ gx_status gx_hashtable_build(gx_hashtable* ht, const int32_t* keys_dev, const in
     const unsigned grid = (unsigned)std::min<uint64_t>(4 * sm_count(), (n + 255) / 256);
     if (ht->layout == GX_HT_DENSE) return hashtable_build_dense(ht, keys_dev, payload_dev, n, bp, grid, s);
     const uint64_t cap = 1ull << ht->log2cap;
+    if (ht->layout == GX_HT_LINEAR && cap <= kSmallHtSlots && n <= kSmallHtRows) {
+        ht_build_small_kernel<<<1, 1024, 0, s>>>(ht->slots, ht->log2cap, keys_dev, payload_dev, n, bp, ht->counters);
+        GX_CK(cudaGetLastError());
+        return GX_OK;
+    }
     fill_u64_kernel<<<(unsigned)std::min<uint64_t>(1024, (cap + 255) / 256), 256, 0, s>>>(ht->slots, cap, kEmptySlot);
     GX_CK(cudaMemsetAsync(ht->counters, 0, 4 * sizeof(unsigned long long), s));
     if (n == 0) return GX_OK;
