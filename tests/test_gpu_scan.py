@@ -94,6 +94,21 @@ def test_q1_config1_sorted_pruned(cuda, S):
             assert q.keep.cpu().numpy().tolist() == O.minmax_keep(mins, maxs, 19940101, 19940131).tolist()
 
 
+def test_q1_pinned_host_residency(cuda):
+    # compressed columns in pinned host memory, read by the kernels over
+    # PCIe: the same results as HBM residency, pruned and over every date
+    f = datagen.fact_q1(8_000_000, True)
+    dd = datagen.date_dim()
+    fact = queries.encode_fact(f, {"date_key": "cascaded"}, residency="pinned")
+    assert all(c.info.on_device == 2 for c in fact.cols.values())
+    ok = dd["d_yearmonthnum"] == 199301
+    q = queries.Q1Query(fact, dd, ok, 19930101, 19930131, 4, 6, 26, 35, prune=True)
+    assert q.run() == _oracle_q1(f, dd, ok, 4, 6, 26, 35)
+    ok_all = np.ones(len(dd["d_key"]), dtype=bool)
+    qa = queries.Q1Query(fact, dd, ok_all, int(dd["d_key"].min()), int(dd["d_key"].max()), 4, 6, 26, 35, prune=False)
+    assert qa.run() == _oracle_q1(f, dd, ok_all, 4, 6, 26, 35)
+
+
 def test_q3_star_join_groupby(cuda):
     # configs[2] shape at 20M fact rows with full-size dimensions
     f = datagen.fact_q3(20_000_000, True)
