@@ -485,7 +485,7 @@ def serving_section(t, rates=(200, 1000, 2000), seconds=2.0, seed=9, max_backlog
                                    ht_layout=autotune.layouts(choices))
     threads = 0  # automatic launch shape per served batch (most resident warps for its footprint)
     out = {"batch_threads": "automatic"}
-    for mode, (inflight, maxb) in (("batched", (4, 64)), ("one_at_a_time", (1, 1))):
+    for mode, (inflight, maxb) in (("batched", (4, 128)), ("one_at_a_time", (1, 1))):
         res = {}
         for rate in rates:
             sv = api.Server(max_inflight=inflight, max_batch=maxb, hbm_budget=120 << 30, batch_threads=threads)

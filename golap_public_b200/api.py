@@ -384,7 +384,7 @@ class Batch:
 class Server:
     """Continuous-batching serving loop (gx_server_* in include/gx.h)."""
 
-    def __init__(self, max_inflight: int = 4, max_batch: int = 64, hbm_budget: int = 120 << 30,
+    def __init__(self, max_inflight: int = 4, max_batch: int = 128, hbm_budget: int = 120 << 30,
                  batch_threads: int = 0, batch_mode: str = "auto"):
         o = L.ServerOpts()
         check(L.lib().gx_server_opts_default(C.byref(o)))

@@ -9,11 +9,14 @@
 // total stays within the HBM budget, and launches it as one persistent
 // multi-query scan (gx_batch_assign + gx_batch_run).  Requests that arrive
 // while other batches run are admitted as slots and memory free up; their
-// work overlaps with the running batches on the device.  Completion is
-// detected with stream events; latency = completion - submit.  Every wait is
-// bounded.
+// work overlaps with the running batches on the device.  Under load (a
+// queue of a quarter of max_batch or more) a free slot waits while another
+// batch runs, so that batches grow and share their decoded tiles among more
+// queries.  Completion is detected with stream events; latency = completion
+// - submit.  Every wait is bounded.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -95,6 +98,11 @@ void gx_server::run() {
         // dispatch to free slots
         for (auto& sl : slots) {
             if (sl.busy || queue.empty()) continue;
+            // under load (a queue of a quarter batch or more) with a batch already
+            // running, wait for it: the next batch then takes more of the queue, and a
+            // larger batch shares each decoded tile among more queries; light load
+            // keeps several small batches in flight for latency
+            if (busy_any && queue.size() >= std::max<size_t>(1, opts.max_batch / 4)) break;
             std::vector<gx_query> qs;
             std::vector<uint64_t> ids;
             uint64_t hbm = 0;
@@ -154,7 +162,7 @@ extern "C" {
 gx_status gx_server_opts_default(gx_server_opts* o) {
     if (!o) return gx::set_error(GX_ERR_INVALID, "null opts");
     o->max_inflight = 4;
-    o->max_batch = 64;
+    o->max_batch = 128;
     o->hbm_budget = 120ull << 30;
     o->batch_threads = 0;
     o->batch_mode = GX_BATCH_AUTO;

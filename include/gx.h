@@ -361,13 +361,15 @@ gx_status gx_batch_rows(gx_batch* b, uint64_t* rows, void* stream);
  * holds while running: its group table and result); a scheduler thread keeps
  * up to max_inflight batches on the device, each formed FIFO from the queue
  * as soon as a slot is free, admitting requests while the admitted bytes stay
- * within hbm_budget.  A request's results land in its own result_dev /
+ * within hbm_budget; under load (a queue of max_batch / 4 or more) a free
+ * slot waits while another batch runs, so that batches grow (larger batches
+ * share each decoded tile among more queries).  A request's results land in its own result_dev /
  * groupby.  wait() blocks (bounded) until the request is done and reports its
  * latency (submit -> completion). */
 typedef struct gx_server gx_server;
 typedef struct gx_server_opts {
     uint32_t max_inflight;  /* batches on the device at once (default 4)       */
-    uint32_t max_batch;     /* requests per batch (default 64)                 */
+    uint32_t max_batch;     /* requests per batch (default 128)                */
     uint64_t hbm_budget;    /* bytes admitted requests may hold (default 120 GiB) */
     uint32_t batch_threads; /* launch shape of shared-form batches (0 = default) */
     uint32_t batch_mode;    /* GX_BATCH_AUTO / QUEUE / SHARED (default AUTO)   */
