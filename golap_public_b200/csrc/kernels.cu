@@ -1893,34 +1893,23 @@ static gx_status scan_launch_shared(const gx_scan_plan* plan, const QueryDesc& q
     shared_layout(P, c0);
     P.rows_scanned = rows_dev;
     const uint32_t n_slots = c0->n_slots;
-    uint32_t* scratch = nullptr;
-    GX_CK(scratch_alloc((void**)&scratch, 4ull * (2ull * n_slots + 2), s));
-    P.n_items = scratch;
-    P.work_counter = scratch + 1;
-    P.items = scratch + 2;
-    P.slot_mask = scratch + 2 + n_slots;
-    cudaError_t e = cudaMemsetAsync(scratch, 0, 8, s);
-    if (e == cudaSuccess) {
-        const unsigned ig = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(8ull * sm_count(), (n_slots + 7) / 8));
-        shared_items_kernel<<<ig, 256, 0, s>>>(P, scratch + 2 + n_slots, scratch + 2, scratch);
-        P.gt_slots = P.q1.grouped ? kShGroupSlots : 0u;
-        const size_t smem = shared_smem_bytes(P.n_cols, 1, 0, 0, P.gt_slots);
-        static int occ[64][kShMaxCols + 1][2] = {};
-        int dev = 0;
-        cudaGetDevice(&dev);
-        int& per_sm = occ[dev & 63][P.n_cols][P.gt_slots ? 1 : 0];
-        if (per_sm == 0) {
-            int v = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, shared_scan_kernel<kShSingleNT, 4, true>, kShSingleNT,
-                                                          smem);
-            per_sm = std::max(1, v);
-        }
-        const uint64_t tiles = (uint64_t)n_slots * P.tiles_per_block;
-        const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm, tiles));
-        shared_scan_kernel<kShSingleNT, 4, true><<<grid, kShSingleNT, smem, s>>>(P);
-        e = cudaGetLastError();
+    // no work list: the kernel's CTAs check their share of the (slot, tile)
+    // items themselves (see sh_single_live), so the launch is one kernel
+    P.gt_slots = P.q1.grouped ? kShGroupSlots : 0u;
+    const size_t smem = shared_smem_bytes(P.n_cols, 1, 0, 0, P.gt_slots);
+    static int occ[64][kShMaxCols + 1][2] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& per_sm = occ[dev & 63][P.n_cols][P.gt_slots ? 1 : 0];
+    if (per_sm == 0) {
+        int v = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, shared_scan_kernel<kShSingleNT, 4, true>, kShSingleNT, smem);
+        per_sm = std::max(1, v);
     }
-    cudaFreeAsync(scratch, s);
+    const uint64_t tiles = (uint64_t)n_slots * P.tiles_per_block;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm, tiles));
+    shared_scan_kernel<kShSingleNT, 4, true><<<grid, kShSingleNT, smem, s>>>(P);
+    const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "shared scan launch: %s", cudaGetErrorString(e));
     *done = true;
     return GX_OK;

@@ -402,6 +402,31 @@ __device__ __forceinline__ uint32_t shared_literal_copy(uint32_t cols, uint32_t 
     return done;
 }
 
+// One-query launches: whether tile `tile` of block slot `slot` is work --
+// the pruning of shared_items_kernel (chunk min/max and keep_in, the slice,
+// the block zone maps) applied per tile; writes the chunk's keep_out flag
+// for the chunk's first tile.
+__device__ __forceinline__ bool sh_single_live(const ShParams& P, uint32_t slot, uint32_t tile) {
+    const ShQuery& Q = P.q1;
+    const uint32_t chunk = slot / P.blocks_per_chunk, j = slot % P.blocks_per_chunk;
+    bool ck = Q.keep_in ? Q.keep_in[chunk] != 0 : true;
+    for (uint32_t p = 0; ck && p < Q.n_prune; ++p) {
+        const PrunePred& pr = Q.prune[p];
+        ck = pr.lo <= pr.maxs[chunk] && pr.hi >= pr.mins[chunk];
+    }
+    if (Q.keep_out && j == 0 && tile == 0) Q.keep_out[chunk] = ck ? 1 : 0;
+    const uint32_t rows = P.dir[slot].n_rows, r0 = tile * P.tile_rows;
+    if (!ck || r0 >= rows) return false;
+    const uint64_t g0 = (uint64_t)chunk * P.rows_per_chunk + (uint64_t)j * P.rows_per_block + r0;
+    const uint32_t n = min(P.tile_rows, rows - r0);
+    if (!(Q.row_lo < g0 + n && Q.row_hi > g0)) return false;
+    for (uint32_t p = 0; p < Q.n_prune; ++p) {
+        const PrunePred& pr = Q.prune[p];
+        if (pr.bmins && !(pr.lo <= pr.bmaxs[slot] && pr.hi >= pr.bmins[slot])) return false;
+    }
+    return true;
+}
+
 // Persistent shared-scan kernel: NT threads, tiles of up to kShTile rows.
 // Per tile, the active queries are evaluated one after another, step-major:
 // a step's fields go to registers, then the step runs over the RPT row
@@ -439,6 +464,8 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
     __shared__ CascTile s_ct;
     __shared__ uint32_t s_seg[2 * (kMaxSegments + 1)];
     __shared__ uint32_t s_cols;                    // batches: columns the tile's active queries read
+    __shared__ uint32_t s_list[SINGLE ? NT : 1];   // one query: this CTA's live items of the round
+    __shared__ uint32_t s_ln, s_li, s_w0;          // their count, the next one, the next round's start
     __shared__ const uint8_t* s_lit[kShMaxCols];   // batches: a literal tile's first byte, or null
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -461,18 +488,56 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
     uint32_t phase = 0;
     unsigned long long local_rows = 0;
     const uint32_t tpb = P.tiles_per_block, tile_rows = P.tile_rows;
-    const uint32_t total = *P.n_items * tpb;
+    // one query: every (slot, tile) item is a candidate, checked by the CTA it
+    // falls to (item w goes to CTA w mod grid); batches: the compacted work
+    // list of shared_items_kernel, taken from a counter
+    const uint32_t total = SINGLE ? P.n_slots * tpb : *P.n_items * tpb;
     const uint32_t MW = P.mask_words;
-    if (tid == 0) s_item = atomicAdd(P.work_counter, 1u);
+    if (tid == 0) {
+        if (SINGLE) {
+            s_ln = 0;
+            s_li = 0;
+            s_w0 = 0;
+        } else {
+            s_item = atomicAdd(P.work_counter, 1u);
+        }
+    }
     __syncthreads();
 
     while (true) {
-        const uint32_t it = s_item;
-        if (it >= total) break;
-        // thread 0 takes the next work item now; its result is needed only at the tile's end
+        uint32_t it;
+        if constexpr (SINGLE) {
+            // the round's list used up: check the next round of candidates, one per thread
+            while (s_li >= s_ln && s_w0 < total) {
+                const uint32_t w = s_w0 + blockIdx.x + tid * gridDim.x;
+                const bool live = w < total && sh_single_live(P, w / tpb, w % tpb);
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, live);
+                if (lane == 0) s_tmp[warp] = __popc(bal);
+                __syncthreads();
+                uint32_t off = 0, cnt = 0;
+                for (uint32_t k = 0; k < (uint32_t)NW; ++k) {
+                    off += k < warp ? s_tmp[k] : 0u;
+                    cnt += s_tmp[k];
+                }
+                if (live) s_list[off + __popc(bal & ((1u << lane) - 1u))] = w;
+                __syncthreads();
+                if (tid == 0) {
+                    s_ln = cnt;
+                    s_li = 0;
+                    s_w0 += gridDim.x * NT;
+                }
+                __syncthreads();
+            }
+            if (s_li >= s_ln) break;
+            it = s_list[s_li];
+        } else {
+            it = s_item;
+            if (it >= total) break;
+        }
+        // batches: thread 0 takes the next work item now; its result is needed only at the tile's end
         uint32_t next_it = 0xFFFFFFFFu;
-        if (tid == 0) next_it = atomicAdd(P.work_counter, 1u);
-        const uint32_t slot = P.items[it / tpb];
+        if (!SINGLE && tid == 0) next_it = atomicAdd(P.work_counter, 1u);
+        const uint32_t slot = SINGLE ? it / tpb : P.items[it / tpb];
         const uint32_t r0 = (it % tpb) * tile_rows;
         const uint32_t rows = P.dir[slot].n_rows;
         if (r0 < rows) {
@@ -481,7 +546,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
         const uint64_t g0 = (uint64_t)chunk * P.rows_per_chunk + (uint64_t)j * P.rows_per_block + r0;
         // active queries of this tile: the block's mask restricted to slices that reach the tile
         for (uint32_t w = tid; w < MW; w += NT) {
-            uint32_t m = P.slot_mask[(size_t)slot * MW + w], keepm = m;
+            uint32_t m = SINGLE ? 1u : P.slot_mask[(size_t)slot * MW + w], keepm = m;
             while (m) {
                 const uint32_t bit = __ffs(m) - 1;
                 m &= m - 1;
@@ -777,8 +842,16 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
         }  // r0 < rows
         __syncthreads();
         if (tid == 0) {
-            s_item = s_fatal ? 0xFFFFFFFFu : next_it;
-            if (!SINGLE) s_cols = 0;
+            if (SINGLE) {
+                ++s_li;
+                if (s_fatal) {  // stop this CTA: nothing left in the list or in later rounds
+                    s_li = s_ln;
+                    s_w0 = total;
+                }
+            } else {
+                s_item = s_fatal ? 0xFFFFFFFFu : next_it;
+                s_cols = 0;
+            }
         }
         __syncthreads();
     }
