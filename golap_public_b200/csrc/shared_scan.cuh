@@ -81,6 +81,8 @@ struct ShParams {
     const ShQuery* qs;
     uint32_t n_queries;
     uint32_t mask_words;        // ceil(n_queries / 32)
+    // batches: the work list of shared_items_kernel (one-query launches prune
+    // their own work and leave these null)
     const uint32_t* slot_mask;  // n_slots * mask_words
     const uint32_t* items;      // compacted slots
     const uint32_t* n_items;
