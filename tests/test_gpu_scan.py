@@ -94,6 +94,23 @@ def test_q1_config1_sorted_pruned(cuda, S):
             assert q.keep.cpu().numpy().tolist() == O.minmax_keep(mins, maxs, 19940101, 19940131).tolist()
 
 
+def test_q1_keep_chunks_in_and_out(cuda):
+    # per-chunk keep flags handed to the scan (MetaChecker output) combine with
+    # the plan's own min/max pruning; keep_out receives keep_in AND min/max
+    f = datagen.fact_q1(7_500_000, True)
+    dd = datagen.date_dim()
+    fact = queries.encode_fact(f, {"date_key": "cascaded"})
+    ok = dd["d_year"] == 1993
+    keep_in = np.array([1, 1, 0, 1, 1, 0, 1, 1], dtype=np.uint16)
+    q = queries.Q1Query(fact, dd, ok, 19930101, 19931231, 1, 3, 0, 24, prune=True)
+    q.plan.keep_chunks = cuda.from_numpy(keep_in).cuda()
+    got = q.run()
+    assert got == _oracle_q1(f, dd, ok, 1, 3, 0, 24, keep=keep_in, rpc=1_000_000)
+    assert got != _oracle_q1(f, dd, ok, 1, 3, 0, 24)  # the dropped chunks held qualifying rows
+    mins, maxs = fact.cols["date_key"].minmax()
+    assert q.keep.cpu().numpy().tolist() == O.minmax_keep(mins, maxs, 19930101, 19931231, keep=keep_in).tolist()
+
+
 def test_q1_pinned_host_residency(cuda):
     # compressed columns in pinned host memory, read by the kernels over
     # PCIe: the same results as HBM residency, pruned and over every date
