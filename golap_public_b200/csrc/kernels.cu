@@ -1,15 +1,19 @@
 // kernels.cu -- sm_100a kernels of the hot path and the C-ABI entry points
 // that launch them.
 //
-//   scan_kernel        fused per-tile decode -> filter -> probe -> aggregate
+//   shared_scan_kernel (shared_scan.cuh) the fused scan: per 2048-row tile,
+//                      decode into shared memory -> filter -> probe ->
+//                      aggregate, one query (which prunes its own work) or a
+//                      batch (work list from shared_items_kernel)
 //                      (replaces ChunkDecompressor + pipeline_q1_lineorder,
 //                      usecases/ssb/queries/01.cuh:27-54, and pipeline_q3,
 //                      usecases/ssb/queries/03.cuh:119-170)
+//   scan_kernel        the per-query (queue) form of the same fused scan
 //   items_kernel       min/max pruning + compaction of surviving chunks
 //                      (check_mmmeta/combine_and, core/metadata.cuh:540-547,632-636)
 //   decompress_kernel  chunk decompression to global memory
 //                      (ChunkDecompressor::step, core/comp.cuh:171-195)
-//   ht_build_kernel / ht_probe_kernel
+//   ht_build_kernel / ht_build_small_kernel / ht_build_dense_kernel / ht_probe_kernel
 //                      (hash_map_build_pred_other core/join.cuh:107-135,
 //                       hash_join_count core/join.cuh:46-59)
 //   groupby_add_kernel (group_by_agg_2col core/group.cuh:15-24 with SumAgg)
