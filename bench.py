@@ -14,19 +14,34 @@ workload's shapes and distributions.
             reference's uncompressed-bytes / time definition), compressed
             columns resident in HBM, device time (CUDA events) per step,
             the step captured once as a CUDA graph and replayed, L2
-            flushed between steps.
+            flushed between steps; surviving_rows_per_s counts only the
+            rows of the tiles the scan reads.
+  latency   p50/p99 of the same step over at least one second of replays.
   e2e       the same query with the compressed columns in pinned host
             memory, read by the kernels over PCIe, timed through the public
             API with the date dimension copied in and the result read back.
-  roofline  the fused scan kernel: algorithmic bytes (compressed bytes of
-            the surviving tiles + their directory/segment index) per launch
-            / launch time, against the measured HBM copy bandwidth.
-  cpu_baseline  the reference's CPU path on the same data: LZ4CPUManager
-            decompression + the query loop over HostHashMap, all host cores.
+  roofline  the fused scan kernel of the step: algorithmic bytes
+            (compressed bytes of the surviving tiles + their directory /
+            side-index entries + min/max metadata) per launch / launch
+            time, against the measured HBM copy bandwidth.
+  full_scan the same plan over every date (no pruning, every tile needs
+            all four columns): the bandwidth-bound case, with its own
+            roofline; full_scan_lz4_matches repeats it with the LZ4 columns
+            encoded with 4-byte matches (token-heavy streams).
+  star_join the 600,000,000-row star join + group-by: three filtered
+            dimension-table builds (customer 3M, supplier 200k, date) and
+            the fused probe/aggregate scan; rows/s, roofline, e2e from
+            pinned host memory, the reference CPU arm on the same bytes.
+  cpu_baseline  the reference's CPU path on the same compressed bytes:
+            LZ4CPUManager decompression (cascaded date_key: the harness's
+            decoder of this build's format) + the query loop over
+            HostHashMap, all host cores.
 
 --impl reference runs only the CPU path (rank 0) and prints its line.
 --gpus N runs N independent replicas (one per GPU; the query does not need
 a collective); value is the total over ranks, time is the max over ranks.
+Clock samples are written as CSV into the directory named by
+GX_BENCH_CLOCKS_DIR when it is set.
 """
 from __future__ import annotations
 
@@ -74,17 +89,18 @@ def profile_traffic():
 class Clocks:
     """Samples SM clocks and clock-event (throttle) reasons through NVML in a
     background thread (every 2 ms) while the timed region runs; the samples
-    are also written to gpurun_out/clocks_bench_<pid>.csv."""
+    are also written as CSV into $GX_BENCH_CLOCKS_DIR when it is set."""
 
     NAMES = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
              ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, gpu: int):
+    def __init__(self, gpu: int, tag: str = "step"):
         self.gpu = gpu
         self.samples = []
         self.max_mhz = None
         self.err = None
-        self.path = ROOT / "gpurun_out" / f"clocks_bench_{os.getpid()}.csv"
+        d = os.environ.get("GX_BENCH_CLOCKS_DIR")
+        self.path = Path(d) / f"clocks_bench_{tag}_{os.getpid()}.csv" if d else None
 
     def _handle(self):
         import pynvml
@@ -133,8 +149,10 @@ class Clocks:
         self.stop.set()
         if self.thread:
             self.thread.join(2.0)
+        if self.path is None:
+            return
         try:
-            self.path.parent.mkdir(exist_ok=True)
+            self.path.parent.mkdir(parents=True, exist_ok=True)
             with open(self.path, "w") as fh:
                 fh.write("t_s,sm_mhz,reasons_hex\n")
                 for t, m, r in self.samples:
@@ -171,6 +189,71 @@ def make_data(seed):
     return datagen.fact_q1(N_ROWS, True, seed=seed), datagen.date_dim()
 
 
+Q1_COLS = ("date_key", "discount", "quantity", "extended_price")
+Q3_COLS = ("date_key", "cust_key", "supp_key", "revenue")
+
+
+def comp_columns(fact, names):
+    """(payload, blocks, codec) of each column: the compressed bytes the GPU scans, for the CPU arm."""
+    return [(fact.cols[n].payload_view(), fact.cols[n].blocks(), 1 if fact.cols[n].codec == "lz4" else 2)
+            for n in names]
+
+
+def present_index(info, n_rows):
+    """Index into the present-block list (gx_column_blocks order) of every block slot, -1 if absent."""
+    bpc = info.blocks_per_chunk
+    idx = np.full(info.n_chunks * bpc, -1, np.int64)
+    k = 0
+    for ch in range(info.n_chunks):
+        rows = min(info.rows_per_chunk, n_rows - ch * info.rows_per_chunk)
+        nb = -(-rows // info.rows_per_block)
+        idx[ch * bpc: ch * bpc + nb] = np.arange(k, k + nb)
+        k += nb
+    return idx
+
+
+def alg_bytes(fact, names, slots, n_chunks_meta, zone_blocks):
+    """Algorithmic bytes of one scan: compressed bytes of the given block slots in the
+    named columns + 16 B of directory per block + 8 B per side-index entry, + 8 B of
+    chunk min/max per chunk and 8 B of zone map per block checked."""
+    tot = 0
+    for name in names:
+        c = fact.cols[name]
+        info = c.info
+        pidx = present_index(info, fact.n_rows)[np.asarray(slots, np.int64)] if len(slots) else []
+        sel = c.blocks()[pidx] if len(slots) else np.zeros((0, 4), np.uint64)
+        per = info.lz4_segments if (c.codec == "lz4" and info.lz4_segments > 1) else (
+            -(-info.rows_per_block // 2048) if c.codec == "cascaded" else 0)
+        tot += int(sel[:, 2].sum()) + 16 * len(sel) + 8 * per * len(sel)
+    return tot + 8 * n_chunks_meta + 8 * zone_blocks
+
+
+def time_launches(fn, reps, stream, flush=None, pre=None):
+    """Device time (ms, CUDA events on `stream`) of fn() per rep, L2 flushed before each."""
+    import torch
+
+    out = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        if pre is not None:
+            pre()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        out.append(a.elapsed_time(b))
+    return out
+
+
+def roofline(bytes_, ms, pk, pk_kind, traffic=None):
+    a = bytes_ / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": a, "peak": pk, "unit": "GB/s", "frac": a / pk, "traffic": traffic,
+            "peak_kind": pk_kind, "algorithmic_bytes_per_launch": int(bytes_)}
+
+
 # ----------------------------------------------------------------- GPU arm
 
 def gpu_arm(args, rank, world):
@@ -194,28 +277,21 @@ def gpu_arm(args, rank, world):
     dk_d = torch.empty_like(dk_h, device="cuda")
     ok_d = torch.empty_like(ok_h, device="cuda")
     stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    pk, pk_kind = peaks()
 
-    def step():
-        # the per-query work of the reference's query1 timed region
-        # (01.hpp:235-430): date table build, pruning, fused scan
+    for _ in range(args.warmup):
         q.ht.build(q._dk, None, preds=[(q._ok, 1, 1)])
         q.launch()
-
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    for _ in range(args.warmup):
-        step()
     torch.cuda.synchronize()
     got = q.run()
-    want = got  # checked against the CPU baseline's result below
     kept = int(q.keep.sum().item())
     kept_chunks = np.nonzero(q.keep.cpu().numpy())[0].tolist()
 
-    # algorithmic bytes of the scan per launch: compressed bytes of the
-    # blocks the query needs (surviving chunks, and within them the blocks
-    # whose date_key zone map meets the predicate) in the 4 columns + their
-    # block directory and segment index entries + the date_key chunk min/max
-    # and block zone maps read by pruning
+    # block slots the pruned scan reads: surviving chunks, and within them the
+    # blocks whose date_key zone map meets the predicate
     bpc = fact.cols["date_key"].info.blocks_per_chunk
+    n_chunks = fact.cols["date_key"].info.n_chunks
 
     def slots_of(chunks, zone=True):
         out = []
@@ -231,14 +307,10 @@ def gpu_arm(args, rank, world):
                 out.append(ch * bpc + j)
         return out
 
-    def alg_bytes(chunks, zone=True):
-        slots = slots_of(chunks, zone)
-        tot = 0
-        for name, c in fact.cols.items():
-            info = c.info
-            sel = c.blocks()[slots]
-            tot += int(sel[:, 2].sum()) + 16 * len(sel) + (8 * info.lz4_segments * len(sel) if info.lz4_segments > 1 else 0)
-        return tot + 8 * fact.cols["date_key"].info.n_chunks + (8 * bpc * len(chunks) if zone else 0)
+    pruned_slots = slots_of(kept_chunks)
+    scan_bytes = alg_bytes(fact, Q1_COLS, pruned_slots, n_chunks, bpc * len(kept_chunks))
+    bi = fact.cols["date_key"].blocks()
+    surviving_rows = int(bi[present_index(fact.cols["date_key"].info, N_ROWS)[pruned_slots], 3].sum())
 
     # the step (date table build, result clear, pruning + fused scan: one
     # library call) captured once as a CUDA graph and replayed per step, so
@@ -284,53 +356,57 @@ def gpu_arm(args, rank, world):
     ms = max_over_ranks(float(np.mean(step_ms)), world, "cuda")
     if int(q.result.item()) != got:
         raise SystemExit("timed steps changed the result")
+
+    # latency distribution: the same graph replayed for at least one second
+    lat_ms, lat_wall = [], time.perf_counter()
+    with Clocks(dev, "latency") as clk_lat:
+        while time.perf_counter() - lat_wall < args.latency_s or len(lat_ms) < 100:
+            lat_ms += time_launches(graph.replay, 200, stream, flush)
+        lat_wall = time.perf_counter() - lat_wall
+
     # the fused scan alone (pruning + scan, one library call), launched directly
-    scan_ms = []
-    for _ in range(args.steps):
-        flush.zero_()
-        q.ht.build(q._dk, None, preds=[(q._ok, 1, 1)])
-        q.result.zero_()
-        b = torch.cuda.Event(enable_timing=True)
-        c = torch.cuda.Event(enable_timing=True)
-        b.record(stream)
-        q.plan.launch()
-        c.record(stream)
-        c.synchronize()
-        scan_ms.append(b.elapsed_time(c))
+    scan_ms = time_launches(q.plan.launch, max(args.steps, 20), stream, flush,
+                            pre=lambda: (q.ht.build(q._dk, None, preds=[(q._ok, 1, 1)]), q.result.zero_()))
     scan_avg = float(np.mean(scan_ms))
 
     # full-table scan: the same Q1 plan over every date (pruning off), so every
-    # tile needs all four columns -- the decode-bound throughput of the kernel
+    # tile needs all four columns -- the bandwidth-bound throughput of the kernel
     ok_all = np.ones(len(dd["d_key"]), dtype=bool)
-    q_all = queries.Q1Query(fact, dd, ok_all, int(dd["d_key"].min()), int(dd["d_key"].max()), *DISC, *QTY,
-                            prune=False)
     m_all = (f["discount"] >= DISC[0]) & (f["discount"] <= DISC[1]) & (f["quantity"] >= QTY[0]) & \
             (f["quantity"] <= QTY[1])
     want_all = int((f["extended_price"][m_all].astype(np.int64) * f["discount"][m_all].astype(np.int64)).sum())
-    if q_all.run() != want_all:
-        raise SystemExit("full scan result differs from the numpy sum")
-    for _ in range(3):
-        q_all.launch()
-    all_ms = []
-    for _ in range(max(3, min(args.steps, 10))):
-        flush.zero_()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        q_all.result.zero_()
-        a.record(stream)
-        q_all.plan.launch()
-        b.record(stream)
-        torch.cuda.synchronize()
-        all_ms.append(a.elapsed_time(b))
-    all_ms_avg = float(np.mean(all_ms))
-    all_bytes = alg_bytes(range(fact.cols["date_key"].info.n_chunks), zone=False)
+    all_slots = slots_of(range(n_chunks), zone=False)
+
+    def full_scan(fct, label):
+        qa = queries.Q1Query(fct, dd, ok_all, int(dd["d_key"].min()), int(dd["d_key"].max()), *DISC, *QTY,
+                             prune=False)
+        if qa.run() != want_all:
+            raise SystemExit(f"{label}: full scan result differs from the numpy sum")
+        for _ in range(3):
+            qa.launch()
+        t = time_launches(qa.launch, max(5, min(args.steps, 20)), stream, flush)
+        avg = float(np.mean(t))
+        nbytes = alg_bytes(fct, Q1_COLS, all_slots, 0, 0)
+        return {"ms": avg, "rows_per_s": N_ROWS / (avg * 1e-3), "comp_gbs": nbytes / (avg * 1e-3) / 1e9,
+                "roofline_frac": nbytes / (avg * 1e-3) / 1e9 / pk, "uncomp_gbs": N_ROWS * 16 / (avg * 1e-3) / 1e9,
+                "roofline": roofline(nbytes, avg, pk, pk_kind),
+                "comp_bytes": {k: c.info.comp_bytes for k, c in fct.cols.items()}}
+
+    full = full_scan(fact, "literal policy")
+    full["lz4_policy"] = "decode-cost-aware (lz4_min_match=0): random-valued columns stored as literal runs"
+    # the same data with the LZ4 columns encoded with 4-byte matches
+    fact_m = queries.encode_fact({k: f[k] for k in Q1_COLS if k != "date_key"}, {}, ROWS_PER_CHUNK, ROWS_PER_BLOCK,
+                                 args.segments, lz4_min_match=4)
+    fact_m.cols["date_key"] = fact.cols["date_key"]
+    full_m = full_scan(fact_m, "4-byte matches")
+    full_m["lz4_policy"] = "lz4_min_match=4 (every 4-byte repeat inside a segment becomes a match)"
 
     # e2e: pinned-host residency, date dimension in, result out
     fact_h = queries.encode_fact(f, {"date_key": "cascaded"}, ROWS_PER_CHUNK, ROWS_PER_BLOCK, args.segments,
                                  residency="pinned")
     qh = queries.Q1Query(fact_h, dd, ok, DATE_LO, DATE_HI, *DISC, *QTY, prune=True)
     res_h = torch.zeros(1, dtype=torch.int64).pin_memory()
-    h2d_scan = alg_bytes(kept_chunks) - 8 * fact.cols["date_key"].info.n_chunks - 8 * bpc * len(kept_chunks)
+    h2d_scan = alg_bytes(fact, Q1_COLS, pruned_slots, 0, 0)
 
     def e2e_step():
         dk_d.copy_(dk_h, non_blocking=True)
@@ -342,24 +418,12 @@ def gpu_arm(args, rank, world):
     for _ in range(args.warmup):
         e2e_step()
     torch.cuda.synchronize()
-    if int(res_h.item()) != want:
+    if int(res_h.item()) != got:
         raise SystemExit("e2e result mismatch")
-    e_ms = []
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        e2e_step()
-        b.record(stream)
-        b.synchronize()
-        e_ms.append(a.elapsed_time(b))
+    e_ms = time_launches(e2e_step, args.steps, stream, flush, pre=torch.cuda.synchronize)
     e2e_ms = max_over_ranks(float(np.mean(e_ms)), world, "cuda")
+    del fact_h, qh
 
-    pk, pk_kind = peaks()
-    scan_bytes = alg_bytes(kept_chunks)
-    achieved = scan_bytes / (scan_avg * 1e-3) / 1e9
     line = {
         "metric": "rows/s & GB/s vs HBM roofline; p50/p99 latency batched vs one-query-at-a-time",
         "value": N_ROWS * world / (ms * 1e-3),
@@ -373,19 +437,21 @@ def gpu_arm(args, rank, world):
         "vs_baseline": None,
         "dtype": "int32",
         "data": "synthetic (seeded, configs[1] shapes and distributions)",
-        "config": {"workload": WORKLOAD, "rows": N_ROWS, "chunks": N_ROWS // ROWS_PER_CHUNK, "chunks_scanned": kept,
-                   "lz4_segments": args.segments, "residency": "hbm", "l2": "flushed between steps (256 MiB write)", "launch": "step replayed from a CUDA graph",
-                   "parallelism": f"replicas x{world}", "comp_bytes": comp},
+        "config": {"workload": WORKLOAD, "rows": N_ROWS, "chunks": n_chunks, "chunks_scanned": kept,
+                   "lz4_segments": args.segments, "residency": "hbm", "l2": "flushed between steps (256 MiB write)",
+                   "launch": "step replayed from a CUDA graph", "parallelism": f"replicas x{world}",
+                   "comp_bytes": comp},
         "result": got,
-        "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
+        "surviving_rows": surviving_rows,
+        "surviving_rows_per_s": surviving_rows * world / (ms * 1e-3),
+        "latency_ms": {"p50": float(np.percentile(lat_ms, 50)), "p99": float(np.percentile(lat_ms, 99)),
+                       "mean": float(np.mean(lat_ms)), "samples": len(lat_ms), "timed_s": lat_wall,
+                       "clocks": clk_lat.summary()},
         "scan_kernel_ms": scan_avg,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk, "unit": "GB/s", "frac": achieved / pk,
-                     "traffic": profile_traffic(), "peak_kind": pk_kind,
-                     "algorithmic_bytes_per_launch": scan_bytes},
-        "full_scan": {"ms": all_ms_avg, "rows_per_s": N_ROWS / (all_ms_avg * 1e-3),
-                      "comp_gbs": all_bytes / (all_ms_avg * 1e-3) / 1e9,
-                      "roofline_frac": all_bytes / (all_ms_avg * 1e-3) / 1e9 / pk,
-                      "uncomp_gbs": N_ROWS * 16 / (all_ms_avg * 1e-3) / 1e9},
+        "roofline": roofline(scan_bytes, scan_avg, pk, pk_kind, profile_traffic()),
+        "roofline_full_scan": full["roofline"],
+        "full_scan": full,
+        "full_scan_lz4_matches": full_m,
         "e2e": {"value": N_ROWS * world / (e2e_ms * 1e-3), "unit": "rows/s",
                 "h2d_bytes_per_step": int(h2d_scan + dd["d_key"].nbytes + ok.astype(np.int32).nbytes),
                 "d2h_bytes_per_step": 8, "ms_per_step": e2e_ms, "residency": "pinned host (zero-copy reads)"},
@@ -393,7 +459,126 @@ def gpu_arm(args, rank, world):
         "clocks": clk.summary(),
         "wall_s_timed": t_wall,
     }
-    return line, f, dd
+    ctx = {"f": f, "dd": dd, "fact": fact, "fact_m": fact_m, "want_all": want_all}
+    return line, ctx
+
+
+def star_join_section(args, pk, pk_kind, world=1):
+    """the 600M-row star join + group-by, one query per step:
+    filtered builds of the customer (3M), supplier (200k) and date tables,
+    then the fused scan probing customer -> supplier -> date and summing
+    revenue per (c_nation, s_nation, year); min/max pruning on date_key."""
+    import torch
+
+    from golap_public_b200 import datagen, queries
+
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    n = args.star_rows
+    t0 = time.perf_counter()
+    g = datagen.fact_q3(n, True, seed=args.seed)
+    cust = datagen.dim_geo(3_000_000, args.seed, 21)
+    supp = datagen.dim_geo(200_000, args.seed, 22)
+    dd = datagen.date_dim()
+    fact = queries.encode_fact({k: g[k] for k in Q3_COLS}, {"date_key": "cascaded"}, ROWS_PER_CHUNK,
+                               ROWS_PER_BLOCK, args.segments)
+    # the customer dimension compressed like the fact table; its join table is
+    # built from the compressed chunks inside every step
+    cust_c = queries.encode_fact(cust, {"key": "cascaded", "nation": "cascaded", "region": "cascaded"},
+                                 ROWS_PER_CHUNK, ROWS_PER_BLOCK, args.segments)
+    build_s = time.perf_counter() - t0
+    region, ylo, yhi = 2, 1992, 1997
+    q = queries.Q3Query(fact, cust_c, supp, dd, region, ylo, yhi, ht_layout=args.star_layout)
+    got = q.run()
+
+    def step():
+        q.build_customer()
+        q.hs.build(q._keep_alive[3], q._keep_alive[4], preds=[(q._keep_alive[5], region, region)])
+        q.hd.build(q._keep_alive[6], q._keep_alive[7], preds=[(q._keep_alive[7], ylo, yhi)])
+        q.launch()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    step_ms = time_launches(step, max(5, min(args.steps, 20)), stream, flush)
+    if q.run() != got:
+        raise SystemExit("star join: repeated steps changed the result")
+    scan_ms = time_launches(q.launch, max(5, min(args.steps, 20)), stream, flush)
+    ms, sms = float(np.mean(step_ms)), float(np.mean(scan_ms))
+    kept = np.nonzero(q.keep.cpu().numpy())[0]
+    info = fact.cols["date_key"].info
+    bpc = info.blocks_per_chunk
+    pidx = present_index(info, n)
+    # blocks of the surviving chunks whose date_key zone map meets the year range
+    bi = fact.cols["date_key"].blocks()
+    lo_key, hi_key = ylo * 10000 + 101, yhi * 10000 + 1231
+    slots = []
+    for c in kept:
+        for j in range(bpc):
+            k = pidx[c * bpc + j]
+            if k < 0:
+                continue
+            r0 = c * ROWS_PER_CHUNK + j * ROWS_PER_BLOCK
+            blk = g["date_key"][r0:r0 + int(bi[k, 3])]
+            if blk.max() >= lo_key and blk.min() <= hi_key:
+                slots.append(c * bpc + j)
+    nbytes = alg_bytes(fact, Q3_COLS, slots, info.n_chunks, bpc * len(kept))
+    rows_scanned = int(bi[pidx[np.asarray(slots)], 3].sum())
+    # dimension side of a step: the compressed customer columns and the supplier /
+    # date key + payload + filter columns read, 8 B per inserted entry written
+    dim_bytes = sum(c.info.comp_bytes for c in cust_c.cols.values()) + 200_000 * 12 + len(dd["d_key"]) * 8 + \
+        8 * (int((cust["region"] == region).sum()) + int((supp["region"] == region).sum()) + 2192)
+    # the customer build alone (one fused decode + filter + insert launch over 3M compressed rows)
+    cust_ms = float(np.mean(time_launches(q.build_customer, 10, stream, flush)))
+    out = {"rows": n, "chunks": fact.cols["date_key"].info.n_chunks, "chunks_scanned": int(len(kept)),
+           "rows_scanned": rows_scanned, "ht_layout": args.star_layout,
+           "workload": "star join + group-by: 600M-row fact (cust_key U[1,3M], supp_key U[1,200k], date_key sorted, "
+                       "revenue U[100,1M]; date_key cascaded, others LZ4), customer 3M / supplier 200k / date 2,556; "
+                       f"c.region == s.region == {region}, year {ylo}..{yhi}; SUM(revenue) GROUP BY "
+                       "(c_nation, s_nation, year)",
+           "table_build_s": build_s, "groups": len(got), "result_total": int(sum(got.values())),
+           "ms_per_step": ms, "rows_per_s": n * world / (ms * 1e-3),
+           "surviving_rows_per_s": rows_scanned * world / (ms * 1e-3),
+           "scan_kernel_ms": sms, "roofline": roofline(nbytes, sms, pk, pk_kind),
+           "step_bytes_incl_dims": nbytes + dim_bytes,
+           "customer_build_ms": cust_ms,
+           "customer_build": "3M-row customer join table built from compressed customer columns (key, nation, "
+                             "region cascaded) in one fused decode + filter + insert launch",
+           "comp_bytes": {k: c.info.comp_bytes for k, c in fact.cols.items()}}
+    # e2e: the fact columns in pinned host memory, dimension columns copied in, groups read back
+    fact_h = queries.encode_fact({k: g[k] for k in Q3_COLS}, {"date_key": "cascaded"}, ROWS_PER_CHUNK,
+                                 ROWS_PER_BLOCK, args.segments, residency="pinned")
+    qh = queries.Q3Query(fact_h, cust, supp, dd, region, ylo, yhi, ht_layout=args.star_layout)
+    host_dims = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in
+                 (cust["key"], cust["nation"], cust["region"], supp["key"], supp["nation"], supp["region"],
+                  dd["d_key"], dd["d_year"])]
+
+    def e2e_step():
+        for hsrc, ddst in zip(host_dims, qh._keep_alive):
+            ddst.copy_(hsrc, non_blocking=True)
+        ck, cn, cr, sk, sn, sr, dk, dy = qh._keep_alive
+        qh.hc.build(ck, cn, preds=[(cr, region, region)])
+        qh.hs.build(sk, sn, preds=[(sr, region, region)])
+        qh.hd.build(dk, dy, preds=[(dy, ylo, yhi)])
+        return qh.run()
+
+    if e2e_step() != got:
+        raise SystemExit("star join e2e result mismatch")
+    e_ms = []
+    for _ in range(3):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        e2e_step()
+        e_ms.append((time.perf_counter() - t) * 1e3)
+    e = float(np.mean(e_ms))
+    out["e2e"] = {"value": n / (e * 1e-3), "unit": "rows/s", "ms_per_step": e,
+                  "h2d_bytes_per_step": int(nbytes + sum(h.numel() * 4 for h in host_dims)),
+                  "d2h_bytes_per_step": 16 * len(got),
+                  "residency": "pinned host (zero-copy reads); host wall clock around each call, groups read back"}
+    del fact_h, qh
+    return out, {"g": g, "cust": cust, "supp": supp, "dd": dd, "fact": fact, "got": got, "region": region,
+                 "ylo": ylo, "yhi": yhi}
 
 
 # --------------------------------------------------- batched and serving forms
@@ -523,61 +708,101 @@ def serving_section(t, rates=(200, 1000, 2000), seconds=2.0, seed=9, max_backlog
 
 # ----------------------------------------------------------------- CPU arm
 
-def cpu_baseline(f, dd, steps=3, warmup=1, threads=None):
-    """The reference's CPU path on the same data (see ref_cpu_q1 in oracle/ref_harness.cu)."""
+def cpu_q1(cols, mins, maxs, dd, ok, lo, hi, steps=3, warmup=1, threads=None):
+    """The reference's CPU path on the Q1 workload's compressed bytes (ref_cpu_q1_comp in
+    oracle/ref_harness.cu): LZ4CPUManager decode + query1inmem's loop over HostHashMap."""
+    import ctypes as C
+
     from oracle import oracle as O
 
     threads = threads or os.cpu_count() or 1
-    ok = (dd["d_yearmonthnum"] == 199401).astype(np.uint8)
-    n_chunks = N_ROWS // ROWS_PER_CHUNK
-    bpc = -(-ROWS_PER_CHUNK // ROWS_PER_BLOCK)
-    mins, maxs = O.chunk_minmax(f["date_key"], ROWS_PER_CHUNK)
-    kind = "reference" if O.ref_available() else "port"
-    if kind == "port":
-        t = []
-        for _ in range(steps):
-            t0 = time.perf_counter()
-            keep = O.minmax_keep(mins, maxs, DATE_LO, DATE_HI)
-            r = O.q1(f["date_key"], f["discount"], f["quantity"], f["extended_price"], dd["d_key"], ok, *DISC, *QTY,
-                     keep_chunk=keep, rows_per_chunk=ROWS_PER_CHUNK)
-            t.append(time.perf_counter() - t0)
-        ms = 1e3 * float(np.mean(t))
-        return {"value": N_ROWS / (ms * 1e-3), "unit": "rows/s", "cores": 1, "kind": "port",
-                "sample": "full query (oracle restatement, 1 thread)", "ms": ms, "result": r}
-    R = O.ref()
-    stride = ROWS_PER_BLOCK * 4 + ROWS_PER_BLOCK * 4 // 255 + 64
-    comp, sizes = [], []
-    for name in ("discount", "quantity", "extended_price"):
-        v = f[name]
-        buf = np.zeros(n_chunks * bpc * stride, np.uint8)
-        sz = np.zeros(n_chunks * bpc, np.int32)
-        for c in range(n_chunks):
-            part = np.ascontiguousarray(v[c * ROWS_PER_CHUNK:(c + 1) * ROWS_PER_CHUNK])
-            assert R.ref_lz4_compress_blocks(O._ptr(part), part.nbytes, ROWS_PER_BLOCK * 4,
-                                             O._ptr(buf[c * bpc * stride:]), stride, O._ptr(sz[c * bpc:])) == 0
-        comp.append(buf)
-        sizes.append(sz)
+    arr = O.comp_cols(cols)
+    okb = ok.astype(np.uint8)
+    times, res = [], None
+    ch, rows = C.c_uint64(), C.c_uint64()
+    for i in range(warmup + steps):
+        el = C.c_double()
+        res = O.ref().ref_cpu_q1_comp(threads, N_ROWS, ROWS_PER_CHUNK, ROWS_PER_BLOCK, arr, O._ptr(mins),
+                                      O._ptr(maxs), O._ptr(dd["d_key"]), O._ptr(okb), len(okb), lo, hi, *DISC, *QTY,
+                                      C.byref(el), C.byref(ch), C.byref(rows))
+        if i >= warmup:
+            times.append(el.value)
+    return float(np.mean(times)), int(res), ch.value, rows.value, threads
+
+
+def cpu_baseline(fact, dd, steps=3, warmup=1, threads=None):
+    """The headline query (January 1994, pruned) on the reference CPU path, same compressed bytes."""
+    from oracle import oracle as O
+
+    ok = dd["d_yearmonthnum"] == 199401
+    mins, maxs = fact.cols["date_key"].minmax()
+    if not O.ref_available():
+        raise SystemExit("reference harness not built: __graft_entry__.build() compiles it where the reference "
+                         "tree is present")
+    ms, res, ch, rows, thr = cpu_q1(comp_columns(fact, Q1_COLS), mins, maxs, dd, ok, DATE_LO, DATE_HI, steps,
+                                    warmup, threads)
+    return {"value": N_ROWS / (ms * 1e-3), "unit": "rows/s", "cores": thr, "kind": "reference",
+            "sample": f"full query: min/max pruning to {ch} of {N_ROWS // ROWS_PER_CHUNK} chunks ({rows} rows), "
+                      "LZ4CPUManager decode of the GPU path's own discount/quantity/extended_price LZ4 blocks, "
+                      "date_key pages decoded by the harness's decoder of this build's cascaded format (the "
+                      "reference has no CPU decoder for its cascaded codec), HostHashMap date join; surviving "
+                      "blocks split over all threads",
+            "ms": ms, "result": res, "surviving_rows_per_s": rows / (ms * 1e-3)}
+
+
+def cpu_full_scan(fact, dd, want, steps=2, warmup=1, threads=None):
+    """The unpruned full scan (every date) on the reference CPU path, same compressed bytes."""
+    ok_all = np.ones(len(dd["d_key"]), dtype=bool)
+    mins, maxs = fact.cols["date_key"].minmax()
+    ms, res, ch, rows, thr = cpu_q1(comp_columns(fact, Q1_COLS), mins, maxs, dd, ok_all, int(dd["d_key"].min()),
+                                    int(dd["d_key"].max()), steps, warmup, threads)
+    if res != want:
+        raise SystemExit(f"cpu full scan result {res} != {want}")
+    return {"value": N_ROWS / (ms * 1e-3), "unit": "rows/s", "cores": thr, "kind": "reference", "ms": ms,
+            "sample": f"all {N_ROWS} rows, every date (no pruning), same compressed bytes as the GPU full scan"}
+
+
+def cpu_star_join(ctx, steps=2, warmup=1, threads=None):
+    """The 600M-row star join on the reference CPU path (ref_cpu_q3_comp in oracle/ref_harness.cu):
+    filtered HostHashMap builds, probes customer -> supplier -> date, thread-local group maps
+    merged through HostHashAggregate, over the GPU path's compressed bytes."""
     import ctypes as C
 
-    comp_ptrs = (C.c_void_p * 3)(*[b.ctypes.data for b in comp])
-    size_ptrs = (C.c_void_p * 3)(*[s.ctypes.data for s in sizes])
-    res = None
+    from oracle import oracle as O
+
+    threads = threads or os.cpu_count() or 1
+    fact, cust, supp, dd = ctx["fact"], ctx["cust"], ctx["supp"], ctx["dd"]
+    region, ylo, yhi = ctx["region"], ctx["ylo"], ctx["yhi"]
+    arr = O.comp_cols(comp_columns(fact, Q3_COLS))
+    mins, maxs = fact.cols["date_key"].minmax()
+    gk = np.zeros(4096, np.int64)
+    gs = np.zeros(4096, np.int64)
+    ng, ch, rows = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    n = fact.n_rows
     times = []
     for i in range(warmup + steps):
         el = C.c_double()
-        scanned = C.c_uint64()
-        r = R.ref_cpu_q1(threads, N_ROWS, ROWS_PER_CHUNK, ROWS_PER_BLOCK, O._ptr(f["date_key"]), O._ptr(mins),
-                         O._ptr(maxs), comp_ptrs, stride, size_ptrs, O._ptr(dd["d_key"]), O._ptr(ok), len(ok),
-                         DATE_LO, DATE_HI, *DISC, *QTY, C.byref(el), C.byref(scanned))
-        res = r
+        O.ref().ref_cpu_q3_comp(threads, n, ROWS_PER_CHUNK, ROWS_PER_BLOCK, arr, O._ptr(mins), O._ptr(maxs),
+                                O._ptr(cust["key"]), O._ptr(cust["nation"]), O._ptr(cust["region"]), len(cust["key"]),
+                                O._ptr(supp["key"]), O._ptr(supp["nation"]), O._ptr(supp["region"]),
+                                len(supp["key"]), O._ptr(dd["d_key"]), O._ptr(dd["d_year"]), len(dd["d_key"]),
+                                region, ylo, yhi, O._ptr(gk), O._ptr(gs), len(gk), C.byref(ng), C.byref(el),
+                                C.byref(ch), C.byref(rows))
         if i >= warmup:
             times.append(el.value)
+    ny = yhi - ylo + 1
+    cpu_groups = {}
+    for i in range(ng.value):
+        k = int(gk[i])
+        cs, y = divmod(k, ny)
+        c, s_ = divmod(cs, 25)
+        cpu_groups[(c, s_, ylo + y)] = int(gs[i])
     ms = float(np.mean(times))
-    return {"value": N_ROWS / (ms * 1e-3), "unit": "rows/s", "cores": threads, "kind": "reference",
-            "sample": f"full query: min/max pruning to {scanned.value} of {n_chunks} chunks, LZ4CPUManager decode of "
-                      "discount/quantity/extended_price (liblz4 blocks of 64 KiB), HostHashMap date join; "
-                      "date_key uncompressed (no reference CPU cascaded decoder)",
-            "ms": ms, "result": int(res)}
+    return {"value": n / (ms * 1e-3), "unit": "rows/s", "cores": threads, "kind": "reference", "ms": ms,
+            "sample": f"full query over all {n} rows ({ch.value} chunks survive min/max pruning): filtered builds "
+                      "of customer/supplier/date, LZ4CPUManager decode of the GPU path's LZ4 blocks, the harness's "
+                      "decoder for the cascaded date_key pages, HostHashMap probes, HostHashAggregate",
+            "groups_equal_gpu": cpu_groups == ctx["got"]}
 
 
 def profile_batch(rows):
@@ -611,10 +836,13 @@ def main():
     ap.add_argument("--impl", default="gx", choices=["gx", "reference"])
     ap.add_argument("--segments", type=int, default=128)
     ap.add_argument("--seed", type=int, default=0xBEE5BEE5)
-    ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched and serving sections")
+    ap.add_argument("--no-star", action="store_true", help="skip the 600M-row star join section")
     ap.add_argument("--batch-rows", type=int, default=100_000_000)
+    ap.add_argument("--star-rows", type=int, default=600_000_000)
+    ap.add_argument("--star-layout", default="dense", choices=["linear", "bucket", "dense"])
+    ap.add_argument("--latency-s", type=float, default=1.0, help="seconds of replays behind p50/p99")
     ap.add_argument("--no-tune", action="store_true", help="batched/serving with the default launch shape")
     ap.add_argument("--rows", type=int, default=N_ROWS,
                     help="fact rows of the Q1 workload (default: the measured 60M-row configuration; smaller "
@@ -636,15 +864,20 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
+        from golap_public_b200 import queries
+
         f, dd = make_data(args.seed)
-        cb = cpu_baseline(f, dd, steps=args.steps, warmup=args.warmup)
+        fact = queries.encode_fact(f, {"date_key": "cascaded"}, ROWS_PER_CHUNK, ROWS_PER_BLOCK, args.segments,
+                                   residency=None)
+        cb = cpu_baseline(fact, dd, steps=args.steps, warmup=args.warmup)
         line = {
             "impl": "reference",
             "metric": "rows/s & GB/s vs HBM roofline; p50/p99 latency batched vs one-query-at-a-time",
             "value": cb["value"], "unit": "rows/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": cb["ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded, configs[1] shapes and distributions)",
-            "config": {"workload": WORKLOAD, "rows": N_ROWS, "chunks": N_ROWS // ROWS_PER_CHUNK},
+            "config": {"workload": WORKLOAD, "rows": N_ROWS, "chunks": N_ROWS // ROWS_PER_CHUNK,
+                       "lz4_segments": args.segments},
             "result": cb["result"],
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -659,7 +892,24 @@ def main():
 
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    line, f, dd = gpu_arm(args, rank, world)
+    line, ctx = gpu_arm(args, rank, world)
+    pk, pk_kind = peaks()
+    if rank == 0 and not args.no_cpu:
+        cb = cpu_baseline(ctx["fact"], ctx["dd"], steps=3, warmup=1)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "ms")}
+        line["cpu_baseline"]["surviving_rows_per_s"] = cb["surviving_rows_per_s"]
+        if cb["result"] != line["result"]:
+            raise SystemExit(f"cpu baseline result {cb['result']} != gpu {line['result']}")
+        line["full_scan"]["cpu_reference"] = cpu_full_scan(ctx["fact"], ctx["dd"], ctx["want_all"])
+    del ctx
+    if not args.no_star:
+        star, sctx = star_join_section(args, pk, pk_kind, world)
+        if rank == 0 and not args.no_cpu:
+            star["cpu_baseline"] = cpu_star_join(sctx)
+            if not star["cpu_baseline"]["groups_equal_gpu"]:
+                raise SystemExit("star join: reference CPU groups differ from the GPU groups")
+        line["star_join"] = star
+        del sctx
     if not args.no_batch:
         from golap_public_b200 import autotune, workload
 
@@ -682,12 +932,6 @@ def main():
         line["batched"]["table_rows_per_chunk"] = cfg["rows_per_chunk"]
         line["batched"]["table_build_s"] = build_s
         del wt
-    if rank == 0 and not args.no_cpu:
-        cb = cpu_baseline(f, dd, steps=3, warmup=1)
-        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
-        line["cpu_baseline"]["ms"] = cb["ms"]
-        if cb["result"] != line["result"]:
-            raise SystemExit(f"cpu baseline result {cb['result']} != gpu {line['result']}")
     if world > 1:
         import torch.distributed as dist
 

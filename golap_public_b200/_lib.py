@@ -17,7 +17,7 @@ u8p = C.POINTER(C.c_uint8)
 GX_OK, GX_ERR_CUDA, GX_ERR_CORRUPT, GX_ERR_CAPACITY, GX_ERR_TIMEOUT, GX_ERR_NOMEM, GX_ERR_INVALID = range(7)
 GX_CODEC_NONE, GX_CODEC_LZ4, GX_CODEC_CASCADED = 0, 1, 2
 GX_STEP_FILTER, GX_STEP_PROBE, GX_STEP_CARRY, GX_STEP_VALUE, GX_STEP_GROUP = 1, 2, 4, 8, 16
-GX_AGG_SUM, GX_AGG_SUM_PRODUCT, GX_AGG_COUNT = 0, 1, 2
+GX_AGG_SUM, GX_AGG_SUM_PRODUCT, GX_AGG_COUNT, GX_AGG_BUILD = 0, 1, 2, 3
 GX_HT_LINEAR, GX_HT_BUCKET, GX_HT_DENSE = 0, 1, 2
 GX_BATCH_AUTO, GX_BATCH_QUEUE, GX_BATCH_SHARED = 0, 1, 2
 GX_MAX_STEPS = 8
@@ -67,7 +67,7 @@ class ScanPrune(C.Structure):
 class ScanPlan(C.Structure):
     _fields_ = [("n_steps", C.c_uint32), ("steps", ScanStep * GX_MAX_STEPS), ("agg", C.c_uint32),
                 ("keep_chunks_dev", P), ("groupby", P), ("result_dev", P), ("n_prune", C.c_uint32),
-                ("prune", ScanPrune * GX_MAX_STEPS), ("keep_out_dev", P)]
+                ("prune", ScanPrune * GX_MAX_STEPS), ("keep_out_dev", P), ("build_ht", P)]
 
 
 class Query(C.Structure):
@@ -113,6 +113,11 @@ _SIGS = {
     "gx_hashtable_count": (C.c_int32, [P, C.POINTER(C.c_uint64), P]),
     "gx_hashtable_probe": (C.c_int32, [P, P, C.c_uint64, P, P, P]),
     "gx_hashtable_view": (C.c_int32, [P, C.POINTER(P), C.POINTER(C.c_uint32)]),
+    "gx_hashtable_view2": (C.c_int32, [P, C.POINTER(P), C.POINTER(C.c_uint32), C.POINTER(P)]),
+    "gx_hashtable_clear": (C.c_int32, [P, P]),
+    "gx_hashtable_keys": (C.c_int32, [P, P, C.c_uint64, P, P]),
+    "gx_check_minmax_points": (C.c_int32, [P, P, P, C.c_uint64, P, P]),
+    "gx_minmax_reduce": (C.c_int32, [P, C.c_uint64, P, P]),
     "gx_groupby_view": (C.c_int32, [P, C.POINTER(P), C.POINTER(P), C.POINTER(C.c_uint32)]),
     "gx_groupby_create": (C.c_int32, [C.c_uint64, C.POINTER(P)]),
     "gx_groupby_free": (C.c_int32, [P]),

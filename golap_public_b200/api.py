@@ -85,10 +85,14 @@ class Column:
         return np.array([(b.offset, b.size, b.payload, b.tuples) for b in arr[:n]], dtype=np.uint64).reshape(-1, 4)
 
     def payload(self) -> np.ndarray:
+        return self.payload_view().copy()
+
+    def payload_view(self) -> np.ndarray:
+        """The host copy of the compressed payload without copying (valid while the column lives)."""
         p = L.u8p()
         n = C.c_uint64()
         check(L.lib().gx_column_payload(self.handle, C.byref(p), C.byref(n)))
-        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+        return np.ctypeslib.as_array(p, shape=(n.value,))
 
     def seg_index(self) -> np.ndarray:
         p = C.POINTER(C.c_uint32)()
@@ -142,6 +146,14 @@ class MetaChecker:
         self.preds.append((col, lo, hi))
         return self
 
+    def add_points(self, col: Column, keys, count, keep_out, stream=None):
+        """Join pruning (check_mmmeta_multiple_pts, core/metadata.cuh:550-560): sets
+        keep_out[c] = 1 where one of the keys (device tensors from HashMap.keys)
+        lies in chunk c's min/max of `col`; AND the result with other flags."""
+        check(L.lib().gx_check_minmax_points(col.handle, _dptr(keys), _dptr(count), keys.numel(), _dptr(keep_out),
+                                             _stream_handle(stream)))
+        return keep_out
+
     def run(self, keep_out, stream=None):
         n = len(self.preds)
         cols = (C.c_void_p * n)(*[c.handle.value for c, _, _ in self.preds])
@@ -174,6 +186,11 @@ class HashMap:
                                          _stream_handle(stream)))
         return self
 
+    def clear(self, stream=None) -> "HashMap":
+        """Empty the table (before GX_AGG_BUILD scans fill it)."""
+        check(L.lib().gx_hashtable_clear(self.handle, _stream_handle(stream)))
+        return self
+
     def count(self, stream=None) -> int:
         n = C.c_uint64()
         check(L.lib().gx_hashtable_count(self.handle, C.byref(n), _stream_handle(stream)))
@@ -182,6 +199,13 @@ class HashMap:
     def probe(self, keys, payload_out=None, hits=None, stream=None):
         check(L.lib().gx_hashtable_probe(self.handle, _dptr(keys), keys.numel(), _dptr(payload_out), _dptr(hits),
                                          _stream_handle(stream)))
+
+    def keys(self, out, count, stream=None):
+        """Keys of the table's entries into the int32 device tensor `out` (any order),
+        their number into the int64 device tensor `count` (collect_hashmap_keys,
+        core/dev_structs.cuh:136-150); no host synchronisation."""
+        check(L.lib().gx_hashtable_keys(self.handle, _dptr(out), out.numel(), _dptr(count), _stream_handle(stream)))
+        return out, count
 
     def free(self):
         if self.handle:
@@ -253,6 +277,7 @@ class ScanPlan:
     result: object = None           # device int64 tensor (1 element)
     prune: list = field(default_factory=list)  # (Column, lo, hi) min/max predicates
     keep_out: object = None         # device uint16 tensor receiving the chunk flags
+    build_ht: "HashMap | None" = None  # GX_AGG_BUILD: the join table the surviving rows go into
 
     def prune_minmax(self, col, lo, hi):
         self.prune.append((col, lo, hi))
@@ -304,6 +329,7 @@ class ScanPlan:
             p.prune[i].lo = lo
             p.prune[i].hi = hi
         p.keep_out_dev = self.keep_out.data_ptr() if self.keep_out is not None else None
+        p.build_ht = self.build_ht.handle.value if self.build_ht is not None else None
         self._c = p  # keep alive
         return p
 

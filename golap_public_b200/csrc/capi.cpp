@@ -118,7 +118,7 @@ gx_status gx_column_info_get(const gx_column* c, gx_column_info* o) {
     o->n_chunks = c->n_chunks;
     o->blocks_per_chunk = c->blocks_per_chunk;
     o->n_blocks = c->n_blocks;
-    o->lz4_segments = c->S;
+    o->lz4_segments = c->codec == GX_CODEC_LZ4 ? c->S : 1u;
     o->on_device = (uint32_t)c->residency;
     return GX_OK;
 }

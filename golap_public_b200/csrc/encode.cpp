@@ -195,8 +195,10 @@ size_t lz4_encode_block_auto(const int32_t* vals, uint32_t W, uint32_t S, uint32
     return best_buf.size();
 }
 
-size_t casc_encode_block(const int32_t* vals, uint32_t rows, bool allow_rle, bool allow_delta,
-                         bool allow_bp, std::vector<uint8_t>& out) {
+// One cascaded page (at most kCascPageRows rows): the smallest of
+// {plain, delta} x {no RLE, RLE with at most kCascPageMaxRuns runs}.
+size_t casc_encode_page(const int32_t* vals, uint32_t rows, bool allow_rle, bool allow_delta,
+                        bool allow_bp, std::vector<uint8_t>& out) {
     // runs
     std::vector<int32_t> rv;
     std::vector<uint32_t> rl;
@@ -207,10 +209,10 @@ size_t casc_encode_block(const int32_t* vals, uint32_t rows, bool allow_rle, boo
             rv.push_back(vals[i]);
             rl.push_back(k - i);
             i = k;
-            if (rv.size() > kCascMaxRuns) break;
+            if (rv.size() > kCascPageMaxRuns) break;
         }
     }
-    const bool rle_ok = allow_rle && rv.size() <= kCascMaxRuns && rows > 0;
+    const bool rle_ok = allow_rle && rv.size() <= kCascPageMaxRuns && rows > 0;
     struct Cand {
         bool rle, delta;
         uint32_t n, vbits, lbits;
@@ -307,6 +309,44 @@ size_t casc_encode_block(const int32_t* vals, uint32_t rows, bool allow_rle, boo
     return best.bytes;
 }
 
+// A cascaded block: the page table, then one page per kCascPageRows rows
+// (format in gx_internal.h).  page_entries receives {page_off, page_bytes}
+// per page (the column's side index).
+size_t casc_encode_block(const int32_t* vals, uint32_t rows, bool allow_rle, bool allow_delta,
+                         bool allow_bp, std::vector<uint8_t>& out, uint32_t* page_entries) {
+    const size_t base = out.size();
+    const uint32_t n_pages = (rows + kCascPageRows - 1) / kCascPageRows;
+    const size_t hdr = (8 + 4 * ((size_t)n_pages + 1) + 15) & ~(size_t)15;
+    out.resize(base + hdr, 0);
+    std::vector<uint32_t> off(n_pages + 1);
+    for (uint32_t p = 0; p < n_pages; ++p) {
+        off[p] = (uint32_t)(out.size() - base);
+        const uint32_t r0 = p * kCascPageRows;
+        casc_encode_page(vals + r0, std::min(kCascPageRows, rows - r0), allow_rle, allow_delta, allow_bp, out);
+        out.resize((out.size() + 15) & ~(size_t)15, 0);  // pages start 16-byte aligned
+        page_entries[2 * p] = off[p];
+        page_entries[2 * p + 1] = (uint32_t)(out.size() - base) - off[p];
+    }
+    off[n_pages] = (uint32_t)(out.size() - base);
+    uint32_t* h = (uint32_t*)(out.data() + base);
+    h[0] = n_pages;
+    h[1] = kCascPageRows;
+    std::memcpy(h + 2, off.data(), 4ull * (n_pages + 1));
+    return out.size() - base;
+}
+
+// Offset of the first literal byte of an LZ4 block that opens with literals
+// (token, then the literal-length extension), or -1.
+static long lz4_first_literal(const uint8_t* blk, size_t n) {
+    if (n == 0 || (blk[0] >> 4) == 0) return -1;
+    size_t p = 1;
+    if ((blk[0] >> 4) == 15) {
+        while (p < n && blk[p] == 255) ++p;
+        ++p;
+    }
+    return p <= n ? (long)p : -1;
+}
+
 int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t rows_per_chunk,
                   uint32_t rows_per_block, uint32_t S, uint32_t min_match, uint32_t depth,
                   bool rle, bool delta, bool bp, uint32_t threads, gx_column* col) {
@@ -322,6 +362,8 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
             return set_error(GX_ERR_INVALID, "segmented LZ4 needs a power-of-two rows_per_block >= segments");
         if (min_match != 0 && (min_match < 4 || (min_match & 3)))
             return set_error(GX_ERR_INVALID, "lz4_min_match must be 0 (decode-cost-aware) or a multiple of 4 >= 4");
+    } else if (codec == GX_CODEC_CASCADED) {
+        S = (rows_per_block + kCascPageRows - 1) / kCascPageRows;  // pages per block
     } else {
         S = 1;
     }
@@ -334,12 +376,14 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
     col->n_slots = col->n_chunks * col->blocks_per_chunk;
     col->S = S;
     col->seg_shift = 0;
-    if (S > 1) {
+    if (codec == GX_CODEC_CASCADED) {
+        col->seg_shift = kCascPageLog2;
+    } else if (S > 1) {
         uint32_t sr = rows_per_block / S;
         while ((1u << col->seg_shift) < sr) ++col->seg_shift;
     }
     col->blocks.assign(col->n_slots, gx_dblock{0, 0, 0});
-    if (S > 1) col->seg.assign((size_t)2 * S * col->n_slots, 0);
+    if (S > 1 || codec == GX_CODEC_CASCADED) col->seg.assign((size_t)2 * S * col->n_slots, 0);
     col->mins.assign(col->n_chunks, 0);
     col->maxs.assign(col->n_chunks, 0);
     col->bmins.assign(col->n_slots, INT32_MAX);  // absent slots keep the empty range
@@ -368,6 +412,7 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
         uint32_t s0 = (uint32_t)((uint64_t)col->n_slots * t / threads);
         uint32_t s1 = (uint32_t)((uint64_t)col->n_slots * (t + 1) / threads);
         auto& buf = bufs[t];
+        std::vector<uint8_t> lz4_tmp;
         for (uint32_t s = s0; s < s1; ++s) {
             uint32_t c = s / col->blocks_per_chunk, j = s % col->blocks_per_chunk;
             uint64_t chunk_r0 = (uint64_t)c * rows_per_chunk;
@@ -391,13 +436,22 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
                 used = (size_t)rows * 4;
             } else if (codec == GX_CODEC_LZ4) {
                 uint32_t tmp_seg[2 * kMaxSegments];
-                used = min_match ? lz4_encode_block(vals + r0, rows, S, rows_per_block / S, min_match, depth, buf,
+                lz4_tmp.clear();
+                used = min_match ? lz4_encode_block(vals + r0, rows, S, rows_per_block / S, min_match, depth, lz4_tmp,
                                                     tmp_seg, nullptr)
-                                 : lz4_encode_block_auto(vals + r0, rows, S, rows_per_block / S, depth, buf, tmp_seg);
+                                 : lz4_encode_block_auto(vals + r0, rows, S, rows_per_block / S, depth, lz4_tmp,
+                                                         tmp_seg);
                 if (used + 16 > kStageBytes) overflow = true;  // cannot happen for <= 16384 int32 rows
                 if (S > 1) std::memcpy(&col->seg[(size_t)2 * S * s], tmp_seg, 8 * S);
+                // place the block so that its first literal byte is 16-byte aligned
+                // (buffers are concatenated at 16-byte multiples, so alignment here
+                // is alignment in the payload)
+                const long lit0 = lz4_first_literal(lz4_tmp.data(), lz4_tmp.size());
+                if (lit0 >= 0) buf.resize(buf.size() + ((16 - (buf.size() + (size_t)lit0) % 16) % 16), 0);
+                start = buf.size();
+                buf.insert(buf.end(), lz4_tmp.begin(), lz4_tmp.end());
             } else {
-                used = casc_encode_block(vals + r0, rows, rle, delta, bp, buf);
+                used = casc_encode_block(vals + r0, rows, rle, delta, bp, buf, &col->seg[(size_t)2 * S * s]);
             }
             buf.resize((buf.size() + kPayloadAlign - 1) & ~(size_t)(kPayloadAlign - 1), 0);
             col->blocks[s].offset = start;  // local, fixed up below

@@ -357,12 +357,26 @@ __device__ __noinline__ int lz4_warp_block(const Src in, uint32_t in_size, uint8
 }
 
 // ------------------------------------------------------ block-wide scans
+// Barrier of a group of NT threads: BAR == 0 is the whole CTA
+// (__syncthreads), otherwise named barrier BAR of exactly NT threads (the
+// consumer warps of a warp-specialised kernel).
+template <int NT, int BAR>
+__device__ __forceinline__ void grp_sync() {
+    if constexpr (BAR == 0) {
+        __syncthreads();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"n"(BAR), "n"(NT) : "memory");
+    }
+}
+
 // Inclusive scan (wrapping uint32 addition) of a[0..n) in shared memory by
-// NT threads; thread t owns the contiguous range [t*per, (t+1)*per).  `tmp`
-// has >= NT/32 words.  Must be called by all NT threads.
-template <int NT>
-__device__ __forceinline__ void block_inclusive_scan(uint32_t* a, uint32_t n, uint32_t* tmp) {
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+// the NT threads of a group (tid = index in the group); thread t owns the
+// contiguous range [t*per, (t+1)*per).  `tmp` has >= NT/32 words.  Must be
+// called by all NT threads.
+template <int NT, int BAR = 0>
+__device__ __forceinline__ void block_inclusive_scan(uint32_t* a, uint32_t n, uint32_t* tmp,
+                                                     uint32_t tid = threadIdx.x) {
+    const uint32_t lane = tid & 31, warp = tid >> 5;
     const uint32_t per = (n + NT - 1) / NT;
     const uint32_t b = min(n, tid * per), e = min(n, b + per);
     uint32_t s = 0;
@@ -374,7 +388,7 @@ __device__ __forceinline__ void block_inclusive_scan(uint32_t* a, uint32_t n, ui
         if (lane >= (uint32_t)d) x += y;
     }
     if (lane == 31) tmp[warp] = x;
-    __syncthreads();
+    grp_sync<NT, BAR>();
     if (warp == 0) {
         uint32_t w = lane < NT / 32 ? tmp[lane] : 0;
 #pragma unroll
@@ -384,52 +398,33 @@ __device__ __forceinline__ void block_inclusive_scan(uint32_t* a, uint32_t n, ui
         }
         if (lane < NT / 32) tmp[lane] = w;
     }
-    __syncthreads();
+    grp_sync<NT, BAR>();
     uint32_t run = (x - s) + (warp ? tmp[warp - 1] : 0);
     for (uint32_t i = b; i < e; ++i) {
         run += a[i];
         a[i] = run;
     }
-    __syncthreads();
+    grp_sync<NT, BAR>();
 }
 
-// Block-wide sum (wrapping uint32) of one value per thread.
-template <int NT>
-__device__ __forceinline__ uint32_t block_sum_u32(uint32_t v, uint32_t* tmp) {
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, d);
-    if (lane == 0) tmp[warp] = v;
-    __syncthreads();
-    uint32_t t = 0;
-    for (uint32_t w = 0; w < NT / 32; ++w) t += tmp[w];
-    __syncthreads();
-    return t;
-}
-
-// ------------------------------------------------------- cascaded blocks
-// Result of decoding one tile [r0, r0+n) of a cascaded block.
-struct CascTile {
-    uint32_t rle;     // 1: values are given as runs (run_val/run_start)
-    uint32_t ra, rb;  // runs intersecting the tile: [ra, rb)
-};
-
-__device__ __forceinline__ bool casc_header_ok(const casc_hdr& h, uint32_t blk_bytes, uint32_t rows) {
+// ------------------------------------------------------- cascaded pages
+__device__ __forceinline__ bool casc_header_ok(const casc_hdr& h, uint32_t pg_bytes, uint32_t rows) {
     const bool rle = (h.flags & CASC_RLE) != 0;
-    if (blk_bytes < 32 || h.n_rows != rows || h.val_bits > 32 || h.len_bits > 32) return false;
-    if (rle ? (h.n_runs == 0 || h.n_runs > kCascMaxRuns) : h.n_runs != rows) return false;
+    if (pg_bytes < 32 || h.n_rows != rows || h.val_bits > 32 || h.len_bits > 32) return false;
+    if (rle ? (h.n_runs == 0 || h.n_runs > kCascPageMaxRuns) : h.n_runs != rows) return false;
     if (h.vals_off < 32 || (h.vals_off & 3) ||
-        (uint64_t)h.vals_off + 4ull * (((uint64_t)h.n_runs * h.val_bits + 31) / 32 + 1) > blk_bytes)
+        (uint64_t)h.vals_off + 4ull * (((uint64_t)h.n_runs * h.val_bits + 31) / 32 + 1) > pg_bytes)
         return false;
     if (rle && ((h.lens_off & 3) || h.lens_off < 32 ||
-                (uint64_t)h.lens_off + 4ull * (((uint64_t)h.n_runs * h.len_bits + 31) / 32 + 1) > blk_bytes))
+                (uint64_t)h.lens_off + 4ull * (((uint64_t)h.n_runs * h.len_bits + 31) / 32 + 1) > pg_bytes))
         return false;
     return true;
 }
 
-__device__ __forceinline__ casc_hdr casc_load_header(const uint8_t* blk) {
-    const uint4* hw = (const uint4*)blk;  // blocks are 16-byte aligned
-    const uint4 a = __ldg(hw), b = __ldg(hw + 1);
+// Header of a page (16-byte aligned; global or shared memory).
+__device__ __forceinline__ casc_hdr casc_load_header(const uint8_t* pg) {
+    const uint4* hw = (const uint4*)pg;
+    const uint4 a = hw[0], b = hw[1];
     casc_hdr h;
     h.n_rows = a.x;
     h.n_runs = a.y;
@@ -445,92 +440,93 @@ __device__ __forceinline__ casc_hdr casc_load_header(const uint8_t* blk) {
     return h;
 }
 
-// Decodes tile [r0, r0+n) of a cascaded block of `rows` rows.  RLE blocks
-// leave their runs in run_val/run_start (block-wide, shared) and report the
-// tile's run range; other blocks write the tile's values to out[0..n).
-// All NT threads call it.  Returns 0 or kErrCorrupt (uniform).
-template <int NT>
-__device__ __forceinline__ int casc_decode_tile(const uint8_t* __restrict__ blk, uint32_t blk_bytes, uint32_t rows,
-                                                uint32_t r0, uint32_t n, int32_t* out, int32_t* run_val,
-                                                uint32_t* run_start, uint32_t* tmp, CascTile* t) {
-    const uint32_t tid = threadIdx.x;
-    const casc_hdr h = casc_load_header(blk);
-    if (!casc_header_ok(h, blk_bytes, rows)) return kErrCorrupt;
+// Decodes one cascaded page of `rows` rows (<= kCascPageRows; global or
+// shared memory, 16-byte aligned) into out[0..rows) in shared memory, plain
+// row order.  RLE pages go through run tables run_val / run_end (shared,
+// kCascPageMaxRuns entries each): run values (with a delta scan), run ends
+// (an inclusive scan of the lengths), then each thread expands a contiguous
+// range of rows from the run that holds its first row (binary search).
+// Called by the NT threads of a group (barrier BAR, tid = index in the
+// group).  Returns 0 or kErrCorrupt (uniform over the group).
+// With FINAL_SYNC false the values are complete only after the caller's
+// next barrier of the group (callers that place one right after save one).
+template <int NT, int BAR = 0, bool FINAL_SYNC = true>
+__device__ __forceinline__ int casc_decode_page(const uint8_t* __restrict__ pg, uint32_t pg_bytes, uint32_t rows,
+                                                int32_t* out, int32_t* run_val, uint32_t* run_end, uint32_t* tmp,
+                                                uint32_t tid = threadIdx.x) {
+    if (pg_bytes < 32) return kErrCorrupt;
+    const casc_hdr h = casc_load_header(pg);
+    if (!casc_header_ok(h, pg_bytes, rows)) return kErrCorrupt;
     const bool rle = (h.flags & CASC_RLE) != 0, delta = (h.flags & CASC_DELTA) != 0;
-    const uint32_t* vw = (const uint32_t*)(blk + h.vals_off);
+    const uint32_t* vw = (const uint32_t*)(pg + h.vals_off);
     if (!rle) {
-        // values of the tile only; with delta, add the sum of the entries before it
-        uint32_t before = 0;
+        for (uint32_t i = tid; i < rows; i += NT)
+            out[i] = (int32_t)((i == 0 && delta) ? 0u : unpack_bits(vw, i, h.val_bits) + (uint32_t)h.val_base);
         if (delta) {
-            uint32_t part = 0;
-            for (uint32_t i = 1 + tid; i < r0 && i < rows; i += NT)  // entries 1..r0-1
-                part += unpack_bits(vw, i, h.val_bits) + (uint32_t)h.val_base;
-            before = block_sum_u32<NT>(part, tmp);
+            grp_sync<NT, BAR>();
+            block_inclusive_scan<NT, BAR>((uint32_t*)out, rows, tmp, tid);
+            for (uint32_t i = tid; i < rows; i += NT) out[i] = (int32_t)((uint32_t)out[i] + (uint32_t)h.first);
         }
-        for (uint32_t i = tid; i < n; i += NT) {
-            const uint32_t e = r0 + i;
-            out[i] = (int32_t)((e == 0 && delta) ? 0u : unpack_bits(vw, e, h.val_bits) + (uint32_t)h.val_base);
-        }
-        __syncthreads();
-        if (delta) {
-            block_inclusive_scan<NT>((uint32_t*)out, n, tmp);
-            const uint32_t add = before + (uint32_t)h.first;
-            for (uint32_t i = tid; i < n; i += NT) out[i] = (int32_t)((uint32_t)out[i] + add);
-            __syncthreads();
-        }
-        if (tid == 0) *t = CascTile{0, 0, 0};
-        __syncthreads();
+        if (FINAL_SYNC) grp_sync<NT, BAR>();
         return 0;
     }
     const uint32_t nr = h.n_runs;
-    const uint32_t* lw = (const uint32_t*)(blk + h.lens_off);
-    for (uint32_t i = tid; i < nr; i += NT) {
-        run_val[i] = (int32_t)((i == 0 && delta) ? 0u : unpack_bits(vw, i, h.val_bits) + (uint32_t)h.val_base);
-        run_start[i + 1] = unpack_bits(lw, i, h.len_bits) + h.len_base;
+    const uint32_t* lw = (const uint32_t*)(pg + h.lens_off);
+    if (nr <= 32) {
+        // few runs (sorted or low-cardinality pages): one warp builds the run
+        // table with shuffle scans, one barrier publishes it
+        if (tid < 32) {
+            const bool in = tid < nr;
+            uint32_t v = in ? ((tid == 0 && delta) ? 0u : unpack_bits(vw, tid, h.val_bits) + (uint32_t)h.val_base) : 0u;
+            uint32_t e = in ? unpack_bits(lw, tid, h.len_bits) + h.len_base : 0u;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t pv = __shfl_up_sync(0xFFFFFFFFu, v, d), pe = __shfl_up_sync(0xFFFFFFFFu, e, d);
+                if (tid >= (uint32_t)d) {
+                    if (delta) v += pv;
+                    e += pe;
+                }
+            }
+            if (in) {
+                run_val[tid] = (int32_t)(delta ? v + (uint32_t)h.first : v);
+                run_end[tid] = e;
+            }
+        }
+        grp_sync<NT, BAR>();
+    } else {
+        for (uint32_t i = tid; i < nr; i += NT) {
+            run_val[i] = (int32_t)((i == 0 && delta) ? 0u : unpack_bits(vw, i, h.val_bits) + (uint32_t)h.val_base);
+            run_end[i] = unpack_bits(lw, i, h.len_bits) + h.len_base;
+        }
+        grp_sync<NT, BAR>();
+        if (delta) {
+            block_inclusive_scan<NT, BAR>((uint32_t*)run_val, nr, tmp, tid);
+            for (uint32_t i = tid; i < nr; i += NT) run_val[i] = (int32_t)((uint32_t)run_val[i] + (uint32_t)h.first);
+        }
+        block_inclusive_scan<NT, BAR>(run_end, nr, tmp, tid);
     }
-    if (tid == 0) run_start[0] = 0;
-    __syncthreads();
-    if (delta) {
-        block_inclusive_scan<NT>((uint32_t*)run_val, nr, tmp);
-        for (uint32_t i = tid; i < nr; i += NT) run_val[i] = (int32_t)((uint32_t)run_val[i] + (uint32_t)h.first);
-    }
-    block_inclusive_scan<NT>(run_start + 1, nr, tmp);
-    if (run_start[nr] != rows) return kErrCorrupt;  // uniform: all threads read the same word
-    if (tid == 0) {
-        // runs intersecting [r0, r0+n): first run ending after r0 .. first run starting at/after r0+n
-        uint32_t lo = 0, hi = nr;
+    if (run_end[nr - 1] != rows) return kErrCorrupt;  // uniform: every thread reads the same word
+    const uint32_t per = (rows + NT - 1) / NT;
+    const uint32_t r_begin = min(rows, tid * per), r_stop = min(rows, r_begin + per);
+    if (r_begin < r_stop) {
+        uint32_t lo = 0, hi = nr - 1;  // first run ending after r_begin
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
-            if (run_start[mid + 1] <= r0) lo = mid + 1; else hi = mid;
+            if (run_end[mid] <= r_begin) lo = mid + 1; else hi = mid;
         }
-        const uint32_t a = lo;
-        hi = nr;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (run_start[mid] < r0 + n) lo = mid + 1; else hi = mid;
+        uint32_t k = lo, e = run_end[k];
+        int32_t v = run_val[k];
+        for (uint32_t r = r_begin; r < r_stop; ++r) {
+            while (r >= e && k + 1 < nr) {
+                ++k;
+                e = run_end[k];
+                v = run_val[k];
+            }
+            out[r] = v;
         }
-        *t = CascTile{1, a, lo};
     }
-    __syncthreads();
+    if (FINAL_SYNC) grp_sync<NT, BAR>();
     return 0;
-}
-
-// Writes the tile's rows from runs into out[0..n): thread-interleaved rows
-// (bank-conflict free), each thread locating its run by binary search over
-// the tile's run range.
-template <int NT>
-__device__ __forceinline__ void casc_runs_to_rows(const CascTile& t, const int32_t* run_val,
-                                                  const uint32_t* run_start, uint32_t r0, uint32_t n, int32_t* out) {
-    for (uint32_t i = threadIdx.x; i < n; i += NT) {
-        const uint32_t r = r0 + i;
-        uint32_t lo = t.ra, hi = t.rb;  // last run with start <= r
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (run_start[mid] <= r) lo = mid; else hi = mid;
-        }
-        out[i] = run_val[lo];
-    }
-    __syncthreads();
 }
 
 // --------------------------------------------------------- join tables

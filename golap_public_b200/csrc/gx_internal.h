@@ -3,14 +3,15 @@
 //
 // Layout of a compressed column in memory (host and HBM alike):
 //
-//   payload   : concatenation of per-block byte streams, each starting on a
-//               16-byte boundary (so cp.async.bulk / 128-bit loads can start
-//               there) and followed by >= 16 bytes of slack at the very end.
+//   payload   : concatenation of per-block byte streams (raw and cascaded
+//               blocks start on a 16-byte boundary, LZ4 blocks see below),
+//               followed by kPayloadSlack bytes of slack at the very end.
 //   directory : one gx_dblock per (chunk, block-in-chunk) slot, padded to
 //               n_chunks * blocks_per_chunk entries; absent blocks of a short
 //               last chunk have n_rows == 0.
 //   seg index : LZ4 columns with S > 1 segments: S pairs of uint32 per block
-//               (see "segmented LZ4" below).
+//               (see "segmented LZ4" below); cascaded columns: one pair
+//               {page offset, page bytes} per page (see "cascaded block").
 //   min/max   : int32 per chunk (inclusive), the MinMaxMeta of the reference
 //               (core/metadata.cuh:110-221).
 //
@@ -30,16 +31,30 @@
 //       token's match-length nibble.  Entry 0 resumes inside the block's
 //       first literal run when the block starts with literals.
 //
+//   LZ4 blocks start anywhere in the payload (not necessarily on a 16-byte
+//   boundary): a block that opens with literals is placed so that its first
+//   literal byte is 16-byte aligned, so the row tiles of a literal run are
+//   16-byte aligned byte ranges that bulk copies move unshifted.
+//
 // Cascaded block (own format; the reference's nvCOMP Cascaded stream format
-// is not available, so only decoded values are comparable):
-//   casc_hdr (32 bytes), then a bit-packed value stream and, with RLE, a
-//   bit-packed run-length stream, each 16-byte aligned, each with one padding
-//   word.  Values: with DELTA, entry 0 is 0 and entry i = v[i]-v[i-1]
-//   (wrapping int32); the stored word is entry - val_base (frame of
-//   reference) in val_bits bits.  Lengths: stored length - len_base in
-//   len_bits bits.  v[i] = first + sum_{k<=i} entry[k] with DELTA, else
-//   entry[i].  Element i of a stream with width w sits at bits [i*w, i*w+w)
-//   of the little-endian uint32 word sequence.
+// is not available, so only decoded values are comparable).  The block is a
+// sequence of independently decodable pages of kCascPageRows rows (the last
+// one shorter), so one row tile never needs the rest of its block:
+//   block header: uint32 n_pages, uint32 page_rows, uint32 page_off[n_pages+1]
+//   (byte offsets from the block start; the last one is the stream end),
+//   padded to 16 bytes; then the pages, each 16-byte aligned.  The column's
+//   side index repeats {page_off, page_bytes} per page (S = pages per block,
+//   seg_shift = log2(kCascPageRows)) so device code locates a page with
+//   independent loads.
+// Cascaded page: casc_hdr (32 bytes), then a bit-packed value stream and,
+//   with RLE (at most kCascPageMaxRuns runs), a bit-packed run-length stream,
+//   each 16-byte aligned, each with one padding word.  Values: with DELTA,
+//   entry 0 is 0 and entry i = v[i]-v[i-1] (wrapping int32); the stored word
+//   is entry - val_base (frame of reference) in val_bits bits.  Lengths:
+//   stored length - len_base in len_bits bits.  v[i] = first +
+//   sum_{k<=i} entry[k] with DELTA, else entry[i].  Element i of a stream
+//   with width w sits at bits [i*w, i*w+w) of the little-endian uint32 word
+//   sequence.
 #pragma once
 #include <stdint.h>
 
@@ -57,7 +72,11 @@ namespace gx {
 
 constexpr uint32_t kMaxRowsPerBlock = 16384;   // 64 KiB of int32: one decode buffer
 constexpr uint32_t kMaxSegments = 128;
-constexpr uint32_t kCascMaxRuns = 2048;        // RLE only when runs <= this
+constexpr uint32_t kCascMaxRuns = 2048;        // run tables of one decode (>= kCascPageMaxRuns)
+constexpr uint32_t kCascPageLog2 = 11;
+constexpr uint32_t kCascPageRows = 1u << kCascPageLog2;  // rows of one cascaded page
+constexpr uint32_t kCascPageMaxRuns = 512;     // RLE pages hold at most this many runs
+constexpr uint32_t kCascMaxPages = kMaxRowsPerBlock / kCascPageRows;
 constexpr uint32_t kStageBytes = 66048;        // shared staging buffer for one compressed block
 constexpr uint32_t kPayloadAlign = 16;
 constexpr uint32_t kPayloadSlack = 64;
@@ -93,13 +112,13 @@ static_assert(sizeof(gx_dblock) == 16, "gx_dblock layout");
 struct gx_dcol {
     const uint8_t* payload;
     const gx_dblock* blocks;
-    const uint32_t* seg;        // 2*S words per block (LZ4 with S > 1), else null
+    const uint32_t* seg;        // 2*S words per block (LZ4 with S > 1, cascaded), else null
     const int32_t* mins;
     const int32_t* maxs;
     uint64_t n_rows;
     uint32_t codec;
-    uint32_t S;                 // LZ4 segments per block (1 = plain LZ4)
-    uint32_t seg_shift;         // log2(rows_per_block / S) when S > 1
+    uint32_t S;                 // LZ4 segments per block (1 = plain LZ4); cascaded: pages per block
+    uint32_t seg_shift;         // log2(rows per segment / page) when the side index exists
     uint32_t rows_per_chunk;
     uint32_t rows_per_block;
     uint32_t blocks_per_chunk;
@@ -189,8 +208,11 @@ size_t lz4_encode_block(const int32_t* vals, uint32_t rows, uint32_t S, uint32_t
                         uint32_t* seg_entries, uint32_t* n_seq);
 size_t lz4_encode_block_auto(const int32_t* vals, uint32_t rows, uint32_t S, uint32_t seg_rows, uint32_t depth,
                              std::vector<uint8_t>& out, uint32_t* seg_entries);
+size_t casc_encode_page(const int32_t* vals, uint32_t rows, bool allow_rle, bool allow_delta,
+                        bool allow_bp, std::vector<uint8_t>& out);
+// A block of pages; page_entries receives {page_off, page_bytes} per page.
 size_t casc_encode_block(const int32_t* vals, uint32_t rows, bool allow_rle, bool allow_delta,
-                         bool allow_bp, std::vector<uint8_t>& out);
+                         bool allow_bp, std::vector<uint8_t>& out, uint32_t* page_entries);
 // Column encoder (encode.cpp): fills layout, payload, directory, min/max.
 int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t rows_per_chunk,
                   uint32_t rows_per_block, uint32_t S, uint32_t min_match, uint32_t depth,

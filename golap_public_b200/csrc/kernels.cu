@@ -160,7 +160,7 @@ struct ItemsParams {
 };
 
 // Layout of a decoded tile in shared memory.
-enum : int { kRows = 0, kSegRows = 1, kRuns = 2 };
+enum : int { kRows = 0, kSegRows = 1 };
 
 // Stage `bytes` bytes from `src` (16-byte aligned, bytes a multiple of 16
 // and within the stage) into shared memory.  HBM-resident columns: thread 0
@@ -195,14 +195,12 @@ __device__ __forceinline__ int stage_bytes(const gx_dcol& c, const uint8_t* src,
 
 // Decode rows [r0, r0+n) of block `slot` of column `c` into shared memory.
 // Returns the layout (kRows: buf[r]; kSegRows: buf[r + ((r >> seg_shift) <<
-// pad_log2)], each segment followed by 2^pad_log2 pad words; kRuns: runs in
-// the stage area, described by *ct) or -1 with *s_err set.  All NT threads
-// call it.
+// pad_log2)], each segment followed by 2^pad_log2 pad words) or -1 with
+// *s_err set.  All NT threads call it.
 template <int NT, int MAXT>
 __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint32_t rows, uint32_t r0, uint32_t n,
                                            uint32_t* buf, uint8_t* stage, uint64_t* mbar, uint32_t& phase,
-                                           uint32_t* tmp, CascTile* ct, int* s_err, uint32_t& pad_log2,
-                                           uint32_t* seg_smem) {
+                                           uint32_t* tmp, int* s_err, uint32_t& pad_log2, uint32_t* seg_smem) {
     using C = Cfg<MAXT>;
     const uint32_t tid = threadIdx.x;
     // segmented LZ4: this thread's entry of the tile's segment index, loaded
@@ -276,14 +274,20 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
             __syncthreads();
             return -1;
         }
-        const uint32_t wbase = lo & ~15u;
-        const uint32_t bytes = ((hi + 15u) & ~15u) - wbase + 16u;
+        // the staged window starts on the 16-byte boundary at or below the tile's
+        // first byte (LZ4 blocks need not start on one); wbase is that boundary
+        // relative to the block start, in wrapping arithmetic (the decoders only
+        // form differences pos - wbase)
+        const uint64_t abs_lo = d.offset + lo;
+        const uint64_t abs_wb = abs_lo & ~15ull;
+        const uint32_t wbase = (uint32_t)(abs_wb - d.offset);
+        const uint32_t bytes = (uint32_t)(((d.offset + hi + 15u) & ~15ull) - abs_wb) + 16u;
         if (bytes > C::kStage) {
             if (tid == 0) *s_err = kErrCorrupt;
             __syncthreads();
             return -1;
         }
-        const int rc = stage_bytes<NT>(c, blk + wbase, bytes, stage, mbar, phase);
+        const int rc = stage_bytes<NT>(c, c.payload + abs_wb, bytes, stage, mbar, phase);
         if (rc && tid == 0) *s_err = rc;
         __syncthreads();
         if (rc) return -1;
@@ -294,7 +298,7 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
             const uint32_t info0 = seg_smem[1];
             if ((info0 & 16u) && (info0 >> 5) >= 4 * n && hi - lo == 4 * n && (n & 3u) == 0 && lo == seg_smem[0]) {
                 const uint32_t* A = (const uint32_t*)stage;
-                const uint32_t rb = lo - wbase, w0 = rb >> 2, sh = (rb & 3u) * 8;
+                const uint32_t rb = (uint32_t)(abs_lo - abs_wb), w0 = rb >> 2, sh = (rb & 3u) * 8;
                 for (uint32_t q4 = tid; q4 < n / 4; q4 += NT) {
                     const uint32_t w = w0 + 4 * q4;
                     const uint32_t a0 = A[w], a1 = A[w + 1], a2 = A[w + 2], a3 = A[w + 3], a4 = A[w + 4];
@@ -331,20 +335,38 @@ __device__ __forceinline__ int decode_tile(const gx_dcol& c, uint32_t slot, uint
             return kSegRows;
         }
         if (tid < 32) {
-            const int r2 = lz4_warp_block(SharedSrc{stage}, d.comp_bytes, (uint8_t*)buf, rows * 4, tid);
+            const int r2 = lz4_warp_block(SharedSrc{stage + (uint32_t)(d.offset - abs_wb)}, d.comp_bytes,
+                                          (uint8_t*)buf, rows * 4, tid);
             if (r2 && tid == 0) *s_err = r2;
         }
         __syncthreads();
         return kRows;
     }
-    // cascaded: run tables live in the (idle) stage area
+    // cascaded: the tile's pages one after another (tiles start on page
+    // boundaries); run tables live in the (idle) stage area
     int32_t* run_val = (int32_t*)stage;
-    uint32_t* run_start = (uint32_t*)(stage + 4 * kCascMaxRuns);
-    const int rc = casc_decode_tile<NT>(blk, d.comp_bytes, rows, r0, n, (int32_t*)buf, run_val, run_start, tmp, ct);
-    if (rc && tid == 0) *s_err = rc;
-    __syncthreads();
-    if (rc) return -1;
-    return ct->rle ? kRuns : kRows;
+    uint32_t* run_end = (uint32_t*)(stage + 4 * kCascMaxRuns);
+    const uint32_t p0 = r0 >> kCascPageLog2, p1 = (r0 + n + kCascPageRows - 1) >> kCascPageLog2;
+    if ((r0 & (kCascPageRows - 1)) || !c.seg || p1 > c.S) {
+        if (tid == 0) *s_err = kErrCorrupt;
+        __syncthreads();
+        return -1;
+    }
+    for (uint32_t p = p0; p < p1; ++p) {
+        const uint32_t* e = c.seg + (size_t)2 * c.S * slot + 2 * p;
+        const uint32_t off = __ldg(e), pb = __ldg(e + 1);
+        const uint32_t pr = min(kCascPageRows, rows - p * kCascPageRows);
+        int rc = kErrCorrupt;
+        if ((off & 15u) == 0 && (uint64_t)off + pb <= d.comp_bytes)
+            rc = casc_decode_page<NT>(blk + off, pb, pr, (int32_t*)buf + (p * kCascPageRows - r0), run_val, run_end,
+                                      tmp);
+        if (rc) {
+            if (tid == 0) *s_err = rc;
+            __syncthreads();
+            return -1;
+        }
+    }
+    return kRows;
 }
 
 // Flush a CTA's partial aggregate of query Q: the scalar sum (one global
@@ -398,8 +420,6 @@ __global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const 
     uint8_t* stage = (uint8_t*)(mask + C::kMaskWords);
     uint32_t* gkeys = (uint32_t*)(stage + C::kStage);
     unsigned long long* gsums = (unsigned long long*)(gkeys + (P.smem_groups ? (1u << kSmemGroupLog2) : 0));
-    const int32_t* run_val = (const int32_t*)stage;
-    const uint32_t* run_start = (const uint32_t*)(stage + 4 * kCascMaxRuns);
 
     __shared__ __align__(8) uint64_t s_mbar;
     __shared__ uint32_t s_item;
@@ -408,7 +428,6 @@ __global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const 
     __shared__ uint32_t s_alive;
     __shared__ uint32_t s_tmp[NW + 1];
     __shared__ unsigned long long s_red[NW];
-    __shared__ CascTile s_ct;
     __shared__ uint32_t s_seg[2 * (kMaxSegments + 1)];
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -476,8 +495,8 @@ __global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const 
         for (uint32_t si = 0; si < Q.n_steps; ++si) {
             const ScanStep& st = Q.steps[si];
             uint32_t pad_log2 = 0;
-            int layout = decode_tile<NT, MAXT>(st.col, slot, rows, r0, n, buf, stage, &s_mbar, phase, s_tmp, &s_ct,
-                                               &s_err, pad_log2, s_seg);
+            const int layout = decode_tile<NT, MAXT>(st.col, slot, rows, r0, n, buf, stage, &s_mbar, phase, s_tmp,
+                                                     &s_err, pad_log2, s_seg);
             const int derr = s_err;
             __syncthreads();  // every thread has read s_err before it is reset
             if (derr) {       // corrupt block: drop the tile, remember the error
@@ -491,39 +510,10 @@ __global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const 
             }
             const uint32_t flags = st.flags;
             const uint32_t dcard = st.digit_card;
-            const bool per_row = (flags & (GX_STEP_CARRY | GX_STEP_VALUE | GX_STEP_GROUP)) || dcard;
-            if (layout == kRuns && per_row) {
-                casc_runs_to_rows<NT>(s_ct, run_val, run_start, r0, n, (int32_t*)buf);
-                layout = kRows;
-            }
             if (tid == 0) s_alive = 0;
             __syncthreads();
             uint32_t alive_w = 0;
-            if (layout == kRuns) {
-                // predicate per run: rows of failing runs leave the mask
-                const CascTile ct = s_ct;
-                for (uint32_t i = ct.ra + tid; i < ct.rb; i += NT) {
-                    const int32_t v = run_val[i];
-                    bool pass = true;
-                    if (flags & GX_STEP_FILTER) pass = v >= st.lo && v <= st.hi;
-                    if ((flags & GX_STEP_PROBE) && pass) {
-                        int32_t p;
-                        pass = ht_probe_any(st.ht, st.ht_log2, st.ht_layout, v, &p);
-                    }
-                    if (!pass) {
-                        const uint32_t ra = max(run_start[i], r0) - r0, rb = min(run_start[i + 1], r0 + n) - r0;
-                        for (uint32_t r = ra; r < rb;) {
-                            const uint32_t w = r >> 5, hb = min(rb, (w + 1) * 32);
-                            const uint32_t bits = (hb - r == 32) ? 0xFFFFFFFFu : (((1u << (hb - r)) - 1u) << (r & 31));
-                            atomicAnd(&mask[w], ~bits);
-                            r = hb;
-                        }
-                    }
-                }
-                __syncthreads();
-                for (uint32_t g = warp; g < ngroups; g += NW)
-                    if (lane == 0) alive_w += __popc(mask[g]);
-            } else {
+            {
                 const uint32_t shift = st.col.seg_shift;
                 for (uint32_t g = warp; g < ngroups; g += NW) {
                     const uint32_t m = mask[g];
@@ -712,7 +702,6 @@ __global__ void __launch_bounds__(NT) decompress_kernel(const __grid_constant__ 
     __shared__ __align__(8) uint64_t s_mbar;
     __shared__ int s_err;
     __shared__ uint32_t s_tmp[NT / 32 + 1];
-    __shared__ CascTile s_ct;
     __shared__ uint32_t s_seg[2 * (kMaxSegments + 1)];
     const uint32_t slot = slot0 + blockIdx.x / tpb;
     const uint32_t r0 = (blockIdx.x % tpb) * tile_rows;
@@ -725,16 +714,11 @@ __global__ void __launch_bounds__(NT) decompress_kernel(const __grid_constant__ 
     }
     __syncthreads();
     uint32_t phase = 0, pad_log2 = 0;
-    int layout = decode_tile<NT, MAXT>(c, slot, d.n_rows, r0, n, buf, stage, &s_mbar, phase, s_tmp, &s_ct, &s_err,
-                                       pad_log2, s_seg);
+    const int layout = decode_tile<NT, MAXT>(c, slot, d.n_rows, r0, n, buf, stage, &s_mbar, phase, s_tmp, &s_err,
+                                             pad_log2, s_seg);
     if (s_err) {
         if (threadIdx.x == 0) raise_error(s_err);
         return;
-    }
-    if (layout == kRuns) {
-        casc_runs_to_rows<NT>(s_ct, (const int32_t*)stage, (const uint32_t*)(stage + 4 * kCascMaxRuns), r0, n,
-                              (int32_t*)buf);
-        layout = kRows;
     }
     const uint32_t chunk = slot / c.blocks_per_chunk, j = slot % c.blocks_per_chunk;
     const uint64_t first = (uint64_t)chunk * c.rows_per_chunk + (uint64_t)j * c.rows_per_block + r0 - row0;
@@ -753,6 +737,85 @@ __global__ void raw_lz4_kernel(const uint8_t* comp, const uint64_t* coff, uint8_
         rc = lz4_warp_block(GlobalSrc{comp + c0}, (uint32_t)(c1 - c0), out + o0, (uint32_t)(o1 - o0),
                             threadIdx.x & 31);
     if ((threadIdx.x & 31) == 0) status[b] = rc;
+}
+
+// Min and max of data[0..n) into range[0] / range[1], which start at
+// INT32_MAX / INT32_MIN (warp reductions, one atomic pair per warp).
+__global__ void minmax_reduce_kernel(const int32_t* data, uint64_t n, int32_t* range) {
+    int32_t lo = INT32_MAX, hi = INT32_MIN;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const bool vec = ((uintptr_t)data & 15u) == 0;
+    if (vec) {
+        const uint64_t n4 = n / 4;
+        for (uint64_t j = i; j < n4; j += stride) {
+            const int4 v = __ldg((const int4*)data + j);
+            lo = min(lo, min(min(v.x, v.y), min(v.z, v.w)));
+            hi = max(hi, max(max(v.x, v.y), max(v.z, v.w)));
+        }
+        i += n4 * 4;
+    }
+    for (; i < n; i += stride) {
+        const int32_t v = __ldg(data + i);
+        lo = min(lo, v);
+        hi = max(hi, v);
+    }
+    lo = __reduce_min_sync(0xFFFFFFFFu, lo);
+    hi = __reduce_max_sync(0xFFFFFFFFu, hi);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&range[0], lo);
+        atomicMax(&range[1], hi);
+    }
+}
+
+// Keys of the occupied slots of a join table, compacted in any order
+// (warp-aggregated counter); a dense table's header slot is skipped.
+__global__ void ht_keys_kernel(const uint64_t* slots, uint64_t n_slots, uint32_t first, int32_t* out, uint64_t cap,
+                               unsigned long long* count) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t n_iter = (n_slots + stride - 1) / stride;  // uniform trip count: every lane reaches the ballot
+    for (uint64_t it = 0; it < n_iter; ++it) {
+        const uint64_t i = it * stride + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+        int32_t k = kEmptyKey;
+        if (i < n_slots && i >= first) k = (int32_t)(uint32_t)slots[i];
+        const bool has = k != kEmptyKey;
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, has);
+        unsigned long long base = 0;
+        if (lane == 0 && m) base = atomicAdd(count, (unsigned long long)__popc(m));
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (has) {
+            const unsigned long long o = base + __popc(m & ((1u << lane) - 1u));
+            if (o < cap) out[o] = k;
+        }
+    }
+}
+
+// Join pruning: out[c] = 1 where chunk c's [min, max] holds one of the keys
+// (the first min(*n_keys, cap) of them, staged through shared memory).
+__global__ void prune_points_kernel(const int32_t* mins, const int32_t* maxs, uint32_t n_chunks, const int32_t* keys,
+                                    const unsigned long long* n_keys, uint64_t cap, uint16_t* out) {
+    __shared__ int32_t s_keys[2048];
+    const uint64_t nk = min((uint64_t)*n_keys, cap);
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int32_t lo = c < n_chunks ? mins[c] : 1, hi = c < n_chunks ? maxs[c] : 0;
+    bool hit = false;
+    for (uint64_t k0 = 0; k0 < nk; k0 += 2048) {
+        const uint32_t m = (uint32_t)min((uint64_t)2048, nk - k0);
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) s_keys[i] = keys[k0 + i];
+        __syncthreads();
+        if (!hit)
+            for (uint32_t i = 0; i < m; ++i) hit |= s_keys[i] >= lo && s_keys[i] <= hi;
+    }
+    if (c < n_chunks && hit) out[c] = 1;
+}
+
+// Slots emptied, counters zeroed (one launch).
+__global__ void ht_clear_kernel(uint64_t* slots, uint64_t n, unsigned long long* counters) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) slots[i] = kEmptySlot;
+    if (blockIdx.x == 0 && threadIdx.x < 4) counters[threadIdx.x] = 0;
 }
 
 __global__ void check_minmax_kernel(const int32_t* mins, const int32_t* maxs, uint32_t n, int32_t lo, int32_t hi,
@@ -1046,6 +1109,7 @@ gx_status allow_smem(K kernel, size_t bytes) {
 }
 
 #include "shared_scan.cuh"
+#include "pipe_scan.cuh"
 
 }  // namespace
 
@@ -1454,6 +1518,61 @@ gx_status gx_hashtable_view(const gx_hashtable* ht, const uint64_t** slots_dev, 
     return GX_OK;
 }
 
+gx_status gx_hashtable_view2(gx_hashtable* ht, uint64_t** slots_dev, uint32_t* log2cap, uint64_t** counters_dev) {
+    if (!ht || !slots_dev || !log2cap || !counters_dev)
+        return set_error(GX_ERR_INVALID, "gx_hashtable_view2: null argument");
+    if (ht->layout != GX_HT_LINEAR) return set_error(GX_ERR_INVALID, "gx_hashtable_view2: linear tables only");
+    *slots_dev = ht->slots;
+    *log2cap = ht->log2cap;
+    *counters_dev = (uint64_t*)ht->counters;
+    return GX_OK;
+}
+
+gx_status gx_hashtable_clear(gx_hashtable* ht, void* stream) {
+    if (!ht) return set_error(GX_ERR_INVALID, "gx_hashtable_clear: null table");
+    const uint64_t cap = 1ull << ht->log2cap;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(4ull * sm_count(), (cap + 255) / 256));
+    ht_clear_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(ht->slots, cap, ht->counters);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+gx_status gx_hashtable_keys(const gx_hashtable* ht, int32_t* keys_dev, uint64_t cap, uint64_t* n_keys_dev,
+                            void* stream) {
+    if (!ht || !n_keys_dev || (cap && !keys_dev)) return set_error(GX_ERR_INVALID, "gx_hashtable_keys: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    GX_CK(cudaMemsetAsync(n_keys_dev, 0, sizeof(uint64_t), s));
+    const uint64_t n = 1ull << ht->log2cap;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(4ull * sm_count(), (n + 255) / 256));
+    ht_keys_kernel<<<grid, 256, 0, s>>>(ht->slots, n, ht->layout == GX_HT_DENSE ? 1u : 0u, keys_dev, cap,
+                                        (unsigned long long*)n_keys_dev);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+gx_status gx_check_minmax_points(const gx_column* col, const int32_t* keys_dev, const uint64_t* n_keys_dev,
+                                 uint64_t cap, uint16_t* out_dev, void* stream) {
+    if (!col || !col->residency || !n_keys_dev || !out_dev || (cap && !keys_dev))
+        return set_error(GX_ERR_INVALID, "gx_check_minmax_points: bad args");
+    const uint32_t n = col->n_chunks;
+    prune_points_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        col->d_mins, col->d_maxs, n, keys_dev, (const unsigned long long*)n_keys_dev, cap, out_dev);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
+gx_status gx_minmax_reduce(const int32_t* data_dev, uint64_t n, int32_t* range_dev, void* stream) {
+    if (!range_dev || (n && !data_dev)) return set_error(GX_ERR_INVALID, "gx_minmax_reduce: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int32_t init[2] = {INT32_MAX, INT32_MIN};
+    GX_CK(cudaMemcpyAsync(range_dev, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    if (n == 0) return GX_OK;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(2ull * sm_count(), (n + 4095) / 4096));
+    minmax_reduce_kernel<<<grid, 512, 0, s>>>(data_dev, n, range_dev);
+    GX_CK(cudaGetLastError());
+    return GX_OK;
+}
+
 gx_status gx_groupby_view(gx_groupby* gb, int64_t** keys_dev, int64_t** sums_dev, uint32_t* log2cap) {
     if (!gb || !keys_dev || !sums_dev || !log2cap) return set_error(GX_ERR_INVALID, "gx_groupby_view: null argument");
     *keys_dev = gb->keys;
@@ -1606,11 +1725,19 @@ static gx_status build_query(const gx_scan_plan* plan, QueryDesc* Q, uint32_t* t
         if (s.flags & GX_STEP_VALUE) any_value = true;
     }
     if (!any_value) return set_error(GX_ERR_INVALID, "scan plan has no VALUE step");
-    if (plan->agg > GX_AGG_COUNT) return set_error(GX_ERR_INVALID, "unknown aggregate");
+    if (plan->agg > GX_AGG_BUILD) return set_error(GX_ERR_INVALID, "unknown aggregate");
+    if (plan->agg == GX_AGG_BUILD) {
+        if (!plan->build_ht) return set_error(GX_ERR_INVALID, "a BUILD plan needs build_ht");
+        if (plan->build_ht->layout == GX_HT_DENSE)
+            return set_error(GX_ERR_INVALID, "a BUILD plan fills linear or bucket tables (dense tables size "
+                                             "themselves from the key range in gx_hashtable_build)");
+        if (plan->groupby || any_digit) return set_error(GX_ERR_INVALID, "a BUILD plan has no group key");
+    }
     if (plan->agg == GX_AGG_SUM_PRODUCT && !any_carry) return set_error(GX_ERR_INVALID, "SUM_PRODUCT needs a CARRY step");
     if (any_carry && any_digit) return set_error(GX_ERR_INVALID, "CARRY and group-key digits cannot be combined");
     if (plan->groupby && !any_digit) return set_error(GX_ERR_INVALID, "grouped scan needs PROBE/GROUP steps with digits");
-    if (!plan->groupby && !plan->result_dev) return set_error(GX_ERR_INVALID, "scan plan needs result_dev or groupby");
+    if (!plan->groupby && !plan->result_dev && plan->agg != GX_AGG_BUILD)
+        return set_error(GX_ERR_INVALID, "scan plan needs result_dev or groupby");
     if (!plan->groupby && any_digit) return set_error(GX_ERR_INVALID, "group-key digits need a groupby table");
     Q->n_steps = plan->n_steps;
     Q->agg = plan->agg;
@@ -1652,6 +1779,7 @@ static gx_status ensure_kernel_attrs() {
     if (!st) st = allow_smem(shared_scan_kernel<512, 1>, sh_max);
     if (!st) st = allow_smem(shared_scan_kernel<1024, 1>, sh_max);
     if (!st) st = allow_smem(shared_scan_kernel<kShSingleNT, 4, true>, sh_max);
+    if (!st) st = allow_smem(pipe_scan_kernel, kPipeMaxDynSmem);
     if (st) return st;
     attr_set[dev & 63] = true;
     return GX_OK;
@@ -1919,6 +2047,65 @@ static gx_status scan_launch_shared(const gx_scan_plan* plan, const QueryDesc& q
     return GX_OK;
 }
 
+// A plan that qualifies for the shared form and reads only HBM-resident
+// columns runs as the warp-specialised pipeline (pipe_scan_kernel): one CTA
+// per SM, a ring of stages sized to the shared memory.  *done = false when the
+// plan does not qualify.
+static gx_status scan_launch_pipe(const gx_scan_plan* plan, const QueryDesc& qd, const gx_column* c0,
+                                  cudaStream_t s, unsigned long long* rows_dev, bool* done) {
+    *done = false;
+    std::vector<const gx_column*> cols;
+    std::string why;
+    PipeParams P;
+    std::memset(&P, 0, sizeof(P));
+    if (!shared_query(*plan, qd, cols, P.q, &why)) return GX_OK;
+    if (cols.size() > kPipeMaxCols) return GX_OK;
+    uint32_t dec = 0, n_dec = 0;
+    for (size_t i = 0; i < cols.size(); ++i) {
+        const gx_column* c = cols[i];
+        if (c->residency != 1) return GX_OK;  // pinned-host columns: zero-copy reads in the shared form
+        if (c->codec != GX_CODEC_NONE) {
+            dec |= 1u << i;
+            ++n_dec;
+        }
+        P.cols[i] = c->view();
+    }
+    P.q.keep_in = plan->keep_chunks_dev;
+    P.q.keep_out = plan->keep_out_dev;
+    P.n_cols = (uint32_t)cols.size();
+    P.n_chunks = c0->n_chunks;
+    P.blocks_per_chunk = c0->blocks_per_chunk;
+    P.rows_per_chunk = c0->rows_per_chunk;
+    P.rows_per_block = c0->rows_per_block;
+    P.tile_rows = std::min<uint32_t>(kPipeTile, c0->rows_per_block);
+    P.tiles_per_block = (c0->rows_per_block + P.tile_rows - 1) / P.tile_rows;
+    P.n_rows = c0->n_rows;
+    P.dec_mask = dec;
+    P.gt_slots = P.q.grouped ? kShGroupSlots : 0u;
+    P.rows_scanned = rows_dev;
+    if (plan->agg == GX_AGG_BUILD) {
+        P.build_rowid = 1;
+        for (uint32_t k = 0; k < plan->n_steps; ++k)
+            if (plan->steps[k].flags & GX_STEP_CARRY) P.build_rowid = 0;
+        P.build_slots = plan->build_ht->slots;
+        P.build_log2 = plan->build_ht->log2cap;
+        P.build_layout = plan->build_ht->layout;
+        P.build_counters = plan->build_ht->counters;
+    }
+    const size_t fixed = 4ull * kShColWords * n_dec + 8ull * kCascPageMaxRuns + 12ull * P.gt_slots;
+    const size_t per_stage = (size_t)kPipeColBytes * P.n_cols;
+    if (fixed + 2 * per_stage > kPipeMaxDynSmem) return GX_OK;
+    P.stages = (uint32_t)std::min<size_t>(kPipeMaxStages, (kPipeMaxDynSmem - fixed) / per_stage);
+    const size_t smem = fixed + P.stages * per_stage;
+    const uint64_t tiles = (uint64_t)c0->n_slots * P.tiles_per_block;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count(), tiles));
+    pipe_scan_kernel<<<grid, kPipeNT, smem, s>>>(P);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "pipelined scan launch: %s", cudaGetErrorString(e));
+    *done = true;
+    return GX_OK;
+}
+
 static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned long long* rows_dev) {
     ScanParams P;
     std::memset(&P, 0, sizeof(P));
@@ -1929,6 +2116,11 @@ static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned 
     st = ensure_kernel_attrs();
     if (st) return st;
     bool done = false;
+    st = scan_launch_pipe(plan, P.q, c0, s, rows_dev, &done);
+    if (st || done) return st;
+    if (plan->agg == GX_AGG_BUILD)
+        return set_error(GX_ERR_INVALID, "a BUILD plan needs HBM-resident columns (LZ4 ones segmented, segments of "
+                                         "at most 2048 rows) and its VALUE step last");
     st = scan_launch_shared(plan, P.q, c0, s, rows_dev, &done);
     if (st || done) return st;
     ItemsParams ip{};
@@ -2002,6 +2194,7 @@ static gx_status scan_launch_static(const gx_scan_plan* plan, cudaStream_t s) {
     uint32_t tile_rows = 0;
     gx_status st = build_query(plan, &P.q, &tile_rows, &c0);
     if (st) return st;
+    if (plan->agg == GX_AGG_BUILD) return set_error(GX_ERR_INVALID, "gx_scan_static: BUILD plans run through gx_scan");
     const uint32_t n_chunks = c0->n_chunks;
     if (n_chunks > kStaticMaxChunks)
         return set_error(GX_ERR_INVALID, "gx_scan_static: %u chunks exceed the static work list of %u chunks", n_chunks,
@@ -2206,6 +2399,8 @@ gx_status gx_batch_assign(gx_batch* b, const gx_query* queries, uint32_t n_queri
         uint32_t tr = 0;
         gx_status st = build_query(&queries[i].plan, &qs[i], &tr, &ci);
         if (st) return st;
+        if (queries[i].plan.agg == GX_AGG_BUILD)
+            return set_error(GX_ERR_INVALID, "query %u: BUILD plans run through gx_scan, not in a batch", i);
         if (c0 && (ci->n_rows != c0->n_rows || ci->rows_per_chunk != c0->rows_per_chunk ||
                    ci->rows_per_block != c0->rows_per_block))
             return set_error(GX_ERR_INVALID, "query %u scans a table with another layout", i);

@@ -291,13 +291,12 @@ __device__ __forceinline__ uint32_t sh_col_index(uint32_t r, uint32_t sh, uint32
 template <int NT>
 __device__ __forceinline__ int shared_decode(const gx_dcol& col, uint32_t c, uint32_t slot, uint32_t rows,
                                              uint32_t r0, uint32_t n, uint32_t* colbuf, uint8_t* stage,
-                                             uint64_t* mbar, uint32_t& phase, uint32_t* s_tmp, CascTile* s_ct,
-                                             int* s_err, int* s_fatal, uint32_t* s_sh, uint32_t* s_pd,
-                                             uint32_t* s_seg) {
+                                             uint64_t* mbar, uint32_t& phase, uint32_t* s_tmp, int* s_err,
+                                             int* s_fatal, uint32_t* s_sh, uint32_t* s_pd, uint32_t* s_seg) {
     uint32_t* buf = colbuf + c * kShColWords;
     uint32_t pad_log2 = 0;
-    int layout = decode_tile<NT, kTileRows>(col, slot, rows, r0, n, buf, stage, mbar, phase, s_tmp, s_ct, s_err,
-                                            pad_log2, s_seg);
+    const int layout = decode_tile<NT, kTileRows>(col, slot, rows, r0, n, buf, stage, mbar, phase, s_tmp, s_err,
+                                                  pad_log2, s_seg);
     const int derr = *s_err;
     __syncthreads();
     if (derr) {
@@ -308,11 +307,6 @@ __device__ __forceinline__ int shared_decode(const gx_dcol& col, uint32_t c, uin
         }
         __syncthreads();
         return derr;
-    }
-    if (layout == kRuns) {
-        casc_runs_to_rows<NT>(*s_ct, (const int32_t*)stage, (const uint32_t*)(stage + 4 * kCascMaxRuns), r0, n,
-                              (int32_t*)buf);
-        layout = kRows;
     }
     s_sh[c] = layout == kSegRows ? col.seg_shift : 31u;
     s_pd[c] = layout == kSegRows ? pad_log2 : 0u;
@@ -357,8 +351,9 @@ __device__ __forceinline__ void shared_literal_locate(const ShParams& P, uint32_
                         src = c.payload + d.offset + lo;
                         if (prefetch) {
                             // the bytes (16-byte aligned cover, inside the payload's slack) into L2
-                            const uint8_t* a = c.payload + d.offset + (lo & ~15u);
-                            const uint32_t bytes = ((hi + 15u) & ~15u) - (lo & ~15u);
+                            const uint64_t a0 = (d.offset + lo) & ~15ull;
+                            const uint8_t* a = c.payload + a0;
+                            const uint32_t bytes = (uint32_t)(((d.offset + hi + 15u) & ~15ull) - a0);
                             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes)
                                          : "memory");
                         }
@@ -463,7 +458,6 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
     __shared__ int s_fatal;
     __shared__ uint32_t s_sh[kShMaxCols], s_pd[kShMaxCols];
     __shared__ uint32_t s_tmp[NW + 1];
-    __shared__ CascTile s_ct;
     __shared__ uint32_t s_seg[2 * (kMaxSegments + 1)];
     __shared__ uint32_t s_cols;                    // batches: columns the tile's active queries read
     __shared__ uint32_t s_list[SINGLE ? NT : 1];   // one query: this CTA's live items of the round
@@ -646,7 +640,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                     }
                     if (!((decoded >> c) & 1u)) {
                         if (shared_decode<NT>(sh_c<SINGLE>(P, c), c, slot, rows, r0, n, colbuf, stage, &s_mbar,
-                                              phase, s_tmp, &s_ct, &s_err, &s_fatal, s_sh, s_pd, s_seg)) {
+                                              phase, s_tmp, &s_err, &s_fatal, s_sh, s_pd, s_seg)) {
                             dropped = true;
                             break;
                         }

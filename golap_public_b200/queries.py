@@ -51,7 +51,7 @@ class Q1Query:
     """Q1-shaped fused scan over a FactTable with columns date_key, discount, quantity, extended_price."""
 
     def __init__(self, fact: FactTable, date: dict, date_ok: np.ndarray, date_lo: int, date_hi: int,
-                 dlo: int, dhi: int, qlo: int, qhi: int, prune: bool = True):
+                 dlo: int, dhi: int, qlo: int, qhi: int, prune: bool = True, join_prune: bool = False):
         import torch
 
         self.fact = fact
@@ -64,7 +64,17 @@ class Q1Query:
         self.keep = torch.zeros(n_chunks, dtype=torch.uint16, device="cuda") if prune else None
         self.result = torch.zeros(1, dtype=torch.int64, device="cuda")
         c = fact.cols
-        self.plan = ScanPlan(agg=L.GX_AGG_SUM_PRODUCT, result=self.result, keep_out=self.keep)
+        # join pruning (usecases/ssb/queries/01.hpp:246-270): chunks whose
+        # date_key min/max holds none of the date table's keys are skipped
+        self.join_prune = join_prune
+        self.join_keep = None
+        if join_prune:
+            self._jkeys = torch.empty(max(1, len(date["d_key"])), dtype=torch.int32, device="cuda")
+            self._jn = torch.zeros(1, dtype=torch.int64, device="cuda")
+            self.join_keep = torch.zeros(n_chunks, dtype=torch.uint16, device="cuda")
+            self.refresh_join_keep()
+        self.plan = ScanPlan(agg=L.GX_AGG_SUM_PRODUCT, result=self.result, keep_out=self.keep,
+                             keep_chunks=self.join_keep)
         if prune:  # MetaChecker::add_minmax on the date column, evaluated by the scan launch
             self.plan.prune_minmax(c["date_key"], date_lo, date_hi)
         self.plan.probe(c["date_key"], self.ht)
@@ -72,6 +82,15 @@ class Q1Query:
         self.plan.filter(c["quantity"], qlo, qhi)
         self.plan.value(c["extended_price"])
         self.plan.to_c()
+
+    def refresh_join_keep(self, stream=None):
+        """Join-pruning flags from the date table's current keys (no host synchronisation)."""
+        from .api import MetaChecker
+
+        self.ht.keys(self._jkeys, self._jn, stream)
+        self.join_keep.zero_()
+        MetaChecker(self.join_keep.numel()).add_points(self.fact.cols["date_key"], self._jkeys, self._jn,
+                                                       self.join_keep, stream)
 
     def launch(self, stream=None):
         """Enqueue: clear result, prune + fused scan (no host synchronisation)."""
@@ -86,25 +105,54 @@ class Q1Query:
         return int(self.result.item())
 
 
-class Q3Query:
-    """Q3-shaped star join + group-by over a FactTable with cust_key, supp_key, date_key, revenue."""
+def build_from_compressed(ht: HashMap, key: Column, payload: Column | None, preds=(), stream=None):
+    """Fill join table `ht` from compressed dimension columns in one fused
+    launch (GX_AGG_BUILD): rows passing the range predicates [(Column, lo, hi)]
+    are inserted with key from `key` and payload from `payload` (or the row
+    number).  Replaces pipeline_customer_q3 and its per-chunk loop
+    (usecases/ssb/queries/03.cuh:94-116, 03.hpp:408-476)."""
+    ht.clear(stream)
+    p = ScanPlan(agg=L.GX_AGG_BUILD, build_ht=ht)
+    for col, lo, hi in preds:
+        p.filter(col, lo, hi)
+    if payload is not None:
+        p.carry(payload)
+    p.value(key)
+    p.launch(stream)
+    return p
 
-    def __init__(self, fact: FactTable, customer: dict, supplier: dict, date: dict, region: int, ylo: int, yhi: int,
+
+class Q3Query:
+    """Q3-shaped star join + group-by over a FactTable with cust_key, supp_key, date_key, revenue.
+
+    `customer` is a dict of host arrays (key, nation, region), built from
+    device copies of them, or a FactTable of compressed customer columns,
+    built from the compressed chunks in one fused launch (build_from_compressed)."""
+
+    def __init__(self, fact: FactTable, customer, supplier: dict, date: dict, region: int, ylo: int, yhi: int,
                  prune: bool = True, n_nations: int = 25, ht_layout: str = "linear"):
         import torch
 
         self.fact = fact
         self.n_nations = n_nations
         self.ylo, self.yhi = ylo, yhi
-        # tables sized for the rows that pass the dimension filters
-        self.hc = HashMap(max(1, int((customer["region"] == region).sum())), ht_layout)
+        self.region = region
+        self.cust_comp = customer if isinstance(customer, FactTable) else None
+        cust_host = None if self.cust_comp else customer
+        # tables sized for the rows that pass the dimension filters (a table
+        # built from compressed columns is sized for every customer)
+        n_c = self.cust_comp.n_rows if self.cust_comp else int((customer["region"] == region).sum())
+        self.hc = HashMap(max(1, n_c), "linear" if self.cust_comp and ht_layout == "dense" else ht_layout)
         self.hs = HashMap(max(1, int((supplier["region"] == region).sum())), ht_layout)
         self.hd = HashMap(max(1, int(((date["d_year"] >= ylo) & (date["d_year"] <= yhi)).sum())), ht_layout)
-        self._keep_alive = [_dev(customer["key"]), _dev(customer["nation"]), _dev(customer["region"]),
+        empty = np.zeros(1, np.int32)
+        self._keep_alive = [_dev(cust_host["key"] if cust_host else empty),
+                            _dev(cust_host["nation"] if cust_host else empty),
+                            _dev(cust_host["region"] if cust_host else empty),
                             _dev(supplier["key"]), _dev(supplier["nation"]), _dev(supplier["region"]),
                             _dev(date["d_key"]), _dev(date["d_year"])]
         ck, cn, cr, sk, sn, sr, dk, dy = self._keep_alive
-        self.hc.build(ck, cn, preds=[(cr, region, region)])
+        self.build_customer()
         self.hs.build(sk, sn, preds=[(sr, region, region)])
         self.hd.build(dk, dy, preds=[(dy, ylo, yhi)])
         n_chunks = fact.cols["date_key"].info.n_chunks
@@ -121,6 +169,16 @@ class Q3Query:
         self.plan.probe(c["date_key"], self.hd, ylo, self.ycard)
         self.plan.value(c["revenue"])
         self.plan.to_c()
+
+    def build_customer(self, stream=None):
+        """The customer join table: filtered build from device arrays, or from the
+        compressed customer columns in one fused launch."""
+        if self.cust_comp:
+            c = self.cust_comp.cols
+            build_from_compressed(self.hc, c["key"], c["nation"], [(c["region"], self.region, self.region)], stream)
+        else:
+            ck, cn, cr = self._keep_alive[:3]
+            self.hc.build(ck, cn, preds=[(cr, self.region, self.region)], stream=stream)
 
     def launch(self, stream=None):
         self.agg.reset(stream)

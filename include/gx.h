@@ -152,6 +152,13 @@ gx_status gx_combine_and(uint16_t* out_dev, const uint16_t* a_dev, const uint16_
 /* Whole MetaChecker pass in one launch: keep_dev[c] = AND over predicates. */
 gx_status gx_prune_minmax(const gx_column* const* cols, const int32_t* lo, const int32_t* hi,
                           uint32_t n_preds, uint16_t* keep_dev, void* stream);
+/* Join pruning, check_mmmeta_multiple_pts (core/metadata.cuh:550-560) as used
+ * behind --join_prune (usecases/ssb/queries/01.hpp:246-270): sets out_dev[c] = 1
+ * where some key lies in chunk c's [min, max] of col, leaves other entries
+ * untouched.  The keys are keys_dev[0 .. min(*n_keys_dev, cap)) with the count
+ * on the device, as gx_hashtable_keys leaves it (no host synchronisation). */
+gx_status gx_check_minmax_points(const gx_column* col, const int32_t* keys_dev, const uint64_t* n_keys_dev,
+                                 uint64_t cap, uint16_t* out_dev, void* stream);
 
 /* --------------------------------------------------------------- hash join
  * Replaces: HashMap (core/dev_structs.cuh:37-132) with its filtered build
@@ -199,6 +206,28 @@ gx_status gx_hashtable_probe(const gx_hashtable* ht, const int32_t* keys_dev, ui
  * passing HashMap by value to a kernel (core/dev_structs.cuh:71-82). */
 gx_status gx_hashtable_view(const gx_hashtable* ht, const uint64_t** slots_dev, uint32_t* log2cap);
 
+/* Writable view for inserting from other kernels (linear tables only):
+ * counters_dev[0] counts inserted keys, [1] duplicates, [2] rows that found
+ * no slot or carried the reserved key (gx_hashtable_count reads them).
+ * Replaces HashMap::insert from a kernel (core/dev_structs.cuh:89-98), used by
+ * hash_map_build_pred_other (core/join.cuh:107-135) and
+ * pipeline_customer_q3 (usecases/ssb/queries/03.cuh:94-116). */
+gx_status gx_hashtable_view2(gx_hashtable* ht, uint64_t** slots_dev, uint32_t* log2cap, uint64_t** counters_dev);
+/* Keys of the table's entries into keys_dev (any order; at most cap written),
+ * their count into *n_keys_dev (device uint64, may exceed cap).  Replaces
+ * collect_hashmap_keys (core/dev_structs.cuh:136-150). */
+gx_status gx_hashtable_keys(const gx_hashtable* ht, int32_t* keys_dev, uint64_t cap, uint64_t* n_keys_dev,
+                            void* stream);
+/* Empty every slot and zero the counters (the cudaMemset of the HashMap
+ * constructor, core/dev_structs.cuh:47-56); gx_hashtable_build clears by itself. */
+gx_status gx_hashtable_clear(gx_hashtable* ht, void* stream);
+
+/* ------------------------------------------------------------ min/max
+ * Replaces: MinMaxMeta::init_chunk (core/metadata.cuh:157-160), the two CUB
+ * reductions per chunk: range_dev[0] = min, range_dev[1] = max of data_dev[0..n)
+ * (device arrays; for n == 0 they stay INT32_MAX / INT32_MIN). */
+gx_status gx_minmax_reduce(const int32_t* data_dev, uint64_t n, int32_t* range_dev, void* stream);
+
 /* ---------------------------------------------------------- hash aggregate
  * Replaces: HashAggregate (core/dev_structs.cuh:158-253) with SumAgg
  * (usecases/ssb/queries/query_common.cuh:24-29) and the group_by_agg kernels
@@ -245,7 +274,18 @@ enum {
     GX_STEP_VALUE = 8,
     GX_STEP_GROUP = 16
 };
-enum { GX_AGG_SUM = 0, GX_AGG_SUM_PRODUCT = 1, GX_AGG_COUNT = 2 };
+enum { GX_AGG_SUM = 0, GX_AGG_SUM_PRODUCT = 1, GX_AGG_COUNT = 2, GX_AGG_BUILD = 3 };
+/* GX_AGG_BUILD fills a join table instead of aggregating: every row that
+ * passes the plan's FILTER / PROBE steps is inserted into plan.build_ht with
+ * the VALUE step's column as the key and the carried value (a CARRY step) as
+ * the payload, or the table row number when the plan carries nothing.  The
+ * scan does not clear the table first (gx_hashtable_clear); duplicate keys
+ * behave as in gx_hashtable_build and gx_hashtable_count reports the rows.
+ * Linear and bucket tables; columns HBM-resident, LZ4 columns segmented.
+ * Replaces: pipeline_customer_q3 (usecases/ssb/queries/03.cuh:94-116) with the
+ * per-chunk loop that feeds it decompressed customer chunks
+ * (usecases/ssb/queries/03.hpp:408-476): decode, filter, compact and insert
+ * become one fused kernel over the compressed dimension columns. */
 
 #define GX_MAX_STEPS 8
 
@@ -275,6 +315,7 @@ typedef struct gx_scan_plan {
     uint32_t n_prune;                 /* min/max predicates ANDed with keep_chunks */
     gx_scan_prune prune[GX_MAX_STEPS];
     uint16_t* keep_out_dev;           /* optional: resulting per-chunk flags     */
+    gx_hashtable* build_ht;           /* GX_AGG_BUILD: the table rows go into    */
 } gx_scan_plan;
 
 /* Run the plan on `stream`.  Does not clear result_dev or the group table

@@ -140,7 +140,7 @@ static uint32_t or_unpack(const uint32_t* w, uint64_t i, uint32_t bits) {
     return (uint32_t)((two >> (bit & 31)) & mask);
 }
 
-OR_EXPORT int64_t or_casc_decode(const uint8_t* blk, uint64_t blk_bytes, int32_t* out, uint64_t max_rows) {
+static int64_t or_casc_decode_page(const uint8_t* blk, uint64_t blk_bytes, int32_t* out, uint64_t max_rows) {
     if (blk_bytes < 32) return -1;
     uint32_t h[8];
     memcpy(h, blk, 32);
@@ -174,6 +174,29 @@ OR_EXPORT int64_t or_casc_decode(const uint8_t* blk, uint64_t blk_bytes, int32_t
     return r == n_rows ? (int64_t)n_rows : -1;
 }
 
+/* A cascaded block is a page table {n_pages, page_rows, page_off[n_pages+1]}
+ * followed by independently coded pages of page_rows rows (the last one
+ * shorter); decodes every page in order.  Returns rows or -1. */
+OR_EXPORT int64_t or_casc_decode(const uint8_t* blk, uint64_t blk_bytes, int32_t* out, uint64_t max_rows) {
+    if (blk_bytes < 8) return -1;
+    uint32_t n_pages, page_rows;
+    memcpy(&n_pages, blk, 4);
+    memcpy(&page_rows, blk + 4, 4);
+    if (page_rows == 0 || (uint64_t)8 + 4ull * ((uint64_t)n_pages + 1) > blk_bytes) return -1;
+    uint64_t rows = 0;
+    for (uint32_t p = 0; p < n_pages; ++p) {
+        uint32_t a, b;
+        memcpy(&a, blk + 8 + 4ull * p, 4);
+        memcpy(&b, blk + 8 + 4ull * (p + 1), 4);
+        if (a > b || b > blk_bytes || (a & 15u)) return -1;
+        uint64_t cap = max_rows - rows < page_rows ? max_rows - rows : page_rows;
+        int64_t got = or_casc_decode_page(blk + a, b - a, out + rows, cap);
+        if (got < 0 || (p + 1 < n_pages && (uint64_t)got != page_rows)) return -1;
+        rows += (uint64_t)got;
+    }
+    return (int64_t)rows;
+}
+
 /* ------------------------------------------------------ min/max pruning
  * MinMaxMeta::check_pred_host / check_pred (core/metadata.cuh:195-211):
  * keep a chunk when lo <= chunk_max && hi >= chunk_min (inclusive);
@@ -185,6 +208,18 @@ OR_EXPORT void or_minmax_keep(const int32_t* mins, const int32_t* maxs, uint64_t
         uint16_t k = (lo <= maxs[c] && hi >= mins[c]) ? 1 : 0;
         keep[c] = and_into ? (uint16_t)(keep[c] & k) : k;
     }
+}
+
+/* check_mmmeta_multiple_pts (core/metadata.cuh:550-560): keep[c] = 1 where
+ * some key lies in [mins[c], maxs[c]] (entries already 1 stay 1). */
+OR_EXPORT void or_minmax_points_keep(const int32_t* mins, const int32_t* maxs, uint64_t n, const int32_t* keys,
+                                     uint64_t n_keys, uint16_t* keep) {
+    for (uint64_t c = 0; c < n; ++c)
+        for (uint64_t i = 0; i < n_keys; ++i)
+            if (keys[i] >= mins[c] && keys[i] <= maxs[c]) {
+                keep[c] = 1;
+                break;
+            }
 }
 
 /* Per-chunk min/max as collected at ingest by MinMaxMeta::init_chunk

@@ -60,6 +60,8 @@ def lib():
         L.or_q3.restype = C.c_int
         L.or_q3.argtypes = [_P, _P, _P, _P, _u64, _P, _P, _P, _u64, _P, _P, _P, _u64, _P, _P, _P, _u64,
                             _i32, _u32, _i32, _u32, _i32, _u32, _P, _P, _P, _u64]
+        L.or_minmax_points_keep.restype = None
+        L.or_minmax_points_keep.argtypes = [_P, _P, _u64, _P, _u64, _P]
         L.or_group_sum_dense.restype = C.c_int
         L.or_group_sum_dense.argtypes = [_P, _P, _u64, _P, _u64]
         L.or_ssb_sizes_for.restype = None
@@ -88,9 +90,14 @@ def ref():
         R.ref_lz4_compress_blocks.argtypes = [_P, _u64, _u64, _P, _u64, _P]
         R.ref_lz4_decompress.restype = C.c_int
         R.ref_lz4_decompress.argtypes = [_P, C.c_int, _P, C.c_int]
-        R.ref_cpu_q1.restype = _i64
-        R.ref_cpu_q1.argtypes = [_u32, _u64, _u64, _u64, _P, _P, _P, _P, _u64, _P, _P, _P, _u64,
-                                 _i32, _i32, _i32, _i32, _i32, _i32, C.POINTER(C.c_double), C.POINTER(_u64)]
+        R.ref_cpu_q1_comp.restype = _i64
+        R.ref_cpu_q1_comp.argtypes = [_u32, _u64, _u64, _u64, _P, _P, _P, _P, _P, _u64,
+                                      _i32, _i32, _i32, _i32, _i32, _i32, C.POINTER(C.c_double), C.POINTER(_u64),
+                                      C.POINTER(_u64)]
+        R.ref_cpu_q3_comp.restype = _i64
+        R.ref_cpu_q3_comp.argtypes = [_u32, _u64, _u64, _u64, _P, _P, _P, _P, _P, _P, _u64, _P, _P, _P, _u64,
+                                      _P, _P, _u64, _i32, _i32, _i32, _P, _P, _u64, C.POINTER(_u64),
+                                      C.POINTER(C.c_double), C.POINTER(_u64), C.POINTER(_u64)]
         _ref = R
     return _ref
 
@@ -116,6 +123,16 @@ def minmax_keep(mins, maxs, lo, hi, keep=None):
         lib().or_minmax_keep(_ptr(mins), _ptr(maxs), n, lo, hi, _ptr(keep), 0)
     else:
         lib().or_minmax_keep(_ptr(mins), _ptr(maxs), n, lo, hi, _ptr(keep), 1)
+    return keep
+
+
+def minmax_points_keep(mins, maxs, keys) -> np.ndarray:
+    """Join-pruning flags (check_mmmeta_multiple_pts)."""
+    keep = np.zeros(len(mins), np.uint16)
+    k = np.ascontiguousarray(keys, np.int32)
+    mn = np.ascontiguousarray(mins, np.int32)
+    mx = np.ascontiguousarray(maxs, np.int32)
+    lib().or_minmax_points_keep(_ptr(mn), _ptr(mx), len(mn), _ptr(k), len(k), _ptr(keep))
     return keep
 
 
@@ -206,3 +223,22 @@ def ssb_queries(t: dict) -> dict:
     r["q3_1_sum"] = int(sums.sum())
     r["q3_1_cells"] = (sums, counts)
     return r
+
+
+# --------------------------------------------- reference CPU baselines over compressed columns
+
+class CompCol(C.Structure):
+    """{payload, blocks, codec} as ref_cpu_*_comp take it (blocks: 4 uint64 per present block)."""
+    _fields_ = [("payload", C.c_void_p), ("blocks", C.c_void_p), ("codec", C.c_uint32)]
+
+
+def comp_cols(cols):
+    """CompCol array over (payload uint8 array, blocks uint64 (n,4) array, codec) triples; the
+    arrays must stay alive while the result is used."""
+    arr = (CompCol * len(cols))()
+    for i, (pl, blocks, codec) in enumerate(cols):
+        arr[i].payload = pl.ctypes.data
+        assert blocks.dtype == np.uint64 and blocks.flags.c_contiguous and pl.flags.c_contiguous
+        arr[i].blocks = blocks.ctypes.data
+        arr[i].codec = codec
+    return arr

@@ -292,70 +292,269 @@ __attribute__((visibility("default"))) int ref_lz4_decompress(const char* in, in
     return m.decompress(out, in, comp_size, decomp_size);
 }
 
-// CPU baseline for a Q1-shaped query over LZ4-compressed chunks, composed of
-// the reference's CPU pieces the way its GPU driver composes its GPU pieces
-// (usecases/ssb/queries/01.hpp:350-424): min/max host pruning
-// (MinMaxMeta::check_pred_host, core/metadata.cuh:195-200) over the
-// per-chunk min/max arrays, then per surviving chunk LZ4CPUManager
-// decompression of the discount / quantity / extended-price blocks and the
-// query1inmem probe loop (01inmem.hpp:109-130) with a HostHashMap date table.
-// date_key is handed over uncompressed: the reference has no CPU cascaded
-// decoder.  Chunks are split over `workers` threads with SliceSeq.
-// Returns the sum; *elapsed_ms receives the wall time of the timed part.
-__attribute__((visibility("default"))) int64_t ref_cpu_q1(
-    uint32_t workers, uint64_t n_rows, uint64_t rows_per_chunk, uint64_t rows_per_block,
-    const int32_t* date_key, const int32_t* date_mins, const int32_t* date_maxs,
-    const char* const* comp_cols /* 3: discount, quantity, extendedprice */, uint64_t comp_stride,
-    const int32_t* const* comp_sizes, const int32_t* d_key, const uint8_t* d_ok, uint64_t n_date, int32_t date_lo,
-    int32_t date_hi, int32_t dlo, int32_t dhi, int32_t qlo, int32_t qhi, double* elapsed_ms, uint64_t* chunks_scanned) {
+// ---------------------------------------------------------------------------
+// CPU baselines over the compressed columns the GPU path scans (the same
+// bytes): LZ4 blocks decoded by the reference's LZ4CPUManager
+// (core/comp_cpu.hpp:22-32); cascaded blocks (the build's own format, for
+// which the reference has no CPU decoder) decoded by casc_cpu_block below,
+// labelled as such by the caller.  Columns arrive as {payload, blocks} where
+// blocks[4*k..] = {offset, size, payload bytes, tuples} of the k-th present
+// block in slot order (gx_column_blocks, the reference's BlockInfo layout,
+// core/comp.cuh:23-32).
+// ---------------------------------------------------------------------------
+
+// Cascaded page / block decode (format in golap_public_b200/csrc/gx_internal.h).
+static inline uint32_t cc_unpack(const uint32_t* w, uint64_t i, uint32_t bits) {
+    if (bits == 0) return 0;
+    const uint64_t bit = i * bits;
+    const uint64_t two = (uint64_t)w[bit >> 5] | ((uint64_t)w[(bit >> 5) + 1] << 32);
+    return (uint32_t)((two >> (bit & 31)) & (bits == 32 ? 0xFFFFFFFFull : ((1ull << bits) - 1)));
+}
+static bool casc_cpu_page(const uint8_t* pg, uint32_t bytes, int32_t* out, uint32_t rows) {
+    if (bytes < 32) return false;
+    uint32_t h[8];
+    std::memcpy(h, pg, 32);
+    const uint32_t n_rows = h[0], n_runs = h[1], flags = h[2] & 255, vbits = (h[2] >> 8) & 255,
+                   lbits = (h[2] >> 16) & 255, vbase = h[4], lbase = h[5], voff = h[6], loff = h[7];
+    const bool rle = flags & 1, delta = flags & 2;
+    if (n_rows != rows || vbits > 32 || lbits > 32 || (!rle && n_runs != rows)) return false;
+    if ((uint64_t)voff + 4ull * (((uint64_t)n_runs * vbits + 31) / 32 + 1) > bytes) return false;
+    if (rle && (uint64_t)loff + 4ull * (((uint64_t)n_runs * lbits + 31) / 32 + 1) > bytes) return false;
+    const uint32_t* vw = (const uint32_t*)(pg + voff);
+    const uint32_t* lw = (const uint32_t*)(pg + loff);
+    uint32_t acc = h[3], r = 0;
+    for (uint32_t i = 0; i < n_runs; ++i) {
+        const uint32_t e = cc_unpack(vw, i, vbits) + vbase;
+        const uint32_t v = delta ? (i ? (acc += e) : acc) : e;
+        const uint32_t len = rle ? cc_unpack(lw, i, lbits) + lbase : 1;
+        if (r + len > rows) return false;
+        for (uint32_t k = 0; k < len; ++k) out[r + k] = (int32_t)v;
+        r += len;
+    }
+    return r == rows;
+}
+static bool casc_cpu_block(const uint8_t* blk, uint64_t bytes, int32_t* out, uint32_t rows) {
+    if (bytes < 8) return false;
+    uint32_t np, pr;
+    std::memcpy(&np, blk, 4);
+    std::memcpy(&pr, blk + 4, 4);
+    if (pr == 0 || 8 + 4ull * (np + 1) > bytes) return false;
+    uint32_t done = 0;
+    for (uint32_t p = 0; p < np; ++p) {
+        uint32_t a, b;
+        std::memcpy(&a, blk + 8 + 4ull * p, 4);
+        std::memcpy(&b, blk + 8 + 4ull * (p + 1), 4);
+        const uint32_t n = std::min(pr, rows - done);
+        if (a > b || b > bytes || !casc_cpu_page(blk + a, b - a, out + done, n)) return false;
+        done += n;
+    }
+    return done == rows;
+}
+
+struct CompCol {
+    const uint8_t* payload;
+    const uint64_t* blocks;  // 4 words per present block
+    uint32_t codec;          // 1 LZ4, 2 cascaded
+};
+
+// Decode present block k of a column into out (rows values).
+static bool decode_block(const CompCol& c, uint64_t k, int32_t* out, uint32_t rows, golap::LZ4CPUManager& m) {
+    const uint64_t off = c.blocks[4 * k], used = c.blocks[4 * k + 2];
+    if (c.codec == 1) return m.decompress((char*)out, (const char*)(c.payload + off), (int)used, (int)(rows * 4)) ==
+                             (int)(rows * 4);
+    return casc_cpu_block(c.payload + off, used, out, rows);
+}
+
+// Present blocks of the table in slot order: first row and row count; those
+// of chunks that pass the min/max check (MinMaxMeta::check_pred_host,
+// core/metadata.cuh:195-200) go into `work`.
+static void table_blocks(uint64_t n_rows, uint64_t rpc, uint64_t rpb, const int32_t* mins, const int32_t* maxs,
+                         int32_t lo, int32_t hi, std::vector<uint64_t>& work, std::vector<uint64_t>& row0,
+                         std::vector<uint32_t>& rows, uint64_t* chunks_kept) {
+    const uint64_t n_chunks = (n_rows + rpc - 1) / rpc;
+    uint64_t kept = 0;
+    for (uint64_t c = 0; c < n_chunks; ++c) {
+        const uint64_t r0 = c * rpc, r1 = std::min(n_rows, r0 + rpc);
+        const bool keep = !mins || (lo <= maxs[c] && hi >= mins[c]);
+        kept += keep;
+        for (uint64_t b0 = r0; b0 < r1; b0 += rpb) {
+            if (keep) work.push_back(row0.size());
+            row0.push_back(b0);
+            rows.push_back((uint32_t)std::min(rpb, r1 - b0));
+        }
+    }
+    *chunks_kept = kept;
+}
+
+// Q1 shape (query1inmem loop body, usecases/ssb/queries/01inmem.hpp:109-130)
+// over compressed date_key / discount / quantity / extended_price: date table
+// HostHashMap built from the flagged dimension rows, chunk pruning on the
+// date_key min/max, then the surviving blocks split evenly over `workers`
+// threads (SliceSeq), each decoding its blocks and running the probe loop.
+__attribute__((visibility("default"))) int64_t ref_cpu_q1_comp(
+    uint32_t workers, uint64_t n_rows, uint64_t rows_per_chunk, uint64_t rows_per_block, const CompCol* cols /* 4 */,
+    const int32_t* date_mins, const int32_t* date_maxs, const int32_t* d_key, const uint8_t* d_ok, uint64_t n_date,
+    int32_t date_lo, int32_t date_hi, int32_t dlo, int32_t dhi, int32_t qlo, int32_t qhi, double* elapsed_ms,
+    uint64_t* chunks_scanned, uint64_t* rows_scanned) {
+    std::vector<uint64_t> work, row0;
+    std::vector<uint32_t> brows;
+    table_blocks(n_rows, rows_per_chunk, rows_per_block, date_mins, date_maxs, date_lo, date_hi, work, row0, brows,
+                 chunks_scanned);
     std::vector<uint64_t> dkeys(n_date);
     for (uint64_t i = 0; i < n_date; ++i) dkeys[i] = (uint64_t)d_key[i];
     util::Timer timer;
     golap::HostHashMap<uint64_t> hm(n_date, dkeys.data());
     for (uint64_t i = 0; i < n_date; ++i)
         if (d_ok[i]) hm.insert(i, dkeys[i]);
-    const uint64_t n_chunks = (n_rows + rows_per_chunk - 1) / rows_per_chunk;
-    const uint64_t bpc = (rows_per_chunk + rows_per_block - 1) / rows_per_block;
-    std::vector<uint64_t> keep;
-    for (uint64_t c = 0; c < n_chunks; ++c)
-        if (date_lo <= date_maxs[c] && date_hi >= date_mins[c]) keep.push_back(c);
-    std::atomic<uint64_t> agg{0};
-    util::SliceSeq sl{keep.size(), workers};
+    std::atomic<uint64_t> agg{0}, scanned{0};
+    std::atomic<int> bad{0};
+    util::SliceSeq sl{work.size(), workers};
     std::vector<std::tuple<uint64_t, uint64_t>> sls(workers);
     for (auto& [s, e] : sls) sl.get(s, e);
     std::vector<std::thread> th;
     for (uint32_t w = 0; w < workers; ++w)
         th.emplace_back([&, w] {
             golap::LZ4CPUManager m;
-            std::vector<int32_t> buf[3];
+            std::vector<int32_t> buf[4];
             for (auto& b : buf) b.resize(rows_per_block);
-            uint64_t part = 0;
+            uint64_t part = 0, nr = 0;
             auto [s, e] = sls[w];
-            for (uint64_t k = s; k < e; ++k) {
-                const uint64_t c = keep[k];
-                const uint64_t r0 = c * rows_per_chunk, r1 = std::min(n_rows, r0 + rows_per_chunk);
-                for (uint64_t j = 0; j < bpc; ++j) {
-                    const uint64_t b0 = r0 + j * rows_per_block;
-                    if (b0 >= r1) break;
-                    const uint64_t rows = std::min(rows_per_block, r1 - b0);
-                    const uint64_t slot = c * bpc + j;
-                    for (int col = 0; col < 3; ++col)
-                        m.decompress((char*)buf[col].data(), comp_cols[col] + slot * comp_stride,
-                                     comp_sizes[col][slot], (int)(rows * 4));
-                    for (uint64_t i = 0; i < rows; ++i) {
-                        int32_t disc = buf[0][i], qty = buf[1][i];
-                        if (disc < dlo || disc > dhi || qty < qlo || qty > qhi) continue;
-                        if (hm.probe((uint64_t)date_key[b0 + i]) == (uint64_t)-1) continue;
-                        part += (uint64_t)((int64_t)buf[2][i] * disc);
-                    }
+            for (uint64_t t = s; t < e; ++t) {
+                const uint64_t k = work[t];
+                const uint32_t rows = brows[k];
+                for (int c = 0; c < 4; ++c)
+                    if (!decode_block(cols[c], k, buf[c].data(), rows, m)) bad = 1;
+                const int32_t *od = buf[0].data(), *disc = buf[1].data(), *qty = buf[2].data(), *ext = buf[3].data();
+                for (uint32_t i = 0; i < rows; ++i) {
+                    if (disc[i] < dlo || disc[i] > dhi || qty[i] < qlo || qty[i] > qhi) continue;
+                    if (hm.probe((uint64_t)od[i]) == (uint64_t)-1) continue;
+                    part += (uint64_t)((int64_t)ext[i] * disc[i]);
                 }
+                nr += rows;
             }
             agg.fetch_add(part, std::memory_order_relaxed);
+            scanned.fetch_add(nr, std::memory_order_relaxed);
         });
     for (auto& x : th) x.join();
     *elapsed_ms = timer.elapsed();
-    *chunks_scanned = keep.size();
-    return (int64_t)agg.load();
+    *rows_scanned = scanned.load();
+    return bad ? INT64_MIN : (int64_t)agg.load();
+}
+
+// Group of the int32 star-join schema: (c_nation, s_nation, year), the
+// integer form of Q3NATION_GROUP (usecases/ssb/queries/03.cuh:29-59) with the
+// same hash shape.
+struct HIGroup {
+    int32_t c_nation, s_nation, year;
+    uint64_t hash() const { return (((uint64_t)(uint32_t)c_nation << 32) | (uint32_t)s_nation) ^ (uint64_t)year; }
+    bool operator==(const HIGroup& o) const {
+        return c_nation == o.c_nation && s_nation == o.s_nation && year == o.year;
+    }
+};
+struct HIGroupHash {
+    std::size_t operator()(const HIGroup& g) const { return g.hash(); }
+};
+
+// Q3 shape (query3_inmem, usecases/ssb/queries/03inmem.hpp:70-226) over
+// compressed date_key / cust_key / supp_key / revenue: filtered HostHashMap
+// builds of customer (region), supplier (region) and date (year range) split
+// over the workers, chunk pruning on the date_key min/max against the year
+// range, then the surviving blocks split over the workers; per row the
+// probes in customer -> supplier -> date order, a thread-local map per group
+// and HostHashAggregate::add of the local sums (the reference's own
+// sequence).  Groups are returned unordered: keys as
+// (c_nation * 25 + s_nation) * n_years + (year - ylo), their sums, *n_groups.
+__attribute__((visibility("default"))) int64_t ref_cpu_q3_comp(
+    uint32_t workers, uint64_t n_rows, uint64_t rows_per_chunk, uint64_t rows_per_block, const CompCol* cols /* 4 */,
+    const int32_t* date_mins, const int32_t* date_maxs, const int32_t* c_key, const int32_t* c_nation,
+    const int32_t* c_region, uint64_t n_cust, const int32_t* s_key, const int32_t* s_nation, const int32_t* s_region,
+    uint64_t n_supp, const int32_t* d_key, const int32_t* d_year, uint64_t n_date, int32_t region, int32_t ylo,
+    int32_t yhi, int64_t* group_keys, int64_t* group_sums, uint64_t cap, uint64_t* n_groups, double* elapsed_ms,
+    uint64_t* chunks_scanned, uint64_t* rows_scanned) {
+    std::vector<uint64_t> work, row0;
+    std::vector<uint32_t> brows;
+    table_blocks(n_rows, rows_per_chunk, rows_per_block, date_mins, date_maxs, ylo * 10000 + 101, yhi * 10000 + 1231,
+                 work, row0, brows, chunks_scanned);
+    std::vector<uint64_t> ck(n_cust), sk(n_supp), dk(n_date);
+    for (uint64_t i = 0; i < n_cust; ++i) ck[i] = (uint64_t)c_key[i];
+    for (uint64_t i = 0; i < n_supp; ++i) sk[i] = (uint64_t)s_key[i];
+    for (uint64_t i = 0; i < n_date; ++i) dk[i] = (uint64_t)d_key[i];
+    const uint64_t num_groups = 800;
+    std::vector<HIGroup> groups(num_groups);
+    auto aggs = std::make_unique<std::atomic<uint64_t>[]>(num_groups);
+    for (uint64_t i = 0; i < num_groups; ++i) aggs[i] = 0;
+    util::Timer timer;
+    golap::HostHashMap<uint64_t> ch(n_cust, ck.data()), sh(n_supp, sk.data()), dh(n_date, dk.data());
+    golap::HostHashAggregate<HIGroup, std::atomic<uint64_t>> ha(num_groups, groups.data(), aggs.get());
+    util::SliceSeq cs{n_cust, workers}, ss{n_supp, workers}, dss{n_date, workers}, ls{work.size(), workers};
+    std::vector<std::tuple<uint64_t, uint64_t>> csl(workers), ssl(workers), dsl(workers), lsl(workers);
+    for (auto& [s, e] : csl) cs.get(s, e);
+    for (auto& [s, e] : ssl) ss.get(s, e);
+    for (auto& [s, e] : dsl) dss.get(s, e);
+    for (auto& [s, e] : lsl) ls.get(s, e);
+    std::vector<std::thread> th;
+    for (uint32_t w = 0; w < workers; ++w)
+        th.emplace_back([&, w] {
+            auto [s, e] = csl[w];
+            for (uint64_t i = s; i < e; ++i)
+                if (c_region[i] == region) ch.insert(i, ck[i]);
+            std::tie(s, e) = ssl[w];
+            for (uint64_t i = s; i < e; ++i)
+                if (s_region[i] == region) sh.insert(i, sk[i]);
+            std::tie(s, e) = dsl[w];
+            for (uint64_t i = s; i < e; ++i)
+                if (d_year[i] >= ylo && d_year[i] <= yhi) dh.insert(i, dk[i]);
+        });
+    for (auto& x : th) x.join();
+    th.clear();
+    std::atomic<uint64_t> scanned{0};
+    std::atomic<int> bad{0};
+    for (uint32_t w = 0; w < workers; ++w)
+        th.emplace_back([&, w] {
+            golap::LZ4CPUManager m;
+            std::vector<int32_t> buf[4];
+            for (auto& b : buf) b.resize(rows_per_block);
+            std::unordered_map<HIGroup, uint64_t, HIGroupHash> local;
+            uint64_t nr = 0;
+            auto [s, e] = lsl[w];
+            for (uint64_t t = s; t < e; ++t) {
+                const uint64_t k = work[t];
+                const uint32_t rows = brows[k];
+                for (int c = 0; c < 4; ++c)
+                    if (!decode_block(cols[c], k, buf[c].data(), rows, m)) bad = 1;
+                const int32_t *od = buf[0].data(), *cu = buf[1].data(), *su = buf[2].data(), *rev = buf[3].data();
+                for (uint32_t i = 0; i < rows; ++i) {
+                    const uint64_t cm = ch.probe((uint64_t)cu[i]);
+                    if (cm == (uint64_t)-1) continue;
+                    const uint64_t sm = sh.probe((uint64_t)su[i]);
+                    if (sm == (uint64_t)-1) continue;
+                    const uint64_t dm = dh.probe((uint64_t)od[i]);
+                    if (dm == (uint64_t)-1) continue;
+                    local[HIGroup{c_nation[cm], s_nation[sm], d_year[dm]}] += (uint64_t)(uint32_t)rev[i];
+                }
+                nr += rows;
+            }
+            for (auto& [g, v] : local) ha.add(g, v, HostSumAtomic());
+            scanned.fetch_add(nr, std::memory_order_relaxed);
+        });
+    for (auto& x : th) x.join();
+    *elapsed_ms = timer.elapsed();
+    *rows_scanned = scanned.load();
+    const int32_t ny = yhi - ylo + 1;
+    uint64_t ng = 0;
+    int64_t total = 0;
+    for (uint64_t i = 0; i < num_groups; ++i) {
+        if (ha.wrote_group[i] == 0) continue;
+        const HIGroup& g = groups[i];
+        if (ng < cap) {
+            group_keys[ng] = ((int64_t)g.c_nation * 25 + g.s_nation) * ny + (g.year - ylo);
+            group_sums[ng] = (int64_t)aggs[i].load();
+        }
+        ++ng;
+        total += (int64_t)aggs[i].load();
+    }
+    *n_groups = ng;
+    return bad ? INT64_MIN : total;
 }
 
 }  // extern "C"

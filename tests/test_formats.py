@@ -31,6 +31,40 @@ def _slots(col, rows_per_chunk, n):
             yield s, r0, min(info.rows_per_block, r1 - r0)
 
 
+def _first_literal(blk):
+    """Offset of the first literal byte of an LZ4 block that opens with literals, else None."""
+    if len(blk) == 0 or (blk[0] >> 4) == 0:
+        return None
+    p = 1
+    if (blk[0] >> 4) == 15:
+        while blk[p] == 255:
+            p += 1
+        p += 1
+    return p
+
+
+def _check_alignment(codec, off, blk):
+    if codec == "lz4":
+        # an LZ4 block that opens with literals is placed so that its first
+        # literal byte is 16-byte aligned (row tiles of a literal run are then
+        # aligned byte ranges); other blocks may start anywhere
+        lit = _first_literal(blk)
+        assert lit is None or (off + lit) % 16 == 0
+    else:
+        assert off % 16 == 0
+
+
+def _check_pages(blk, ent, rows):
+    """Cascaded block: the page table in the stream equals the side index; pages are 16-byte aligned."""
+    n_pages, page_rows = (int(x) for x in blk[:8].view(np.uint32))
+    assert page_rows == 2048 and n_pages == -(-rows // 2048)
+    offs = blk[8:8 + 4 * (n_pages + 1)].view(np.uint32).astype(np.int64)
+    assert offs[-1] == len(blk)
+    for p in range(n_pages):
+        assert offs[p] % 16 == 0
+        assert int(ent[2 * p]) == offs[p] and int(ent[2 * p + 1]) == offs[p + 1] - offs[p]
+
+
 def roundtrip(vals, codec, rows_per_chunk=100_000, rows_per_block=16384, S=32, **kw):
     col = api.Column(vals, codec, rows_per_chunk=rows_per_chunk, rows_per_block=rows_per_block, lz4_segments=S, **kw)
     info = col.info
@@ -42,8 +76,9 @@ def roundtrip(vals, codec, rows_per_chunk=100_000, rows_per_block=16384, S=32, *
     assert np.array_equal(mins, em) and np.array_equal(maxs, ex)
     for k, (s, r0, rows) in enumerate(_slots(col, rows_per_chunk, len(vals))):
         off, size, used, tuples = (int(x) for x in blocks[k])
-        assert tuples == rows and off % 16 == 0 and size >= used
+        assert tuples == rows and size >= used
         blk = pl[off:off + used]
+        _check_alignment(codec, off, blk)
         want = np.ascontiguousarray(vals[r0:r0 + rows], np.int32)
         if codec == "lz4":
             got = O.lz4_decode(blk, rows * 4)
@@ -59,6 +94,8 @@ def roundtrip(vals, codec, rows_per_chunk=100_000, rows_per_block=16384, S=32, *
         elif codec == "cascaded":
             got = O.casc_decode(blk, rows)
             assert got is not None and np.array_equal(got, want)
+            pages = -(-rows_per_block // 2048)
+            _check_pages(blk, seg[2 * pages * s: 2 * pages * (s + 1)], rows)
         else:
             assert np.array_equal(blk.view(np.int32), want)
     return col
@@ -144,5 +181,7 @@ def test_block_directory_matches_reference_blockinfo_layout():
     info = col.info
     assert info.n_chunks == 4 and info.blocks_per_chunk == 16
     assert int(b[:, 3].sum()) == 1_000_000
-    assert all(int(x) % 16 == 0 for x in b[:, 0])
+    pl = col.payload()
+    for off, _, used, _ in b:
+        _check_alignment("lz4", int(off), pl[int(off):int(off) + int(used)])
     assert np.all(b[1:, 0] >= b[:-1, 0] + b[:-1, 2])

@@ -141,8 +141,12 @@ def test_corrupt_blocks_are_reported(cuda, codec, S):
         assert info & 16
         _corrupt_payload(col, first + lit_pos + (info >> 5), 0xFF)
         _corrupt_payload(col, first + lit_pos + (info >> 5) + 1, 0xFF)
+    elif codec == "cascaded":
+        # the first page's run count (pages are located through the side index)
+        page = int(col.seg_index()[0])
+        _corrupt_payload(col, first + page + 5, 0xFF)
     else:
-        _corrupt_payload(col, first + (1 if codec == "cascaded" else 0), 0xFF)  # n_runs / first token
+        _corrupt_payload(col, first, 0xFF)  # first token
     col.to_device()
     out = cuda.zeros(300_000, dtype=cuda.int32, device="cuda")
     api.ChunkDecompressor(col).chunks(0, col.info.n_chunks, out)

@@ -163,3 +163,92 @@ def test_groupby_vs_oracle_and_overflow(cuda):
     with pytest.raises(GxError) as e:
         api.scan_check()
     assert e.value.status == L.GX_ERR_CAPACITY
+
+
+@pytest.mark.parametrize("layout", ["linear", "bucket", "dense"])
+def test_hashtable_keys_collects_filtered_build_keys(cuda, layout):
+    # collect_hashmap_keys (core/dev_structs.cuh:136-150): the keys of the rows
+    # the filtered build inserted, in any order, count on the device
+    rng = np.random.default_rng(12)
+    keys = rng.permutation(np.arange(100, 100 + 50_000, dtype=np.int32))
+    flag = rng.integers(0, 3, len(keys), dtype=np.int32)
+    kd, fd = cuda.from_numpy(keys).cuda(), cuda.from_numpy(flag).cuda()
+    hm = api.HashMap(len(keys), layout).build(kd, None, preds=[(fd, 1, 1)])
+    out = cuda.empty(len(keys), dtype=cuda.int32, device="cuda")
+    cnt = cuda.zeros(1, dtype=cuda.int64, device="cuda")
+    hm.keys(out, cnt)
+    n = int(cnt.item())
+    assert sorted(out[:n].cpu().numpy().tolist()) == sorted(keys[flag == 1].tolist())
+    # a too-small output: the count is still the full count, nothing written past cap
+    small = cuda.full((10,), -7, dtype=cuda.int32, device="cuda")
+    hm.keys(small, cnt)
+    assert int(cnt.item()) == n and set(small.cpu().numpy().tolist()) <= set(keys[flag == 1].tolist())
+
+
+def test_join_pruning_points_vs_oracle(cuda):
+    # check_mmmeta_multiple_pts (core/metadata.cuh:550-560) behind --join_prune
+    # (usecases/ssb/queries/01.hpp:246-270): a chunk stays when one of the
+    # build side's keys lies in its min/max
+    rng = np.random.default_rng(5)
+    v = np.sort(rng.integers(0, 1_000_000, 3_000_000, dtype=np.int32))
+    col = api.Column(v, "cascaded", rows_per_chunk=20_000).to_device()
+    mins, maxs = col.minmax()
+    n = col.info.n_chunks
+    for keys in (np.array([5, 500_000, 999_999], np.int32), rng.integers(-5, 1_100_000, 5000, dtype=np.int32),
+                 np.zeros(0, np.int32), rng.integers(0, 1_000_000, 3000, dtype=np.int32)):
+        kd = cuda.from_numpy(np.ascontiguousarray(keys)).cuda() if len(keys) else cuda.zeros(1, dtype=cuda.int32,
+                                                                                           device="cuda")
+        cnt = cuda.tensor([len(keys)], dtype=cuda.int64, device="cuda")
+        keep = cuda.zeros(n, dtype=cuda.uint16, device="cuda")
+        api.MetaChecker(n).add_points(col, kd, cnt, keep)
+        assert keep.cpu().numpy().tolist() == O.minmax_points_keep(mins, maxs, keys).tolist()
+
+
+def test_minmax_reduce_and_clear(cuda):
+    # MinMaxMeta::init_chunk (core/metadata.cuh:157-160) on device data
+    rng = np.random.default_rng(8)
+    for n in (1, 3, 1000, 1 << 20, 3_000_001):
+        v = rng.integers(-2**31, 2**31 - 1, n, dtype=np.int64).astype(np.int32)
+        vd = cuda.from_numpy(v).cuda()
+        for off in (0, 1):  # aligned and unaligned starts
+            if off >= n:
+                continue
+            r = cuda.zeros(2, dtype=cuda.int32, device="cuda")
+            L.check(L.lib().gx_minmax_reduce(C.c_void_p(vd.data_ptr() + 4 * off), n - off, C.c_void_p(r.data_ptr()),
+                                             None))
+            assert r.cpu().numpy().tolist() == [int(v[off:].min()), int(v[off:].max())]
+    hm = api.HashMap(1000).build(cuda.arange(1000, dtype=cuda.int32, device="cuda"))
+    assert hm.count() == 1000
+    L.check(L.lib().gx_hashtable_clear(hm.handle, None))
+    assert hm.count() == 0
+    hits = cuda.zeros(1, dtype=cuda.int64, device="cuda")
+    hm.probe(cuda.arange(1000, dtype=cuda.int32, device="cuda"), None, hits)
+    assert int(hits.item()) == 0
+
+
+@pytest.mark.parametrize("layout", ["linear", "bucket"])
+@pytest.mark.parametrize("carry,key_codec", [(True, "cascaded"), (False, "lz4"), (True, "lz4")])
+def test_build_from_compressed_dimension(cuda, layout, carry, key_codec):
+    # GX_AGG_BUILD: pipeline_customer_q3 (usecases/ssb/queries/03.cuh:94-116)
+    # fused with the decompression of the customer chunks -- filter on region,
+    # insert key -> nation (CARRY) or key -> row number
+    from golap_public_b200 import datagen, queries
+
+    n = 1_200_000
+    cust = datagen.dim_geo(n, datagen.SEED, 21)
+    keys = cust["key"] if key_codec == "cascaded" else np.random.default_rng(3).permutation(cust["key"])
+    cc = queries.encode_fact({"key": keys, "nation": cust["nation"], "region": cust["region"]},
+                             {"key": key_codec, "nation": "cascaded", "region": "cascaded"}, rows_per_chunk=500_000)
+    ht = api.HashMap(n, layout)
+    queries.build_from_compressed(ht, cc.cols["key"], cc.cols["nation"] if carry else None,
+                                  [(cc.cols["region"], 2, 2)])
+    sel = cust["region"] == 2
+    assert ht.count() == int(sel.sum())
+    probe = cuda.from_numpy(keys).cuda()
+    out = cuda.empty_like(probe)
+    ht.probe(probe, out)
+    exp = np.where(sel, cust["nation"] if carry else np.arange(n, dtype=np.int32), np.iinfo(np.int32).min)
+    assert np.array_equal(out.cpu().numpy(), exp)
+    # a dense table cannot be filled this way (it sizes itself from the key range)
+    with pytest.raises(GxError):
+        queries.build_from_compressed(api.HashMap(n, "dense"), cc.cols["key"], None)

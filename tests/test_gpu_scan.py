@@ -94,6 +94,28 @@ def test_q1_config1_sorted_pruned(cuda, S):
             assert q.keep.cpu().numpy().tolist() == O.minmax_keep(mins, maxs, 19940101, 19940131).tolist()
 
 
+def test_q1_join_pruning(cuda):
+    # join pruning (usecases/ssb/queries/01.hpp:246-270): the filtered date
+    # table's keys prune the chunks whose date_key min/max holds none of them;
+    # two months three years apart keep only their own chunks, where min/max
+    # pruning on the key range would keep everything in between
+    f = datagen.fact_q1(30_000_000, True)
+    dd = datagen.date_dim()
+    fact = queries.encode_fact(f, {"date_key": "cascaded"})
+    ok = np.isin(dd["d_yearmonthnum"], [199302, 199607])
+    want = _oracle_q1(f, dd, ok, 4, 6, 26, 35)
+    q = queries.Q1Query(fact, dd, ok, int(dd["d_key"][ok].min()), int(dd["d_key"][ok].max()), 4, 6, 26, 35,
+                        prune=True, join_prune=True)
+    assert q.run() == want
+    mins, maxs = fact.cols["date_key"].minmax()
+    jk = q.join_keep.cpu().numpy()
+    assert jk.tolist() == O.minmax_points_keep(mins, maxs, dd["d_key"][ok]).tolist()
+    range_keep = O.minmax_keep(mins, maxs, int(dd["d_key"][ok].min()), int(dd["d_key"][ok].max()))
+    assert jk.sum() < range_keep.sum() // 4
+    # keep_out = join flags AND the plan's own min/max pruning
+    assert q.keep.cpu().numpy().tolist() == (jk & range_keep).tolist()
+
+
 def test_q1_keep_chunks_in_and_out(cuda):
     # per-chunk keep flags handed to the scan (MetaChecker output) combine with
     # the plan's own min/max pruning; keep_out receives keep_in AND min/max
@@ -146,6 +168,30 @@ def test_q3_star_join_groupby(cuda):
         assert 100 <= len(got) <= 150
 
 
+def test_q3_customer_from_compressed_chunks(cuda):
+    # the customer join table filled from compressed customer columns in one
+    # fused launch (GX_AGG_BUILD), then the star join: same groups as the oracle
+    f = datagen.fact_q3(6_000_000, True)
+    cust = datagen.dim_geo(3_000_000, datagen.SEED, 21)
+    supp = datagen.dim_geo(200_000, datagen.SEED, 22)
+    dd = datagen.date_dim()
+    fact = queries.encode_fact(f, {"date_key": "cascaded"})
+    cc = queries.encode_fact(cust, {"key": "cascaded", "nation": "cascaded", "region": "cascaded"})
+    for region in (0, 3):
+        q = queries.Q3Query(fact, cc, supp, dd, region, 1993, 1996)
+        got = q.run()
+        sums, counts = O.q3(f["cust_key"], f["supp_key"], f["date_key"], f["revenue"],
+                            cust["key"], cust["nation"], cust["region"] == region,
+                            supp["key"], supp["nation"], supp["region"] == region,
+                            dd["d_key"], dd["d_year"], (dd["d_year"] >= 1993) & (dd["d_year"] <= 1996),
+                            0, 25, 0, 25, 1993, 4)
+        want = {(c, s, 1993 + y): int(sums[c, s, y]) for c, s, y in zip(*np.nonzero(counts))}
+        assert got == want
+        q.build_customer()  # rebuilt in place: the same table again
+        assert q.hc.count() == int((cust["region"] == region).sum())
+        assert q.run() == want
+
+
 def test_scan_plan_validation(cuda):
     f = datagen.fact_q1(100_000, False)
     fact = queries.encode_fact(f, {})
@@ -191,7 +237,9 @@ def test_scan_reports_corrupt_tile_and_recovers(cuda):
             n = C.c_uint64()
             L.check(L.lib().gx_column_payload(c.handle, C.byref(p), C.byref(n)))
             off = int(c.blocks()[3][0])
-            p[off + 4] = 0xFF  # n_runs of block 3 -> invalid header
+            pages = -(-c.info.rows_per_block // 2048)
+            page = int(c.seg_index()[2 * pages * 3])  # first page of block 3 (side index entry)
+            p[off + page + 4] = 0xFF  # its n_runs -> invalid page header
         bad_cols[k] = c.to_device()
     bad = queries.FactTable(bad_cols, len(f["date_key"]))
     ok = dd["d_year"] == 1995
