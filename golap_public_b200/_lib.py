@@ -17,7 +17,7 @@ u8p = C.POINTER(C.c_uint8)
 GX_OK, GX_ERR_CUDA, GX_ERR_CORRUPT, GX_ERR_CAPACITY, GX_ERR_TIMEOUT, GX_ERR_NOMEM, GX_ERR_INVALID = range(7)
 GX_CODEC_NONE, GX_CODEC_LZ4, GX_CODEC_CASCADED = 0, 1, 2
 GX_STEP_FILTER, GX_STEP_PROBE, GX_STEP_CARRY, GX_STEP_VALUE, GX_STEP_GROUP = 1, 2, 4, 8, 16
-GX_AGG_SUM, GX_AGG_SUM_PRODUCT, GX_AGG_COUNT, GX_AGG_BUILD = 0, 1, 2, 3
+GX_AGG_SUM, GX_AGG_SUM_PRODUCT, GX_AGG_COUNT, GX_AGG_BUILD, GX_AGG_SUM_DIFF = 0, 1, 2, 3, 4
 GX_HT_LINEAR, GX_HT_BUCKET, GX_HT_DENSE = 0, 1, 2
 GX_BATCH_AUTO, GX_BATCH_QUEUE, GX_BATCH_SHARED = 0, 1, 2
 GX_MAX_STEPS = 8

@@ -55,26 +55,33 @@ __device__ __forceinline__ void raise_error(int code) { atomicCAS(&g_gx_error, 0
 // pool that keeps up to 256 MiB cached across synchronisations: the default
 // pool returns its memory at every synchronisation, so every call after one
 // would map fresh memory (hundreds of microseconds).
+// Per-device caches (memory pools, kernel attributes, occupancies, the
+// static scratch address) hold kMaxDevices entries; every one of them
+// refuses a device index outside that range in the same way.
+constexpr int kMaxDevices = 64;
+static inline bool device_index_ok(int dev) { return dev >= 0 && dev < kMaxDevices; }
+
 static cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
     static std::mutex mu;
-    static cudaMemPool_t pools[64] = {};
+    static cudaMemPool_t pools[kMaxDevices] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
+    if (!device_index_ok(dev)) return cudaErrorInvalidDevice;
     cudaMemPool_t pool;
     {
         std::lock_guard<std::mutex> lk(mu);
-        if (!pools[dev & 63]) {
+        if (!pools[dev]) {
             cudaMemPoolProps props{};
             props.allocType = cudaMemAllocationTypePinned;
             props.location.type = cudaMemLocationTypeDevice;
             props.location.id = dev;
-            e = cudaMemPoolCreate(&pools[dev & 63], &props);
+            e = cudaMemPoolCreate(&pools[dev], &props);
             if (e != cudaSuccess) return e;
             uint64_t keep = 256ull << 20;
-            cudaMemPoolSetAttribute(pools[dev & 63], cudaMemPoolAttrReleaseThreshold, &keep);
+            cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
         }
-        pool = pools[dev & 63];
+        pool = pools[dev];
     }
     return cudaMallocFromPoolAsync(p, bytes, pool, s);
 }
@@ -122,6 +129,7 @@ struct QueryDesc {
     uint32_t agg;
     uint32_t grouped;       // sums per group key
     uint32_t need_aux;      // aux array (carry or group key) in shared memory
+    uint32_t carry_digits;  // a carried value and group-key digits (not in the queue form's one aux array)
     uint64_t row_lo, row_hi;
     int64_t* result;
     int64_t* g_keys;
@@ -539,6 +547,7 @@ __global__ void __launch_bounds__(NT, (MAXT < 16384 ? 4 : 1)) scan_kernel(const 
                         int64_t val = 0;
                         if (keep) {
                             if (Q.agg == GX_AGG_SUM_PRODUCT) val = (int64_t)v * (int64_t)(int32_t)aux[r];
+                            else if (Q.agg == GX_AGG_SUM_DIFF) val = (int64_t)v - (int64_t)(int32_t)aux[r];
                             else if (Q.agg == GX_AGG_COUNT) val = 1;
                             else val = v;
                         }
@@ -1042,10 +1051,14 @@ __global__ void groupby_compact_kernel(const int64_t* gk, const int64_t* gs, uin
 // ------------------------------------------------------------ host helpers
 
 int sm_count() {
-    static int cached[64] = {0};
+    static int cached[kMaxDevices] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) dev = 0;
+    if (!device_index_ok(dev)) {  // callers reject such devices; answer without caching
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n > 0 ? n : 1;
+    }
     if (!cached[dev]) {
         int n = 0;
         cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
@@ -1291,14 +1304,15 @@ gx_status gx_decompress_chunks(const gx_column* col, uint64_t first_chunk, uint6
     if (!col->residency) return set_error(GX_ERR_INVALID, "column is not on the device");
     if (first_chunk + n_chunks > col->n_chunks) return set_error(GX_ERR_INVALID, "chunk range out of bounds");
     if (n_chunks == 0) return GX_OK;
-    static bool attr_set[64] = {false};
+    static bool attr_set[kMaxDevices] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (!attr_set[dev & 63]) {
+    if (!device_index_ok(dev)) return set_error(GX_ERR_INVALID, "device %d out of range", dev);
+    if (!attr_set[dev]) {
         gx_status st = allow_smem(decompress_kernel<128, kTileRows>, dec_smem_bytes<kTileRows>());
         if (!st) st = allow_smem(decompress_kernel<256, kMaxRowsPerBlock>, dec_smem_bytes<kMaxRowsPerBlock>());
         if (st) return st;
-        attr_set[dev & 63] = true;
+        attr_set[dev] = true;
     }
     const uint32_t slot0 = (uint32_t)(first_chunk * col->blocks_per_chunk);
     const uint32_t nslots = (uint32_t)(n_chunks * col->blocks_per_chunk);
@@ -1725,7 +1739,7 @@ static gx_status build_query(const gx_scan_plan* plan, QueryDesc* Q, uint32_t* t
         if (s.flags & GX_STEP_VALUE) any_value = true;
     }
     if (!any_value) return set_error(GX_ERR_INVALID, "scan plan has no VALUE step");
-    if (plan->agg > GX_AGG_BUILD) return set_error(GX_ERR_INVALID, "unknown aggregate");
+    if (plan->agg > GX_AGG_SUM_DIFF) return set_error(GX_ERR_INVALID, "unknown aggregate");
     if (plan->agg == GX_AGG_BUILD) {
         if (!plan->build_ht) return set_error(GX_ERR_INVALID, "a BUILD plan needs build_ht");
         if (plan->build_ht->layout == GX_HT_DENSE)
@@ -1733,8 +1747,9 @@ static gx_status build_query(const gx_scan_plan* plan, QueryDesc* Q, uint32_t* t
                                              "themselves from the key range in gx_hashtable_build)");
         if (plan->groupby || any_digit) return set_error(GX_ERR_INVALID, "a BUILD plan has no group key");
     }
-    if (plan->agg == GX_AGG_SUM_PRODUCT && !any_carry) return set_error(GX_ERR_INVALID, "SUM_PRODUCT needs a CARRY step");
-    if (any_carry && any_digit) return set_error(GX_ERR_INVALID, "CARRY and group-key digits cannot be combined");
+    if ((plan->agg == GX_AGG_SUM_PRODUCT || plan->agg == GX_AGG_SUM_DIFF) && !any_carry)
+        return set_error(GX_ERR_INVALID, "SUM_PRODUCT / SUM_DIFF need a CARRY step");
+    Q->carry_digits = any_carry && any_digit ? 1 : 0;  // only the shared and pipelined forms keep both
     if (plan->groupby && !any_digit) return set_error(GX_ERR_INVALID, "grouped scan needs PROBE/GROUP steps with digits");
     if (!plan->groupby && !plan->result_dev && plan->agg != GX_AGG_BUILD)
         return set_error(GX_ERR_INVALID, "scan plan needs result_dev or groupby");
@@ -1765,10 +1780,11 @@ static gx_status build_query(const gx_scan_plan* plan, QueryDesc* Q, uint32_t* t
 }
 
 static gx_status ensure_kernel_attrs() {
-    static bool attr_set[64] = {false};
+    static bool attr_set[kMaxDevices] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (attr_set[dev & 63]) return GX_OK;
+    if (!device_index_ok(dev)) return set_error(GX_ERR_INVALID, "device %d out of range", dev);
+    if (attr_set[dev]) return GX_OK;
     gx_status st = allow_smem(scan_kernel<128, kTileRows, false>, scan_smem_bytes<kTileRows>(true, true));
     if (!st) st = allow_smem(scan_kernel<128, kTileRows, true>, scan_smem_bytes<kTileRows>(true, true));
     if (!st) st = allow_smem(scan_kernel<256, kMaxRowsPerBlock, false>, scan_smem_bytes<kMaxRowsPerBlock>(true, true));
@@ -1781,7 +1797,7 @@ static gx_status ensure_kernel_attrs() {
     if (!st) st = allow_smem(shared_scan_kernel<kShSingleNT, 4, true>, sh_max);
     if (!st) st = allow_smem(pipe_scan_kernel, kPipeMaxDynSmem);
     if (st) return st;
-    attr_set[dev & 63] = true;
+    attr_set[dev] = true;
     return GX_OK;
 }
 
@@ -1792,10 +1808,10 @@ static void scan_geometry(uint32_t tile_rows, bool aux, bool groups, uint64_t ti
     if (tile_rows <= kTileRows) {
         *smem = scan_smem_bytes<kTileRows>(aux, groups);
         // resident CTAs per SM, per device and shared-memory layout (queried once)
-        static int occ[64][2][2] = {};
+        static int occ[kMaxDevices][2][2] = {};  // ensure_kernel_attrs has checked the device
         int dev = 0;
         cudaGetDevice(&dev);
-        int& per_sm = occ[dev & 63][aux][groups];
+        int& per_sm = occ[dev][aux][groups];
         if (per_sm == 0) {
             int v = 1;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, scan_kernel<128, kTileRows, BATCH>, 128, *smem);
@@ -2029,10 +2045,10 @@ static gx_status scan_launch_shared(const gx_scan_plan* plan, const QueryDesc& q
     // items themselves (see sh_single_live), so the launch is one kernel
     P.gt_slots = P.q1.grouped ? kShGroupSlots : 0u;
     const size_t smem = shared_smem_bytes(P.n_cols, 1, 0, 0, P.gt_slots);
-    static int occ[64][kShMaxCols + 1][2] = {};
+    static int occ[kMaxDevices][kShMaxCols + 1][2] = {};  // ensure_kernel_attrs has checked the device
     int dev = 0;
     cudaGetDevice(&dev);
-    int& per_sm = occ[dev & 63][P.n_cols][P.gt_slots ? 1 : 0];
+    int& per_sm = occ[dev][P.n_cols][P.gt_slots ? 1 : 0];
     if (per_sm == 0) {
         int v = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, shared_scan_kernel<kShSingleNT, 4, true>, kShSingleNT, smem);
@@ -2123,6 +2139,9 @@ static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned 
                                          "at most 2048 rows) and its VALUE step last");
     st = scan_launch_shared(plan, P.q, c0, s, rows_dev, &done);
     if (st || done) return st;
+    if (P.q.carry_digits)
+        return set_error(GX_ERR_INVALID, "a plan with a carried value and group-key digits needs the shared or "
+                                         "pipelined form (segmented LZ4 columns, its only VALUE step last)");
     ItemsParams ip{};
     for (uint32_t i = 0; i < P.q.n_prune; ++i) ip.preds[i] = P.q.prune[i];
     ip.n_preds = P.q.n_prune;
@@ -2169,11 +2188,11 @@ static __device__ __align__(256) uint32_t g_scan_static_scratch[4 + kStaticMaxCh
 // once per device (with that device current) and cached.
 static gx_status static_scratch(uint32_t** out) {
     static std::mutex mu;
-    static uint32_t* addr[64] = {nullptr};
+    static uint32_t* addr[kMaxDevices] = {nullptr};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "gx_scan_static: cudaGetDevice: %s", cudaGetErrorString(e));
-    if (dev < 0 || dev >= 64) return set_error(GX_ERR_INVALID, "gx_scan_static: device %d out of range", dev);
+    if (!device_index_ok(dev)) return set_error(GX_ERR_INVALID, "gx_scan_static: device %d out of range", dev);
     std::lock_guard<std::mutex> lk(mu);
     if (!addr[dev]) {
         void* p = nullptr;
@@ -2195,6 +2214,8 @@ static gx_status scan_launch_static(const gx_scan_plan* plan, cudaStream_t s) {
     gx_status st = build_query(plan, &P.q, &tile_rows, &c0);
     if (st) return st;
     if (plan->agg == GX_AGG_BUILD) return set_error(GX_ERR_INVALID, "gx_scan_static: BUILD plans run through gx_scan");
+    if (P.q.carry_digits)
+        return set_error(GX_ERR_INVALID, "gx_scan_static: a carried value with group-key digits runs through gx_scan");
     const uint32_t n_chunks = c0->n_chunks;
     if (n_chunks > kStaticMaxChunks)
         return set_error(GX_ERR_INVALID, "gx_scan_static: %u chunks exceed the static work list of %u chunks", n_chunks,
@@ -2495,6 +2516,12 @@ gx_status gx_batch_assign(gx_batch* b, const gx_query* queries, uint32_t n_queri
         else if (b->mode_pref == GX_BATCH_SHARED)
             return set_error(GX_ERR_INVALID, "batch cannot run in the shared form: %s", why.c_str());
     }
+    if (b->mode == GX_BATCH_QUEUE)
+        for (uint32_t i = 0; i < n_queries; ++i)
+            if (qs[i].carry_digits)
+                return set_error(GX_ERR_INVALID, "query %u carries a value and group-key digits: the queue form "
+                                                 "keeps one of them per row",
+                                 i);
     return GX_OK;
 }
 

@@ -604,14 +604,14 @@ __global__ void __launch_bounds__(kPipeNT, 1) pipe_scan_kernel(const __grid_cons
                         keep = kk ? keep : (keep & ~(1u << i));
                     }
                 } else if (simple && last && !grouped && agg != GX_AGG_COUNT && agg != GX_AGG_BUILD) {
-                    const bool prod = agg == GX_AGG_SUM_PRODUCT;
+                    const bool prod = agg == GX_AGG_SUM_PRODUCT, diff = agg == GX_AGG_SUM_DIFF;
 #pragma unroll
                     for (uint32_t i = 0; i < RPT; ++i) {
                         const uint32_t r = (i * NW + warp) * 32 + lane;
                         const int32_t v = (int32_t)col[sh_col_index(r, sh, pd)];
                         const bool kk = ((keep >> i) & 1u) && (!filt || (v >= lo && v <= hi));
                         const int32_t c2 = carry_step ? v : carry[i];
-                        const int64_t val = prod ? (int64_t)v * c2 : (int64_t)v;
+                        const int64_t val = prod ? (int64_t)v * c2 : diff ? (int64_t)v - c2 : (int64_t)v;
                         local += kk ? val : 0;
                     }
                 } else if ((flags & GX_STEP_PROBE) && htlay != GX_HT_BUCKET && !last) {
@@ -722,6 +722,7 @@ __global__ void __launch_bounds__(kPipeNT, 1) pipe_scan_kernel(const __grid_cons
                         } else if (last) {
                             const int64_t val = !kk                          ? 0
                                                 : agg == GX_AGG_SUM_PRODUCT ? (int64_t)v * carry[i]
+                                                : agg == GX_AGG_SUM_DIFF    ? (int64_t)v - carry[i]
                                                 : agg == GX_AGG_COUNT        ? 1
                                                                              : (int64_t)v;
                             if (!grouped) local += val;

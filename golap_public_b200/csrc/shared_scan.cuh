@@ -667,14 +667,14 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                         }
                     } else if (simple && last && !grouped && agg != GX_AGG_COUNT) {
                         // the VALUE step of a scalar SUM / SUM_PRODUCT
-                        const bool prod = agg == GX_AGG_SUM_PRODUCT;
+                        const bool prod = agg == GX_AGG_SUM_PRODUCT, diff = agg == GX_AGG_SUM_DIFF;
 #pragma unroll
                         for (int i = 0; i < RPT; ++i) {
                             const uint32_t r = (i * NW + warp) * 32 + lane;
                             const int32_t v = (int32_t)col[sh_col_index(r, sh, pd)];
                             const bool k = ((keep >> i) & 1u) && (!filt || (v >= lo && v <= hi));
                             const int32_t c2 = carry_step ? v : carry[i];
-                            const int64_t val = prod ? (int64_t)v * c2 : (int64_t)v;
+                            const int64_t val = prod ? (int64_t)v * c2 : diff ? (int64_t)v - c2 : (int64_t)v;
                             local += k ? val : 0;
                         }
                     } else if (RPT <= 8 && (flags & GX_STEP_PROBE) && htlay != GX_HT_BUCKET && !last) {
@@ -795,6 +795,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                             if (last) {  // the VALUE step: aggregate the row
                                 const int64_t val = !k ? 0
                                                   : agg == GX_AGG_SUM_PRODUCT ? (int64_t)v * carry[i]
+                                                  : agg == GX_AGG_SUM_DIFF    ? (int64_t)v - carry[i]
                                                   : agg == GX_AGG_COUNT        ? 1
                                                                                : (int64_t)v;
                                 if (!grouped) local += val;

@@ -12,7 +12,8 @@ independent stream per column, default seed 0xBEE5BEE5):
                    date_key, revenue U[100,1000000]
   customer / supplier: key 1..N, nation U[0,25), region = region of nation
                    (5 nations per region, the SSB nation->region map)
-  part:            key 1..N, category U[0,25), brand U[0,1000)
+  part:            key 1..N, category U[0,25), mfgr = category // 5,
+                   brand = 40 * category + U[0,40)
   date:            2,556 rows: key, year, yearmonthnum
 Sorted facts are produced directly in date order (multinomial day counts),
 which is the same distribution as sorting the unsorted table by date_key.
@@ -60,14 +61,19 @@ def fact_q1(n: int, sorted_by_date: bool, seed: int = SEED) -> dict:
 
 
 def fact_q3(n: int, sorted_by_date: bool = True, seed: int = SEED, n_customer: int = 3_000_000,
-            n_supplier: int = 200_000, n_part: int = 1_400_000) -> dict:
-    return {
+            n_supplier: int = 200_000, n_part: int = 1_400_000, supplycost: bool = False) -> dict:
+    """Star-schema fact table; with supplycost=True also supplycost U[100, 600,000]
+    (the profit column of the Q4 shape)."""
+    t = {
         "date_key": _date_column(n, sorted_by_date, _rng(seed, 11)),
         "cust_key": _rng(seed, 12).integers(1, n_customer + 1, n, dtype=np.int32),
         "supp_key": _rng(seed, 13).integers(1, n_supplier + 1, n, dtype=np.int32),
         "part_key": _rng(seed, 14).integers(1, n_part + 1, n, dtype=np.int32),
         "revenue": _rng(seed, 15).integers(100, 1_000_001, n, dtype=np.int32),
     }
+    if supplycost:
+        t["supplycost"] = _rng(seed, 16).integers(100, 600_001, n, dtype=np.int32)
+    return t
 
 
 def dim_geo(n: int, seed: int, stream: int) -> dict:
@@ -76,9 +82,12 @@ def dim_geo(n: int, seed: int, stream: int) -> dict:
 
 
 def dim_part(n: int, seed: int = SEED) -> dict:
+    """key 1..n, category U[0,25), mfgr = category // 5 (the SSB MFGR#m of
+    category MFGR#mn), brand = 40 * category + U[0,40) (the SSB MFGR#mnbb)."""
     r = _rng(seed, 23)
-    return {"key": np.arange(1, n + 1, dtype=np.int32), "category": r.integers(0, 25, n, dtype=np.int32),
-            "brand": r.integers(0, 1000, n, dtype=np.int32)}
+    cat = r.integers(0, 25, n, dtype=np.int32)
+    return {"key": np.arange(1, n + 1, dtype=np.int32), "category": cat, "mfgr": (cat // 5).astype(np.int32),
+            "brand": (40 * cat + r.integers(0, 40, n, dtype=np.int32)).astype(np.int32)}
 
 
 def zipf_keys(n: int, n_keys: int, s: float = 1.1, seed: int = SEED, stream: int = 31) -> np.ndarray:

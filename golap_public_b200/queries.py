@@ -12,6 +12,16 @@ Q3 shape -- usecases/ssb/queries/03.hpp:80-592 (query3) with pipeline_q3
     SUM(revenue) GROUP BY (customer.nation, supplier.nation, year)
     WHERE customer.region = r AND supplier.region = r AND year in [ylo,yhi]
   probes in customer -> supplier -> date order, like the reference.
+
+Q2 shape -- usecases/ssb/queries/02.cuh:103 (pipeline_q2, part -> supplier
+-> date) and 02inmem.hpp:100-180:
+    SUM(revenue) GROUP BY (part.brand, year)
+    WHERE part.category = c AND supplier.region = r
+
+Q4 shape -- usecases/ssb/queries/04.cuh:100 (pipeline_q4) and
+04inmem.hpp:120-160 (customer -> supplier -> date -> part):
+    SUM(revenue - supplycost) GROUP BY (customer.nation, year)
+    WHERE customer.region = r AND supplier.region = r AND part.mfgr in [m0,m1]
 """
 from __future__ import annotations
 
@@ -198,3 +208,85 @@ class Q3Query:
         scan_check(stream)
         raw = self.agg.read(stream=stream)
         return {self.decode_key(k): v for k, v in raw.items()}
+
+
+class _StarQuery:
+    """Common part of the star-join shapes: join tables, group table, plan."""
+
+    def launch(self, stream=None):
+        self.agg.reset(stream)
+        self.plan.launch(stream)
+
+    def run(self, stream=None) -> dict:
+        self.launch(stream)
+        from .api import scan_check
+
+        scan_check(stream)
+        return {self.decode_key(k): v for k, v in self.agg.read(stream=stream).items()}
+
+    def _tables(self, dims, ht_layout):
+        """dims: name -> (keys, payload or None, filter column or None, lo, hi); builds one table each."""
+        self.ht = {}
+        self._keep_alive = []
+        for name, (keys, pay, fcol, lo, hi) in dims.items():
+            ok = np.ones(len(keys), bool) if fcol is None else (fcol >= lo) & (fcol <= hi)
+            ht = HashMap(max(1, int(ok.sum())), ht_layout)
+            kd = _dev(keys)
+            pd = _dev(pay) if pay is not None else None
+            preds = []
+            if fcol is not None:
+                fd = _dev(fcol)
+                preds = [(fd, lo, hi)]
+                self._keep_alive.append(fd)
+            ht.build(kd, pd, preds=preds)
+            self._keep_alive += [kd, pd]
+            self.ht[name] = ht
+
+
+class Q2Query(_StarQuery):
+    """Q2-shaped star join over a FactTable with part_key, supp_key, date_key, revenue."""
+
+    def __init__(self, fact: FactTable, part: dict, supplier: dict, date: dict, category: int, region: int,
+                 year0: int = 1992, n_years: int = 7, n_brands: int = 1000, ht_layout: str = "linear"):
+        self.year0, self.n_years = year0, n_years
+        self._tables({"part": (part["key"], part["brand"], part["category"], category, category),
+                      "supp": (supplier["key"], None, supplier["region"], region, region),
+                      "date": (date["d_key"], date["d_year"], None, 0, 0)}, ht_layout)
+        self.agg = HashAggregate(n_brands * n_years)
+        c = fact.cols
+        self.plan = ScanPlan(agg=L.GX_AGG_SUM, groupby=self.agg)
+        self.plan.probe(c["part_key"], self.ht["part"], 0, n_brands)
+        self.plan.probe(c["supp_key"], self.ht["supp"])
+        self.plan.probe(c["date_key"], self.ht["date"], year0, n_years)
+        self.plan.value(c["revenue"])
+        self.plan.to_c()
+
+    def decode_key(self, k: int):
+        """(brand, year)"""
+        return k // self.n_years, self.year0 + k % self.n_years
+
+
+class Q4Query(_StarQuery):
+    """Q4-shaped star join over a FactTable with cust_key, supp_key, part_key, date_key, revenue, supplycost."""
+
+    def __init__(self, fact: FactTable, customer: dict, supplier: dict, part: dict, date: dict, region: int,
+                 mfgr_lo: int, mfgr_hi: int, year0: int = 1992, n_years: int = 7, ht_layout: str = "linear"):
+        self.year0, self.n_years = year0, n_years
+        self._tables({"cust": (customer["key"], customer["nation"], customer["region"], region, region),
+                      "supp": (supplier["key"], None, supplier["region"], region, region),
+                      "date": (date["d_key"], date["d_year"], None, 0, 0),
+                      "part": (part["key"], None, part["mfgr"], mfgr_lo, mfgr_hi)}, ht_layout)
+        self.agg = HashAggregate(25 * n_years)
+        c = fact.cols
+        self.plan = ScanPlan(agg=L.GX_AGG_SUM_DIFF, groupby=self.agg)
+        self.plan.probe(c["cust_key"], self.ht["cust"], 0, 25)
+        self.plan.probe(c["supp_key"], self.ht["supp"])
+        self.plan.probe(c["date_key"], self.ht["date"], year0, n_years)
+        self.plan.probe(c["part_key"], self.ht["part"])
+        self.plan.carry(c["supplycost"])
+        self.plan.value(c["revenue"])
+        self.plan.to_c()
+
+    def decode_key(self, k: int):
+        """(c_nation, year)"""
+        return k // self.n_years, self.year0 + k % self.n_years

@@ -261,8 +261,9 @@ gx_status gx_groupby_read(gx_groupby* gb, int64_t* keys_host, int64_t* sums_host
  *   FILTER  : keep rows with lo <= v <= hi
  *   PROBE   : keep rows whose value is a key of ht; if digit_card > 0 the
  *             payload p extends the group key: g = g*digit_card + (p-digit_base)
- *   CARRY   : remember v for the product aggregate
- *   VALUE   : aggregate v (times the carried value when agg == SUM_PRODUCT)
+ *   CARRY   : remember v (for SUM_PRODUCT / SUM_DIFF, or as a BUILD payload)
+ *   VALUE   : aggregate v (times the carried value when agg == SUM_PRODUCT,
+ *             minus it when agg == SUM_DIFF)
  *   GROUP   : the value itself extends the group key like a PROBE payload
  *             (g = g*digit_card + (v-digit_base)); GROUP BY a fact column
  * Flags may be OR-ed (FILTER|CARRY).  The aggregate is int64:
@@ -274,7 +275,12 @@ enum {
     GX_STEP_VALUE = 8,
     GX_STEP_GROUP = 16
 };
-enum { GX_AGG_SUM = 0, GX_AGG_SUM_PRODUCT = 1, GX_AGG_COUNT = 2, GX_AGG_BUILD = 3 };
+enum { GX_AGG_SUM = 0, GX_AGG_SUM_PRODUCT = 1, GX_AGG_COUNT = 2, GX_AGG_BUILD = 3, GX_AGG_SUM_DIFF = 4 };
+/* GX_AGG_SUM_DIFF sums v - carried (SUM(lo_revenue - lo_supplycost) of
+ * usecases/ssb/queries/04inmem.hpp:146).  A plan may carry a value and build
+ * a group key at once only where gx_scan runs it in the shared or pipelined
+ * form (segmented LZ4, its only VALUE step last); gx_scan_static and queue-form
+ * batches refuse such plans. */
 /* GX_AGG_BUILD fills a join table instead of aggregating: every row that
  * passes the plan's FILTER / PROBE steps is inserted into plan.build_ht with
  * the VALUE step's column as the key and the carried value (a CARRY step) as
@@ -329,10 +335,13 @@ gx_status gx_scan_check(void* stream);
 
 /* Allocation-free form of gx_scan.  No reference counterpart: the reference
  * has no scan entry point whose scratch avoids the allocator.
- * Identical results to gx_scan, but the chunk work list lives in one
- * file-scope device array per device (GX_SCAN_STATIC_MAX_CHUNKS chunk ids,
- * 64 KiB) instead of stream-ordered pool memory, so the call never allocates
- * or frees device memory.  It is for callers that own every byte of device
+ * Identical results to gx_scan, but always through the two-launch queue form
+ * (a pruning/work-list kernel, then the per-query scan kernel), whose chunk
+ * work list lives in one file-scope device array per device
+ * (GX_SCAN_STATIC_MAX_CHUNKS chunk ids, 64 KiB) instead of stream-ordered
+ * pool memory, so the call never allocates or frees device memory.  (Plans
+ * that gx_scan runs as a single pipelined or shared-form launch take no
+ * scratch there either; this entry point keeps them on the queue form.)  It is for callers that own every byte of device
  * memory through their own budget (tables carved out of HBM up front, with
  * the driver's pool kept empty) and for callers that cannot afford a pool
  * allocation that may fail or map new memory in the middle of a query.

@@ -392,6 +392,81 @@ OR_EXPORT int or_q3(const int32_t* lo_custkey, const int32_t* lo_suppkey, const 
  * HashAggregate::add with SumAgg (core/dev_structs.cuh:210-244,
  * usecases/ssb/queries/query_common.cuh:24-29) as a sort-free CPU sum over a
  * dense key range [0, n_keys). */
+/* Q2 shape, the query2 loop (usecases/ssb/queries/02inmem.hpp:100-180):
+ * part rows passing part_ok and supplier rows passing supp_ok are joined,
+ * every date joins (its year is the group attribute); SUM(revenue) GROUP BY
+ * (brand, year) into sums[brand_card][n_years], counts likewise.  Keys are
+ * row indexes of the dimension arrays (fact keys index them directly).
+ * Returns 0, or -1 on a key outside a dimension. */
+OR_EXPORT int or_q2(const int32_t* lo_partkey, const int32_t* lo_suppkey, const int32_t* lo_orderdate,
+                    const int32_t* lo_revenue, uint64_t n, const uint8_t* part_ok, const int32_t* p_brand,
+                    uint64_t n_part, const uint8_t* supp_ok, uint64_t n_supp, const int32_t* d_key,
+                    const int32_t* d_year, uint64_t n_date, int32_t brand_card, int32_t year0, int32_t n_years,
+                    int64_t* sums, int64_t* counts) {
+    int32_t dmin = INT32_MAX, dmax = INT32_MIN;
+    for (uint64_t i = 0; i < n_date; ++i) {
+        if (d_key[i] < dmin) dmin = d_key[i];
+        if (d_key[i] > dmax) dmax = d_key[i];
+    }
+    if (n_date == 0) return 0;
+    int32_t* dy = (int32_t*)malloc(sizeof(int32_t) * (uint64_t)(dmax - dmin + 1));
+    for (int64_t k = 0; k <= (int64_t)dmax - dmin; ++k) dy[k] = INT32_MIN;
+    for (uint64_t i = 0; i < n_date; ++i) dy[d_key[i] - dmin] = d_year[i];
+    int rc = 0;
+    for (uint64_t r = 0; r < n; ++r) {
+        const int64_t pk = lo_partkey[r], sk = lo_suppkey[r];
+        if (pk < 0 || (uint64_t)pk >= n_part || sk < 0 || (uint64_t)sk >= n_supp) { rc = -1; break; }
+        if (!part_ok[pk] || !supp_ok[sk]) continue;
+        const int32_t dk = lo_orderdate[r];
+        if (dk < dmin || dk > dmax || dy[dk - dmin] == INT32_MIN) continue;
+        const int32_t y = dy[dk - dmin] - year0, b = p_brand[pk];
+        if (y < 0 || y >= n_years || b < 0 || b >= brand_card) { rc = -1; break; }
+        sums[(int64_t)b * n_years + y] += lo_revenue[r];
+        counts[(int64_t)b * n_years + y] += 1;
+    }
+    free(dy);
+    return rc;
+}
+
+/* Q4 shape, the query4inmem loop (usecases/ssb/queries/04inmem.hpp:120-160):
+ * customer / supplier / part rows passing their flags join, dates pass
+ * date_ok; SUM(revenue - supplycost) GROUP BY (year, c_nation) into
+ * sums[n_years][25], counts likewise. */
+OR_EXPORT int or_q4(const int32_t* lo_custkey, const int32_t* lo_suppkey, const int32_t* lo_partkey,
+                    const int32_t* lo_orderdate, const int32_t* lo_revenue, const int32_t* lo_supplycost, uint64_t n,
+                    const uint8_t* cust_ok, const int32_t* c_nation, uint64_t n_cust, const uint8_t* supp_ok,
+                    uint64_t n_supp, const uint8_t* part_ok, uint64_t n_part, const int32_t* d_key,
+                    const int32_t* d_year, const uint8_t* date_ok, uint64_t n_date, int32_t year0, int32_t n_years,
+                    int64_t* sums, int64_t* counts) {
+    int32_t dmin = INT32_MAX, dmax = INT32_MIN;
+    for (uint64_t i = 0; i < n_date; ++i) {
+        if (d_key[i] < dmin) dmin = d_key[i];
+        if (d_key[i] > dmax) dmax = d_key[i];
+    }
+    if (n_date == 0) return 0;
+    int32_t* dy = (int32_t*)malloc(sizeof(int32_t) * (uint64_t)(dmax - dmin + 1));
+    for (int64_t k = 0; k <= (int64_t)dmax - dmin; ++k) dy[k] = INT32_MIN;
+    for (uint64_t i = 0; i < n_date; ++i)
+        if (date_ok[i]) dy[d_key[i] - dmin] = d_year[i];
+    int rc = 0;
+    for (uint64_t r = 0; r < n; ++r) {
+        const int64_t ck = lo_custkey[r], sk = lo_suppkey[r], pk = lo_partkey[r];
+        if (ck < 0 || (uint64_t)ck >= n_cust || sk < 0 || (uint64_t)sk >= n_supp || pk < 0 || (uint64_t)pk >= n_part) {
+            rc = -1;
+            break;
+        }
+        if (!cust_ok[ck] || !supp_ok[sk] || !part_ok[pk]) continue;
+        const int32_t dk = lo_orderdate[r];
+        if (dk < dmin || dk > dmax || dy[dk - dmin] == INT32_MIN) continue;
+        const int32_t y = dy[dk - dmin] - year0, c = c_nation[ck];
+        if (y < 0 || y >= n_years || c < 0 || c >= 25) { rc = -1; break; }
+        sums[(int64_t)y * 25 + c] += (int64_t)lo_revenue[r] - lo_supplycost[r];
+        counts[(int64_t)y * 25 + c] += 1;
+    }
+    free(dy);
+    return rc;
+}
+
 OR_EXPORT int or_group_sum_dense(const int64_t* keys, const int64_t* vals, uint64_t n, int64_t* sums, uint64_t n_keys) {
     memset(sums, 0, 8 * n_keys);
     for (uint64_t i = 0; i < n; ++i) {
@@ -443,14 +518,18 @@ static uint32_t or_partkey_to_price(uint64_t p) {
 
 /* Fills caller arrays (sized from or_ssb_sizes_for; lineorder arrays need
  * n_orders*7 entries).  Returns the number of lineorder rows. */
+/* Part columns are integer codes of the reference strings: p_mfgr
+ * "MFGR#m" -> m-1 (0..4), p_category "MFGR#mn" -> 5*(m-1)+(n-1) (0..24),
+ * p_brand1 "MFGR#mnbb" -> 40*p_category + (bb-1) (0..999). */
 OR_EXPORT int64_t or_ssb_generate(uint32_t sf, uint64_t seed,
                                   /* date */ int32_t* d_key, int32_t* d_year, int32_t* d_yearmonthnum,
                                   int32_t* d_weeknuminyear,
                                   /* customer */ int32_t* c_nation, int32_t* c_region,
                                   /* supplier */ int32_t* s_nation, int32_t* s_region,
+                                  /* part (may be NULL) */ int32_t* p_mfgr, int32_t* p_category, int32_t* p_brand1,
                                   /* lineorder */ int32_t* lo_orderdate, int32_t* lo_custkey, int32_t* lo_suppkey,
                                   int32_t* lo_quantity, int32_t* lo_discount, int32_t* lo_extendedprice,
-                                  int32_t* lo_revenue) {
+                                  int32_t* lo_revenue, int32_t* lo_partkey, int32_t* lo_supplycost) {
     uint64_t n_orders, n_c, n_s, n_p, n_d;
     or_ssb_sizes_for(sf, &n_orders, &n_c, &n_s, &n_p, &n_d);
     /* populate_date (SSB_def.hpp:372-399): no RNG */
@@ -480,9 +559,19 @@ OR_EXPORT int64_t or_ssb_generate(uint32_t sf, uint64_t seed,
         s_nation[t] = (int32_t)nat;
         s_region[t] = OR_NATION_REGION[nat];
     }
-    /* populate_part (:282-318): 12 draws per part */
-    for (uint64_t t = 0; t < n_p; ++t)
-        for (int k = 0; k < 12; ++k) (void)or_uniform_int(&seed, 0, 10);
+    /* populate_part (:282-318): size, num1, num2, num3, then 8 draws for the
+       type / container / name / colour strings */
+    for (uint64_t t = 0; t < n_p; ++t) {
+        (void)or_uniform_int(&seed, 1, 51);
+        uint32_t num1 = or_uniform_int(&seed, 1, 6), num2 = or_uniform_int(&seed, 1, 6);
+        uint32_t num3 = or_uniform_int(&seed, 1, 41);
+        for (int k = 0; k < 8; ++k) (void)or_uniform_int(&seed, 0, 10);
+        if (p_mfgr) {
+            p_mfgr[t] = (int32_t)num1 - 1;
+            p_category[t] = 5 * ((int32_t)num1 - 1) + (int32_t)num2 - 1;
+            p_brand1[t] = 40 * p_category[t] + (int32_t)num3 - 1;
+        }
+    }
     /* populate_lineorder (:201-279) */
     uint64_t total = 0;
     for (uint64_t oi = 0; oi < n_orders; ++oi) {
@@ -509,6 +598,10 @@ OR_EXPORT int64_t or_ssb_generate(uint32_t sf, uint64_t seed,
             lo_discount[r] = (int32_t)d;
             lo_extendedprice[r] = (int32_t)ext;
             lo_revenue[r] = (int32_t)(uint32_t)(ext * (100.0 - d) / 100);
+            if (lo_partkey) {
+                lo_partkey[r] = (int32_t)pk;
+                lo_supplycost[r] = (int32_t)(6 * or_partkey_to_price(pk) / 10);
+            }
         }
         total += lines;
     }

@@ -24,9 +24,17 @@ _P = C.c_void_p
 _u64, _i64, _i32, _u32 = C.c_uint64, C.c_int64, C.c_int32, C.c_uint32
 
 
+# The reference source tree of this checkout's build container (absent on
+# machines that only run the prebuilt libraries); GX_REFERENCE_TREE overrides.
+_REF_TREE = os.environ.get("GX_REFERENCE_TREE", "/root/reference")
+
+
 def build() -> None:
-    """Compile liboracle.so (and the reference harness where the tree exists)."""
-    subprocess.run(["make", "-s", "-C", str(HERE), "-f", "Makefile", "all"], check=True)
+    """Compile liboracle.so, and the reference harness where the reference tree exists."""
+    cmd = ["make", "-s", "-C", str(HERE), "-f", "Makefile", "all"]
+    if Path(_REF_TREE, "core").is_dir():
+        cmd.append(f"REF={_REF_TREE}")
+    subprocess.run(cmd, check=True)
 
 
 def _ptr(a):
@@ -67,7 +75,12 @@ def lib():
         L.or_ssb_sizes_for.restype = None
         L.or_ssb_sizes_for.argtypes = [_u32] + [C.POINTER(_u64)] * 5
         L.or_ssb_generate.restype = _i64
-        L.or_ssb_generate.argtypes = [_u32, _u64] + [_P] * 15
+        L.or_ssb_generate.argtypes = [_u32, _u64] + [_P] * 20
+        L.or_q2.restype = C.c_int
+        L.or_q2.argtypes = [_P, _P, _P, _P, _u64, _P, _P, _u64, _P, _u64, _P, _P, _u64, _i32, _i32, _i32, _P, _P]
+        L.or_q4.restype = C.c_int
+        L.or_q4.argtypes = [_P, _P, _P, _P, _P, _P, _u64, _P, _P, _u64, _P, _u64, _P, _u64, _P, _P, _P, _u64,
+                            _i32, _i32, _P, _P]
         _lib = L
     return _lib
 
@@ -86,6 +99,10 @@ def ref():
         R.ref_ssb_golden.argtypes = [_u32, _u32, _P]
         R.ref_ssb_columns.restype = _i64
         R.ref_ssb_columns.argtypes = [_u32] + [_P] * 11
+        R.ref_ssb_golden_flights.restype = C.c_int
+        R.ref_ssb_golden_flights.argtypes = [_u32, _u32, _P]
+        R.ref_ssb_part_columns.restype = _i64
+        R.ref_ssb_part_columns.argtypes = [_u32] + [_P] * 5
         R.ref_lz4_compress_blocks.restype = C.c_int
         R.ref_lz4_compress_blocks.argtypes = [_P, _u64, _u64, _P, _u64, _P]
         R.ref_lz4_decompress.restype = C.c_int
@@ -185,8 +202,59 @@ def q3(custkey, suppkey, orderdate, revenue, c_key, c_attr, c_ok, s_key, s_attr,
     return sums.reshape(c_card, s_card, d_card), counts.reshape(c_card, s_card, d_card)
 
 
+def _keyed(keys, attr, ok, n):
+    """Dimension arrays indexed by key (0..n-1): attribute and pass flag; keys outside stay unset."""
+    a = np.zeros(n, np.int32)
+    f = np.zeros(n, np.uint8)
+    k = np.asarray(keys, np.int64)
+    a[k] = attr
+    f[k] = np.asarray(ok, np.uint8)
+    return a, f
+
+
+def q2(partkey, suppkey, orderdate, revenue, p_key, p_brand, p_ok, s_key, s_ok, d_key, d_year, brand_card, year0,
+       n_years):
+    """Q2 shape (02inmem.hpp:100-180): (sums, counts) of shape (brand_card, n_years)."""
+    f = [np.ascontiguousarray(x, np.int32) for x in (partkey, suppkey, orderdate, revenue)]
+    npk = int(max(np.max(p_key), np.max(f[0]))) + 1
+    nsk = int(max(np.max(s_key), np.max(f[1]))) + 1
+    pb, pok = _keyed(p_key, p_brand, p_ok, npk)
+    _, sok = _keyed(s_key, np.zeros(len(s_key), np.int32), s_ok, nsk)
+    d = [np.ascontiguousarray(x, np.int32) for x in (d_key, d_year)]
+    sums = np.zeros(brand_card * n_years, np.int64)
+    counts = np.zeros_like(sums)
+    rc = lib().or_q2(_ptr(f[0]), _ptr(f[1]), _ptr(f[2]), _ptr(f[3]), len(f[0]), _ptr(pok), _ptr(pb), npk, _ptr(sok),
+                     nsk, _ptr(d[0]), _ptr(d[1]), len(d[0]), brand_card, year0, n_years, _ptr(sums), _ptr(counts))
+    if rc != 0:
+        raise ValueError(f"or_q2 failed: {rc}")
+    return sums.reshape(brand_card, n_years), counts.reshape(brand_card, n_years)
+
+
+def q4(custkey, suppkey, partkey, orderdate, revenue, supplycost, c_key, c_nation, c_ok, s_key, s_ok, p_key, p_ok,
+       d_key, d_year, d_ok, year0, n_years):
+    """Q4 shape (04inmem.hpp:120-160): (sums, counts) of SUM(revenue - supplycost), shape (n_years, 25)."""
+    f = [np.ascontiguousarray(x, np.int32) for x in (custkey, suppkey, partkey, orderdate, revenue, supplycost)]
+    nck = int(max(np.max(c_key), np.max(f[0]))) + 1
+    nsk = int(max(np.max(s_key), np.max(f[1]))) + 1
+    npk = int(max(np.max(p_key), np.max(f[2]))) + 1
+    cn, cok = _keyed(c_key, c_nation, c_ok, nck)
+    _, sok = _keyed(s_key, np.zeros(len(s_key), np.int32), s_ok, nsk)
+    _, pok = _keyed(p_key, np.zeros(len(p_key), np.int32), p_ok, npk)
+    d = [np.ascontiguousarray(x, np.int32) for x in (d_key, d_year)]
+    dok = np.ascontiguousarray(d_ok, np.uint8)
+    sums = np.zeros(n_years * 25, np.int64)
+    counts = np.zeros_like(sums)
+    rc = lib().or_q4(_ptr(f[0]), _ptr(f[1]), _ptr(f[2]), _ptr(f[3]), _ptr(f[4]), _ptr(f[5]), len(f[0]), _ptr(cok),
+                     _ptr(cn), nck, _ptr(sok), nsk, _ptr(pok), npk, _ptr(d[0]), _ptr(d[1]), _ptr(dok), len(d[0]),
+                     year0, n_years, _ptr(sums), _ptr(counts))
+    if rc != 0:
+        raise ValueError(f"or_q4 failed: {rc}")
+    return sums.reshape(n_years, 25), counts.reshape(n_years, 25)
+
+
 def ssb_generate(sf: int, seed: int = 0xBEE5BEE5) -> dict:
-    """Oracle restatement of the reference SSB generator (int32 columns)."""
+    """Oracle restatement of the reference SSB generator (int32 columns; part
+    strings as integer codes: p_mfgr 0..4, p_category 0..24, p_brand1 0..999)."""
     L = lib()
     vals = [_u64() for _ in range(5)]
     L.or_ssb_sizes_for(sf, *[C.byref(v) for v in vals])
@@ -195,14 +263,18 @@ def ssb_generate(sf: int, seed: int = 0xBEE5BEE5) -> dict:
     t = {k: np.zeros(n_d, np.int32) for k in ("d_key", "d_year", "d_yearmonthnum", "d_weeknuminyear")}
     t.update({k: np.zeros(n_c, np.int32) for k in ("c_nation", "c_region")})
     t.update({k: np.zeros(n_s, np.int32) for k in ("s_nation", "s_region")})
-    lo = ("lo_orderdate", "lo_custkey", "lo_suppkey", "lo_quantity", "lo_discount", "lo_extendedprice", "lo_revenue")
+    t.update({k: np.zeros(n_p, np.int32) for k in ("p_mfgr", "p_category", "p_brand1")})
+    lo = ("lo_orderdate", "lo_custkey", "lo_suppkey", "lo_quantity", "lo_discount", "lo_extendedprice", "lo_revenue",
+          "lo_partkey", "lo_supplycost")
     t.update({k: np.zeros(cap, np.int32) for k in lo})
     n = L.or_ssb_generate(sf, seed, *[_ptr(t[k]) for k in ("d_key", "d_year", "d_yearmonthnum", "d_weeknuminyear",
-                                                          "c_nation", "c_region", "s_nation", "s_region") + lo])
+                                                          "c_nation", "c_region", "s_nation", "s_region",
+                                                          "p_mfgr", "p_category", "p_brand1") + lo])
     for k in lo:
         t[k] = t[k][:n]
     t["c_key"] = np.arange(n_c, dtype=np.int32)
     t["s_key"] = np.arange(n_s, dtype=np.int32)
+    t["p_key"] = np.arange(n_p, dtype=np.int32)
     return t
 
 
@@ -222,6 +294,21 @@ def ssb_queries(t: dict) -> dict:
     r["q3_1_groups"] = int((counts > 0).sum())
     r["q3_1_sum"] = int(sums.sum())
     r["q3_1_cells"] = (sums, counts)
+    # Q2.1 (02inmem.hpp:208-210): p_category = MFGR#12 (code 1), s_region AMERICA (1)
+    sums, counts = q2(t["lo_partkey"], t["lo_suppkey"], t["lo_orderdate"], t["lo_revenue"], t["p_key"],
+                      t["p_brand1"], t["p_category"] == 1, t["s_key"], t["s_region"] == 1, t["d_key"], t["d_year"],
+                      1000, 1992, 7)
+    r["q2_1_groups"] = int((counts > 0).sum())
+    r["q2_1_sum"] = int(sums.sum())
+    r["q2_1_cells"] = (sums, counts)
+    # Q4.1 (04inmem.hpp:204-210): c_region, s_region AMERICA, p_mfgr MFGR#1 or MFGR#2 (codes 0, 1)
+    sums, counts = q4(t["lo_custkey"], t["lo_suppkey"], t["lo_partkey"], t["lo_orderdate"], t["lo_revenue"],
+                      t["lo_supplycost"], t["c_key"], t["c_nation"], t["c_region"] == 1, t["s_key"],
+                      t["s_region"] == 1, t["p_key"], t["p_mfgr"] <= 1, t["d_key"], t["d_year"],
+                      np.ones(len(t["d_key"]), bool), 1992, 7)
+    r["q4_1_groups"] = int((counts > 0).sum())
+    r["q4_1_sum"] = int(sums.sum())
+    r["q4_1_cells"] = (sums, counts)
     return r
 
 

@@ -213,6 +213,183 @@ static void run_q31(Tables& t, uint32_t workers, uint64_t* n_groups, uint64_t* t
     *total = sum;
 }
 
+// Restatement of YEARBRAND_GROUP (usecases/ssb/queries/02.cuh:45-62) and
+// Q41_GROUP (usecases/ssb/queries/04.cuh:12-31).
+struct HYearBrand {
+    uint16_t d_year;
+    util::Padded<char[10]> p_brand1;
+    uint64_t hash() const {
+        uint64_t h = 0;
+        std::memcpy(&h, p_brand1.d, 8);
+        return h ^ d_year;
+    }
+    bool operator==(const HYearBrand& o) const {  // brands are 9 characters, never shorter
+        for (int i = 0; i < 9; ++i)
+            if (p_brand1.d[i] == '\0' || p_brand1.d[i] != o.p_brand1.d[i]) return false;
+        return d_year == o.d_year;
+    }
+};
+struct HYearBrandHash {
+    std::size_t operator()(const HYearBrand& g) const { return g.hash(); }
+};
+struct HQ41 {
+    uint16_t d_year;
+    util::Padded<char[16]> c_nation;
+    uint64_t hash() const {
+        uint64_t h = (*(uint32_t*)c_nation.d);
+        h <<= 32;
+        h ^= d_year;
+        return h;
+    }
+    bool operator==(const HQ41& o) const {
+        for (int i = 0; i < 16; ++i) {
+            if (c_nation.d[i] != o.c_nation.d[i]) return false;
+            if (c_nation.d[i] == '\0') break;
+        }
+        return d_year == o.d_year;
+    }
+};
+struct HQ41Hash {
+    std::size_t operator()(const HQ41& g) const { return g.hash(); }
+};
+
+static bool str_is(const char* d, const char* s, int n) { return std::strncmp(d, s, n) == 0; }
+
+// query2 body for Q2.1 (usecases/ssb/queries/02inmem.hpp:100-180, predicates
+// of query2_1inmem :208-210: p_category MFGR#12, s_region AMERICA; every date).
+static void run_q21(Tables& t, uint32_t workers, uint64_t* n_groups, uint64_t* total) {
+    golap::HostHashMap ph(t.part.num_tuples, t.part.col<Part::KEY>().data());
+    golap::HostHashMap sh(t.supplier.num_tuples, t.supplier.col<Supplier::KEY>().data());
+    golap::HostHashMap dh(t.date.num_tuples, t.date.col<Date::KEY>().data());
+    const uint64_t num_groups = 500;
+    std::vector<HYearBrand> groups(num_groups);
+    auto aggs = std::make_unique<std::atomic<uint64_t>[]>(num_groups);
+    for (uint64_t i = 0; i < num_groups; ++i) aggs[i] = 0;
+    golap::HostHashAggregate<HYearBrand, std::atomic<uint64_t>> ha(num_groups, groups.data(), aggs.get());
+    util::SliceSeq ps{t.part.num_tuples, workers}, ss{t.supplier.num_tuples, workers}, dss{t.date.num_tuples, workers},
+        ls{t.lineorder.num_tuples, workers};
+    std::vector<std::tuple<uint64_t, uint64_t>> psl(workers), ssl(workers), dsl(workers), lsl(workers);
+    for (auto& [s, e] : psl) ps.get(s, e);
+    for (auto& [s, e] : ssl) ss.get(s, e);
+    for (auto& [s, e] : dsl) dss.get(s, e);
+    for (auto& [s, e] : lsl) ls.get(s, e);
+    std::vector<std::thread> th;
+    for (uint32_t w = 0; w < workers; ++w)
+        th.emplace_back([&, w] {
+            auto [s, e] = psl[w];
+            for (uint64_t i = s; i < e; ++i)
+                if (str_is(t.part.col<Part::CATEGORY>().data()[i].d, "MFGR#12", 8))
+                    ph.insert(i, t.part.col<Part::KEY>().data()[i]);
+            std::tie(s, e) = ssl[w];
+            for (uint64_t i = s; i < e; ++i)
+                if (region_is(t.supplier.col<Supplier::REGION>().data()[i], "AMERICA"))
+                    sh.insert(i, t.supplier.col<Supplier::KEY>().data()[i]);
+            std::tie(s, e) = dsl[w];
+            for (uint64_t i = s; i < e; ++i) dh.insert(i, t.date.col<Date::KEY>().data()[i]);
+        });
+    for (auto& x : th) x.join();
+    th.clear();
+    for (uint32_t w = 0; w < workers; ++w)
+        th.emplace_back([&, w] {
+            auto [s, e] = lsl[w];
+            std::unordered_map<HYearBrand, uint64_t, HYearBrandHash> local;
+            for (uint64_t i = s; i < e; ++i) {
+                const uint64_t pm = ph.probe(t.lineorder.col<Lineorder::PARTKEY>().data()[i]);
+                if (pm == (uint64_t)-1) continue;
+                const uint64_t sm = sh.probe(t.lineorder.col<Lineorder::SUPPKEY>().data()[i]);
+                if (sm == (uint64_t)-1) continue;
+                const uint64_t dm = dh.probe(t.lineorder.col<Lineorder::ORDERDATE>().data()[i]);
+                local[HYearBrand{t.date.col<Date::YEAR>().data()[dm], t.part.col<Part::BRAND1>().data()[pm]}] +=
+                    t.lineorder.col<Lineorder::REVENUE>().data()[i];
+            }
+            for (auto& [k, v] : local) ha.add(k, v, HostSumAtomic());
+        });
+    for (auto& x : th) x.join();
+    uint64_t ng = 0, sum = 0;
+    for (uint64_t i = 0; i < num_groups; ++i) {
+        if (ha.wrote_group[i] == 0) continue;
+        ++ng;
+        sum += aggs[i];
+    }
+    *n_groups = ng;
+    *total = sum;
+}
+
+// query4inmem body for Q4.1 (usecases/ssb/queries/04inmem.hpp:80-160,
+// predicates of query4_1inmem :204-210: c_region and s_region AMERICA,
+// p_mfgr MFGR#1 or MFGR#2, every date); profit = revenue - supplycost.
+static void run_q41(Tables& t, uint32_t workers, uint64_t* n_groups, uint64_t* total) {
+    golap::HostHashMap ch(t.customer.num_tuples, t.customer.col<Customer::KEY>().data());
+    golap::HostHashMap sh(t.supplier.num_tuples, t.supplier.col<Supplier::KEY>().data());
+    golap::HostHashMap dh(t.date.num_tuples, t.date.col<Date::KEY>().data());
+    golap::HostHashMap ph(t.part.num_tuples, t.part.col<Part::KEY>().data());
+    const uint64_t num_groups = 800;
+    std::vector<HQ41> groups(num_groups);
+    auto aggs = std::make_unique<std::atomic<uint64_t>[]>(num_groups);
+    for (uint64_t i = 0; i < num_groups; ++i) aggs[i] = 0;
+    golap::HostHashAggregate<HQ41, std::atomic<uint64_t>> ha(num_groups, groups.data(), aggs.get());
+    util::SliceSeq cs{t.customer.num_tuples, workers}, ss{t.supplier.num_tuples, workers},
+        dss{t.date.num_tuples, workers}, ps{t.part.num_tuples, workers}, ls{t.lineorder.num_tuples, workers};
+    std::vector<std::tuple<uint64_t, uint64_t>> csl(workers), ssl(workers), dsl(workers), psl(workers), lsl(workers);
+    for (auto& [s, e] : csl) cs.get(s, e);
+    for (auto& [s, e] : ssl) ss.get(s, e);
+    for (auto& [s, e] : dsl) dss.get(s, e);
+    for (auto& [s, e] : psl) ps.get(s, e);
+    for (auto& [s, e] : lsl) ls.get(s, e);
+    std::vector<std::thread> th;
+    for (uint32_t w = 0; w < workers; ++w)
+        th.emplace_back([&, w] {
+            auto [s, e] = csl[w];
+            for (uint64_t i = s; i < e; ++i)
+                if (region_is(t.customer.col<Customer::REGION>().data()[i], "AMERICA"))
+                    ch.insert(i, t.customer.col<Customer::KEY>().data()[i]);
+            std::tie(s, e) = ssl[w];
+            for (uint64_t i = s; i < e; ++i)
+                if (region_is(t.supplier.col<Supplier::REGION>().data()[i], "AMERICA"))
+                    sh.insert(i, t.supplier.col<Supplier::KEY>().data()[i]);
+            std::tie(s, e) = dsl[w];
+            for (uint64_t i = s; i < e; ++i) dh.insert(i, t.date.col<Date::KEY>().data()[i]);
+            std::tie(s, e) = psl[w];
+            for (uint64_t i = s; i < e; ++i) {
+                const char* m = t.part.col<Part::MFGR>().data()[i].d;
+                if (str_is(m, "MFGR#1", 7) || str_is(m, "MFGR#2", 7)) ph.insert(i, t.part.col<Part::KEY>().data()[i]);
+            }
+        });
+    for (auto& x : th) x.join();
+    th.clear();
+    for (uint32_t w = 0; w < workers; ++w)
+        th.emplace_back([&, w] {
+            auto [s, e] = lsl[w];
+            std::unordered_map<HQ41, uint64_t, HQ41Hash> local;
+            for (uint64_t i = s; i < e; ++i) {
+                const uint64_t cm = ch.probe(t.lineorder.col<Lineorder::CUSTKEY>().data()[i]);
+                if (cm == (uint64_t)-1) continue;
+                const uint64_t sm = sh.probe(t.lineorder.col<Lineorder::SUPPKEY>().data()[i]);
+                if (sm == (uint64_t)-1) continue;
+                const uint64_t dm = dh.probe(t.lineorder.col<Lineorder::ORDERDATE>().data()[i]);
+                if (dm == (uint64_t)-1) continue;
+                const uint64_t pm = ph.probe(t.lineorder.col<Lineorder::PARTKEY>().data()[i]);
+                if (pm == (uint64_t)-1) continue;
+                const uint64_t profit = t.lineorder.col<Lineorder::REVENUE>().data()[i] -
+                                        t.lineorder.col<Lineorder::SUPPLYCOST>().data()[i];
+                local[HQ41{t.date.col<Date::YEAR>().data()[dm], t.customer.col<Customer::NATION>().data()[cm]}] +=
+                    profit;
+            }
+            for (auto& [k, v] : local) ha.add(k, v, HostSumAtomic());
+        });
+    for (auto& x : th) x.join();
+    uint64_t ng = 0, sum = 0;
+    for (uint64_t i = 0; i < num_groups; ++i) {
+        if (ha.wrote_group[i] == 0) continue;
+        ++ng;
+        sum += aggs[i];
+    }
+    *n_groups = ng;
+    *total = sum;
+}
+
+static int part_code(const char* mfgr_str) { return mfgr_str[5] - '1'; }
+
 static int nation_index(const util::Padded<char[16]>& n) {
     int i = 0;
     for (auto& kv : NATION) {
@@ -267,6 +444,46 @@ __attribute__((visibility("default"))) int64_t ref_ssb_columns(uint32_t sf, int3
         lo_discount[i] = t.lineorder.col<Lineorder::DISCOUNT>().data()[i];
         lo_extendedprice[i] = (int32_t)t.lineorder.col<Lineorder::EXTENDEDPRICE>().data()[i];
         lo_revenue[i] = (int32_t)t.lineorder.col<Lineorder::REVENUE>().data()[i];
+    }
+    return (int64_t)t.lineorder.num_tuples;
+}
+
+// Q2.1 and Q4.1 on the reference tables: out = {q21_groups, q21_sum,
+// q41_groups, q41_sum}.
+__attribute__((visibility("default"))) int ref_ssb_golden_flights(uint32_t sf, uint32_t workers, int64_t* out) {
+    Tables t(sf, 1);
+    t.init();
+    t.populate();
+    uint64_t ng = 0, tot = 0;
+    run_q21(t, workers, &ng, &tot);
+    out[0] = (int64_t)ng;
+    out[1] = (int64_t)tot;
+    run_q41(t, workers, &ng, &tot);
+    out[2] = (int64_t)ng;
+    out[3] = (int64_t)tot;
+    return 0;
+}
+
+// The part and lineorder columns the Q2/Q4 flights read, as integer codes
+// (p_mfgr "MFGR#m" -> m-1, p_category "MFGR#mn" -> 5(m-1)+(n-1), p_brand1
+// "MFGR#mnbb" -> 40*category + bb-1) for cross-checking the oracle.
+__attribute__((visibility("default"))) int64_t ref_ssb_part_columns(uint32_t sf, int32_t* p_mfgr, int32_t* p_category,
+                                                                    int32_t* p_brand1, int32_t* lo_partkey,
+                                                                    int32_t* lo_supplycost) {
+    Tables t(sf, 1);
+    t.init();
+    t.populate();
+    for (uint64_t i = 0; i < t.part.num_tuples; ++i) {
+        const char* m = t.part.col<Part::MFGR>().data()[i].d;
+        const char* c = t.part.col<Part::CATEGORY>().data()[i].d;
+        const char* b = t.part.col<Part::BRAND1>().data()[i].d;
+        p_mfgr[i] = part_code(m);
+        p_category[i] = 5 * part_code(m) + (c[6] - '1');
+        p_brand1[i] = 40 * p_category[i] + (b[7] - '0') * 10 + (b[8] - '0') - 1;
+    }
+    for (uint64_t i = 0; i < t.lineorder.num_tuples; ++i) {
+        lo_partkey[i] = (int32_t)t.lineorder.col<Lineorder::PARTKEY>().data()[i];
+        lo_supplycost[i] = (int32_t)t.lineorder.col<Lineorder::SUPPLYCOST>().data()[i];
     }
     return (int64_t)t.lineorder.num_tuples;
 }

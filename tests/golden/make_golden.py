@@ -2,10 +2,10 @@
 code (oracle/_ref/libgolapref.so, compiled from the GOLAP sources by
 oracle/Makefile): the SSB tables from the reference generator
 (usecases/ssb/data/SSB_def.hpp, seed 0xBEE5BEE5, scale factor 1) and the
-Q1.1/Q1.2/Q1.3/Q3.1 results of the query loops over the reference's
-HostHashMap/HostHashAggregate.  Also records per-column checksums of the
-generated table so the oracle's generator restatement can be compared
-without the reference tree.
+Q1.1/Q1.2/Q1.3/Q3.1/Q2.1/Q4.1 results of the query loops over the
+reference's HostHashMap/HostHashAggregate.  Also records per-column
+checksums of the generated table (part strings as integer codes) so the
+oracle's generator restatement can be compared without the reference tree.
 
 Run: python tests/golden/make_golden.py
 """
@@ -36,6 +36,17 @@ def main():
     for k in COLS:
         a = arrs[k][:n] if k.startswith("lo_") else arrs[k]
         digests[k] = hashlib.sha256(a.tobytes()).hexdigest()
+    fl = np.zeros(4, np.int64)
+    R.ref_ssb_golden_flights(1, 8, O._ptr(fl))
+    n_part = 200_000
+    parts = {k: np.zeros(n_part, np.int32) for k in ("p_mfgr", "p_category", "p_brand1")}
+    lo2 = {k: np.zeros(1_500_000 * 7, np.int32) for k in ("lo_partkey", "lo_supplycost")}
+    n2 = R.ref_ssb_part_columns(1, *[O._ptr(parts[k]) for k in parts], *[O._ptr(lo2[k]) for k in lo2])
+    assert n2 == n
+    for k, a in parts.items():
+        digests[k] = hashlib.sha256(a.tobytes()).hexdigest()
+    for k, a in lo2.items():
+        digests[k] = hashlib.sha256(a[:n].tobytes()).hexdigest()
     doc = {
         "source": "reference CPU code compiled from the GOLAP sources (oracle/ref_harness.cu)",
         "scale_factor": 1,
@@ -46,6 +57,10 @@ def main():
         "q1_3": int(out[2]),
         "q3_1_groups": int(out[3]),
         "q3_1_sum": int(out[4]),
+        "q2_1_groups": int(fl[0]),
+        "q2_1_sum": int(fl[1]),
+        "q4_1_groups": int(fl[2]),
+        "q4_1_sum": int(fl[3]),
         "column_sha256": digests,
     }
     (Path(__file__).parent / "ssb_sf1_reference.json").write_text(json.dumps(doc, indent=1) + "\n")

@@ -3,8 +3,9 @@
 * SSB generator restatement vs the reference generator: per-column sha256 of
   the scale-factor-1 tables recorded from the reference's own code
   (tests/golden/ssb_sf1_reference.json, made by tests/golden/make_golden.py).
-* Q1.1 / Q1.2 / Q1.3 / Q3.1 restatements vs the reference results on the
-  same data (same fixture; the values agree with the published survey run).
+* Q1.1 / Q1.2 / Q1.3 / Q3.1 / Q2.1 / Q4.1 restatements vs the reference
+  results on the same data (same fixture; the Q1/Q3 values agree with the
+  published survey run).
 * LZ4 decoder restatement vs blocks produced by the reference's
   LZ4CPUManager::compress (liblz4), tests/golden/lz4_reference_blocks.npz.
 * Where the reference harness is built in this checkout, it is also run
@@ -45,6 +46,10 @@ def test_queries_match_reference(sf1, golden):
     assert r["q1_3"] == golden["q1_3"] == 25077436727
     assert r["q3_1_groups"] == golden["q3_1_groups"] == 150
     assert r["q3_1_sum"] == golden["q3_1_sum"] == 772685826017
+    assert r["q2_1_groups"] == golden["q2_1_groups"] == 280
+    assert r["q2_1_sum"] == golden["q2_1_sum"] == 173123930382
+    assert r["q4_1_groups"] == golden["q4_1_groups"] == 35
+    assert r["q4_1_sum"] == golden["q4_1_sum"] == 330407033455
 
 
 def test_lz4_decoder_on_reference_blocks():
@@ -97,3 +102,10 @@ def test_reference_harness_live(golden):
     O.ref().ref_ssb_golden(1, 4, O._ptr(out))
     assert out.tolist() == [golden["q1_1"], golden["q1_2"], golden["q1_3"], golden["q3_1_groups"],
                             golden["q3_1_sum"], golden["lineorder_rows"]]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference harness not built here")
+def test_reference_harness_flights_live(golden):
+    out = np.zeros(4, np.int64)
+    O.ref().ref_ssb_golden_flights(1, 4, O._ptr(out))
+    assert out.tolist() == [golden["q2_1_groups"], golden["q2_1_sum"], golden["q4_1_groups"], golden["q4_1_sum"]]

@@ -46,6 +46,24 @@ def test_static_equals_scan_q1_pruned(cuda):
     assert 1 <= sum(got[0][1]) < len(got[0][1])
 
 
+def test_static_leaves_device_memory_unchanged(cuda):
+    # the property the entry point exists for: after a first call (which loads
+    # the kernels' code and looks up the array's address), further calls take
+    # no device memory -- no pool allocation, no cudaMalloc
+    f = datagen.fact_q1(6_000_000, True)
+    dd = datagen.date_dim()
+    fact = queries.encode_fact(f, {"date_key": "cascaded"})
+    ok = dd["d_year"] == 1996
+    q = queries.Q1Query(fact, dd, ok, 19960101, 19961231, 1, 3, 0, 24, prune=True)
+    first = _run("gx_scan_static", q.plan, q.result, q.keep)
+    cuda.cuda.synchronize()
+    free0 = cuda.cuda.mem_get_info()[0]
+    for _ in range(5):
+        assert _run("gx_scan_static", q.plan, q.result, q.keep) == first
+    cuda.cuda.synchronize()
+    assert cuda.cuda.mem_get_info()[0] == free0
+
+
 def test_static_equals_scan_grouped(cuda):
     f = datagen.fact_q3(5_000_000, True, n_customer=300_000, n_supplier=20_000)
     cust = datagen.dim_geo(300_000, datagen.SEED, 21)
