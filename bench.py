@@ -248,6 +248,40 @@ def time_launches(fn, reps, stream, flush=None, pre=None):
     return out
 
 
+REF_GPU = ROOT / "baseline" / "_ref" / "libgolaprefgpu.so"
+
+
+def ref_gpu_lib():
+    """The same-box GPU reference point (baseline/refgpu/ref_gpu.cu), or None when not built."""
+    import ctypes as C
+
+    if not REF_GPU.exists():
+        return None
+    R = C.CDLL(str(REF_GPU))
+    P, u64, i32 = C.c_void_p, C.c_uint64, C.c_int32
+    R.ref_gpu_q1.restype = C.c_int64
+    R.ref_gpu_q1.argtypes = [P, P, P, P, u64, P, P, u64, P, C.c_uint32, C.c_int, C.POINTER(C.c_double)]
+    R.ref_gpu_q3.restype = C.c_int64
+    R.ref_gpu_q3.argtypes = [P, P, P, P, u64, P, P, P, u64, P, P, P, u64, P, P, u64, i32, i32, i32, P, C.c_uint32,
+                             C.c_int, P, P, u64, C.POINTER(u64), C.POINTER(C.c_double)]
+    return R
+
+
+def decompressed(fact, names):
+    """The named columns decoded into int32 device tensors (one library call each)."""
+    import torch
+
+    from golap_public_b200 import api
+
+    out = {}
+    for k in names:
+        t = torch.empty(fact.n_rows, dtype=torch.int32, device="cuda")
+        api.ChunkDecompressor(fact.cols[k]).chunks(0, fact.cols[k].info.n_chunks, t)
+        out[k] = t
+    api.scan_check()
+    return out
+
+
 def roofline(bytes_, ms, pk, pk_kind, traffic=None):
     a = bytes_ / (ms * 1e-3) / 1e9
     return {"bound": "hbm", "achieved": a, "peak": pk, "unit": "GB/s", "frac": a / pk, "traffic": traffic,
@@ -401,6 +435,32 @@ def gpu_arm(args, rank, world):
     full_m = full_scan(fact_m, "4-byte matches")
     full_m["lz4_policy"] = "lz4_min_match=4 (every 4-byte repeat inside a segment becomes a match)"
 
+    # same-box GPU reference point: the reference's own pipeline_q1_lineorder and
+    # hash_map_build_pred_other compiled for sm_100a, on the decompressed columns
+    ref_gpu = None
+    R = ref_gpu_lib()
+    if R is not None:
+        import ctypes as C
+
+        cols = decompressed(fact, Q1_COLS)
+        ptrs = [C.c_void_p(cols[k].data_ptr()) for k in Q1_COLS]
+        dkd = torch.from_numpy(dd["d_key"]).cuda()
+        ref_gpu = {"what": "the reference's hash_map_build_pred_other + pipeline_q1_lineorder (one launch per "
+                           "surviving 1M-row chunk, 512-thread CTAs) compiled for sm_100a, on columns already "
+                           "decompressed into the reference's types (decompression not counted: a lower bound)"}
+        for label, okv, chunks in (("pruned", ok, kept_chunks), ("full_scan", ok_all, list(range(n_chunks)))):
+            ch = np.ascontiguousarray(chunks, np.uint32)
+            okb = np.ascontiguousarray(okv.astype(np.uint8))
+            rms = C.c_double()
+            r = R.ref_gpu_q1(*ptrs, N_ROWS, C.c_void_p(dkd.data_ptr()), okb.ctypes.data_as(C.c_void_p), len(okb),
+                             ch.ctypes.data_as(C.c_void_p), len(ch), 5, C.byref(rms))
+            want_r = got if label == "pruned" else want_all
+            ref_gpu[label] = {"ms": rms.value, "rows_per_s": N_ROWS / (rms.value * 1e-3), "result_equal": r == want_r,
+                              "gx_ms": ms if label == "pruned" else full["ms"]}
+            if r != want_r:
+                raise SystemExit(f"reference GPU kernels gave {r}, the fused scan {want_r}")
+        del cols
+
     # e2e: pinned-host residency, date dimension in, result out
     fact_h = queries.encode_fact(f, {"date_key": "cascaded"}, ROWS_PER_CHUNK, ROWS_PER_BLOCK, args.segments,
                                  residency="pinned")
@@ -452,6 +512,7 @@ def gpu_arm(args, rank, world):
         "roofline_full_scan": full["roofline"],
         "full_scan": full,
         "full_scan_lz4_matches": full_m,
+        "reference_gpu": ref_gpu,
         "e2e": {"value": N_ROWS * world / (e2e_ms * 1e-3), "unit": "rows/s",
                 "h2d_bytes_per_step": int(h2d_scan + dd["d_key"].nbytes + ok.astype(np.int32).nbytes),
                 "d2h_bytes_per_step": 8, "ms_per_step": e2e_ms, "residency": "pinned host (zero-copy reads)"},
@@ -545,6 +606,42 @@ def star_join_section(args, pk, pk_kind, world=1):
            "customer_build": "3M-row customer join table built from compressed customer columns (key, nation, "
                              "region cascaded) in one fused decode + filter + insert launch",
            "comp_bytes": {k: c.info.comp_bytes for k, c in fact.cols.items()}}
+    # same-box GPU reference point (the reference's HashMap / HashAggregate /
+    # hash_map_build_pred_other and pipeline_q3's loop body, sm_100a)
+    R = ref_gpu_lib()
+    if R is not None:
+        import ctypes as C
+
+        cols = decompressed(fact, Q3_COLS)
+        dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in
+               (("ck", cust["key"]), ("cn", cust["nation"]), ("cr", cust["region"]), ("sk", supp["key"]),
+                ("sn", supp["nation"]), ("sr", supp["region"]), ("dk", dd["d_key"]), ("dy", dd["d_year"]))}
+        ch = np.ascontiguousarray(kept, np.uint32)
+        gk = np.zeros(4096, np.int64)
+        gs = np.zeros(4096, np.int64)
+        ng, rms = C.c_uint64(), C.c_double()
+        vp = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+        R.ref_gpu_q3(vp(cols["date_key"]), vp(cols["cust_key"]), vp(cols["supp_key"]), vp(cols["revenue"]), n,
+                     vp(dev["ck"]), vp(dev["cn"]), vp(dev["cr"]), len(cust["key"]), vp(dev["sk"]), vp(dev["sn"]),
+                     vp(dev["sr"]), len(supp["key"]), vp(dev["dk"]), vp(dev["dy"]), len(dd["d_key"]), region, ylo, yhi,
+                     ch.ctypes.data_as(C.c_void_p), len(ch), 3, gk.ctypes.data_as(C.c_void_p),
+                     gs.ctypes.data_as(C.c_void_p), len(gk), C.byref(ng), C.byref(rms))
+        ny = yhi - ylo + 1
+        rg = {}
+        for i in range(ng.value):
+            cs_, y = divmod(int(gk[i]), ny)
+            c, s_ = divmod(cs_, 25)
+            rg[(c, s_, ylo + y)] = int(gs[i])
+        out["reference_gpu"] = {
+            "what": "the reference's hash_map_build_pred_other (customer/supplier/date), HashMap probes and "
+                    "HashAggregate::add in pipeline_q3's loop body (one launch per surviving 1M-row chunk) compiled "
+                    "for sm_100a, on columns already decompressed into the reference's types (decompression not "
+                    "counted: a lower bound)",
+            "ms": rms.value, "rows_per_s": n / (rms.value * 1e-3), "groups_equal": rg == got, "gx_ms": ms}
+        if rg != got:
+            raise SystemExit("star join: reference GPU kernels' groups differ from the fused scan's")
+        del cols, dev
+
     # e2e: the fact columns in pinned host memory, dimension columns copied in, groups read back
     fact_h = queries.encode_fact({k: g[k] for k in Q3_COLS}, {"date_key": "cascaded"}, ROWS_PER_CHUNK,
                                  ROWS_PER_BLOCK, args.segments, residency="pinned")
