@@ -117,6 +117,12 @@ _SIGS = {
     "gx_hashtable_clear": (C.c_int32, [P, P]),
     "gx_hashtable_keys": (C.c_int32, [P, P, C.c_uint64, P, P]),
     "gx_check_minmax_points": (C.c_int32, [P, P, P, C.c_uint64, P, P]),
+    "gx_column_build_hist": (C.c_int32, [P, C.c_uint32, P]),
+    "gx_check_hist": (C.c_int32, [P, C.c_int32, C.c_int32, P, P]),
+    "gx_column_build_bloom": (C.c_int32, [P, C.c_uint64, C.c_double, P]),
+    "gx_check_bloom": (C.c_int32, [P, C.c_int32, P, P]),
+    "gx_column_meta_read": (C.c_int32, [P, P, P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
+                                        C.POINTER(C.c_uint32), P]),
     "gx_minmax_reduce": (C.c_int32, [P, C.c_uint64, P, P]),
     "gx_groupby_view": (C.c_int32, [P, C.POINTER(P), C.POINTER(P), C.POINTER(C.c_uint32)]),
     "gx_groupby_create": (C.c_int32, [C.c_uint64, C.POINTER(P)]),

@@ -102,6 +102,30 @@ class Column:
             return np.zeros(0, np.uint32)
         return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
 
+    # --- richer pruning metadata (built on the device)
+    def build_hist(self, n_buckets: int, stream=None) -> "Column":
+        """Equal-width histograms of n_buckets per chunk (EqHistogram)."""
+        check(L.lib().gx_column_build_hist(self.handle, n_buckets, _stream_handle(stream)))
+        return self
+
+    def build_bloom(self, m_bytes: int, p: float, stream=None) -> "Column":
+        """A Bloom filter of m_bytes per chunk for false-positive rate p (BloomMeta)."""
+        check(L.lib().gx_column_build_bloom(self.handle, m_bytes, p, _stream_handle(stream)))
+        return self
+
+    def meta(self, stream=None):
+        """(histogram counts (n_chunks, n_buckets) or None, Bloom words (n_chunks, m/4) or None, k)."""
+        nb, mb, k = C.c_uint32(), C.c_uint64(), C.c_uint32()
+        check(L.lib().gx_column_meta_read(self.handle, None, None, C.byref(nb), C.byref(mb), C.byref(k),
+                                          _stream_handle(stream)))
+        nc = self.info.n_chunks
+        h = np.zeros((nc, nb.value), np.uint64) if nb.value else None
+        w = np.zeros((nc, mb.value // 4), np.uint32) if mb.value else None
+        check(L.lib().gx_column_meta_read(self.handle, h.ctypes.data_as(C.c_void_p) if h is not None else None,
+                                          w.ctypes.data_as(C.c_void_p) if w is not None else None, None, None, None,
+                                          _stream_handle(stream)))
+        return h, w, k.value
+
     # --- device residency
     def to_device(self, residency: str = "hbm", stream=None) -> "Column":
         check(L.lib().gx_column_to_device(self.handle, 1 if residency == "hbm" else 2, _stream_handle(stream)))
@@ -152,6 +176,18 @@ class MetaChecker:
         lies in chunk c's min/max of `col`; AND the result with other flags."""
         check(L.lib().gx_check_minmax_points(col.handle, _dptr(keys), _dptr(count), keys.numel(), _dptr(keep_out),
                                              _stream_handle(stream)))
+        return keep_out
+
+    def add_hist(self, col: Column, lo: int, hi: int, keep_out, stream=None):
+        """check_hist (core/metadata.cuh:584-595): sets keep_out[c] = 1 where a
+        non-empty bucket of chunk c overlaps [lo, hi] (col.build_hist first)."""
+        check(L.lib().gx_check_hist(col.handle, lo, hi, _dptr(keep_out), _stream_handle(stream)))
+        return keep_out
+
+    def add_bloom(self, col: Column, value: int, keep_out, stream=None):
+        """check_bloom (core/metadata.cuh:612-620): sets keep_out[c] = 1 where
+        value may be in chunk c (col.build_bloom first)."""
+        check(L.lib().gx_check_bloom(col.handle, value, _dptr(keep_out), _stream_handle(stream)))
         return keep_out
 
     def run(self, keep_out, stream=None):

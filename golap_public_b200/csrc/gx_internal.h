@@ -170,6 +170,14 @@ struct gx_column {
     uint32_t* d_seg = nullptr;
     int32_t* d_mins = nullptr;
     int32_t* d_maxs = nullptr;
+    // richer pruning metadata built on the device (meta.cu): equal-width
+    // histograms (hist_buckets counts per chunk) and Bloom filters
+    // (bloom_bytes per chunk, bloom_k hash functions)
+    uint32_t hist_buckets = 0;
+    uint64_t* d_hist = nullptr;
+    uint64_t bloom_bytes = 0;
+    uint32_t bloom_k = 0;
+    uint32_t* d_bloom = nullptr;
     int32_t* d_bmins = nullptr;
     int32_t* d_bmaxs = nullptr;
     int device = -1;

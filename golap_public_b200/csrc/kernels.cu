@@ -1288,6 +1288,13 @@ gx_status gx_column_release_device(gx_column* col) {
     if (col->d_maxs) cudaFree(col->d_maxs);
     if (col->d_bmins) cudaFree(col->d_bmins);
     if (col->d_bmaxs) cudaFree(col->d_bmaxs);
+    if (col->d_hist) cudaFree(col->d_hist);
+    if (col->d_bloom) cudaFree(col->d_bloom);
+    col->d_hist = nullptr;
+    col->d_bloom = nullptr;
+    col->hist_buckets = 0;
+    col->bloom_bytes = 0;
+    col->bloom_k = 0;
     col->d_bmins = col->d_bmaxs = nullptr;
     col->d_payload = nullptr;
     col->h_pinned = nullptr;

@@ -160,6 +160,25 @@ gx_status gx_prune_minmax(const gx_column* const* cols, const int32_t* lo, const
 gx_status gx_check_minmax_points(const gx_column* col, const int32_t* keys_dev, const uint64_t* n_keys_dev,
                                  uint64_t cap, uint16_t* out_dev, void* stream);
 
+/* Richer per-chunk metadata, built on the device from the (device-resident)
+ * compressed column and checked with the same flag convention.
+ * Replaces: EqHistogram (core/metadata.cuh:225-382) with fill_hist /
+ * check_hist (:573-595), and BloomMeta (:385-537) with fill_bloom /
+ * check_bloom (:602-620), as MetaChecker::add_hist / add_bloom use them. */
+/* n_buckets (1..4096) equal-width buckets per chunk between its min and max. */
+gx_status gx_column_build_hist(gx_column* col, uint32_t n_buckets, void* stream);
+/* out_dev[c] = 1 where a non-empty bucket of chunk c overlaps [lo, hi]; other entries untouched. */
+gx_status gx_check_hist(const gx_column* col, int32_t lo, int32_t hi, uint16_t* out_dev, void* stream);
+/* A Bloom filter of m_bytes (a multiple of 4, at most 32 KiB) per chunk for
+ * false-positive rate p (the reference's (p, m) parameters). */
+gx_status gx_column_build_bloom(gx_column* col, uint64_t m_bytes, double p, void* stream);
+/* out_dev[c] = 1 where value may be in chunk c; other entries untouched. */
+gx_status gx_check_bloom(const gx_column* col, int32_t value, uint16_t* out_dev, void* stream);
+/* Host copies of the built metadata (each pointer may be NULL): counts
+ * (n_chunks x n_buckets), filter words (n_chunks x bloom_bytes / 4), sizes. */
+gx_status gx_column_meta_read(const gx_column* col, uint64_t* hist_host, uint32_t* bloom_host, uint32_t* n_buckets,
+                              uint64_t* bloom_bytes, uint32_t* bloom_k, void* stream);
+
 /* --------------------------------------------------------------- hash join
  * Replaces: HashMap (core/dev_structs.cuh:37-132) with its filtered build
  * hash_map_build_pred_other (core/join.cuh:107-135) and the probe kernels

@@ -11,6 +11,7 @@
  * against liblz4-produced blocks.
  */
 #include <stdint.h>
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
@@ -220,6 +221,78 @@ OR_EXPORT void or_minmax_points_keep(const int32_t* mins, const int32_t* maxs, u
                 keep[c] = 1;
                 break;
             }
+}
+
+/* EqHistogram (core/metadata.cuh:225-382): per chunk n_buckets equal-width
+ * buckets between the chunk's min and max (add :305-322, double arithmetic),
+ * and check_pred (:325-350).  counts has n_chunks * nb entries. */
+OR_EXPORT void or_hist_counts(const int32_t* v, uint64_t n, uint64_t rpc, uint32_t nb, const int32_t* mins,
+                              const int32_t* maxs, uint64_t* counts) {
+    for (uint64_t r = 0; r < n; ++r) {
+        const uint64_t c = r / rpc;
+        uint64_t b = 0;
+        if (maxs[c] != mins[c]) {
+            const double inv = (double)nb / (double)((int64_t)maxs[c] - mins[c]);
+            b = (uint64_t)((double)((int64_t)v[r] - mins[c]) * inv);
+            if (b > nb - 1) b = nb - 1;
+        }
+        counts[c * nb + b] += 1;
+    }
+}
+OR_EXPORT void or_hist_keep(const int32_t* mins, const int32_t* maxs, const uint64_t* counts, uint64_t n_chunks,
+                            uint32_t nb, int32_t lo, int32_t hi, uint16_t* keep) {
+    for (uint64_t c = 0; c < n_chunks; ++c) {
+        if (mins[c] == maxs[c]) {
+            if (lo <= mins[c] && hi >= maxs[c] && counts[c * nb] != 0) keep[c] = 1;
+            continue;
+        }
+        const double inv = (double)nb / (double)((int64_t)maxs[c] - mins[c]);
+        int64_t first = (int64_t)(((double)lo - mins[c]) * inv);
+        const int64_t last = (int64_t)(((double)hi - mins[c]) * inv);
+        if (lo == maxs[c]) first = (int64_t)nb - 1;
+        for (int64_t b = 0; b < (int64_t)nb; ++b)
+            if (first <= b && last >= b && counts[c * nb + b] != 0) keep[c] = 1;
+    }
+}
+
+/* BloomMeta (core/metadata.cuh:385-537): (p, m) parameters, the 64-bit
+ * finaliser hash (:464-472) and k bits per value per chunk. */
+OR_EXPORT uint32_t or_bloom_k(uint64_t m_bytes, double p) {
+    const uint64_t mbits = m_bytes << 3;
+    const uint64_t nn = (uint64_t)ceil(((double)mbits * log(pow(0.5, log(2.0))) / log(p)));
+    return (uint32_t)ceil(log(2.0) * (double)mbits / (double)nn);
+}
+static uint64_t or_bloom_hash(uint64_t v, uint64_t mbits) {
+    v ^= v >> 33;
+    v *= 0xff51afd7ed558ccdull;
+    v ^= v >> 33;
+    v *= 0xc4ceb9fe1a85ec53ull;
+    v ^= v >> 33;
+    return v % mbits;
+}
+OR_EXPORT void or_bloom_words(const int32_t* v, uint64_t n, uint64_t rpc, uint64_t m_bytes, uint32_t k,
+                              uint32_t* words) {
+    const uint64_t mbits = m_bytes << 3, per = m_bytes / 4;
+    for (uint64_t r = 0; r < n; ++r) {
+        const uint64_t lv = (uint64_t)(int64_t)v[r];
+        for (uint32_t i = 0; i < k; ++i) {
+            const uint64_t bit = or_bloom_hash(lv + i, mbits);
+            words[(r / rpc) * per + (bit >> 5)] |= 1u << (bit & 31);
+        }
+    }
+}
+OR_EXPORT void or_bloom_keep(const uint32_t* words, uint64_t n_chunks, uint64_t m_bytes, uint32_t k, int32_t val,
+                             uint16_t* keep) {
+    const uint64_t mbits = m_bytes << 3, per = m_bytes / 4;
+    const uint64_t lv = (uint64_t)(int64_t)val;
+    for (uint64_t c = 0; c < n_chunks; ++c) {
+        int res = 1;
+        for (uint32_t i = 0; i < k; ++i) {
+            const uint64_t bit = or_bloom_hash(lv + i, mbits);
+            if (!(words[c * per + (bit >> 5)] & (1u << (bit & 31)))) res = 0;
+        }
+        if (res) keep[c] = 1;
+    }
 }
 
 /* Per-chunk min/max as collected at ingest by MinMaxMeta::init_chunk

@@ -70,6 +70,16 @@ def lib():
                             _i32, _u32, _i32, _u32, _i32, _u32, _P, _P, _P, _u64]
         L.or_minmax_points_keep.restype = None
         L.or_minmax_points_keep.argtypes = [_P, _P, _u64, _P, _u64, _P]
+        L.or_hist_counts.restype = None
+        L.or_hist_counts.argtypes = [_P, _u64, _u64, _u32, _P, _P, _P]
+        L.or_hist_keep.restype = None
+        L.or_hist_keep.argtypes = [_P, _P, _P, _u64, _u32, _i32, _i32, _P]
+        L.or_bloom_k.restype = _u32
+        L.or_bloom_k.argtypes = [_u64, C.c_double]
+        L.or_bloom_words.restype = None
+        L.or_bloom_words.argtypes = [_P, _u64, _u64, _u64, _u32, _P]
+        L.or_bloom_keep.restype = None
+        L.or_bloom_keep.argtypes = [_P, _u64, _u64, _u32, _i32, _P]
         L.or_group_sum_dense.restype = C.c_int
         L.or_group_sum_dense.argtypes = [_P, _P, _u64, _P, _u64]
         L.or_ssb_sizes_for.restype = None
@@ -150,6 +160,40 @@ def minmax_points_keep(mins, maxs, keys) -> np.ndarray:
     mn = np.ascontiguousarray(mins, np.int32)
     mx = np.ascontiguousarray(maxs, np.int32)
     lib().or_minmax_points_keep(_ptr(mn), _ptr(mx), len(mn), _ptr(k), len(k), _ptr(keep))
+    return keep
+
+
+def hist_counts(v, rows_per_chunk, n_buckets):
+    """EqHistogram counts per chunk (n_chunks, n_buckets)."""
+    v = np.ascontiguousarray(v, np.int32)
+    mins, maxs = chunk_minmax(v, rows_per_chunk)
+    counts = np.zeros(len(mins) * n_buckets, np.uint64)
+    lib().or_hist_counts(_ptr(v), len(v), rows_per_chunk, n_buckets, _ptr(mins), _ptr(maxs), _ptr(counts))
+    return counts.reshape(len(mins), n_buckets)
+
+
+def hist_keep(mins, maxs, counts, lo, hi):
+    keep = np.zeros(len(mins), np.uint16)
+    c = np.ascontiguousarray(counts, np.uint64)
+    mn, mx = np.ascontiguousarray(mins, np.int32), np.ascontiguousarray(maxs, np.int32)
+    lib().or_hist_keep(_ptr(mn), _ptr(mx), _ptr(c), len(mn), c.shape[1], lo, hi, _ptr(keep))
+    return keep
+
+
+def bloom_words(v, rows_per_chunk, m_bytes, p):
+    """BloomMeta filters (n_chunks, m_bytes / 4 words) and k."""
+    v = np.ascontiguousarray(v, np.int32)
+    k = lib().or_bloom_k(m_bytes, p)
+    nc = -(-len(v) // rows_per_chunk)
+    words = np.zeros(nc * (m_bytes // 4), np.uint32)
+    lib().or_bloom_words(_ptr(v), len(v), rows_per_chunk, m_bytes, k, _ptr(words))
+    return words.reshape(nc, m_bytes // 4), k
+
+
+def bloom_keep(words, m_bytes, k, val):
+    w = np.ascontiguousarray(words, np.uint32)
+    keep = np.zeros(w.shape[0], np.uint16)
+    lib().or_bloom_keep(_ptr(w), w.shape[0], m_bytes, k, val, _ptr(keep))
     return keep
 
 

@@ -252,3 +252,51 @@ def test_build_from_compressed_dimension(cuda, layout, carry, key_codec):
     # a dense table cannot be filled this way (it sizes itself from the key range)
     with pytest.raises(GxError):
         queries.build_from_compressed(api.HashMap(n, "dense"), cc.cols["key"], None)
+
+
+@pytest.mark.parametrize("kind", ["sorted_date", "random", "constant_chunks"])
+def test_histogram_metadata_vs_oracle(cuda, kind):
+    # EqHistogram + fill_hist / check_hist (core/metadata.cuh:225-382, 573-595)
+    from golap_public_b200 import datagen
+
+    rng = np.random.default_rng(21)
+    n, rpc = 1_000_000, 100_000
+    if kind == "sorted_date":
+        v = datagen.fact_q1(n, True)["date_key"]
+    elif kind == "random":
+        v = rng.integers(-50_000, 50_000, n, dtype=np.int32)
+    else:
+        v = np.repeat(rng.integers(0, 100, n // rpc, dtype=np.int32), rpc)
+    col = api.Column(v, "cascaded" if kind != "random" else "lz4", rows_per_chunk=rpc).to_device()
+    for nb in (1, 16, 1000):
+        col.build_hist(nb)
+        h, _, _ = col.meta()
+        want = O.hist_counts(v, rpc, nb)
+        assert np.array_equal(h, want)
+        mins, maxs = col.minmax()
+        med = int(np.median(v))
+        for lo, hi in [(int(v.min()), int(v.min())), (int(v.max()), int(v.max())), (med, med + 3),
+                       (int(v.min()) - 10, int(v.min()) - 1), (-100, 100), (19940101, 19940131)]:
+            flags = cuda.zeros(len(mins), dtype=cuda.uint16, device="cuda")
+            api.MetaChecker(len(mins)).add_hist(col, lo, hi, flags)
+            assert flags.cpu().numpy().tolist() == O.hist_keep(mins, maxs, want, lo, hi).tolist()
+
+
+@pytest.mark.parametrize("m_bytes,p", [(64, 0.05), (1024, 0.01), (8192, 0.001)])
+def test_bloom_metadata_vs_oracle(cuda, m_bytes, p):
+    # BloomMeta + fill_bloom / check_bloom (core/metadata.cuh:385-537, 602-620)
+    rng = np.random.default_rng(22)
+    n, rpc = 600_000, 50_000
+    v = rng.integers(0, 200_000, n, dtype=np.int32)
+    col = api.Column(v, "lz4", rows_per_chunk=rpc).to_device().build_bloom(m_bytes, p)
+    _, w, k = col.meta()
+    want_w, want_k = O.bloom_words(v, rpc, m_bytes, p)
+    assert k == want_k and np.array_equal(w, want_w)
+    nc = col.info.n_chunks
+    for val in [int(v[0]), int(v[-1]), -1, 123_456, 199_999, int(v[rpc * 3 + 7])]:
+        flags = cuda.zeros(nc, dtype=cuda.uint16, device="cuda")
+        api.MetaChecker(nc).add_bloom(col, val, flags)
+        got = flags.cpu().numpy()
+        assert got.tolist() == O.bloom_keep(want_w, m_bytes, k, val).tolist()
+        present = np.array([(v[c * rpc:(c + 1) * rpc] == val).any() for c in range(nc)])
+        assert np.all(got[present] == 1)  # no false negatives
