@@ -132,6 +132,7 @@ _SIGS = {
     "gx_groupby_read": (C.c_int32, [P, P, P, C.c_uint64, C.POINTER(C.c_uint64), P]),
     "gx_scan": (C.c_int32, [C.POINTER(ScanPlan), P]),
     "gx_scan_static": (C.c_int32, [C.POINTER(ScanPlan), P]),
+    "gx_scan_streamed": (C.c_int32, [C.POINTER(ScanPlan), C.c_uint32, P]),
     "gx_scan_sync": (C.c_int32, [C.POINTER(ScanPlan), P, C.POINTER(C.c_uint64)]),
     "gx_scan_check": (C.c_int32, [P]),
     "gx_batch_create": (C.c_int32, [C.POINTER(Query), C.c_uint32, C.POINTER(P)]),

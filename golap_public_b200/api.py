@@ -372,6 +372,11 @@ class ScanPlan:
     def launch(self, stream=None):
         check(L.lib().gx_scan(C.byref(self.to_c()), _stream_handle(stream)))
 
+    def launch_streamed(self, chunks_per_group: int = 16, stream=None):
+        """Scan pinned-host columns through double-buffered HBM staging:
+        only the chunks that survive the min/max predicates are copied."""
+        check(L.lib().gx_scan_streamed(C.byref(self.to_c()), chunks_per_group, _stream_handle(stream)))
+
     def run_sync(self, stream=None) -> int:
         rows = C.c_uint64()
         check(L.lib().gx_scan_sync(C.byref(self.to_c()), _stream_handle(stream), C.byref(rows)))

@@ -2074,8 +2074,19 @@ static gx_status scan_launch_shared(const gx_scan_plan* plan, const QueryDesc& q
 // columns runs as the warp-specialised pipeline (pipe_scan_kernel): one CTA
 // per SM, a ring of stages sized to the shared memory.  *done = false when the
 // plan does not qualify.
+// A streamed scan's chunk group: chunks [chunk_lo, chunk_hi) of the table,
+// with the payloads of the listed (pinned-host) columns staged in HBM; a
+// staged view's payload pointer stands for payload offset 0.
+struct PipeGroup {
+    uint32_t chunk_lo, chunk_hi;
+    uint32_t n;
+    const gx_column* col[kPipeMaxCols];
+    const uint8_t* payload[kPipeMaxCols];
+};
+
 static gx_status scan_launch_pipe(const gx_scan_plan* plan, const QueryDesc& qd, const gx_column* c0,
-                                  cudaStream_t s, unsigned long long* rows_dev, bool* done) {
+                                  cudaStream_t s, unsigned long long* rows_dev, bool* done,
+                                  const PipeGroup* grp = nullptr) {
     *done = false;
     std::vector<const gx_column*> cols;
     std::string why;
@@ -2086,17 +2097,26 @@ static gx_status scan_launch_pipe(const gx_scan_plan* plan, const QueryDesc& qd,
     uint32_t dec = 0, n_dec = 0;
     for (size_t i = 0; i < cols.size(); ++i) {
         const gx_column* c = cols[i];
-        if (c->residency != 1) return GX_OK;  // pinned-host columns: zero-copy reads in the shared form
+        const uint8_t* staged = nullptr;
+        for (uint32_t k = 0; grp && k < grp->n; ++k)
+            if (grp->col[k] == c) staged = grp->payload[k];
+        if (c->residency != 1 && !staged) return GX_OK;  // pinned-host columns: zero-copy reads in the shared form
         if (c->codec != GX_CODEC_NONE) {
             dec |= 1u << i;
             ++n_dec;
         }
         P.cols[i] = c->view();
+        if (staged) {
+            P.cols[i].payload = staged;
+            P.cols[i].host_mapped = 0;
+        }
     }
     P.q.keep_in = plan->keep_chunks_dev;
     P.q.keep_out = plan->keep_out_dev;
     P.n_cols = (uint32_t)cols.size();
     P.n_chunks = c0->n_chunks;
+    P.chunk_lo = grp ? grp->chunk_lo : 0u;
+    P.chunk_hi = grp ? grp->chunk_hi : c0->n_chunks;
     P.blocks_per_chunk = c0->blocks_per_chunk;
     P.rows_per_chunk = c0->rows_per_chunk;
     P.rows_per_block = c0->rows_per_block;
@@ -2120,7 +2140,7 @@ static gx_status scan_launch_pipe(const gx_scan_plan* plan, const QueryDesc& qd,
     if (fixed + 2 * per_stage > kPipeMaxDynSmem) return GX_OK;
     P.stages = (uint32_t)std::min<size_t>(kPipeMaxStages, (kPipeMaxDynSmem - fixed) / per_stage);
     const size_t smem = fixed + P.stages * per_stage;
-    const uint64_t tiles = (uint64_t)c0->n_slots * P.tiles_per_block;
+    const uint64_t tiles = (uint64_t)(P.chunk_hi - P.chunk_lo) * c0->blocks_per_chunk * P.tiles_per_block;
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count(), tiles));
     pipe_scan_kernel<<<grid, kPipeNT, smem, s>>>(P);
     const cudaError_t e = cudaGetLastError();
@@ -2182,6 +2202,133 @@ static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned 
     cudaFreeAsync(scratch, s);
     if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "scan launch: %s", cudaGetErrorString(e));
     return GX_OK;
+}
+
+// Streamed scan of pinned-host columns (gx_scan_streamed): chunk groups
+// whose surviving chunks' compressed bytes are copied to HBM on a copy
+// stream (double-buffered), each group scanned by the pipelined kernel while
+// the next one is copied.
+static gx_status scan_streamed(const gx_scan_plan* plan, uint32_t per_group, cudaStream_t s) {
+    QueryDesc qd;
+    uint32_t tile_rows = 0;
+    const gx_column* c0 = nullptr;
+    gx_status st = build_query(plan, &qd, &tile_rows, &c0);
+    if (st) return st;
+    st = ensure_kernel_attrs();
+    if (st) return st;
+    if (per_group == 0) return set_error(GX_ERR_INVALID, "gx_scan_streamed: chunks_per_group must be > 0");
+    // the plan's distinct pinned-host columns
+    std::vector<gx_column*> staged;
+    for (uint32_t i = 0; i < plan->n_steps; ++i) {
+        gx_column* c = const_cast<gx_column*>(plan->steps[i].col);
+        if (c->residency == 2 && std::find(staged.begin(), staged.end(), c) == staged.end()) staged.push_back(c);
+    }
+    const uint32_t n_chunks = c0->n_chunks, bpc = c0->blocks_per_chunk;
+    // chunk keep on the host: the plan's min/max predicates (the kernel applies
+    // them again together with keep_chunks_dev)
+    std::vector<uint8_t> keep(n_chunks, 1);
+    for (uint32_t p = 0; p < plan->n_prune; ++p) {
+        const gx_column* pc = plan->prune[p].col;
+        for (uint32_t c = 0; c < n_chunks; ++c)
+            if (!(plan->prune[p].lo <= pc->maxs[c] && plan->prune[p].hi >= pc->mins[c])) keep[c] = 0;
+    }
+    // byte range of chunk c of column col: [first block offset, last block end)
+    auto chunk_range = [&](const gx_column* col, uint32_t c, uint64_t* a, uint64_t* b) {
+        *a = col->blocks[(size_t)c * bpc].offset;
+        *b = *a;
+        for (uint32_t j = 0; j < bpc; ++j) {
+            const gx_dblock& d = col->blocks[(size_t)c * bpc + j];
+            if (d.n_rows) *b = std::max<uint64_t>(*b, d.offset + d.comp_bytes);
+        }
+    };
+    // groups with a surviving chunk, and the staging bytes each column needs
+    struct Group {
+        uint32_t lo, hi;
+    };
+    std::vector<Group> groups;
+    std::vector<uint64_t> cap(staged.size(), 0);
+    for (uint32_t g0 = 0; g0 < n_chunks; g0 += per_group) {
+        const uint32_t g1 = std::min(n_chunks, g0 + per_group);
+        uint32_t first = g1, last = g0;
+        for (uint32_t c = g0; c < g1; ++c)
+            if (keep[c]) {
+                first = std::min(first, c);
+                last = c;
+            }
+        if (first == g1) continue;
+        groups.push_back({first, last + 1});
+        for (size_t k = 0; k < staged.size(); ++k) {
+            uint64_t a0, b0, a1, b1;
+            chunk_range(staged[k], first, &a0, &b0);
+            chunk_range(staged[k], last, &a1, &b1);
+            cap[k] = std::max<uint64_t>(cap[k], b1 - (a0 & ~15ull) + kPayloadSlack);
+        }
+    }
+    if (plan->agg == GX_AGG_BUILD) return set_error(GX_ERR_INVALID, "gx_scan_streamed: BUILD plans are not streamed");
+    // chunks outside every group's [first, last] range are pruned; the
+    // launches write the flags of the chunks inside the ranges
+    if (plan->keep_out_dev) GX_CK(cudaMemsetAsync(plan->keep_out_dev, 0, 2ull * n_chunks, s));
+    if (groups.empty()) return GX_OK;
+    std::vector<uint8_t*> buf(2 * staged.size(), nullptr);
+    for (size_t k = 0; k < staged.size(); ++k)
+        for (int b = 0; b < 2; ++b) GX_CK(scratch_alloc((void**)&buf[2 * k + b], cap[k], s));
+    cudaStream_t cs = nullptr;
+    cudaEvent_t ready, copied[2], consumed[2];
+    GX_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    GX_CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    for (int b = 0; b < 2; ++b) {
+        GX_CK(cudaEventCreateWithFlags(&copied[b], cudaEventDisableTiming));
+        GX_CK(cudaEventCreateWithFlags(&consumed[b], cudaEventDisableTiming));
+    }
+    GX_CK(cudaEventRecord(ready, s));  // staging allocated (stream-ordered) before the first copy
+    GX_CK(cudaStreamWaitEvent(cs, ready, 0));
+    for (size_t gi = 0; gi < groups.size() && !st; ++gi) {
+        const int b = (int)(gi & 1);
+        const Group& G = groups[gi];
+        if (gi >= 2) GX_CK(cudaStreamWaitEvent(cs, consumed[b], 0));
+        PipeGroup pg{};
+        pg.chunk_lo = G.lo;
+        pg.chunk_hi = G.hi;
+        for (size_t k = 0; k < staged.size(); ++k) {
+            const gx_column* col = staged[k];
+            uint64_t a0, b0;
+            chunk_range(col, G.lo, &a0, &b0);
+            const uint64_t base = a0 & ~15ull;
+            // runs of surviving chunks, each copied at its offset in the group's range
+            for (uint32_t c = G.lo; c < G.hi;) {
+                if (!keep[c]) {
+                    ++c;
+                    continue;
+                }
+                uint32_t e = c;
+                while (e + 1 < G.hi && keep[e + 1]) ++e;
+                uint64_t ra, rb, ea, eb;
+                chunk_range(col, c, &ra, &rb);
+                chunk_range(col, e, &ea, &eb);
+                ra &= ~15ull;
+                const uint64_t end = std::min<uint64_t>(col->payload.size(), eb + kPayloadSlack);
+                GX_CK(cudaMemcpyAsync(buf[2 * k + b] + (ra - base), (const uint8_t*)col->h_pinned + ra, end - ra,
+                                      cudaMemcpyHostToDevice, cs));
+                c = e + 1;
+            }
+            pg.col[pg.n] = col;
+            pg.payload[pg.n++] = buf[2 * k + b] - base;
+        }
+        GX_CK(cudaEventRecord(copied[b], cs));
+        GX_CK(cudaStreamWaitEvent(s, copied[b], 0));
+        bool done = false;
+        st = scan_launch_pipe(plan, qd, c0, s, nullptr, &done, &pg);
+        if (!st && !done) st = set_error(GX_ERR_INVALID, "gx_scan_streamed: the plan needs the pipelined form");
+        if (!st) GX_CK(cudaEventRecord(consumed[b], s));
+    }
+    for (uint8_t* p : buf) cudaFreeAsync(p, s);  // after the last kernel on s
+    cudaEventDestroy(ready);
+    for (int b = 0; b < 2; ++b) {
+        cudaEventDestroy(copied[b]);
+        cudaEventDestroy(consumed[b]);
+    }
+    cudaStreamDestroy(cs);
+    return st;
 }
 
 // Work-list scratch of gx_scan_static, one per device: word 0 = surviving
@@ -2271,6 +2418,10 @@ gx_status gx_scan_static(const gx_scan_plan* plan, void* stream) {
 
 gx_status gx_scan(const gx_scan_plan* plan, void* stream) {
     return scan_launch(plan, (cudaStream_t)stream, nullptr);
+}
+
+gx_status gx_scan_streamed(const gx_scan_plan* plan, uint32_t chunks_per_group, void* stream) {
+    return scan_streamed(plan, chunks_per_group, (cudaStream_t)stream);
 }
 
 gx_status gx_scan_check(void* stream) {

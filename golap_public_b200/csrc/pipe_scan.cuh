@@ -94,6 +94,7 @@ struct PipeParams {
     unsigned long long* build_counters;  // inserted, duplicates, dropped
     uint32_t build_log2, build_layout;
     uint32_t build_rowid;           // 1: the payload is the table row (no CARRY step)
+    uint32_t chunk_lo, chunk_hi;    // chunks [chunk_lo, chunk_hi) are scanned (a streamed group, or all)
 };
 
 // One insert of a GX_AGG_BUILD plan into a linear or bucket join table
@@ -306,10 +307,10 @@ __global__ void __launch_bounds__(kPipeNT, 1) pipe_scan_kernel(const __grid_cons
         const uint32_t K = (PC + G - 1) / G;          // most candidates of one CTA in one chunk
         uint32_t k = 0;                               // tiles issued
         bool abort = false;
-        for (uint32_t cb = 0; cb < P.n_chunks && !abort; cb += 32) {
+        for (uint32_t cb = P.chunk_lo; cb < P.chunk_hi && !abort; cb += 32) {
             const uint32_t cc = cb + lane;
             bool ck = false;
-            if (cc < P.n_chunks) {
+            if (cc < P.chunk_hi) {
                 ck = pipe_chunk_keep(Q, cc);
                 if (b == 0 && Q.keep_out) Q.keep_out[cc] = ck ? 1 : 0;
             }

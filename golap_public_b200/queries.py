@@ -57,6 +57,13 @@ def encode_fact(data: dict, codecs: dict, rows_per_chunk=1_000_000, rows_per_blo
     return FactTable(cols, len(next(iter(data.values()))))
 
 
+def _launch(plan: ScanPlan, stream_group: int, stream):
+    if stream_group:
+        plan.launch_streamed(stream_group, stream)
+    else:
+        plan.launch(stream)
+
+
 class Q1Query:
     """Q1-shaped fused scan over a FactTable with columns date_key, discount, quantity, extended_price."""
 
@@ -102,10 +109,14 @@ class Q1Query:
         MetaChecker(self.join_keep.numel()).add_points(self.fact.cols["date_key"], self._jkeys, self._jn,
                                                        self.join_keep, stream)
 
+    # >0: columns in pinned host memory are streamed to HBM in groups of this
+    # many chunks (gx_scan_streamed); only chunks that survive pruning cross PCIe
+    stream_group = 0
+
     def launch(self, stream=None):
         """Enqueue: clear result, prune + fused scan (no host synchronisation)."""
         self.result.zero_()
-        self.plan.launch(stream)
+        _launch(self.plan, self.stream_group, stream)
 
     def run(self, stream=None) -> int:
         self.launch(stream)
@@ -190,9 +201,11 @@ class Q3Query:
             ck, cn, cr = self._keep_alive[:3]
             self.hc.build(ck, cn, preds=[(cr, self.region, self.region)], stream=stream)
 
+    stream_group = 0  # as Q1Query.stream_group
+
     def launch(self, stream=None):
         self.agg.reset(stream)
-        self.plan.launch(stream)
+        _launch(self.plan, self.stream_group, stream)
 
     def decode_key(self, k: int):
         y = k % self.ycard
@@ -213,9 +226,11 @@ class Q3Query:
 class _StarQuery:
     """Common part of the star-join shapes: join tables, group table, plan."""
 
+    stream_group = 0  # as Q1Query.stream_group
+
     def launch(self, stream=None):
         self.agg.reset(stream)
-        self.plan.launch(stream)
+        _launch(self.plan, self.stream_group, stream)
 
     def run(self, stream=None) -> dict:
         self.launch(stream)

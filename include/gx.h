@@ -352,6 +352,23 @@ gx_status gx_scan_sync(const gx_scan_plan* plan, void* stream, uint64_t* rows_sc
 /* Read and clear the device error word of the scan engine. */
 gx_status gx_scan_check(void* stream);
 
+/* Streamed scan of a plan whose columns are in pinned host memory
+ * (gx_column_to_device with residency 2).  Replaces the reference's load-then-decompress chain
+ * for host-resident columns (DataCopy / VarLoader / BatchLoader feeding the
+ * decompressor: core/access.hpp:17-60, 190-435, one chunk per pipeline step):
+ * the table is cut into groups of `chunks_per_group` chunks; the compressed
+ * bytes of each group's chunks that survive the plan's min/max predicates
+ * are copied host->HBM with cudaMemcpyAsync on an internal copy stream into
+ * one of two staging buffers, and the group is scanned from HBM by the
+ * pipelined kernel while the next group's bytes are copied.  Pruned chunks
+ * are never copied.  Results equal gx_scan's.  keep_chunks_dev is applied by
+ * the kernel (chunks it drops are still copied).  HBM-resident columns of
+ * the plan are read in place.  Plans the pipelined kernel does not run
+ * (GX_AGG_BUILD, queue-only shapes) are rejected with GX_ERR_INVALID.
+ * Staging memory (two buffers per host column, each the largest group's
+ * bytes) comes from the stream-ordered pool and is released on `stream`. */
+gx_status gx_scan_streamed(const gx_scan_plan* plan, uint32_t chunks_per_group, void* stream);
+
 /* Allocation-free form of gx_scan.  No reference counterpart: the reference
  * has no scan entry point whose scratch avoids the allocator.
  * Identical results to gx_scan, but always through the two-launch queue form

@@ -148,6 +148,50 @@ def test_q1_pinned_host_residency(cuda):
     assert qa.run() == _oracle_q1(f, dd, ok_all, 4, 6, 26, 35)
 
 
+@pytest.mark.parametrize("group", [1, 3, 16])
+def test_q1_streamed_from_pinned_host(cuda, group):
+    # gx_scan_streamed: surviving chunks' bytes are staged in HBM group by
+    # group; results and chunk flags equal the oracle's, pruned and unpruned
+    f = datagen.fact_q1(9_500_000, True)
+    dd = datagen.date_dim()
+    fact = queries.encode_fact(f, {"date_key": "cascaded"}, residency="pinned", lz4_segments=32)
+    for ym, lo, hi in ((199301, 19930101, 19930131), (199712, 19971201, 19971231)):
+        ok = dd["d_yearmonthnum"] == ym
+        q = queries.Q1Query(fact, dd, ok, lo, hi, 4, 6, 26, 35, prune=True)
+        q.stream_group = group
+        assert q.run() == _oracle_q1(f, dd, ok, 4, 6, 26, 35)
+        mins, maxs = fact.cols["date_key"].minmax()
+        assert q.keep.cpu().numpy().tolist() == O.minmax_keep(mins, maxs, lo, hi).tolist()
+    ok_all = np.ones(len(dd["d_key"]), dtype=bool)
+    qa = queries.Q1Query(fact, dd, ok_all, int(dd["d_key"].min()), int(dd["d_key"].max()), 1, 3, 0, 24, prune=False)
+    qa.stream_group = group
+    assert qa.run() == _oracle_q1(f, dd, ok_all, 1, 3, 0, 24)
+
+
+def test_q3_streamed_from_pinned_host(cuda):
+    f = datagen.fact_q3(5_000_000, True, n_customer=300_000, n_supplier=20_000)
+    cust = datagen.dim_geo(300_000, datagen.SEED, 21)
+    supp = datagen.dim_geo(20_000, datagen.SEED, 22)
+    dd = datagen.date_dim()
+    fact = queries.encode_fact(f, {"date_key": "cascaded"}, residency="pinned", lz4_segments=32)
+    q = queries.Q3Query(fact, cust, supp, dd, 2, 1994, 1995)
+    q.stream_group = 2
+    sums, counts = O.q3(f["cust_key"], f["supp_key"], f["date_key"], f["revenue"], cust["key"], cust["nation"],
+                        cust["region"] == 2, supp["key"], supp["nation"], supp["region"] == 2, dd["d_key"],
+                        dd["d_year"], (dd["d_year"] >= 1994) & (dd["d_year"] <= 1995), 0, 25, 0, 25, 1994, 2)
+    assert q.run() == {(c, s, 1994 + y): int(sums[c, s, y]) for c, s, y in zip(*np.nonzero(counts))}
+
+
+def test_streamed_rejects_hbm_only_shapes(cuda):
+    f = datagen.fact_q1(300_000, True)
+    dd = datagen.date_dim()
+    fact = queries.encode_fact(f, {"date_key": "cascaded"}, residency="pinned", lz4_segments=1)
+    q = queries.Q1Query(fact, dd, dd["d_yearmonthnum"] == 199301, 19930101, 19930131, 4, 6, 26, 35)
+    q.stream_group = 4
+    with pytest.raises(GxError):
+        q.run()  # plain LZ4 blocks: not a pipelined-kernel shape
+
+
 def test_q3_star_join_groupby(cuda):
     # configs[2] shape at 20M fact rows with full-size dimensions
     f = datagen.fact_q3(20_000_000, True)
