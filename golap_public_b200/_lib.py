@@ -20,6 +20,7 @@ GX_STEP_FILTER, GX_STEP_PROBE, GX_STEP_CARRY, GX_STEP_VALUE, GX_STEP_GROUP = 1, 
 GX_AGG_SUM, GX_AGG_SUM_PRODUCT, GX_AGG_COUNT, GX_AGG_BUILD, GX_AGG_SUM_DIFF = 0, 1, 2, 3, 4
 GX_HT_LINEAR, GX_HT_BUCKET, GX_HT_DENSE = 0, 1, 2
 GX_BATCH_AUTO, GX_BATCH_QUEUE, GX_BATCH_SHARED = 0, 1, 2
+GX_FORM_AUTO, GX_FORM_WARP, GX_FORM_PIPE, GX_FORM_SHARED, GX_FORM_QUEUE = range(5)
 GX_MAX_STEPS = 8
 
 
@@ -133,6 +134,7 @@ _SIGS = {
     "gx_scan": (C.c_int32, [C.POINTER(ScanPlan), P]),
     "gx_scan_static": (C.c_int32, [C.POINTER(ScanPlan), P]),
     "gx_scan_streamed": (C.c_int32, [C.POINTER(ScanPlan), C.c_uint32, P]),
+    "gx_scan_set_form": (C.c_int32, [C.c_uint32]),
     "gx_scan_sync": (C.c_int32, [C.POINTER(ScanPlan), P, C.POINTER(C.c_uint64)]),
     "gx_scan_check": (C.c_int32, [P]),
     "gx_batch_create": (C.c_int32, [C.POINTER(Query), C.c_uint32, C.POINTER(P)]),

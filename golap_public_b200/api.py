@@ -383,6 +383,17 @@ class ScanPlan:
         return rows.value
 
 
+SCAN_FORMS = {"auto": L.GX_FORM_AUTO, "warp": L.GX_FORM_WARP, "pipe": L.GX_FORM_PIPE, "shared": L.GX_FORM_SHARED,
+              "queue": L.GX_FORM_QUEUE}
+
+
+def set_scan_form(form: str = "auto"):
+    """Kernel form of single-plan scans (process-wide): "auto" or one forced
+    form ("warp", "pipe", "shared", "queue"); a forced form that cannot run a
+    plan makes the launch fail instead of falling back."""
+    check(L.lib().gx_scan_set_form(SCAN_FORMS[form]))
+
+
 def scan_check(stream=None):
     check(L.lib().gx_scan_check(_stream_handle(stream)))
 

@@ -178,6 +178,8 @@ struct gx_column {
     uint64_t bloom_bytes = 0;
     uint32_t bloom_k = 0;
     uint32_t* d_bloom = nullptr;
+    // LZ4: every block is one 16-byte aligned literal run (-1 = not known yet)
+    mutable int lz4_direct = -1;
     int32_t* d_bmins = nullptr;
     int32_t* d_bmaxs = nullptr;
     int device = -1;

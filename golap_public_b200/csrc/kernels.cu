@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstring>
 #include <mutex>
@@ -1123,6 +1124,7 @@ gx_status allow_smem(K kernel, size_t bytes) {
 
 #include "shared_scan.cuh"
 #include "pipe_scan.cuh"
+#include "warp_scan.cuh"
 
 }  // namespace
 
@@ -1803,6 +1805,7 @@ static gx_status ensure_kernel_attrs() {
     if (!st) st = allow_smem(shared_scan_kernel<1024, 1>, sh_max);
     if (!st) st = allow_smem(shared_scan_kernel<kShSingleNT, 4, true>, sh_max);
     if (!st) st = allow_smem(pipe_scan_kernel, kPipeMaxDynSmem);
+    if (!st) st = allow_smem(warp_scan_kernel, kWsMaxDynSmem);
     if (st) return st;
     attr_set[dev] = true;
     return GX_OK;
@@ -2149,6 +2152,104 @@ static gx_status scan_launch_pipe(const gx_scan_plan* plan, const QueryDesc& qd,
     return GX_OK;
 }
 
+// Form selection of gx_scan (gx_scan_set_form): process-wide.
+static std::atomic<uint32_t> g_scan_form{GX_FORM_AUTO};
+
+// 1 when every block of an LZ4 column is one literal run whose first byte is
+// 16-byte aligned in the payload (the warp-tile scan then reads the column in
+// place and gives it no decode buffer).  Computed once from the host copy.
+static bool lz4_all_direct(const gx_column* c) {
+    if (c->lz4_direct >= 0) return c->lz4_direct != 0;
+    bool ok = c->codec == GX_CODEC_LZ4;
+    for (uint32_t sl = 0; ok && sl < c->n_slots; ++sl) {
+        const gx::gx_dblock& d = c->blocks[sl];
+        if (!d.n_rows) continue;
+        if (d.offset + d.comp_bytes > c->payload.size() || d.comp_bytes == 0) {
+            ok = false;
+            break;
+        }
+        const uint8_t* p = c->payload.data() + d.offset;
+        uint64_t pos = 1, lit = p[0] >> 4;
+        if ((p[0] & 15u) != 0 && lit != 15) {
+            ok = false;
+            break;
+        }
+        if (lit == 15) {
+            uint8_t x;
+            do {
+                if (pos >= d.comp_bytes) break;
+                x = p[pos++];
+                lit += x;
+            } while (x == 255);
+        }
+        ok = lit == 4ull * d.n_rows && pos + lit == d.comp_bytes && ((d.offset + pos) & 15u) == 0;
+    }
+    c->lz4_direct = ok ? 1 : 0;
+    return ok;
+}
+
+// The warp-tile scan (warp_scan_kernel) for a plan, or *done = false when
+// the plan is not of its shape: HBM-resident (or staged) columns, LZ4 ones
+// segmented with segments of at most kWsTile rows, no BUILD, and the warps'
+// decode buffers within the shared memory of two CTAs per SM.
+static gx_status scan_launch_warp(const gx_scan_plan* plan, const QueryDesc& qd, const gx_column* c0, cudaStream_t s,
+                                  unsigned long long* rows_dev, bool* done, const PipeGroup* grp = nullptr) {
+    *done = false;
+    if (plan->agg == GX_AGG_BUILD) return GX_OK;
+    std::vector<const gx_column*> cols;
+    std::string why;
+    WsParams P;
+    std::memset(&P, 0, sizeof(P));
+    if (!shared_query(*plan, qd, cols, P.q, &why)) return GX_OK;
+    if (cols.size() > kWsMaxCols) return GX_OK;
+    uint32_t nb = 0;
+    for (size_t i = 0; i < cols.size(); ++i) {
+        const gx_column* c = cols[i];
+        const uint8_t* staged = nullptr;
+        for (uint32_t k = 0; grp && k < grp->n; ++k)
+            if (grp->col[k] == c) staged = grp->payload[k];
+        if (c->residency != 1 && !staged) return GX_OK;
+        if (c->rows_per_block != c0->rows_per_block || c->rows_per_chunk != c0->rows_per_chunk) return GX_OK;
+        if (c->codec == GX_CODEC_LZ4 && (c->S <= 1 || c->seg_shift > kWsLog2)) return GX_OK;
+        P.cols[i] = c->view();
+        if (staged) {
+            P.cols[i].payload = staged;
+            P.cols[i].host_mapped = 0;
+        }
+        const bool direct = c->codec == GX_CODEC_NONE || (c->codec == GX_CODEC_LZ4 && lz4_all_direct(c));
+        P.buf_of[i] = direct ? kWsNoBuf : nb++;
+    }
+    for (size_t i = cols.size(); i < kWsMaxCols; ++i) P.buf_of[i] = kWsNoBuf;
+    P.q.keep_in = plan->keep_chunks_dev;
+    P.q.keep_out = plan->keep_out_dev;
+    P.n_cols = (uint32_t)cols.size();
+    P.blocks_per_chunk = c0->blocks_per_chunk;
+    P.rows_per_chunk = c0->rows_per_chunk;
+    P.rows_per_block = c0->rows_per_block;
+    P.tiles_per_block = (c0->rows_per_block + kWsTile - 1) / kWsTile;
+    P.n_rows = c0->n_rows;
+    P.chunk_lo = grp ? grp->chunk_lo : 0u;
+    P.chunk_hi = grp ? grp->chunk_hi : c0->n_chunks;
+    P.n_bufs = nb;
+    P.grouped_tab = P.q.grouped ? 1u : 0u;
+    P.warp_words = 4 * kWsMaxCols + nb * kWsTile + (P.grouped_tab ? 3 * kWsGroupSlots : 0u);
+    P.rows_scanned = rows_dev;
+    const size_t smem = 4ull * P.warp_words * kWsWarps;
+    if (smem > kWsMaxDynSmem / 2) return GX_OK;  // fewer than two CTAs (16 warps) per SM: the pipelined form
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, warp_scan_kernel, kWsNT, smem) != cudaSuccess ||
+        per_sm < 1)
+        return set_error(GX_ERR_CUDA, "warp scan occupancy query failed");
+    const uint64_t tiles = (uint64_t)(P.chunk_hi - P.chunk_lo) * c0->blocks_per_chunk * P.tiles_per_block;
+    const uint64_t want = (tiles + kWsWarps - 1) / kWsWarps;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm, want));
+    warp_scan_kernel<<<grid, kWsNT, smem, s>>>(P);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "warp scan launch: %s", cudaGetErrorString(e));
+    *done = true;
+    return GX_OK;
+}
+
 static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned long long* rows_dev) {
     ScanParams P;
     std::memset(&P, 0, sizeof(P));
@@ -2159,13 +2260,25 @@ static gx_status scan_launch(const gx_scan_plan* plan, cudaStream_t s, unsigned 
     st = ensure_kernel_attrs();
     if (st) return st;
     bool done = false;
-    st = scan_launch_pipe(plan, P.q, c0, s, rows_dev, &done);
-    if (st || done) return st;
+    const uint32_t form = g_scan_form.load(std::memory_order_relaxed);
+    if (form == GX_FORM_AUTO || form == GX_FORM_WARP) {
+        st = scan_launch_warp(plan, P.q, c0, s, rows_dev, &done);
+        if (st || done) return st;
+        if (form == GX_FORM_WARP) return set_error(GX_ERR_INVALID, "the plan is not of the warp-tile form's shape");
+    }
+    if (form == GX_FORM_AUTO || form == GX_FORM_PIPE) {
+        st = scan_launch_pipe(plan, P.q, c0, s, rows_dev, &done);
+        if (st || done) return st;
+        if (form == GX_FORM_PIPE) return set_error(GX_ERR_INVALID, "the plan is not of the pipelined form's shape");
+    }
     if (plan->agg == GX_AGG_BUILD)
         return set_error(GX_ERR_INVALID, "a BUILD plan needs HBM-resident columns (LZ4 ones segmented, segments of "
                                          "at most 2048 rows) and its VALUE step last");
-    st = scan_launch_shared(plan, P.q, c0, s, rows_dev, &done);
-    if (st || done) return st;
+    if (form == GX_FORM_AUTO || form == GX_FORM_SHARED) {
+        st = scan_launch_shared(plan, P.q, c0, s, rows_dev, &done);
+        if (st || done) return st;
+        if (form == GX_FORM_SHARED) return set_error(GX_ERR_INVALID, "the plan is not of the shared form's shape");
+    }
     if (P.q.carry_digits)
         return set_error(GX_ERR_INVALID, "a plan with a carried value and group-key digits needs the shared or "
                                          "pipelined form (segmented LZ4 columns, its only VALUE step last)");
@@ -2317,7 +2430,9 @@ static gx_status scan_streamed(const gx_scan_plan* plan, uint32_t per_group, cud
         GX_CK(cudaEventRecord(copied[b], cs));
         GX_CK(cudaStreamWaitEvent(s, copied[b], 0));
         bool done = false;
-        st = scan_launch_pipe(plan, qd, c0, s, nullptr, &done, &pg);
+        const uint32_t form = g_scan_form.load(std::memory_order_relaxed);
+        if (form != GX_FORM_PIPE) st = scan_launch_warp(plan, qd, c0, s, nullptr, &done, &pg);
+        if (!st && !done && form != GX_FORM_WARP) st = scan_launch_pipe(plan, qd, c0, s, nullptr, &done, &pg);
         if (!st && !done) st = set_error(GX_ERR_INVALID, "gx_scan_streamed: the plan needs the pipelined form");
         if (!st) GX_CK(cudaEventRecord(consumed[b], s));
     }
@@ -2418,6 +2533,12 @@ gx_status gx_scan_static(const gx_scan_plan* plan, void* stream) {
 
 gx_status gx_scan(const gx_scan_plan* plan, void* stream) {
     return scan_launch(plan, (cudaStream_t)stream, nullptr);
+}
+
+gx_status gx_scan_set_form(uint32_t form) {
+    if (form > GX_FORM_QUEUE) return set_error(GX_ERR_INVALID, "unknown scan form %u", form);
+    g_scan_form.store(form, std::memory_order_relaxed);
+    return GX_OK;
 }
 
 gx_status gx_scan_streamed(const gx_scan_plan* plan, uint32_t chunks_per_group, void* stream) {

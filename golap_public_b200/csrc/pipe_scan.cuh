@@ -445,19 +445,24 @@ __global__ void __launch_bounds__(kPipeNT, 1) pipe_scan_kernel(const __grid_cons
                         abort = true;
                         break;
                     }
-                    if (lane == 0) {
+                    // the warp copies the descriptor into the slot (a word per lane) and
+                    // lane c issues column c's copy, after lane 0 announced the bytes
+                    {
                         const uint32_t* from = (const uint32_t*)&s_cand[L];
                         uint32_t* to = (uint32_t*)&s_desc[st];
-                        for (uint32_t w = 0; w < sizeof(PipeTile) / 4; ++w) to[w] = from[w];
-                        fence_proxy_async_smem();
-                        uint32_t total = 0;
-                        for (uint32_t c = 0; c < ncols; ++c) total += s_cbytes[L][c];
-                        mbar_expect_tx_arrive(&s_full[st], total);
-                        for (uint32_t c = 0; c < ncols; ++c)
-                            if (s_cbytes[L][c])
-                                bulk_copy_1d(ring + ((size_t)st * ncols + c) * kPipeColBytes, s_csrc[L][c],
-                                             s_cbytes[L][c], &s_full[st]);
+                        for (uint32_t w = lane; w < sizeof(PipeTile) / 4; w += 32) to[w] = from[w];
                     }
+                    const uint32_t cbytes = lane < ncols ? s_cbytes[L][lane] : 0u;
+                    const uint32_t total = __reduce_add_sync(0xFFFFFFFFu, cbytes);
+                    __syncwarp();
+                    if (lane == 0) {
+                        fence_proxy_async_smem();
+                        mbar_expect_tx_arrive(&s_full[st], total);
+                    }
+                    __syncwarp();
+                    if (cbytes)
+                        bulk_copy_1d(ring + ((size_t)st * ncols + lane) * kPipeColBytes, s_csrc[L][lane], cbytes,
+                                     &s_full[st]);
                     __syncwarp();
                     ++k;
                 }

@@ -352,6 +352,20 @@ gx_status gx_scan_sync(const gx_scan_plan* plan, void* stream, uint64_t* rows_sc
 /* Read and clear the device error word of the scan engine. */
 gx_status gx_scan_check(void* stream);
 
+/* Which kernel form gx_scan / gx_scan_sync / gx_scan_streamed use.  No
+ * reference counterpart (the reference has one kernel per query shape).
+ * GX_FORM_AUTO (default) tries, in this order: the warp-tile scan (one warp
+ * per 1024-row tile, no block-wide barriers; LZ4 columns segmented with
+ * segments of at most 1024 rows, no GX_AGG_BUILD), the pipelined scan (a
+ * producer warp staging tiles with bulk copies for 16 consumer warps), the
+ * shared form (one CTA per 2048-row tile) and the queue form (any plan).
+ * Any other value forces that form: plans it cannot run fail with
+ * GX_ERR_INVALID (the queue form accepts what gx_scan accepts, except a
+ * carried value combined with group-key digits).  Every form gives identical
+ * results.  Process-wide setting, for tests and measurements. */
+enum { GX_FORM_AUTO = 0, GX_FORM_WARP = 1, GX_FORM_PIPE = 2, GX_FORM_SHARED = 3, GX_FORM_QUEUE = 4 };
+gx_status gx_scan_set_form(uint32_t form);
+
 /* Streamed scan of a plan whose columns are in pinned host memory
  * (gx_column_to_device with residency 2).  Replaces the reference's load-then-decompress chain
  * for host-resident columns (DataCopy / VarLoader / BatchLoader feeding the
@@ -360,11 +374,12 @@ gx_status gx_scan_check(void* stream);
  * bytes of each group's chunks that survive the plan's min/max predicates
  * are copied host->HBM with cudaMemcpyAsync on an internal copy stream into
  * one of two staging buffers, and the group is scanned from HBM by the
- * pipelined kernel while the next group's bytes are copied.  Pruned chunks
- * are never copied.  Results equal gx_scan's.  keep_chunks_dev is applied by
- * the kernel (chunks it drops are still copied).  HBM-resident columns of
- * the plan are read in place.  Plans the pipelined kernel does not run
- * (GX_AGG_BUILD, queue-only shapes) are rejected with GX_ERR_INVALID.
+ * warp-tile kernel (else the pipelined one; see gx_scan_set_form) while the
+ * next group's bytes are copied.  Pruned chunks are never copied.  Results
+ * equal gx_scan's.  keep_chunks_dev is applied by the kernel (chunks it drops
+ * are still copied).  HBM-resident columns of the plan are read in place.
+ * Plans neither kernel runs (GX_AGG_BUILD, queue-only shapes) are rejected
+ * with GX_ERR_INVALID.
  * Staging memory (two buffers per host column, each the largest group's
  * bytes) comes from the stream-ordered pool and is released on `stream`. */
 gx_status gx_scan_streamed(const gx_scan_plan* plan, uint32_t chunks_per_group, void* stream);
