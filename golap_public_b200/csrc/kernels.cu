@@ -2189,9 +2189,12 @@ static bool lz4_all_direct(const gx_column* c) {
 }
 
 // The warp-tile scan (warp_scan_kernel) for a plan, or *done = false when
-// the plan is not of its shape: HBM-resident (or staged) columns, LZ4 ones
-// segmented with segments of at most kWsTile rows, no BUILD, and the warps'
-// decode buffers within the shared memory of two CTAs per SM.
+// the plan is not of its shape: HBM-resident (or staged) columns sharing the
+// table layout, LZ4 ones segmented with segments of at most kWsTile rows, no
+// BUILD, at most 32768 chunks.  Shared memory per warp: one kWsTile-row area
+// per column (a stage area for raw and all-literal LZ4 columns, a decode
+// buffer for cascaded and other LZ4 columns) and a group table for grouped
+// plans.
 static gx_status scan_launch_warp(const gx_scan_plan* plan, const QueryDesc& qd, const gx_column* c0, cudaStream_t s,
                                   unsigned long long* rows_dev, bool* done, const PipeGroup* grp = nullptr) {
     *done = false;
@@ -2202,7 +2205,8 @@ static gx_status scan_launch_warp(const gx_scan_plan* plan, const QueryDesc& qd,
     std::memset(&P, 0, sizeof(P));
     if (!shared_query(*plan, qd, cols, P.q, &why)) return GX_OK;
     if (cols.size() > kWsMaxCols) return GX_OK;
-    uint32_t nb = 0;
+    uint32_t areas = 0;
+    for (size_t i = 0; i < kWsMaxCols; ++i) P.stage_of[i] = P.buf_of[i] = kWsNone;
     for (size_t i = 0; i < cols.size(); ++i) {
         const gx_column* c = cols[i];
         const uint8_t* staged = nullptr;
@@ -2216,10 +2220,11 @@ static gx_status scan_launch_warp(const gx_scan_plan* plan, const QueryDesc& qd,
             P.cols[i].payload = staged;
             P.cols[i].host_mapped = 0;
         }
-        const bool direct = c->codec == GX_CODEC_NONE || (c->codec == GX_CODEC_LZ4 && lz4_all_direct(c));
-        P.buf_of[i] = direct ? kWsNoBuf : nb++;
+        if (c->codec == GX_CODEC_NONE || (c->codec == GX_CODEC_LZ4 && lz4_all_direct(c)))
+            P.stage_of[i] = areas++;
+        else
+            P.buf_of[i] = areas++;
     }
-    for (size_t i = cols.size(); i < kWsMaxCols; ++i) P.buf_of[i] = kWsNoBuf;
     P.q.keep_in = plan->keep_chunks_dev;
     P.q.keep_out = plan->keep_out_dev;
     P.n_cols = (uint32_t)cols.size();
@@ -2230,17 +2235,20 @@ static gx_status scan_launch_warp(const gx_scan_plan* plan, const QueryDesc& qd,
     P.n_rows = c0->n_rows;
     P.chunk_lo = grp ? grp->chunk_lo : 0u;
     P.chunk_hi = grp ? grp->chunk_hi : c0->n_chunks;
-    P.n_bufs = nb;
+    const uint32_t n_range = P.chunk_hi - P.chunk_lo;
+    P.chunk_words = ((n_range + 31) / 32 + 3) & ~3u;
+    if (P.chunk_words > kWsMaxChunkWords) return GX_OK;
+    P.n_areas = areas;
     P.grouped_tab = P.q.grouped ? 1u : 0u;
-    P.warp_words = 4 * kWsMaxCols + nb * kWsTile + (P.grouped_tab ? 3 * kWsGroupSlots : 0u);
+    P.warp_words = kWsHead + areas * kWsTile + (P.grouped_tab ? kWsTile + 3 * kWsGroupSlots : 0u);
     P.rows_scanned = rows_dev;
-    const size_t smem = 4ull * P.warp_words * kWsWarps;
-    if (smem > kWsMaxDynSmem / 2) return GX_OK;  // fewer than two CTAs (16 warps) per SM: the pipelined form
+    const size_t smem = 4ull * (2ull * P.chunk_words + (size_t)P.warp_words * kWsWarps);
+    if (smem > kWsMaxDynSmem) return GX_OK;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, warp_scan_kernel, kWsNT, smem) != cudaSuccess ||
         per_sm < 1)
         return set_error(GX_ERR_CUDA, "warp scan occupancy query failed");
-    const uint64_t tiles = (uint64_t)(P.chunk_hi - P.chunk_lo) * c0->blocks_per_chunk * P.tiles_per_block;
+    const uint64_t tiles = (uint64_t)n_range * c0->blocks_per_chunk * P.tiles_per_block;
     const uint64_t want = (tiles + kWsWarps - 1) / kWsWarps;
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm, want));
     warp_scan_kernel<<<grid, kWsNT, smem, s>>>(P);

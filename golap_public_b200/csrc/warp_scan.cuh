@@ -31,15 +31,17 @@
 
 constexpr uint32_t kWsLog2 = 10;
 constexpr uint32_t kWsTile = 1u << kWsLog2;    // rows of one warp tile
-constexpr uint32_t kWsNT = 256;                // threads per CTA (8 independent warps)
+constexpr uint32_t kWsNT = 128;                // threads per CTA (4 independent warps)
 constexpr uint32_t kWsWarps = kWsNT / 32;
 constexpr uint32_t kWsBatch = 128;             // rows per evaluation batch (4 per lane)
 constexpr uint32_t kWsMaxCols = kPipeMaxCols;
 constexpr uint32_t kWsGroupLog2 = 7;           // warp group table: 128 slots
 constexpr uint32_t kWsGroupSlots = 1u << kWsGroupLog2;
 constexpr uint32_t kWsGroupProbes = 16;
-constexpr uint32_t kWsNoBuf = 0xFFFFFFFFu;
+constexpr uint32_t kWsNone = 0xFFFFFFFFu;
 constexpr uint32_t kWsMaxDynSmem = 200u << 10;  // dynamic shared memory of one CTA at most
+constexpr uint32_t kWsMaxChunkWords = 1024;     // chunk keep bits of one launch: 32768 chunks
+constexpr uint32_t kWsHead = 36;                // per-warp words before the stage: 8 constant slots, the mbarrier
 static_assert(kWsTile <= kCascPageRows && kCascPageRows % kWsTile == 0, "a warp tile lies in one cascaded page");
 
 struct WsParams {
@@ -49,15 +51,17 @@ struct WsParams {
     uint32_t blocks_per_chunk, rows_per_chunk, rows_per_block, tiles_per_block;
     uint64_t n_rows;                // rows of the table
     uint32_t chunk_lo, chunk_hi;    // chunks [chunk_lo, chunk_hi) are scanned
-    uint32_t buf_of[kWsMaxCols];    // the warp buffer column c decodes into, or kWsNoBuf (always read in place)
-    uint32_t n_bufs;                // decode buffers per warp (kWsTile words each)
+    uint32_t stage_of[kWsMaxCols];  // stage area column c is copied into (raw / aligned-literal LZ4), or kWsNone
+    uint32_t buf_of[kWsMaxCols];    // decode buffer of column c (cascaded / LZ4 with matches), or kWsNone
+    uint32_t n_areas;               // stage areas + decode buffers per warp (kWsTile words each)
     uint32_t warp_words;            // shared memory words per warp
+    uint32_t chunk_words;           // words of the chunk keep bitmap (and of its prefix counts)
     uint32_t grouped_tab;           // 1: the warp has a group table
     unsigned long long* rows_scanned;
 };
 
 // Column read modes of one tile.
-enum : uint32_t { kWmDirect = 0, kWmConst = 1, kWmLz4 = 2, kWmCasc = 3, kWmBad = 4 };
+enum : uint32_t { kWmStage = 0, kWmConst = 1, kWmLz4 = 2, kWmCasc = 3, kWmBad = 4 };
 
 __device__ __forceinline__ uint64_t ws_shfl64(uint64_t v, uint32_t src) {
     return ((uint64_t)__shfl_sync(0xFFFFFFFFu, (uint32_t)(v >> 32), src) << 32) |
@@ -160,23 +164,23 @@ __device__ __noinline__ int ws_casc_rows(const uint8_t* __restrict__ pg, uint32_
 }
 
 // The warp's per-segment LZ4 decode of a tile: segments j0 .. j0+nseg-1 of
-// the block into out (segment t at out + t * seg_rows), G lanes per segment.
-// Returns 0 or kErrCorrupt (uniform).
-__device__ __noinline__ int ws_lz4_rows(const gx_dcol& c, uint32_t slot, uint64_t blk_off, uint32_t blk_bytes,
+// the block that starts at address blk (blk_bytes compressed bytes; side
+// index entries e) into out (segment t at out + t * seg_rows), G lanes per
+// segment.  Returns 0 or kErrCorrupt (uniform).
+__device__ __noinline__ int ws_lz4_rows(const uint8_t* blk, uint32_t blk_bytes, const uint32_t* e, uint32_t seg_shift,
                                         uint32_t rows, uint32_t r0, uint32_t n, uint32_t lo, uint32_t hi,
                                         uint32_t* out, uint32_t lane) {
-    const uint32_t seg_rows = 1u << c.seg_shift;
-    const uint32_t j0 = r0 >> c.seg_shift, nseg = (n + seg_rows - 1) >> c.seg_shift;
-    const uint64_t abs_wb = (blk_off + lo) & ~15ull;
-    const uint32_t* A = (const uint32_t*)(c.payload + abs_wb);
-    const uint32_t wbase = (uint32_t)(abs_wb - blk_off);
-    const uint32_t* e = c.seg + (size_t)2 * c.S * slot;
-    uint32_t glog = seg_group_log2(nseg, 32);
+    const uint32_t seg_rows = 1u << seg_shift;
+    const uint32_t j0 = r0 >> seg_shift, nseg = (n + seg_rows - 1) >> seg_shift;
+    // payload addresses keep the payload offsets' alignment modulo 16
+    const uintptr_t a_wb = ((uintptr_t)blk + lo) & ~(uintptr_t)15;
+    const uint32_t* A = (const uint32_t*)a_wb;
+    const uint32_t wbase = (uint32_t)(a_wb - (uintptr_t)blk);
+    const uint32_t glog = seg_group_log2(nseg, 32);
     const uint32_t G = 1u << glog;
     const uint32_t gl = lane & (G - 1u);
     const uint32_t gmask = G >= 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (lane & ~(G - 1u)));
     int err = 0;
-    // all groups run the same number of rounds (the shuffles inside stay converged per group)
     for (uint32_t t0 = 0; t0 < nseg; t0 += (32u >> glog)) {
         const uint32_t t = t0 + (lane >> glog);
         if (t < nseg) {
@@ -210,322 +214,558 @@ __device__ __noinline__ void ws_group_add(uint32_t gk, int64_t val, uint32_t* tk
     if (!group_add_global(keys, sums, log2cap, (int64_t)gk, val)) raise_error(kErrCapacity);
 }
 
-__global__ void __launch_bounds__(kWsNT, 2) warp_scan_kernel(const __grid_constant__ WsParams P) {
+// Position of the k-th set bit of m (k < popc(m)).
+__device__ __forceinline__ uint32_t ws_select(uint32_t m, uint32_t k) {
+    uint32_t pos = 0;
+#pragma unroll
+    for (uint32_t width = 16; width >= 1; width >>= 1) {
+        const uint32_t low = __popc(m & ((1u << width) - 1u));
+        if (k >= low) {
+            k -= low;
+            m >>= width;
+            pos += width;
+        }
+    }
+    return pos;
+}
+
+// One row tile: block slot, first row in the block, rows, block rows, and
+// the rows [a, b) of the tile inside the query's row slice.
+struct WsTile {
+    uint32_t slot, r0, n, rows, a, b;
+};
+
+// How one column of one tile is read.
+struct WsCol {
+    uint32_t mode;        // kWm*
+    const uint8_t* src;   // stage: the rows; LZ4: the block; cascaded: the page
+    uint32_t aux0, aux1;  // LZ4: [lo, hi) in the block; cascaded: page bytes, page rows
+    uint32_t bytes;       // stage: bytes copied; LZ4: the block's compressed bytes
+    int32_t cval;         // kWmConst: the value
+};
+
+// Rank-space tile t (t-th tile of the surviving chunks, chunk-major) ->
+// its tile; false when t is past the end or the tile has no rows of the
+// query's slice.
+__device__ __forceinline__ bool ws_locate(const WsParams& P, const uint32_t* s_kbits, const uint32_t* s_kpre,
+                                          uint64_t t, uint64_t t_end, WsTile& T) {
+    if (t >= t_end) return false;
+    const uint32_t tpb = P.tiles_per_block, bpc = P.blocks_per_chunk;
+    const uint64_t PC = (uint64_t)bpc * tpb;
+    const uint32_t k = (uint32_t)(t / PC), loc = (uint32_t)(t % PC);
+    uint32_t lo = 0, hi = P.chunk_words - 1;  // the bitmap word holding the k-th surviving chunk
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (s_kpre[mid] <= k) lo = mid; else hi = mid - 1;
+    }
+    const uint32_t chunk = P.chunk_lo + lo * 32 + ws_select(s_kbits[lo], k - s_kpre[lo]);
+    const uint32_t jb = loc / tpb, tile = loc % tpb;
+    const uint64_t c_r0 = (uint64_t)chunk * P.rows_per_chunk;
+    const uint64_t c_rows = min((uint64_t)P.rows_per_chunk, P.n_rows - c_r0);
+    const uint64_t jrow = (uint64_t)jb * P.rows_per_block;
+    T.rows = jrow < c_rows ? (uint32_t)min((uint64_t)P.rows_per_block, c_rows - jrow) : 0u;
+    T.r0 = tile * kWsTile;
+    T.slot = chunk * bpc + jb;
+    if (T.r0 >= T.rows) return false;
+    T.n = min(kWsTile, T.rows - T.r0);
+    const uint64_t g0 = c_r0 + jrow + T.r0;
+    const ShQuery& Q = P.q;
+    T.a = Q.row_lo > g0 ? (uint32_t)min((uint64_t)T.n, Q.row_lo - g0) : 0u;
+    T.b = Q.row_hi > g0 ? (uint32_t)min((uint64_t)T.n, Q.row_hi - g0) : 0u;
+    return T.a < T.b;
+}
+
+// Column c's read decision for tile T (directory entry, side-index
+// entries, a cascaded page's header: a single-run page needs no decode).
+__device__ __noinline__ WsCol ws_column(const WsParams& P, const gx_dcol& col, uint32_t c, const WsTile& T) {
+    WsCol C;
+    C.mode = kWmBad;
+    C.src = nullptr;
+    C.aux0 = C.aux1 = C.bytes = 0;
+    C.cval = 0;
+    const uint32_t slot = T.slot, r0 = T.r0, n = T.n, rows = T.rows;
+    const uint4 dw = __ldg((const uint4*)(col.blocks + slot));
+    const uint64_t d_off = ((uint64_t)dw.y << 32) | dw.x;
+    const uint32_t d_bytes = dw.z, d_rows = dw.w;
+    const bool dir_ok =
+        d_rows == rows && d_off <= col.payload_bytes && (uint64_t)d_bytes + 32 <= col.payload_bytes - d_off;
+    const uint8_t* blk = col.payload + d_off;
+    if (col.codec == GX_CODEC_NONE) {
+        if (dir_ok && d_bytes == rows * 4 && (d_off & 15u) == 0 && P.stage_of[c] != kWsNone) {
+            C.mode = kWmStage;
+            C.src = blk + 4ull * r0;
+            C.bytes = (4 * n + 15u) & ~15u;
+        }
+    } else if (col.codec == GX_CODEC_LZ4) {
+        const uint32_t sr = 1u << col.seg_shift;
+        const uint32_t j0 = r0 >> col.seg_shift, nseg = (n + sr - 1) >> col.seg_shift;
+        if ((r0 & (sr - 1u)) == 0 && j0 + nseg <= col.S) {
+            const uint32_t* e = col.seg + (size_t)2 * col.S * slot;
+            const uint32_t e0 = __ldg(e + 2 * j0), e1 = __ldg(e + 2 * j0 + 1);
+            const uint32_t e2 = j0 + nseg < col.S ? __ldg(e + 2 * (j0 + nseg)) : 0u;
+            const uint32_t hi = j0 + nseg < col.S ? e2 : d_bytes;
+            if (dir_ok && e0 <= hi && hi <= d_bytes) {
+                const bool lit = (e1 & 16u) && (e1 >> 5) >= 4 * n && hi - e0 == 4 * n;
+                if (lit && ((d_off + e0) & 15u) == 0 && P.stage_of[c] != kWsNone) {
+                    C.mode = kWmStage;
+                    C.src = blk + e0;
+                    C.bytes = (4 * n + 15u) & ~15u;
+                } else if (P.buf_of[c] != kWsNone) {
+                    C.mode = kWmLz4;
+                    C.src = blk;
+                    C.aux0 = e0;
+                    C.aux1 = hi;
+                    C.bytes = d_bytes;
+                }
+            }
+        }
+    } else if (col.codec == GX_CODEC_CASCADED) {
+        const uint32_t page = r0 >> kCascPageLog2;
+        if (page < col.S && P.buf_of[c] != kWsNone) {
+            const uint32_t* e = col.seg + (size_t)2 * col.S * slot + 2 * page;
+            const uint32_t po = __ldg(e), pb = __ldg(e + 1);
+            if (dir_ok && (d_off & 15u) == 0 && (po & 15u) == 0 && (uint64_t)po + pb <= d_bytes && pb >= 32) {
+                const uint8_t* pg = blk + po;
+                C.mode = kWmCasc;
+                C.src = pg;
+                C.aux0 = pb;
+                C.aux1 = min(kCascPageRows, rows - page * kCascPageRows);
+                // pages that hold one value need no decode: zero-width values
+                // without RLE (with DELTA: zero steps), or one run of the whole page
+                const casc_hdr h = casc_load_header(pg);
+                if (casc_header_ok(h, pb, C.aux1) && h.val_bits == 0) {
+                    const bool rle = (h.flags & CASC_RLE) != 0, delta = (h.flags & CASC_DELTA) != 0;
+                    const bool one = rle ? (h.n_runs == 1 && h.len_bits == 0 && h.len_base == C.aux1)
+                                         : (!delta || h.val_base == 0);
+                    if (one) {
+                        C.mode = kWmConst;
+                        C.cval = delta ? h.first : h.val_base;
+                    }
+                }
+            }
+        }
+    }
+    return C;
+}
+
+// Decisions for the four tiles t0 + q*W (q = 0..3) at once: lane 8q + c
+// decides column c of tile q (and checks prune predicate c's zone map), so
+// the four tiles cost one round of dependent loads.  Returns the mask of
+// the tiles to scan; every lane of group q holds tile q in T.
+__device__ __forceinline__ uint32_t ws_decide(const WsParams& P, const gx_dcol* s_cols, const uint32_t* s_kbits,
+                                              const uint32_t* s_kpre, uint64_t t0, uint64_t W, uint64_t t_end,
+                                              uint32_t lane, WsTile& T, WsCol& C) {
+    const ShQuery& Q = P.q;
+    const uint32_t q = lane >> 3, c = lane & 7;
+    const bool ok = ws_locate(P, s_kbits, s_kpre, t0 + q * W, t_end, T);
+    bool zfail = false;
+    if (ok && c < Q.n_prune) {
+        const PrunePred& pr = Q.prune[c];
+        if (pr.bmins) zfail = !(pr.lo <= __ldg(pr.bmaxs + T.slot) && pr.hi >= __ldg(pr.bmins + T.slot));
+    }
+    C.mode = kWmBad;
+    if (ok && c < P.n_cols) C = ws_column(P, s_cols[c], c, T);
+    const uint32_t oks = __ballot_sync(0xFFFFFFFFu, ok), fails = __ballot_sync(0xFFFFFFFFu, zfail);
+    uint32_t vm = 0;
+#pragma unroll
+    for (uint32_t g = 0; g < 4; ++g)
+        if (((oks >> (8 * g)) & 1u) && ((fails >> (8 * g)) & 0xFFu) == 0) vm |= 1u << g;
+    return vm;
+}
+
+// L2 prefetch of the directory and side-index lines of the four tiles
+// t0 + q*W (lane 8q + c: column c), so that their decisions read L2.
+__device__ __forceinline__ void ws_prefetch_meta(const WsParams& P, const gx_dcol* s_cols, const uint32_t* s_kbits,
+                                                 const uint32_t* s_kpre, uint64_t t0, uint64_t W, uint64_t t_end,
+                                                 uint32_t lane) {
+    const uint32_t q = lane >> 3, c = lane & 7;
+    WsTile T;
+    if (c >= P.n_cols || !ws_locate(P, s_kbits, s_kpre, t0 + q * W, t_end, T)) return;
+    const gx_dcol& col = s_cols[c];
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(col.blocks + T.slot));
+    if (col.codec == GX_CODEC_LZ4)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(col.seg + (size_t)2 * col.S * T.slot + 2 * (T.r0 >> col.seg_shift)));
+    else if (col.codec == GX_CODEC_CASCADED)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(col.seg + (size_t)2 * col.S * T.slot + 2 * (T.r0 >> kCascPageLog2)));
+}
+
+__device__ __forceinline__ void ws_bulk_prefetch_l2(const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
+// A step over a column that holds one value v on the whole tile: decided
+// once.  Returns true when the tile's rows are all dropped; else multiplies
+// in the group-key digit of every kept row.
+__device__ __noinline__ bool ws_step_const(const ShStep& stp, int32_t v, uint32_t keep, uint32_t* gkb, bool grouped,
+                                           uint32_t lane) {
+    const uint32_t flags = stp.flags, dcard = stp.digit_card;
+    bool f = !(flags & GX_STEP_FILTER) || (v >= stp.lo && v <= stp.hi);
+    int32_t pp = v;
+    if (f && (flags & GX_STEP_PROBE)) f = sh_probe(stp.ht, stp.ht_log2, stp.ht_layout, v, &pp);
+    if (!f) return true;
+    if (dcard && grouped) {
+        const uint32_t dgt = (uint32_t)(pp - stp.digit_base);
+        if (dgt >= dcard) {
+            if (lane == 0) raise_error(kErrInvalid);
+            return true;
+        }
+#pragma unroll 1
+        for (uint32_t j = 0; j < 8; ++j) {
+            if (!((keep >> (4 * j)) & 15u)) continue;
+            uint4* g = (uint4*)(gkb + 128 * j + 4 * lane);
+            uint4 x = *g;
+            x.x = x.x * dcard + dgt;
+            x.y = x.y * dcard + dgt;
+            x.z = x.z * dcard + dgt;
+            x.w = x.w * dcard + dgt;
+            *g = x;
+        }
+    }
+    return false;
+}
+
+// A filter / probe / digit step over the tile's rows of a column at `col`
+// (shared memory, kWsTile rows).  Probes issue the first-slot reads of a
+// row group's distinct keys together and reuse the lane's last result for a
+// repeated key.  Returns the new keep bits.
+__device__ __noinline__ uint32_t ws_step_rows(const ShStep& stp, const uint8_t* col, uint32_t keep, uint32_t* gkb,
+                                              bool grouped, uint32_t lane) {
+    const uint32_t flags = stp.flags, dcard = stp.digit_card;
+    const int32_t lo = stp.lo, hi = stp.hi, dbase = stp.digit_base;
+    const bool filt = (flags & GX_STEP_FILTER) != 0, probe = (flags & GX_STEP_PROBE) != 0;
+    const uint64_t* const ht = stp.ht;
+    const uint32_t htlog = stp.ht_log2, htlay = stp.ht_layout;
+    const bool dense = htlay == GX_HT_DENSE, bucket = htlay == GX_HT_BUCKET;
+    uint32_t hbase = 0, hspan = 0;
+    if (probe && dense) {
+        const uint64_t hdr = __ldg((const unsigned long long*)ht);
+        hbase = (uint32_t)hdr;
+        hspan = (uint32_t)(hdr >> 32);
+    }
+    int32_t mv = 0, mp = 0;  // the lane's last probed key and its result
+    bool mhave = false, mf = false;
+#pragma unroll 1
+    for (uint32_t j = 0; j < 8; ++j) {
+        uint32_t kk = (keep >> (4 * j)) & 15u;
+        if (!kk) continue;
+        const uint4 w4 = *(const uint4*)(col + (128 * j + 4 * lane) * 4);
+        const int32_t v[4] = {(int32_t)w4.x, (int32_t)w4.y, (int32_t)w4.z, (int32_t)w4.w};
+        if (filt) {
+#pragma unroll
+            for (uint32_t i = 0; i < 4; ++i)
+                if (!(v[i] >= lo && v[i] <= hi)) kk &= ~(1u << i);
+        }
+        int32_t pp[4] = {v[0], v[1], v[2], v[3]};
+        if (probe && kk) {
+            uint64_t ee[4];
+            uint32_t rd = 0;
+#pragma unroll
+            for (uint32_t i = 0; i < 4; ++i) {
+                const bool again =
+                    (i > 0 && v[i] == v[i - 1] && ((kk >> (i - 1)) & 1u)) || (mhave && v[i] == mv);
+                const uint32_t u = (uint32_t)v[i] - hbase;
+                const bool r = ((kk >> i) & 1u) && !again && !bucket && v[i] != kEmptyKey && (!dense || u < hspan);
+                const unsigned long long* sl = (const unsigned long long*)ht + (dense ? 1 + u : hash_key32(v[i], htlog));
+                ee[i] = r ? __ldg(sl) : (unsigned long long)kEmptySlot;
+                rd |= r ? 1u << i : 0u;
+            }
+#pragma unroll
+            for (uint32_t i = 0; i < 4; ++i) {
+                if (!((kk >> i) & 1u)) continue;
+                bool f;
+                int32_t p = v[i];
+                if (mhave && v[i] == mv) {
+                    f = mf;
+                    p = mp;
+                } else if ((rd >> i) & 1u) {
+                    const int32_t ek = (int32_t)(uint32_t)ee[i];
+                    if (ek == v[i]) {
+                        f = true;
+                        p = (int32_t)(uint32_t)(ee[i] >> 32);
+                    } else if (dense || ek == kEmptyKey) {
+                        f = false;
+                    } else {
+                        f = sh_probe(ht, htlog, htlay, v[i], &p);
+                    }
+                } else {
+                    // bucket tables, keys the memo held when the reads were issued,
+                    // the reserved key, keys outside a dense range
+                    f = sh_probe(ht, htlog, htlay, v[i], &p);
+                }
+                mhave = true;
+                mv = v[i];
+                mf = f;
+                mp = p;
+                pp[i] = p;
+                if (!f) kk &= ~(1u << i);
+            }
+        }
+        if (dcard && grouped && kk) {
+            uint4* g = (uint4*)(gkb + 128 * j + 4 * lane);
+            const uint4 x = *g;
+            uint32_t xg[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+            for (uint32_t i = 0; i < 4; ++i) {
+                if (!((kk >> i) & 1u)) continue;
+                const uint32_t dgt = (uint32_t)(pp[i] - dbase);
+                if (dgt >= dcard) {
+                    raise_error(kErrInvalid);
+                    kk &= ~(1u << i);
+                } else {
+                    xg[i] = xg[i] * dcard + dgt;
+                }
+            }
+            *g = make_uint4(xg[0], xg[1], xg[2], xg[3]);
+        }
+        keep = (keep & ~(15u << (4 * j))) | (kk << (4 * j));
+    }
+    return keep;
+}
+
+// The aggregate over the kept rows of the tile: the value column at `col`
+// (mask 0: one value), the carried column at `ccol`.  Returns the scalar
+// part; grouped sums go to the warp's group table.
+__device__ __noinline__ int64_t ws_aggregate(uint32_t agg, bool grouped, bool carried, const uint8_t* col, uint32_t msk,
+                                             const uint8_t* ccol, uint32_t cmask, uint32_t keep, const uint32_t* gkb,
+                                             uint32_t* tkey, unsigned long long* tsum, int64_t* g_keys,
+                                             int64_t* g_sums, uint32_t g_log2, uint32_t lane) {
+    if (!grouped && agg == GX_AGG_COUNT) return __popc(keep);
+    if (!grouped && agg == GX_AGG_SUM && msk == 0) return (int64_t)__popc(keep) * *(const int32_t*)col;
+    int64_t acc = 0;
+#pragma unroll 1
+    for (uint32_t j = 0; j < 8; ++j) {
+        const uint32_t kk = (keep >> (4 * j)) & 15u;
+        if (!kk) continue;
+        const uint32_t ro = (128 * j + 4 * lane) * 4;
+        const uint4 w4 = *(const uint4*)(col + (ro & msk));
+        const uint4 cw = carried ? *(const uint4*)(ccol + (ro & cmask)) : make_uint4(0, 0, 0, 0);
+        const int32_t v[4] = {(int32_t)w4.x, (int32_t)w4.y, (int32_t)w4.z, (int32_t)w4.w};
+        const int32_t cv[4] = {(int32_t)cw.x, (int32_t)cw.y, (int32_t)cw.z, (int32_t)cw.w};
+        if (!grouped) {
+            if (agg == GX_AGG_SUM_PRODUCT) {
+#pragma unroll
+                for (uint32_t i = 0; i < 4; ++i) acc += ((kk >> i) & 1u) ? (int64_t)v[i] * cv[i] : 0;
+            } else if (agg == GX_AGG_SUM_DIFF) {
+#pragma unroll
+                for (uint32_t i = 0; i < 4; ++i) acc += ((kk >> i) & 1u) ? (int64_t)v[i] - cv[i] : 0;
+            } else {
+#pragma unroll
+                for (uint32_t i = 0; i < 4; ++i) acc += ((kk >> i) & 1u) ? (int64_t)v[i] : 0;
+            }
+        } else {
+            const uint4 gw = *(const uint4*)(gkb + 128 * j + 4 * lane);
+            const uint32_t g[4] = {gw.x, gw.y, gw.z, gw.w};
+#pragma unroll
+            for (uint32_t i = 0; i < 4; ++i) {
+                if (!((kk >> i) & 1u)) continue;
+                const int64_t val = agg == GX_AGG_SUM_PRODUCT ? (int64_t)v[i] * cv[i]
+                                    : agg == GX_AGG_SUM_DIFF  ? (int64_t)v[i] - cv[i]
+                                    : agg == GX_AGG_COUNT      ? 1
+                                                               : (int64_t)v[i];
+                ws_group_add(g[i], val, tkey, tsum, g_keys, g_sums, g_log2);
+            }
+        }
+    }
+    return acc;
+}
+
+__global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_constant__ WsParams P) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ gx_dcol s_cols[kWsMaxCols];
+    __shared__ uint32_t s_nsurv;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t ncols = P.n_cols;
-    if (tid < ncols * (sizeof(gx_dcol) / 4))
-        ((uint32_t*)s_cols)[tid] = ((const uint32_t*)P.cols)[tid];
-    __syncthreads();  // the only block-wide barrier: the column table is read-only from here on
-
-    uint32_t* const wmem = (uint32_t*)smem + (size_t)warp * P.warp_words;
-    uint4* const cslot = (uint4*)wmem;                       // kWsMaxCols broadcast slots (constant columns)
-    uint32_t* const bufs = wmem + 4 * kWsMaxCols;            // n_bufs x kWsTile words
-    uint32_t* const tkey = bufs + (size_t)P.n_bufs * kWsTile;  // group table: keys, then sums (8-byte aligned)
+    const ShQuery& Q = P.q;
+    uint32_t* const s_kbits = (uint32_t*)smem;               // chunk keep bits of [chunk_lo, chunk_hi)
+    uint32_t* const s_kpre = s_kbits + P.chunk_words;        // surviving chunks before each word
+    uint32_t* const wmem = s_kpre + P.chunk_words + (size_t)warp * P.warp_words;
+    uint4* const cslot = (uint4*)wmem;                       // constant columns (4 copies of the value)
+    uint64_t* const bar = (uint64_t*)(wmem + 4 * kWsMaxCols);  // the warp's stage mbarrier
+    uint32_t* const areas = wmem + kWsHead;                  // n_areas x kWsTile words
+    uint32_t* const gkb = areas + (size_t)P.n_areas * kWsTile;  // grouped: group key of each row of the tile
+    uint32_t* const tkey = gkb + kWsTile;                    // grouped: group table keys, then sums
     unsigned long long* const tsum = (unsigned long long*)(tkey + kWsGroupSlots);
+
+    for (uint32_t i = tid; i < ncols * (uint32_t)(sizeof(gx_dcol) / 4); i += kWsNT)
+        ((uint32_t*)s_cols)[i] = ((const uint32_t*)P.cols)[i];
+    // chunk keep (keep_in and the prune predicates' chunk min/max, the
+    // reference's granularity), one ballot word per 32 chunks; CTA 0 writes keep_out
+    const uint32_t n_range = P.chunk_hi - P.chunk_lo;
+    for (uint32_t wb = warp * 32; wb < P.chunk_words * 32; wb += kWsNT) {
+        const uint32_t i = wb + lane, chunk = P.chunk_lo + i;
+        bool ck = i < n_range;
+        if (ck) {
+            if (Q.keep_in) ck = __ldg(Q.keep_in + chunk) != 0;
+            for (uint32_t p = 0; p < Q.n_prune; ++p) {
+                const PrunePred& pr = Q.prune[p];
+                ck = ck && pr.lo <= __ldg(pr.maxs + chunk) && pr.hi >= __ldg(pr.mins + chunk);
+            }
+            if (blockIdx.x == 0 && Q.keep_out) Q.keep_out[chunk] = ck ? 1 : 0;
+        }
+        const uint32_t word = __ballot_sync(0xFFFFFFFFu, ck);
+        if (lane == 0) s_kbits[wb / 32] = word;
+    }
+    if (lane == 0) mbar_init(bar, 1);
     if (P.grouped_tab) {
         for (uint32_t i = lane; i < kWsGroupSlots; i += 32) {
             tkey[i] = kEmptyGKey;
             tsum[i] = 0;
         }
     }
-    __syncwarp();
+    __syncthreads();
+    if (warp == 0) {  // exclusive prefix of the popcounts: per lane a run of words, then a warp scan
+        const uint32_t per = (P.chunk_words + 31) / 32, w0 = min(P.chunk_words, lane * per),
+                       w1 = min(P.chunk_words, w0 + per);
+        uint32_t cnt = 0;
+        for (uint32_t i = w0; i < w1; ++i) cnt += __popc(s_kbits[i]);
+        uint32_t run = ws_scan(cnt, lane) - cnt;
+        for (uint32_t i = w0; i < w1; ++i) {
+            s_kpre[i] = run;
+            run += __popc(s_kbits[i]);
+        }
+        if (lane == 31) s_nsurv = run;
+    }
+    __syncthreads();  // the last block-wide barrier: warps are independent from here on
 
-    const ShQuery& Q = P.q;
+    const uint64_t PC = (uint64_t)P.blocks_per_chunk * P.tiles_per_block;
+    const uint64_t t_end = (uint64_t)s_nsurv * PC;
     const uint32_t ns = Q.n_steps, agg = Q.agg;
     const bool grouped = Q.grouped != 0;
-    const uint32_t tpb = P.tiles_per_block, bpc = P.blocks_per_chunk;
-    const uint64_t PC = (uint64_t)bpc * tpb;  // tiles per chunk
-    const uint64_t t_begin = (uint64_t)P.chunk_lo * PC, t_end = (uint64_t)P.chunk_hi * PC;
     const uint64_t W = (uint64_t)gridDim.x * kWsWarps;
     int64_t local = 0;
     unsigned long long local_rows = 0;
-
-    for (uint64_t w = t_begin + (uint64_t)blockIdx.x * kWsWarps + warp; w < t_end; w += W) {
-        const uint32_t chunk = (uint32_t)(w / PC), loc = (uint32_t)(w % PC);
-        const uint32_t jb = loc / tpb, tile = loc % tpb;
-        const uint32_t slot = chunk * bpc + jb;
-        const uint64_t c_r0 = (uint64_t)chunk * P.rows_per_chunk;
-        const uint64_t c_rows = min((uint64_t)P.rows_per_chunk, P.n_rows - c_r0);
-        const uint64_t jrow = (uint64_t)jb * P.rows_per_block;
-        const uint32_t rows = jrow < c_rows ? (uint32_t)min((uint64_t)P.rows_per_block, c_rows - jrow) : 0u;
-        const uint32_t r0 = tile * kWsTile;
-        // chunk keep (keep_in and the prune predicates' chunk min/max); the
-        // warp of the chunk's first tile publishes it
-        bool ck = Q.keep_in ? __ldg(Q.keep_in + chunk) != 0 : true;
-        for (uint32_t p = 0; p < Q.n_prune; ++p) {
-            const PrunePred& pr = Q.prune[p];
-            ck = ck && pr.lo <= __ldg(pr.maxs + chunk) && pr.hi >= __ldg(pr.mins + chunk);
-        }
-        if (loc == 0 && lane == 0 && Q.keep_out) Q.keep_out[chunk] = ck ? 1 : 0;
-        if (!ck || r0 >= rows) continue;
-        const uint32_t n = min(kWsTile, rows - r0);
-        const uint64_t g0 = c_r0 + jrow + r0;
-        const uint32_t a = Q.row_lo > g0 ? (uint32_t)min((uint64_t)n, Q.row_lo - g0) : 0u;
-        const uint32_t b = Q.row_hi > g0 ? (uint32_t)min((uint64_t)n, Q.row_hi - g0) : 0u;
-        if (a >= b) continue;
-        bool zk = true;
-        for (uint32_t p = 0; p < Q.n_prune; ++p) {
-            const PrunePred& pr = Q.prune[p];
-            if (pr.bmins) zk = zk && pr.lo <= __ldg(pr.bmaxs + slot) && pr.hi >= __ldg(pr.bmins + slot);
-        }
-        if (!zk) continue;
-
-        // ---- columns: lane c decides how column c is read
-        uint32_t mode = kWmBad;
-        const uint8_t* cptr = nullptr;   // direct: the tile's first row; casc: the page
-        uint32_t aux0 = 0, aux1 = 0;     // LZ4: [lo, hi); casc: page bytes, page rows
-        uint64_t blk_off = 0;
-        uint32_t blk_bytes = 0;
-        if (lane < ncols) {
-            const gx_dcol& col = s_cols[lane];
-            const uint4 dw = __ldg((const uint4*)(col.blocks + slot));
-            const uint64_t d_off = ((uint64_t)dw.y << 32) | dw.x;
-            const uint32_t d_bytes = dw.z, d_rows = dw.w;
-            blk_off = d_off;
-            blk_bytes = d_bytes;
-            const bool dir_ok = d_rows == rows && d_off <= col.payload_bytes &&
-                                (uint64_t)d_bytes + 32 <= col.payload_bytes - d_off;
-            if (dir_ok && col.codec == GX_CODEC_NONE) {
-                if (d_bytes == rows * 4 && (d_off & 15u) == 0) {
-                    mode = kWmDirect;
-                    cptr = col.payload + d_off + 4ull * r0;
-                }
-            } else if (dir_ok && col.codec == GX_CODEC_LZ4) {
-                const uint32_t sr = 1u << col.seg_shift;
-                const uint32_t j0 = r0 >> col.seg_shift, nseg = (n + sr - 1) >> col.seg_shift;
-                if ((r0 & (sr - 1u)) == 0 && j0 + nseg <= col.S) {
-                    const uint32_t* e = col.seg + (size_t)2 * col.S * slot;
-                    const uint32_t e0 = __ldg(e + 2 * j0), e1 = __ldg(e + 2 * j0 + 1);
-                    const uint32_t hi = j0 + nseg < col.S ? __ldg(e + 2 * (j0 + nseg)) : d_bytes;
-                    if (e0 <= hi && hi <= d_bytes) {
-                        const bool lit = (e1 & 16u) && (e1 >> 5) >= 4 * n && hi - e0 == 4 * n;
-                        if (lit && ((d_off + e0) & 15u) == 0) {
-                            mode = kWmDirect;
-                            cptr = col.payload + d_off + e0;
-                        } else if (P.buf_of[lane] != kWsNoBuf) {
-                            mode = kWmLz4;
-                            aux0 = e0;
-                            aux1 = hi;
-                        }
-                    }
-                }
-            } else if (dir_ok && col.codec == GX_CODEC_CASCADED) {
-                const uint32_t page = r0 >> kCascPageLog2;
-                const uint32_t* e = col.seg + (size_t)2 * col.S * slot + 2 * page;
-                const uint32_t po = __ldg(e), pb = __ldg(e + 1);
-                if ((po & 15u) == 0 && (uint64_t)po + pb <= d_bytes && (d_off & 15u) == 0 &&
-                    P.buf_of[lane] != kWsNoBuf && page < col.S) {
-                    mode = kWmCasc;
-                    cptr = col.payload + d_off + po;
-                    aux0 = pb;
-                    aux1 = min(kCascPageRows, rows - page * kCascPageRows);
-                }
+    uint32_t ph = 0;
+    bool stop = false;
+    for (uint64_t t0 = (uint64_t)blockIdx.x * kWsWarps + warp; t0 < t_end && !stop; t0 += 4 * W) {
+        WsTile T;
+        WsCol C;
+        const uint32_t vm = ws_decide(P, s_cols, s_kbits, s_kpre, t0, W, t_end, lane, T, C);
+        ws_prefetch_meta(P, s_cols, s_kbits, s_kpre, t0 + 4 * W, W, t_end, lane);
+        // the staged ranges of every tile of the four go to L2 now
+        if (((vm >> (lane >> 3)) & 1u) && (lane & 7) < ncols && C.mode == kWmStage) ws_bulk_prefetch_l2(C.src, C.bytes);
+        for (uint32_t q = 0; q < 4 && !stop; ++q) {
+            if (!((vm >> q) & 1u)) continue;
+            const uint32_t L0 = 8 * q, Lc = 8 * q + (lane & 7);
+            const uint32_t slot = __shfl_sync(0xFFFFFFFFu, T.slot, L0), r0 = __shfl_sync(0xFFFFFFFFu, T.r0, L0);
+            const uint32_t n = __shfl_sync(0xFFFFFFFFu, T.n, L0), rows = __shfl_sync(0xFFFFFFFFu, T.rows, L0);
+            const uint32_t a = __shfl_sync(0xFFFFFFFFu, T.a, L0), b = __shfl_sync(0xFFFFFFFFu, T.b, L0);
+            // lane c (< ncols): column c of this tile
+            const uint32_t mode = __shfl_sync(0xFFFFFFFFu, C.mode, Lc);
+            const uint8_t* src = (const uint8_t*)ws_shfl64((uint64_t)C.src, Lc);
+            const uint32_t aux0 = __shfl_sync(0xFFFFFFFFu, C.aux0, Lc), aux1 = __shfl_sync(0xFFFFFFFFu, C.aux1, Lc);
+            const uint32_t cbytes = __shfl_sync(0xFFFFFFFFu, C.bytes, Lc);
+            const int32_t cval = (int32_t)__shfl_sync(0xFFFFFFFFu, (uint32_t)C.cval, Lc);
+            const bool mine = lane < ncols;
+            // ---- stage copies (one bulk copy per in-place column)
+            const uint32_t my = (mine && mode == kWmStage) ? cbytes : 0u;
+            const uint32_t total = __reduce_add_sync(0xFFFFFFFFu, my);
+            if (total) {
+                if (lane == 0) mbar_expect_tx_arrive(bar, total);
+                __syncwarp();
+                if (my) bulk_copy_1d(areas + (size_t)P.stage_of[lane] * kWsTile, src, my, bar);
             }
-            // in-place rows go to L2 now; the batches read them from there
-        }
-        if (__any_sync(0xFFFFFFFFu, lane < ncols && mode == kWmBad)) {
-            if (lane == 0) raise_error(kErrCorrupt);
-            continue;
-        }
-        for (uint32_t c = 0; c < ncols; ++c) {
-            const uint32_t m = __shfl_sync(0xFFFFFFFFu, mode, c);
-            if (m != kWmDirect) continue;
-            const uint8_t* p = (const uint8_t*)ws_shfl64((uint64_t)cptr, c);
-            if (lane * 128 < 4 * n) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + lane * 128));
-        }
-        // decodes (one column at a time, the whole warp)
-        int terr = 0;
-        const uint8_t* rptr = cptr;  // lane c: where column c's rows are read
-        uint32_t rmask = 0xFFFFFFFFu;
-        for (uint32_t c = 0; c < ncols && !terr; ++c) {
-            const uint32_t m = __shfl_sync(0xFFFFFFFFu, mode, c);
-            if (m == kWmDirect) continue;
-            uint32_t* buf = bufs + (size_t)P.buf_of[c] * kWsTile;
-            const uint32_t x0 = __shfl_sync(0xFFFFFFFFu, aux0, c), x1 = __shfl_sync(0xFFFFFFFFu, aux1, c);
-            int r;
-            int32_t cv = 0;
-            if (m == kWmCasc) {
-                const uint8_t* pg = (const uint8_t*)ws_shfl64((uint64_t)cptr, c);
-                r = ws_casc_rows(pg, x0, x1, r0 & (kCascPageRows - 1u), n, (int32_t*)buf, &cv, lane);
-            } else {
-                const uint64_t bo = ws_shfl64(blk_off, c);
-                const uint32_t bb = __shfl_sync(0xFFFFFFFFu, blk_bytes, c);
-                r = ws_lz4_rows(s_cols[c], slot, bo, bb, rows, r0, n, x0, x1, buf, lane);
-            }
-            if (r == 1) {  // one value for the whole tile
-                if (lane == 0) cslot[c] = make_uint4((uint32_t)cv, (uint32_t)cv, (uint32_t)cv, (uint32_t)cv);
-                if (lane == c) {
-                    rptr = (const uint8_t*)&cslot[c];
+            // ---- decodes, one column at a time by the whole warp
+            int terr = __any_sync(0xFFFFFFFFu, mine && mode == kWmBad) ? kErrCorrupt : 0;
+            uint32_t roff = 0, rmask = 0xFFFFFFFFu;  // lane c: shared-memory byte offset of column c's rows
+            if (mine) {
+                if (mode == kWmStage) {
+                    roff = (uint32_t)((uint8_t*)(areas + (size_t)P.stage_of[lane] * kWsTile) - smem);
+                } else if (mode == kWmConst) {
+                    cslot[lane] = make_uint4((uint32_t)cval, (uint32_t)cval, (uint32_t)cval, (uint32_t)cval);
+                    roff = (uint32_t)((uint8_t*)&cslot[lane] - smem);
                     rmask = 0;
                 }
-            } else if (r) {
-                terr = r;
-            } else if (lane == c) {
-                rptr = (const uint8_t*)buf;
             }
-        }
-        __syncwarp();
-        if (terr) {
-            if (lane == 0) raise_error(terr);
-            continue;
-        }
-        local_rows += b - a;  // lane-uniform; counted once per warp below
-
-        // ---- evaluation
-        const uint8_t* sp[GX_MAX_STEPS];
-        uint32_t sm[GX_MAX_STEPS];
-#pragma unroll
-        for (uint32_t s = 0; s < GX_MAX_STEPS; ++s) {
-            if (s < ns) {
-                const uint32_t c = Q.steps[s].col;
-                sp[s] = (const uint8_t*)ws_shfl64((uint64_t)rptr, c);
-                sm[s] = __shfl_sync(0xFFFFFFFFu, rmask, c);
-            }
-        }
-        for (uint32_t rb = 0; rb < n; rb += kWsBatch) {
-            const uint32_t r_first = rb + lane * 4;
-            uint4 vals[GX_MAX_STEPS];
-#pragma unroll
-            for (uint32_t s = 0; s < GX_MAX_STEPS; ++s)
-                if (s < ns)
-                    vals[s] = r_first < n ? *(const uint4*)(sp[s] + ((r_first * 4) & sm[s])) : make_uint4(0, 0, 0, 0);
-            uint32_t keep = 0;
-#pragma unroll
-            for (uint32_t i = 0; i < 4; ++i) keep |= (r_first + i >= a && r_first + i < b) ? 1u << i : 0u;
-            uint32_t gk[4] = {0, 0, 0, 0};
-            int32_t carry[4] = {0, 0, 0, 0};
-#pragma unroll
-            for (uint32_t s = 0; s < GX_MAX_STEPS; ++s) {
-                if (s >= ns || !__any_sync(0xFFFFFFFFu, keep)) break;
-                const ShStep& stp = Q.steps[s];
-                const uint32_t flags = stp.flags, dcard = stp.digit_card;
-                const int32_t lo = stp.lo, hi = stp.hi, dbase = stp.digit_base;
-                const bool last = s + 1 == ns;
-                const bool filt = (flags & GX_STEP_FILTER) != 0, carry_step = (flags & GX_STEP_CARRY) != 0;
-                const bool probe = (flags & GX_STEP_PROBE) != 0;
-                const int32_t v[4] = {(int32_t)vals[s].x, (int32_t)vals[s].y, (int32_t)vals[s].z, (int32_t)vals[s].w};
-                uint32_t kk = keep;
-                if (filt) {
-#pragma unroll
-                    for (uint32_t i = 0; i < 4; ++i)
-                        if (!(v[i] >= lo && v[i] <= hi)) kk &= ~(1u << i);
+            for (uint32_t c = 0; c < ncols && !terr; ++c) {
+                const uint32_t m = __shfl_sync(0xFFFFFFFFu, mode, c);
+                if (m != kWmLz4 && m != kWmCasc) continue;
+                uint32_t* buf = areas + (size_t)P.buf_of[c] * kWsTile;
+                const uint8_t* cs = (const uint8_t*)ws_shfl64((uint64_t)src, c);
+                const uint32_t x0 = __shfl_sync(0xFFFFFFFFu, aux0, c), x1 = __shfl_sync(0xFFFFFFFFu, aux1, c);
+                int r;
+                int32_t cv = 0;
+                if (m == kWmCasc) {
+                    r = ws_casc_rows(cs, x0, x1, r0 & (kCascPageRows - 1u), n, (int32_t*)buf, &cv, lane);
+                } else {
+                    const uint32_t bb = __shfl_sync(0xFFFFFFFFu, cbytes, c);
+                    const gx_dcol& col = s_cols[c];
+                    r = ws_lz4_rows(cs, bb, col.seg + (size_t)2 * col.S * slot, col.seg_shift, rows, r0, n, x0, x1,
+                                    buf, lane);
                 }
-                int32_t pp[4] = {v[0], v[1], v[2], v[3]};
-                if (probe) {
-                    const uint64_t* const ht = stp.ht;
-                    const uint32_t htlog = stp.ht_log2, htlay = stp.ht_layout;
-                    if (htlay == GX_HT_BUCKET) {
-                        int32_t mv = kEmptyKey, mp = 0;
-                        bool mk = false;
-#pragma unroll
-                        for (uint32_t i = 0; i < 4; ++i) {
-                            if (!((kk >> i) & 1u)) continue;
-                            if (v[i] != mv || i == 0) {
-                                mp = v[i];
-                                mk = sh_probe(ht, htlog, htlay, v[i], &mp);
-                                mv = v[i];
-                            }
-                            pp[i] = mp;
-                            if (!mk) kk &= ~(1u << i);
-                        }
-                    } else {
-                        // first-slot reads of the lane's distinct keys, all issued before use
-                        const bool dense = htlay == GX_HT_DENSE;
-                        uint32_t hbase = 0, hspan = 0;
-                        if (dense) {
-                            const uint64_t hdr = __ldg((const unsigned long long*)ht);
-                            hbase = (uint32_t)hdr;
-                            hspan = (uint32_t)(hdr >> 32);
-                        }
-                        uint64_t ee[4];
-                        uint32_t rd = 0;
-                        const uint32_t kf = kk;  // rows kept up to the probe
-#pragma unroll
-                        for (uint32_t i = 0; i < 4; ++i) {
-                            const bool again = i > 0 && v[i] == v[i - 1] && ((kf >> (i - 1)) & 1u);
-                            const uint32_t u = (uint32_t)v[i] - hbase;
-                            const bool r = ((kk >> i) & 1u) && !again && v[i] != kEmptyKey && (!dense || u < hspan);
-                            const unsigned long long* slotp =
-                                (const unsigned long long*)ht + (dense ? 1 + u : hash_key32(v[i], htlog));
-                            ee[i] = r ? __ldg(slotp) : (unsigned long long)kEmptySlot;
-                            rd |= r ? 1u << i : 0u;
-                        }
-                        bool pf = false;  // the previous kept row's key was found
-                        int32_t pv = 0;
-#pragma unroll
-                        for (uint32_t i = 0; i < 4; ++i) {
-                            if (!((kk >> i) & 1u)) continue;
-                            const bool again = i > 0 && v[i] == v[i - 1] && ((kf >> (i - 1)) & 1u);
-                            bool f;
-                            int32_t p = v[i];
-                            if (again) {
-                                f = pf;
-                                p = pv;
-                            } else if (!((rd >> i) & 1u)) {
-                                f = false;
-                            } else {
-                                const int32_t ek = (int32_t)(uint32_t)ee[i];
-                                if (ek == v[i]) {
-                                    f = true;
-                                    p = (int32_t)(uint32_t)(ee[i] >> 32);
-                                } else if (dense || ek == kEmptyKey) {
-                                    f = false;
-                                } else {
-                                    f = sh_probe(ht, htlog, htlay, v[i], &p);
-                                }
-                            }
-                            pf = f;
-                            pv = p;
-                            pp[i] = p;
-                            if (!f) kk &= ~(1u << i);
-                        }
+                if (r == 1) {  // one value for the whole tile
+                    if (lane == c) {
+                        cslot[c] = make_uint4((uint32_t)cv, (uint32_t)cv, (uint32_t)cv, (uint32_t)cv);
+                        roff = (uint32_t)((uint8_t*)&cslot[c] - smem);
+                        rmask = 0;
                     }
-                }
-                if (dcard) {
-#pragma unroll
-                    for (uint32_t i = 0; i < 4; ++i) {
-                        if (!((kk >> i) & 1u)) continue;
-                        const uint32_t dgt = (uint32_t)(pp[i] - dbase);
-                        if (dgt >= dcard) {
-                            raise_error(kErrInvalid);
-                            kk &= ~(1u << i);
-                        } else {
-                            gk[i] = gk[i] * dcard + dgt;
-                        }
-                    }
-                }
-                if (carry_step) {
-#pragma unroll
-                    for (uint32_t i = 0; i < 4; ++i) carry[i] = v[i];
-                }
-                keep = kk;
-                if (last) {
-#pragma unroll
-                    for (uint32_t i = 0; i < 4; ++i) {
-                        const bool k = (kk >> i) & 1u;
-                        const int64_t val = agg == GX_AGG_SUM_PRODUCT ? (int64_t)v[i] * carry[i]
-                                            : agg == GX_AGG_SUM_DIFF  ? (int64_t)v[i] - carry[i]
-                                            : agg == GX_AGG_COUNT      ? 1
-                                                                       : (int64_t)v[i];
-                        if (!grouped) {
-                            local += k ? val : 0;
-                        } else if (k) {
-                            if (P.grouped_tab)
-                                ws_group_add(gk[i], val, tkey, tsum, Q.g_keys, Q.g_sums, Q.g_log2);
-                            else if (!group_add_global(Q.g_keys, Q.g_sums, Q.g_log2, (int64_t)gk[i], val))
-                                raise_error(kErrCapacity);
-                        }
-                    }
+                } else if (r) {
+                    terr = r;
+                } else if (lane == c) {
+                    roff = (uint32_t)((uint8_t*)buf - smem);
                 }
             }
+            // ---- the staged bytes
+            if (total) {
+                const bool ok = __all_sync(0xFFFFFFFFu, mbar_wait_bounded(bar, ph));
+                ph ^= 1u;
+                if (!ok) {
+                    // the copies did not land: stop this warp (after one more bounded
+                    // wait, so that no copy is left in flight into its shared memory)
+                    if (lane == 0) raise_error(kErrTimeout);
+                    mbar_wait_bounded(bar, ph ^ 1u);
+                    stop = true;
+                    break;
+                }
+            }
+            __syncwarp();
+            if (terr) {
+                if (lane == 0) raise_error(terr);
+            } else {
+                local_rows += b - a;  // lane-uniform; lane 0's count is the warp's
+                // ---- evaluation, step-major over the tile: the lane's rows are
+                // 128 j + 4 lane + i (j < 8, i < 4), keep bit 4 j + i
+                uint32_t keep = 0;
+#pragma unroll 1
+                for (uint32_t j = 0; j < 8; ++j) {
+                    const int32_t base = (int32_t)(128 * j + 4 * lane);
+                    const int32_t l = min(4, max(0, (int32_t)a - base)), h = min(4, max(0, (int32_t)b - base));
+                    keep |= (h > l ? ((1u << h) - 1u) & ~((1u << l) - 1u) : 0u) << (4 * j);
+                }
+                if (grouped) {
+#pragma unroll 1
+                    for (uint32_t j = 0; j < 8; ++j) *(uint4*)(gkb + 128 * j + 4 * lane) = make_uint4(0, 0, 0, 0);
+                }
+                uint32_t coff = 0, cmask = 0;  // the carried column (none: carried values are 0)
+                bool carried = false;
+                for (uint32_t s = 0; s < ns; ++s) {
+                    if (!__any_sync(0xFFFFFFFFu, keep)) break;
+                    const ShStep& stp = Q.steps[s];
+                    const uint32_t flags = stp.flags;
+                    const uint32_t c = stp.col;
+                    const uint32_t off = __shfl_sync(0xFFFFFFFFu, roff, c), msk = __shfl_sync(0xFFFFFFFFu, rmask, c);
+                    if (flags & GX_STEP_CARRY) {
+                        coff = off;
+                        cmask = msk;
+                        carried = true;
+                    }
+                    if (msk == 0) {
+                        if (ws_step_const(stp, *(const int32_t*)(smem + off), keep, gkb, grouped, lane)) keep = 0;
+                    } else if ((flags & (GX_STEP_FILTER | GX_STEP_PROBE)) || stp.digit_card) {
+                        keep = ws_step_rows(stp, smem + off, keep, gkb, grouped, lane);
+                    }
+                    if (s + 1 == ns && keep)
+                        local += ws_aggregate(agg, grouped, carried, smem + off, msk, smem + coff, cmask, keep, gkb,
+                                              tkey, tsum, Q.g_keys, Q.g_sums, Q.g_log2, lane);
+                }
+            }
+            // every lane is done with the tile's areas before the next copies overwrite them
+            __syncwarp();
+            if (lane == 0) fence_proxy_async_smem();
         }
-        __syncwarp();
     }
     // ---- the warp's results
+    __syncwarp();
     if (grouped && P.grouped_tab) {
-        __syncwarp();
         for (uint32_t i = lane; i < kWsGroupSlots; i += 32) {
             const uint32_t key = tkey[i];
             if (key != kEmptyGKey && !group_add_global(Q.g_keys, Q.g_sums, Q.g_log2, (int64_t)key, (int64_t)tsum[i]))
