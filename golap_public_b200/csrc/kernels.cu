@@ -1805,7 +1805,11 @@ static gx_status ensure_kernel_attrs() {
     if (!st) st = allow_smem(shared_scan_kernel<1024, 1>, sh_max);
     if (!st) st = allow_smem(shared_scan_kernel<kShSingleNT, 4, true>, sh_max);
     if (!st) st = allow_smem(pipe_scan_kernel, kPipeMaxDynSmem);
-    if (!st) st = allow_smem(warp_scan_kernel, kWsMaxDynSmem);
+    if (!st) st = allow_smem(warp_scan_kernel<0>, kWsMaxDynSmem);
+    if (!st) st = allow_smem(warp_scan_kernel<kSigQ1>, kWsMaxDynSmem);
+    if (!st) st = allow_smem(warp_scan_kernel<kSigQ2>, kWsMaxDynSmem);
+    if (!st) st = allow_smem(warp_scan_kernel<kSigQ3>, kWsMaxDynSmem);
+    if (!st) st = allow_smem(warp_scan_kernel<kSigQ4>, kWsMaxDynSmem);
     if (st) return st;
     attr_set[dev] = true;
     return GX_OK;
@@ -2244,14 +2248,28 @@ static gx_status scan_launch_warp(const gx_scan_plan* plan, const QueryDesc& qd,
     P.rows_scanned = rows_dev;
     const size_t smem = 4ull * (2ull * P.chunk_words + (size_t)P.warp_words * kWsWarps);
     if (smem > kWsMaxDynSmem) return GX_OK;
+    // the plan's signature: a compile-time evaluator when one matches
+    uint32_t kinds[GX_MAX_STEPS] = {};
+    for (uint32_t k = 0; k < plan->n_steps; ++k) {
+        const uint32_t f = plan->steps[k].flags;
+        kinds[k] = ((f & GX_STEP_FILTER) ? kWkF : 0u) | ((f & GX_STEP_PROBE) ? kWkP : 0u) |
+                   ((f & GX_STEP_CARRY) ? kWkC : 0u) | (P.q.steps[k].digit_card ? kWkD : 0u);
+    }
+    const uint32_t sig = plan->n_steps <= 6 ? ws_sig(plan->n_steps, P.q.agg, P.q.grouped != 0, kinds[0], kinds[1],
+                                                     kinds[2], kinds[3], kinds[4], kinds[5])
+                                            : 0u;
+    void (*kern)(WsParams) = warp_scan_kernel<0>;
+    if (sig == kSigQ1) kern = warp_scan_kernel<kSigQ1>;
+    else if (sig == kSigQ2) kern = warp_scan_kernel<kSigQ2>;
+    else if (sig == kSigQ3) kern = warp_scan_kernel<kSigQ3>;
+    else if (sig == kSigQ4) kern = warp_scan_kernel<kSigQ4>;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, warp_scan_kernel, kWsNT, smem) != cudaSuccess ||
-        per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWsNT, smem) != cudaSuccess || per_sm < 1)
         return set_error(GX_ERR_CUDA, "warp scan occupancy query failed");
     const uint64_t tiles = (uint64_t)n_range * c0->blocks_per_chunk * P.tiles_per_block;
     const uint64_t want = (tiles + kWsWarps - 1) / kWsWarps;
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm, want));
-    warp_scan_kernel<<<grid, kWsNT, smem, s>>>(P);
+    kern<<<grid, kWsNT, smem, s>>>(P);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "warp scan launch: %s", cudaGetErrorString(e));
     *done = true;

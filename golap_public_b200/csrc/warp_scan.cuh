@@ -33,7 +33,9 @@ constexpr uint32_t kWsLog2 = 10;
 constexpr uint32_t kWsTile = 1u << kWsLog2;    // rows of one warp tile
 constexpr uint32_t kWsNT = 128;                // threads per CTA (4 independent warps)
 constexpr uint32_t kWsWarps = kWsNT / 32;
-constexpr uint32_t kWsBatch = 128;             // rows per evaluation batch (4 per lane)
+constexpr uint32_t kWsBatch = 128;             // rows of one row group (4 per lane)
+constexpr uint32_t kWsGroups = kWsTile / kWsBatch;  // row groups of a tile (4 keep bits each)
+static_assert(kWsGroups * 4 <= 32, "the keep bits of a tile fit one word");
 constexpr uint32_t kWsMaxCols = kPipeMaxCols;
 constexpr uint32_t kWsGroupLog2 = 7;           // warp group table: 128 slots
 constexpr uint32_t kWsGroupSlots = 1u << kWsGroupLog2;
@@ -277,7 +279,7 @@ __device__ __forceinline__ bool ws_locate(const WsParams& P, const uint32_t* s_k
 
 // Column c's read decision for tile T (directory entry, side-index
 // entries, a cascaded page's header: a single-run page needs no decode).
-__device__ __noinline__ WsCol ws_column(const WsParams& P, const gx_dcol& col, uint32_t c, const WsTile& T) {
+__device__ __forceinline__ WsCol ws_column(const WsParams& P, const gx_dcol& col, uint32_t c, const WsTile& T) {
     WsCol C;
     C.mode = kWmBad;
     C.src = nullptr;
@@ -333,13 +335,32 @@ __device__ __noinline__ WsCol ws_column(const WsParams& P, const gx_dcol& col, u
                 // pages that hold one value need no decode: zero-width values
                 // without RLE (with DELTA: zero steps), or one run of the whole page
                 const casc_hdr h = casc_load_header(pg);
-                if (casc_header_ok(h, pb, C.aux1) && h.val_bits == 0) {
-                    const bool rle = (h.flags & CASC_RLE) != 0, delta = (h.flags & CASC_DELTA) != 0;
-                    const bool one = rle ? (h.n_runs == 1 && h.len_bits == 0 && h.len_base == C.aux1)
-                                         : (!delta || h.val_base == 0);
-                    if (one) {
+                const bool rle = (h.flags & CASC_RLE) != 0, delta = (h.flags & CASC_DELTA) != 0;
+                if (casc_header_ok(h, pb, C.aux1)) {
+                    if (!rle && h.val_bits == 0 && (!delta || h.val_base == 0)) {
                         C.mode = kWmConst;
                         C.cval = delta ? h.first : h.val_base;
+                    } else if (rle && h.n_runs <= 8) {
+                        // a few runs (sorted columns): the run holding the tile's first
+                        // row, and whether it also holds the last
+                        const uint32_t* vw = (const uint32_t*)(pg + h.vals_off);
+                        const uint32_t* lw = (const uint32_t*)(pg + h.lens_off);
+                        const uint32_t h0 = r0 & (kCascPageRows - 1u), h1 = h0 + n;
+                        uint32_t end = 0, val = 0;
+                        for (uint32_t k = 0; k < h.n_runs; ++k) {
+                            const uint32_t start = end;
+                            end += unpack_bits(lw, k, h.len_bits) + h.len_base;
+                            const uint32_t e =
+                                (delta && k == 0) ? 0u : unpack_bits(vw, k, h.val_bits) + (uint32_t)h.val_base;
+                            val = delta ? val + e : e;
+                            if (start <= h0 && h0 < end) {
+                                if (h1 <= end) {
+                                    C.mode = kWmConst;
+                                    C.cval = (int32_t)(delta ? val + (uint32_t)h.first : val);
+                                }
+                                break;
+                            }
+                        }
                     }
                 }
             }
@@ -396,12 +417,12 @@ __device__ __forceinline__ void ws_bulk_prefetch_l2(const void* src, uint32_t by
 // A step over a column that holds one value v on the whole tile: decided
 // once.  Returns true when the tile's rows are all dropped; else multiplies
 // in the group-key digit of every kept row.
-__device__ __noinline__ bool ws_step_const(const ShStep& stp, int32_t v, uint32_t keep, uint32_t* gkb, bool grouped,
+__device__ __forceinline__ bool ws_step_const(const ShStep& stp, int32_t v, uint32_t keep, uint32_t* gkb, bool grouped,
                                            uint32_t lane) {
     const uint32_t flags = stp.flags, dcard = stp.digit_card;
     bool f = !(flags & GX_STEP_FILTER) || (v >= stp.lo && v <= stp.hi);
     int32_t pp = v;
-    if (f && (flags & GX_STEP_PROBE)) f = sh_probe(stp.ht, stp.ht_log2, stp.ht_layout, v, &pp);
+    if (f && (flags & GX_STEP_PROBE)) f = ht_probe_any(stp.ht, stp.ht_log2, stp.ht_layout, v, &pp);
     if (!f) return true;
     if (dcard && grouped) {
         const uint32_t dgt = (uint32_t)(pp - stp.digit_base);
@@ -410,7 +431,7 @@ __device__ __noinline__ bool ws_step_const(const ShStep& stp, int32_t v, uint32_
             return true;
         }
 #pragma unroll 1
-        for (uint32_t j = 0; j < 8; ++j) {
+        for (uint32_t j = 0; j < kWsGroups; ++j) {
             if (!((keep >> (4 * j)) & 15u)) continue;
             uint4* g = (uint4*)(gkb + 128 * j + 4 * lane);
             uint4 x = *g;
@@ -428,7 +449,7 @@ __device__ __noinline__ bool ws_step_const(const ShStep& stp, int32_t v, uint32_
 // (shared memory, kWsTile rows).  Probes issue the first-slot reads of a
 // row group's distinct keys together and reuse the lane's last result for a
 // repeated key.  Returns the new keep bits.
-__device__ __noinline__ uint32_t ws_step_rows(const ShStep& stp, const uint8_t* col, uint32_t keep, uint32_t* gkb,
+__device__ __forceinline__ uint32_t ws_step_rows(const ShStep& stp, const uint8_t* col, uint32_t keep, uint32_t* gkb,
                                               bool grouped, uint32_t lane) {
     const uint32_t flags = stp.flags, dcard = stp.digit_card;
     const int32_t lo = stp.lo, hi = stp.hi, dbase = stp.digit_base;
@@ -445,7 +466,7 @@ __device__ __noinline__ uint32_t ws_step_rows(const ShStep& stp, const uint8_t* 
     int32_t mv = 0, mp = 0;  // the lane's last probed key and its result
     bool mhave = false, mf = false;
 #pragma unroll 1
-    for (uint32_t j = 0; j < 8; ++j) {
+    for (uint32_t j = 0; j < kWsGroups; ++j) {
         uint32_t kk = (keep >> (4 * j)) & 15u;
         if (!kk) continue;
         const uint4 w4 = *(const uint4*)(col + (128 * j + 4 * lane) * 4);
@@ -525,7 +546,7 @@ __device__ __noinline__ uint32_t ws_step_rows(const ShStep& stp, const uint8_t* 
 // The aggregate over the kept rows of the tile: the value column at `col`
 // (mask 0: one value), the carried column at `ccol`.  Returns the scalar
 // part; grouped sums go to the warp's group table.
-__device__ __noinline__ int64_t ws_aggregate(uint32_t agg, bool grouped, bool carried, const uint8_t* col, uint32_t msk,
+__device__ __forceinline__ int64_t ws_aggregate(uint32_t agg, bool grouped, bool carried, const uint8_t* col, uint32_t msk,
                                              const uint8_t* ccol, uint32_t cmask, uint32_t keep, const uint32_t* gkb,
                                              uint32_t* tkey, unsigned long long* tsum, int64_t* g_keys,
                                              int64_t* g_sums, uint32_t g_log2, uint32_t lane) {
@@ -533,7 +554,7 @@ __device__ __noinline__ int64_t ws_aggregate(uint32_t agg, bool grouped, bool ca
     if (!grouped && agg == GX_AGG_SUM && msk == 0) return (int64_t)__popc(keep) * *(const int32_t*)col;
     int64_t acc = 0;
 #pragma unroll 1
-    for (uint32_t j = 0; j < 8; ++j) {
+    for (uint32_t j = 0; j < kWsGroups; ++j) {
         const uint32_t kk = (keep >> (4 * j)) & 15u;
         if (!kk) continue;
         const uint32_t ro = (128 * j + 4 * lane) * 4;
@@ -569,6 +590,200 @@ __device__ __noinline__ int64_t ws_aggregate(uint32_t agg, bool grouped, bool ca
     return acc;
 }
 
+// ---- plan signatures: compile-time evaluators for the known query shapes
+// A signature packs the step count (bits 0-2), the aggregate (3-5), grouped
+// (6) and per step s a kind nibble at bit 7 + 4 s: 1 FILTER, 2 PROBE,
+// 4 CARRY, 8 group-key digit.  Signature 0 is the run-time evaluator.
+constexpr uint32_t kWkF = 1, kWkP = 2, kWkC = 4, kWkD = 8;
+constexpr uint32_t ws_sig(uint32_t ns, uint32_t agg, bool grouped, uint32_t k0, uint32_t k1 = 0, uint32_t k2 = 0,
+                          uint32_t k3 = 0, uint32_t k4 = 0, uint32_t k5 = 0) {
+    return ns | (agg << 3) | ((grouped ? 1u : 0u) << 6) | (k0 << 7) | (k1 << 11) | (k2 << 15) | (k3 << 19) |
+           (k4 << 23) | (k5 << 27);
+}
+// pipeline_q1_lineorder: date probe, discount filter carried, quantity filter, price x discount
+constexpr uint32_t kSigQ1 = ws_sig(4, GX_AGG_SUM_PRODUCT, false, kWkP, kWkF | kWkC, kWkF, 0);
+// pipeline_q3: customer / supplier / date probes with digits, revenue grouped
+constexpr uint32_t kSigQ3 = ws_sig(4, GX_AGG_SUM, true, kWkP | kWkD, kWkP | kWkD, kWkP | kWkD, 0);
+// pipeline_q2: part probe (brand digit), supplier probe, date probe (year digit), revenue grouped
+constexpr uint32_t kSigQ2 = ws_sig(4, GX_AGG_SUM, true, kWkP | kWkD, kWkP, kWkP | kWkD, 0);
+// pipeline_q4: customer (nation digit), supplier, date (year digit), part probes, supplycost carried, profit grouped
+constexpr uint32_t kSigQ4 = ws_sig(6, GX_AGG_SUM_DIFF, true, kWkP | kWkD, kWkP, kWkP | kWkD, kWkP, kWkC, 0);
+
+// The tile's rows evaluated through all steps of a compile-time signature,
+// one 128-row group at a time: every column's 4 values of the lane are
+// loaded first, then the steps run on registers (carried values and group
+// keys included).  Steps over a column that holds one value on the tile
+// (other than the last) are decided once for the tile.  Returns the scalar
+// part; grouped sums go to the warp's group table.
+template <uint32_t SIG>
+__device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* sbase, const uint32_t* off,
+                                               const uint32_t* msk, uint32_t keep, uint32_t* tkey,
+                                               unsigned long long* tsum, uint32_t lane) {
+    constexpr uint32_t NS = SIG & 7, AGG = (SIG >> 3) & 7;
+    constexpr bool GR = ((SIG >> 6) & 1) != 0;
+    int64_t acc = 0;
+    int32_t mv[NS], mp[NS];  // per probe step: the lane's last key and its result
+    bool mh[NS], mf[NS];
+    uint32_t cd[NS];  // constant steps: the group-key digit
+    int32_t cv[NS];   // constant steps: the value
+#pragma unroll
+    for (uint32_t s = 0; s < NS; ++s) {
+        mh[s] = false;
+        mf[s] = false;
+        mv[s] = 0;
+        mp[s] = 0;
+        cd[s] = 0;
+        cv[s] = 0;
+        if (s + 1 < NS && msk[s] == 0) {
+            const uint32_t K = (SIG >> (7 + 4 * s)) & 15u;
+            const ShStep& stp = Q.steps[s];
+            const int32_t v = *(const int32_t*)(sbase + off[s]);
+            cv[s] = v;
+            bool f = !(K & kWkF) || (v >= stp.lo && v <= stp.hi);
+            int32_t pp = v;
+            if ((K & kWkP) && f) f = ht_probe_any(stp.ht, stp.ht_log2, stp.ht_layout, v, &pp);
+            if ((K & kWkD) && f) {
+                cd[s] = (uint32_t)(pp - stp.digit_base);
+                if (cd[s] >= stp.digit_card) {
+                    if (lane == 0) raise_error(kErrInvalid);
+                    f = false;
+                }
+            }
+            if (!f) return 0;  // no row of the tile passes
+        }
+    }
+#pragma unroll 1
+    for (uint32_t j = 0; j < kWsGroups; ++j) {
+        uint32_t kk = (keep >> (4 * j)) & 15u;
+        if (!kk) continue;
+        const uint32_t ro = (128 * j + 4 * lane) * 4;
+        uint4 w[NS];
+#pragma unroll
+        for (uint32_t s = 0; s < NS; ++s)
+            w[s] = (s + 1 < NS && msk[s] == 0) ? make_uint4(0, 0, 0, 0)
+                                               : *(const uint4*)(sbase + off[s] + (ro & msk[s]));
+        int32_t carry[4] = {0, 0, 0, 0};
+        uint32_t g[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (uint32_t s = 0; s < NS; ++s) {
+            const uint32_t K = (SIG >> (7 + 4 * s)) & 15u;
+            const ShStep& stp = Q.steps[s];
+            if (s + 1 < NS && msk[s] == 0) {  // decided for the tile
+                if (K & kWkD) {
+                    const uint32_t dcard = stp.digit_card;
+#pragma unroll
+                    for (uint32_t i = 0; i < 4; ++i) g[i] = g[i] * dcard + cd[s];
+                }
+                if (K & kWkC) {
+#pragma unroll
+                    for (uint32_t i = 0; i < 4; ++i) carry[i] = cv[s];
+                }
+                continue;
+            }
+            const int32_t v[4] = {(int32_t)w[s].x, (int32_t)w[s].y, (int32_t)w[s].z, (int32_t)w[s].w};
+            if (K & kWkF) {
+                const int32_t lo = stp.lo, hi = stp.hi;
+#pragma unroll
+                for (uint32_t i = 0; i < 4; ++i)
+                    if (!(v[i] >= lo && v[i] <= hi)) kk &= ~(1u << i);
+            }
+            int32_t pp[4] = {v[0], v[1], v[2], v[3]};
+            if (K & kWkP) {
+                const uint64_t* const ht = stp.ht;
+                const uint32_t htlog = stp.ht_log2, htlay = stp.ht_layout;
+                const bool dense = htlay == GX_HT_DENSE, bucket = htlay == GX_HT_BUCKET;
+                uint32_t hbase = 0, hspan = 0;
+                if (dense) {
+                    const uint64_t hdr = __ldg((const unsigned long long*)ht);
+                    hbase = (uint32_t)hdr;
+                    hspan = (uint32_t)(hdr >> 32);
+                }
+                // first-slot reads of the lane's distinct keys, all issued before use
+                uint64_t ee[4];
+                uint32_t rd = 0;
+#pragma unroll
+                for (uint32_t i = 0; i < 4; ++i) {
+                    const bool again =
+                        (i > 0 && v[i] == v[i - 1] && ((kk >> (i - 1)) & 1u)) || (mh[s] && v[i] == mv[s]);
+                    const uint32_t u = (uint32_t)v[i] - hbase;
+                    const bool r =
+                        ((kk >> i) & 1u) && !again && !bucket && v[i] != kEmptyKey && (!dense || u < hspan);
+                    const unsigned long long* sl =
+                        (const unsigned long long*)ht + (dense ? 1 + u : hash_key32(v[i], htlog));
+                    ee[i] = r ? __ldg(sl) : (unsigned long long)kEmptySlot;
+                    rd |= r ? 1u << i : 0u;
+                }
+#pragma unroll
+                for (uint32_t i = 0; i < 4; ++i) {
+                    if (!((kk >> i) & 1u)) continue;
+                    bool f;
+                    int32_t p = v[i];
+                    if (mh[s] && v[i] == mv[s]) {
+                        f = mf[s];
+                        p = mp[s];
+                    } else if ((rd >> i) & 1u) {
+                        const int32_t ek = (int32_t)(uint32_t)ee[i];
+                        if (ek == v[i]) {
+                            f = true;
+                            p = (int32_t)(uint32_t)(ee[i] >> 32);
+                        } else if (dense || ek == kEmptyKey) {
+                            f = false;
+                        } else {
+                            f = sh_probe(ht, htlog, htlay, v[i], &p);
+                        }
+                    } else {
+                        // bucket tables, keys the memo held when the reads were issued,
+                        // the reserved key, keys outside a dense range
+                        f = sh_probe(ht, htlog, htlay, v[i], &p);
+                    }
+                    mh[s] = true;
+                    mv[s] = v[i];
+                    mf[s] = f;
+                    mp[s] = p;
+                    pp[i] = p;
+                    if (!f) kk &= ~(1u << i);
+                }
+            }
+            if (K & kWkD) {
+                const uint32_t dcard = stp.digit_card;
+                const int32_t dbase = stp.digit_base;
+#pragma unroll
+                for (uint32_t i = 0; i < 4; ++i) {
+                    if (!((kk >> i) & 1u)) continue;
+                    const uint32_t dgt = (uint32_t)(pp[i] - dbase);
+                    if (dgt >= dcard) {
+                        raise_error(kErrInvalid);
+                        kk &= ~(1u << i);
+                    } else {
+                        g[i] = g[i] * dcard + dgt;
+                    }
+                }
+            }
+            if (K & kWkC) {
+#pragma unroll
+                for (uint32_t i = 0; i < 4; ++i) carry[i] = v[i];
+            }
+            if (!kk) break;
+            if (s + 1 == NS) {
+#pragma unroll
+                for (uint32_t i = 0; i < 4; ++i) {
+                    if (!((kk >> i) & 1u)) continue;
+                    const int64_t val = AGG == GX_AGG_SUM_PRODUCT ? (int64_t)v[i] * carry[i]
+                                        : AGG == GX_AGG_SUM_DIFF  ? (int64_t)v[i] - carry[i]
+                                        : AGG == GX_AGG_COUNT      ? 1
+                                                                   : (int64_t)v[i];
+                    if (GR)
+                        ws_group_add(g[i], val, tkey, tsum, Q.g_keys, Q.g_sums, Q.g_log2);
+                    else
+                        acc += val;
+                }
+            }
+        }
+    }
+    return acc;
+}
+
+template <uint32_t SIG>
 __global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_constant__ WsParams P) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ gx_dcol s_cols[kWsMaxCols];
@@ -723,21 +938,35 @@ __global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_consta
             } else {
                 local_rows += b - a;  // lane-uniform; lane 0's count is the warp's
                 // ---- evaluation, step-major over the tile: the lane's rows are
-                // 128 j + 4 lane + i (j < 8, i < 4), keep bit 4 j + i
-                uint32_t keep = 0;
+                // 128 j + 4 lane + i (j < kWsGroups, i < 4), keep bit 4 j + i
+                uint32_t keep = kWsGroups == 8 ? 0xFFFFFFFFu : (1u << (4 * kWsGroups)) - 1u;
+                if (a != 0 || b != kWsTile) {
+                    keep = 0;
 #pragma unroll 1
-                for (uint32_t j = 0; j < 8; ++j) {
-                    const int32_t base = (int32_t)(128 * j + 4 * lane);
-                    const int32_t l = min(4, max(0, (int32_t)a - base)), h = min(4, max(0, (int32_t)b - base));
-                    keep |= (h > l ? ((1u << h) - 1u) & ~((1u << l) - 1u) : 0u) << (4 * j);
+                    for (uint32_t j = 0; j < kWsGroups; ++j) {
+                        const int32_t base = (int32_t)(128 * j + 4 * lane);
+                        const int32_t l = min(4, max(0, (int32_t)a - base)), h = min(4, max(0, (int32_t)b - base));
+                        keep |= (h > l ? ((1u << h) - 1u) & ~((1u << l) - 1u) : 0u) << (4 * j);
+                    }
                 }
-                if (grouped) {
+                if (SIG == 0 && grouped) {
 #pragma unroll 1
-                    for (uint32_t j = 0; j < 8; ++j) *(uint4*)(gkb + 128 * j + 4 * lane) = make_uint4(0, 0, 0, 0);
+                    for (uint32_t j = 0; j < kWsGroups; ++j) *(uint4*)(gkb + 128 * j + 4 * lane) = make_uint4(0, 0, 0, 0);
+                }
+                if constexpr (SIG != 0) {
+                    constexpr uint32_t NS = SIG & 7;
+                    uint32_t off[NS], msk[NS];
+#pragma unroll
+                    for (uint32_t s = 0; s < NS; ++s) {
+                        const uint32_t c = Q.steps[s].col;
+                        off[s] = __shfl_sync(0xFFFFFFFFu, roff, c);
+                        msk[s] = __shfl_sync(0xFFFFFFFFu, rmask, c);
+                    }
+                    local += ws_eval_sig<SIG>(Q, smem, off, msk, keep, tkey, tsum, lane);
                 }
                 uint32_t coff = 0, cmask = 0;  // the carried column (none: carried values are 0)
                 bool carried = false;
-                for (uint32_t s = 0; s < ns; ++s) {
+                for (uint32_t s = 0; SIG == 0 && s < ns; ++s) {
                     if (!__any_sync(0xFFFFFFFFu, keep)) break;
                     const ShStep& stp = Q.steps[s];
                     const uint32_t flags = stp.flags;
