@@ -919,7 +919,8 @@ def cpu_star_join(ctx, steps=2, warmup=1, threads=None):
     threads = threads or os.cpu_count() or 1
     fact, cust, supp, dd = ctx["fact"], ctx["cust"], ctx["supp"], ctx["dd"]
     region, ylo, yhi = ctx["region"], ctx["ylo"], ctx["yhi"]
-    arr = O.comp_cols(comp_columns(fact, Q3_COLS))
+    keep = comp_columns(fact, Q3_COLS)  # the arrays stay alive while the harness reads them
+    arr = O.comp_cols(keep)
     mins, maxs = fact.cols["date_key"].minmax()
     gk = np.zeros(4096, np.int64)
     gs = np.zeros(4096, np.int64)
