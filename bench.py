@@ -974,6 +974,44 @@ def profile_batch(rows):
         print(json.dumps({"profile_batch": i, "rows": rows, "threads": batch.threads, "ms": a.elapsed_time(b)}))
 
 
+def profile_scan(kind, rows, segments):
+    """One single-plan scan of the Q1 workload's shape on `rows` rows, for a
+    profiler: "q1full" (every date, no pruning: every tile needs all four
+    columns), "q1pruned" (the headline month) or "q3" (the star join with
+    dense join tables); three untimed launches, then three timed ones."""
+    import torch
+
+    from golap_public_b200 import api, datagen, queries
+
+    dd = datagen.date_dim()
+    if kind == "q3":
+        g = datagen.fact_q3(rows, True)
+        fact = queries.encode_fact({k: g[k] for k in Q3_COLS}, {"date_key": "cascaded"}, ROWS_PER_CHUNK,
+                                   ROWS_PER_BLOCK, segments)
+        q = queries.Q3Query(fact, datagen.dim_geo(3_000_000, datagen.SEED, 21),
+                            datagen.dim_geo(200_000, datagen.SEED, 22), dd, 2, 1992, 1997, ht_layout="dense")
+    else:
+        f = datagen.fact_q1(rows, True)
+        fact = queries.encode_fact(f, {"date_key": "cascaded"}, ROWS_PER_CHUNK, ROWS_PER_BLOCK, segments)
+        if kind == "q1full":
+            ok = np.ones(len(dd["d_key"]), dtype=bool)
+            q = queries.Q1Query(fact, dd, ok, int(dd["d_key"].min()), int(dd["d_key"].max()), *DISC, *QTY,
+                                prune=False)
+        else:
+            q = queries.Q1Query(fact, dd, dd["d_yearmonthnum"] == 199401, DATE_LO, DATE_HI, *DISC, *QTY)
+    stream = torch.cuda.current_stream()
+    for i in range(6):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        q.launch()
+        b.record(stream)
+        b.synchronize()
+        api.scan_check()
+        if i >= 3:
+            print(json.dumps({"profile_scan": kind, "rows": rows, "launch": i, "ms": a.elapsed_time(b)}))
+
+
 def main():
     global N_ROWS
     ap = argparse.ArgumentParser()
@@ -995,6 +1033,8 @@ def main():
                     help="fact rows of the Q1 workload (default: the measured 60M-row configuration; smaller "
                          "values are for profiler captures)")
     ap.add_argument("--tune-rows", type=int, default=20_000_000)
+    ap.add_argument("--profile-scan", choices=["q1full", "q1pruned", "q3"],
+                    help="run one single-plan scan six times on --rows rows (for a profiler) and exit")
     ap.add_argument("--profile-batch", action="store_true",
                     help="only build the batch table and run the 256-query mixed batch (shared form, dense join "
                          "tables, automatic launch shape) three times: the command profiler captures use")
@@ -1004,6 +1044,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
 
+    if args.profile_scan:
+        profile_scan(args.profile_scan, args.rows, args.segments)
+        return
     if args.profile_batch:
         profile_batch(args.batch_rows)
         return

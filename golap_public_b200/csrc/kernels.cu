@@ -2244,10 +2244,7 @@ static gx_status scan_launch_warp(const gx_scan_plan* plan, const QueryDesc& qd,
     if (P.chunk_words > kWsMaxChunkWords) return GX_OK;
     P.n_areas = areas;
     P.grouped_tab = P.q.grouped ? 1u : 0u;
-    P.warp_words = kWsHead + areas * kWsTile + (P.grouped_tab ? kWsTile + 3 * kWsGroupSlots : 0u);
     P.rows_scanned = rows_dev;
-    const size_t smem = 4ull * (2ull * P.chunk_words + (size_t)P.warp_words * kWsWarps);
-    if (smem > kWsMaxDynSmem) return GX_OK;
     // the plan's signature: a compile-time evaluator when one matches
     uint32_t kinds[GX_MAX_STEPS] = {};
     for (uint32_t k = 0; k < plan->n_steps; ++k) {
@@ -2263,6 +2260,13 @@ static gx_status scan_launch_warp(const gx_scan_plan* plan, const QueryDesc& qd,
     else if (sig == kSigQ2) kern = warp_scan_kernel<kSigQ2>;
     else if (sig == kSigQ3) kern = warp_scan_kernel<kSigQ3>;
     else if (sig == kSigQ4) kern = warp_scan_kernel<kSigQ4>;
+    // shared memory per warp: the areas, then (grouped) the run-time
+    // evaluator's per-row group keys and the group table
+    const bool rt_eval = kern == warp_scan_kernel<0>;
+    P.warp_words = kWsHead + areas * kWsTile + (P.grouped_tab && rt_eval ? kWsTile : 0u);
+    const size_t smem = 4ull * (2ull * P.chunk_words + (size_t)P.warp_words * kWsWarps +
+                                (P.grouped_tab ? 3ull * kWsGroupSlots : 0ull));
+    if (smem > kWsMaxDynSmem) return GX_OK;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWsNT, smem) != cudaSuccess || per_sm < 1)
         return set_error(GX_ERR_CUDA, "warp scan occupancy query failed");

@@ -25,9 +25,11 @@
 //     batch is issued before the first step runs), filters, join probes
 //     (each lane probes a repeated key once), group-key digits, carried
 //     value, and the aggregate.
-// Scalar sums stay in registers; grouped sums go to the warp's own group
-// table in shared memory (keys that find no slot go to the global table) and
-// are flushed when the warp is done.  Nothing waits on another warp.
+// Scalar sums stay in registers; grouped sums go to the CTA's group table in
+// shared memory (keys that find no slot go to the global table), flushed when
+// the CTA is done.  Join-table reads carry an L2 evict-last policy and the
+// streamed column bytes an evict-first one, so that the tables stay in L2
+// while the fact columns pass through it.  Nothing waits on another warp.
 
 constexpr uint32_t kWsLog2 = 10;
 constexpr uint32_t kWsTile = 1u << kWsLog2;    // rows of one warp tile
@@ -37,11 +39,11 @@ constexpr uint32_t kWsBatch = 128;             // rows of one row group (4 per l
 constexpr uint32_t kWsGroups = kWsTile / kWsBatch;  // row groups of a tile (4 keep bits each)
 static_assert(kWsGroups * 4 <= 32, "the keep bits of a tile fit one word");
 constexpr uint32_t kWsMaxCols = kPipeMaxCols;
-constexpr uint32_t kWsGroupLog2 = 7;           // warp group table: 128 slots
+constexpr uint32_t kWsGroupLog2 = 9;           // the CTA's group table: 512 slots
 constexpr uint32_t kWsGroupSlots = 1u << kWsGroupLog2;
 constexpr uint32_t kWsGroupProbes = 16;
 constexpr uint32_t kWsNone = 0xFFFFFFFFu;
-constexpr uint32_t kWsMaxDynSmem = 200u << 10;  // dynamic shared memory of one CTA at most
+constexpr uint32_t kWsMaxDynSmem = 220u << 10;  // dynamic shared memory of one CTA at most
 constexpr uint32_t kWsMaxChunkWords = 1024;     // chunk keep bits of one launch: 32768 chunks
 constexpr uint32_t kWsHead = 36;                // per-warp words before the stage: 8 constant slots, the mbarrier
 static_assert(kWsTile <= kCascPageRows && kCascPageRows % kWsTile == 0, "a warp tile lies in one cascaded page");
@@ -78,6 +80,32 @@ __device__ __forceinline__ uint32_t ws_scan(uint32_t x, uint32_t lane) {
         if (lane >= (uint32_t)d) x += y;
     }
     return x;
+}
+
+// L2 cache policies: join tables stay (evict last), streamed bytes go first.
+__device__ __forceinline__ uint64_t ws_policy_keep() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t ws_policy_stream() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// A join-table slot read under policy pol (read-only path).
+__device__ __forceinline__ unsigned long long ws_ld_slot(const unsigned long long* a, uint64_t pol) {
+    unsigned long long v;
+    asm("ld.global.nc.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(pol));
+    return v;
+}
+// One bulk copy (no multicast) completing on m, its lines read under policy pol.
+__device__ __forceinline__ void ws_bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* m, uint64_t pol) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(m)), "l"(pol)
+        : "memory");
 }
 
 // Rows [h0, h0 + n) of a cascaded page decoded by one warp into out[0..n),
@@ -199,7 +227,7 @@ __device__ __noinline__ int ws_lz4_rows(const uint8_t* blk, uint32_t blk_bytes, 
 
 // Add of (gk, val) to the warp's group table; keys that find no slot within
 // kWsGroupProbes go to the global table.
-__device__ __noinline__ void ws_group_add(uint32_t gk, int64_t val, uint32_t* tkey, unsigned long long* tsum,
+__device__ __forceinline__ void ws_group_add(uint32_t gk, int64_t val, uint32_t* tkey, unsigned long long* tsum,
                                           int64_t* keys, int64_t* sums, uint32_t log2cap) {
     if (gk != kEmptyGKey) {
         uint32_t s = hash_key32((int32_t)gk, kWsGroupLog2);
@@ -410,8 +438,9 @@ __device__ __forceinline__ void ws_prefetch_meta(const WsParams& P, const gx_dco
         asm volatile("prefetch.global.L2 [%0];" ::"l"(col.seg + (size_t)2 * col.S * T.slot + 2 * (T.r0 >> kCascPageLog2)));
 }
 
-__device__ __forceinline__ void ws_bulk_prefetch_l2(const void* src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+__device__ __forceinline__ void ws_bulk_prefetch_l2(const void* src, uint32_t bytes, uint64_t pol) {
+    asm volatile("cp.async.bulk.prefetch.L2.global.L2::cache_hint [%0], %1, %2;" ::"l"(src), "r"(bytes), "l"(pol)
+                 : "memory");
 }
 
 // A step over a column that holds one value v on the whole tile: decided
@@ -450,7 +479,7 @@ __device__ __forceinline__ bool ws_step_const(const ShStep& stp, int32_t v, uint
 // row group's distinct keys together and reuse the lane's last result for a
 // repeated key.  Returns the new keep bits.
 __device__ __forceinline__ uint32_t ws_step_rows(const ShStep& stp, const uint8_t* col, uint32_t keep, uint32_t* gkb,
-                                              bool grouped, uint32_t lane) {
+                                              bool grouped, uint64_t pol_keep, uint32_t lane) {
     const uint32_t flags = stp.flags, dcard = stp.digit_card;
     const int32_t lo = stp.lo, hi = stp.hi, dbase = stp.digit_base;
     const bool filt = (flags & GX_STEP_FILTER) != 0, probe = (flags & GX_STEP_PROBE) != 0;
@@ -487,7 +516,7 @@ __device__ __forceinline__ uint32_t ws_step_rows(const ShStep& stp, const uint8_
                 const uint32_t u = (uint32_t)v[i] - hbase;
                 const bool r = ((kk >> i) & 1u) && !again && !bucket && v[i] != kEmptyKey && (!dense || u < hspan);
                 const unsigned long long* sl = (const unsigned long long*)ht + (dense ? 1 + u : hash_key32(v[i], htlog));
-                ee[i] = r ? __ldg(sl) : (unsigned long long)kEmptySlot;
+                ee[i] = r ? ws_ld_slot(sl, pol_keep) : (unsigned long long)kEmptySlot;
                 rd |= r ? 1u << i : 0u;
             }
 #pragma unroll
@@ -618,20 +647,14 @@ constexpr uint32_t kSigQ4 = ws_sig(6, GX_AGG_SUM_DIFF, true, kWkP | kWkD, kWkP, 
 template <uint32_t SIG>
 __device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* sbase, const uint32_t* off,
                                                const uint32_t* msk, uint32_t keep, uint32_t* tkey,
-                                               unsigned long long* tsum, uint32_t lane) {
+                                               unsigned long long* tsum, uint64_t pol_keep, uint32_t lane) {
     constexpr uint32_t NS = SIG & 7, AGG = (SIG >> 3) & 7;
     constexpr bool GR = ((SIG >> 6) & 1) != 0;
     int64_t acc = 0;
-    int32_t mv[NS], mp[NS];  // per probe step: the lane's last key and its result
-    bool mh[NS], mf[NS];
     uint32_t cd[NS];  // constant steps: the group-key digit
     int32_t cv[NS];   // constant steps: the value
 #pragma unroll
     for (uint32_t s = 0; s < NS; ++s) {
-        mh[s] = false;
-        mf[s] = false;
-        mv[s] = 0;
-        mp[s] = 0;
         cd[s] = 0;
         cv[s] = 0;
         if (s + 1 < NS && msk[s] == 0) {
@@ -698,48 +721,30 @@ __device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* 
                     hbase = (uint32_t)hdr;
                     hspan = (uint32_t)(hdr >> 32);
                 }
-                // first-slot reads of the lane's distinct keys, all issued before use
+                // the first slot of every kept row's key, all read before any is used
                 uint64_t ee[4];
-                uint32_t rd = 0;
 #pragma unroll
                 for (uint32_t i = 0; i < 4; ++i) {
-                    const bool again =
-                        (i > 0 && v[i] == v[i - 1] && ((kk >> (i - 1)) & 1u)) || (mh[s] && v[i] == mv[s]);
                     const uint32_t u = (uint32_t)v[i] - hbase;
-                    const bool r =
-                        ((kk >> i) & 1u) && !again && !bucket && v[i] != kEmptyKey && (!dense || u < hspan);
+                    const bool r = ((kk >> i) & 1u) && !bucket && v[i] != kEmptyKey && (!dense || u < hspan);
                     const unsigned long long* sl =
                         (const unsigned long long*)ht + (dense ? 1 + u : hash_key32(v[i], htlog));
-                    ee[i] = r ? __ldg(sl) : (unsigned long long)kEmptySlot;
-                    rd |= r ? 1u << i : 0u;
+                    ee[i] = r ? ws_ld_slot(sl, pol_keep) : (unsigned long long)kEmptySlot;
                 }
 #pragma unroll
                 for (uint32_t i = 0; i < 4; ++i) {
                     if (!((kk >> i) & 1u)) continue;
+                    const int32_t ek = (int32_t)(uint32_t)ee[i];
                     bool f;
                     int32_t p = v[i];
-                    if (mh[s] && v[i] == mv[s]) {
-                        f = mf[s];
-                        p = mp[s];
-                    } else if ((rd >> i) & 1u) {
-                        const int32_t ek = (int32_t)(uint32_t)ee[i];
-                        if (ek == v[i]) {
-                            f = true;
-                            p = (int32_t)(uint32_t)(ee[i] >> 32);
-                        } else if (dense || ek == kEmptyKey) {
-                            f = false;
-                        } else {
-                            f = sh_probe(ht, htlog, htlay, v[i], &p);
-                        }
+                    if (ek == v[i] && v[i] != kEmptyKey) {
+                        f = true;
+                        p = (int32_t)(uint32_t)(ee[i] >> 32);
+                    } else if (!bucket && (dense || ek == kEmptyKey)) {
+                        f = false;  // an empty first slot, or a dense table's slot of another key
                     } else {
-                        // bucket tables, keys the memo held when the reads were issued,
-                        // the reserved key, keys outside a dense range
-                        f = sh_probe(ht, htlog, htlay, v[i], &p);
+                        f = sh_probe(ht, htlog, htlay, v[i], &p);  // a linear chain, or a bucket table
                     }
-                    mh[s] = true;
-                    mv[s] = v[i];
-                    mf[s] = f;
-                    mp[s] = p;
                     pp[i] = p;
                     if (!f) kk &= ~(1u << i);
                 }
@@ -797,9 +802,13 @@ __global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_consta
     uint4* const cslot = (uint4*)wmem;                       // constant columns (4 copies of the value)
     uint64_t* const bar = (uint64_t*)(wmem + 4 * kWsMaxCols);  // the warp's stage mbarrier
     uint32_t* const areas = wmem + kWsHead;                  // n_areas x kWsTile words
-    uint32_t* const gkb = areas + (size_t)P.n_areas * kWsTile;  // grouped: group key of each row of the tile
-    uint32_t* const tkey = gkb + kWsTile;                    // grouped: group table keys, then sums
+    // grouped plans: the run-time evaluator's group key of each row of the tile
+    // (compile-time evaluators keep keys in registers), then the group table
+    uint32_t* const gkb = areas + (size_t)P.n_areas * kWsTile;
+    // grouped: the CTA's group table (keys, then sums) after the warps' regions
+    uint32_t* const tkey = s_kpre + P.chunk_words + (size_t)kWsWarps * P.warp_words;
     unsigned long long* const tsum = (unsigned long long*)(tkey + kWsGroupSlots);
+    const uint64_t pol_keep = ws_policy_keep(), pol_stream = ws_policy_stream();
 
     for (uint32_t i = tid; i < ncols * (uint32_t)(sizeof(gx_dcol) / 4); i += kWsNT)
         ((uint32_t*)s_cols)[i] = ((const uint32_t*)P.cols)[i];
@@ -822,7 +831,7 @@ __global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_consta
     }
     if (lane == 0) mbar_init(bar, 1);
     if (P.grouped_tab) {
-        for (uint32_t i = lane; i < kWsGroupSlots; i += 32) {
+        for (uint32_t i = tid; i < kWsGroupSlots; i += kWsNT) {
             tkey[i] = kEmptyGKey;
             tsum[i] = 0;
         }
@@ -857,7 +866,7 @@ __global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_consta
         const uint32_t vm = ws_decide(P, s_cols, s_kbits, s_kpre, t0, W, t_end, lane, T, C);
         ws_prefetch_meta(P, s_cols, s_kbits, s_kpre, t0 + 4 * W, W, t_end, lane);
         // the staged ranges of every tile of the four go to L2 now
-        if (((vm >> (lane >> 3)) & 1u) && (lane & 7) < ncols && C.mode == kWmStage) ws_bulk_prefetch_l2(C.src, C.bytes);
+        if (((vm >> (lane >> 3)) & 1u) && (lane & 7) < ncols && C.mode == kWmStage) ws_bulk_prefetch_l2(C.src, C.bytes, pol_stream);
         for (uint32_t q = 0; q < 4 && !stop; ++q) {
             if (!((vm >> q) & 1u)) continue;
             const uint32_t L0 = 8 * q, Lc = 8 * q + (lane & 7);
@@ -877,7 +886,7 @@ __global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_consta
             if (total) {
                 if (lane == 0) mbar_expect_tx_arrive(bar, total);
                 __syncwarp();
-                if (my) bulk_copy_1d(areas + (size_t)P.stage_of[lane] * kWsTile, src, my, bar);
+                if (my) ws_bulk_copy(areas + (size_t)P.stage_of[lane] * kWsTile, src, my, bar, pol_stream);
             }
             // ---- decodes, one column at a time by the whole warp
             int terr = __any_sync(0xFFFFFFFFu, mine && mode == kWmBad) ? kErrCorrupt : 0;
@@ -962,7 +971,7 @@ __global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_consta
                         off[s] = __shfl_sync(0xFFFFFFFFu, roff, c);
                         msk[s] = __shfl_sync(0xFFFFFFFFu, rmask, c);
                     }
-                    local += ws_eval_sig<SIG>(Q, smem, off, msk, keep, tkey, tsum, lane);
+                    local += ws_eval_sig<SIG>(Q, smem, off, msk, keep, tkey, tsum, pol_keep, lane);
                 }
                 uint32_t coff = 0, cmask = 0;  // the carried column (none: carried values are 0)
                 bool carried = false;
@@ -980,7 +989,7 @@ __global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_consta
                     if (msk == 0) {
                         if (ws_step_const(stp, *(const int32_t*)(smem + off), keep, gkb, grouped, lane)) keep = 0;
                     } else if ((flags & (GX_STEP_FILTER | GX_STEP_PROBE)) || stp.digit_card) {
-                        keep = ws_step_rows(stp, smem + off, keep, gkb, grouped, lane);
+                        keep = ws_step_rows(stp, smem + off, keep, gkb, grouped, pol_keep, lane);
                     }
                     if (s + 1 == ns && keep)
                         local += ws_aggregate(agg, grouped, carried, smem + off, msk, smem + coff, cmask, keep, gkb,
@@ -992,10 +1001,11 @@ __global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_consta
             if (lane == 0) fence_proxy_async_smem();
         }
     }
-    // ---- the warp's results
+    // ---- results: the CTA's group table once every warp is done, else the warp's sum
     __syncwarp();
     if (grouped && P.grouped_tab) {
-        for (uint32_t i = lane; i < kWsGroupSlots; i += 32) {
+        __syncthreads();
+        for (uint32_t i = tid; i < kWsGroupSlots; i += kWsNT) {
             const uint32_t key = tkey[i];
             if (key != kEmptyGKey && !group_add_global(Q.g_keys, Q.g_sums, Q.g_log2, (int64_t)key, (int64_t)tsum[i]))
                 raise_error(kErrCapacity);
