@@ -90,6 +90,23 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* m, uint32_t phase) {
     return false;
 }
 
+// L2 cache policies: join tables stay (evict last), streamed bytes go first.
+__device__ __forceinline__ uint64_t ws_policy_keep() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t ws_policy_stream() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// A join-table slot read under policy pol (read-only path).
+__device__ __forceinline__ unsigned long long ws_ld_slot(const unsigned long long* a, uint64_t pol) {
+    unsigned long long v;
+    asm("ld.global.nc.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(pol));
+    return v;
+}
 // ------------------------------------------------- segmented LZ4, one lane
 // Decodes the K output words of one segment of a segmented LZ4 block (format
 // in gx_internal.h) into out[0..K).  The block's compressed bytes from

@@ -473,6 +473,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
         s_gsum[i] = 0;
         s_gkey[i] = kEmptyGKey;
     }
+    const uint64_t pol_keep = ws_policy_keep();  // join tables stay in L2 while the columns stream through
     if (!SINGLE)
         for (uint32_t i = tid; i < P.qc_bytes / 16; i += NT) ((uint4*)s_qc)[i] = __ldg(P.qc + i);
     if (tid == 0) {
@@ -703,7 +704,7 @@ __global__ void __launch_bounds__(NT, MINB) shared_scan_kernel(const __grid_cons
                             const unsigned long long* sp =
                                 (const unsigned long long*)ht + (dense ? 1 + u : hash_key32(v, htlog));
                             vv[i] = v;
-                            ee[i] = rd ? __ldg(sp) : (unsigned long long)kEmptySlot;
+                            ee[i] = rd ? ws_ld_slot(sp, pol_keep) : (unsigned long long)kEmptySlot;
                             fk |= rd ? 1u << i : 0u;
                         }
 #pragma unroll

@@ -9,27 +9,32 @@
 // (core/metadata.cuh:638-658) and the per-chunk worker loop of
 // usecases/ssb/queries/01.hpp:350-424 folded into the same launch.
 //
-// Every warp is an independent worker: there is no block-wide barrier and no
-// producer.  Warp w of the grid takes the row tiles w, w + W, w + 2W, ... of
-// the table (kWsTile rows of one block each; W warps in the grid).  Per tile:
-//   * lane c loads column c's directory entry and the tile's side-index
-//     entries, and decides how the column's rows are read: in place from
-//     HBM (raw rows, or an LZ4 literal run whose first byte is 16-byte
-//     aligned), as one value for the whole tile (a cascaded run covering the
-//     tile), or decoded by the warp into the warp's buffer in shared memory
-//     (an LZ4 range with matches: groups of lanes per segment; a cascaded
-//     page: run windows of 32 runs, one run per lane);
-//   * the in-place ranges are prefetched into L2 (one line per lane);
-//   * the plan's steps run over batches of 128 rows, 4 consecutive rows per
-//     lane read with one 16-byte load per column (every column's load of a
-//     batch is issued before the first step runs), filters, join probes
-//     (each lane probes a repeated key once), group-key digits, carried
-//     value, and the aggregate.
+// Every warp is an independent worker: after one block-wide barrier at the
+// start (chunk keep bits of the launch and their prefix counts, computed by
+// each CTA) no warp waits for another.  The 1024-row tiles of the surviving
+// chunks form a dense rank space; warp w of the grid takes tiles w, w + W,
+// w + 2W, ... (W warps), four at a time:
+//   * one decision round per four tiles: lane 8q + c reads column c's
+//     directory entry and side-index entries for tile q (a cascaded page's
+//     header and up to 8 runs too) and picks how the column is read --
+//     staged (raw rows or a 16-byte aligned LZ4 literal run: one bulk copy
+//     of the tile's rows into the warp's stage area), constant (a cascaded
+//     page or run that holds one value on the tile), or decoded by the warp
+//     into its buffer (LZ4 ranges with matches: groups of lanes per
+//     segment; other cascaded pages: run windows of 32 runs, one per lane);
+//     the round's staged ranges are bulk-prefetched into L2 and the next
+//     round's directory lines prefetched;
+//   * per tile: the bulk copies on the warp's mbarrier, the decodes, then the
+//     plan's steps over row groups of 128 rows (4 consecutive rows per lane,
+//     one 16-byte shared load per column).  Plans of the SSB shapes run a
+//     compile-time evaluator selected by their signature (all values of a
+//     row group in registers, steps over a constant column decided once per
+//     tile); other plans a run-time step-major evaluator.
 // Scalar sums stay in registers; grouped sums go to the CTA's group table in
 // shared memory (keys that find no slot go to the global table), flushed when
 // the CTA is done.  Join-table reads carry an L2 evict-last policy and the
 // streamed column bytes an evict-first one, so that the tables stay in L2
-// while the fact columns pass through it.  Nothing waits on another warp.
+// while the fact columns pass through it.
 
 constexpr uint32_t kWsLog2 = 10;
 constexpr uint32_t kWsTile = 1u << kWsLog2;    // rows of one warp tile
@@ -82,23 +87,6 @@ __device__ __forceinline__ uint32_t ws_scan(uint32_t x, uint32_t lane) {
     return x;
 }
 
-// L2 cache policies: join tables stay (evict last), streamed bytes go first.
-__device__ __forceinline__ uint64_t ws_policy_keep() {
-    uint64_t p;
-    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-__device__ __forceinline__ uint64_t ws_policy_stream() {
-    uint64_t p;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-// A join-table slot read under policy pol (read-only path).
-__device__ __forceinline__ unsigned long long ws_ld_slot(const unsigned long long* a, uint64_t pol) {
-    unsigned long long v;
-    asm("ld.global.nc.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(pol));
-    return v;
-}
 // One bulk copy (no multicast) completing on m, its lines read under policy pol.
 __device__ __forceinline__ void ws_bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* m, uint64_t pol) {
     asm volatile(
