@@ -635,7 +635,8 @@ constexpr uint32_t kSigQ4 = ws_sig(6, GX_AGG_SUM_DIFF, true, kWkP | kWkD, kWkP, 
 template <uint32_t SIG>
 __device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* sbase, const uint32_t* off,
                                                const uint32_t* msk, uint32_t keep, uint32_t* tkey,
-                                               unsigned long long* tsum, uint64_t pol_keep, uint32_t lane) {
+                                               unsigned long long* tsum, uint64_t pol_keep, const uint64_t* s_hdr,
+                                               uint32_t lane) {
     constexpr uint32_t NS = SIG & 7, AGG = (SIG >> 3) & 7;
     constexpr bool GR = ((SIG >> 6) & 1) != 0;
     int64_t acc = 0;
@@ -652,7 +653,20 @@ __device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* 
             cv[s] = v;
             bool f = !(K & kWkF) || (v >= stp.lo && v <= stp.hi);
             int32_t pp = v;
-            if ((K & kWkP) && f) f = ht_probe_any(stp.ht, stp.ht_log2, stp.ht_layout, v, &pp);
+            if ((K & kWkP) && f) {
+                if (stp.ht_layout == GX_HT_DENSE) {  // one read: the table header is cached
+                    const uint64_t hdr = s_hdr[s];
+                    const uint32_t u = (uint32_t)v - (uint32_t)hdr;
+                    f = false;
+                    if (v != kEmptyKey && u < (uint32_t)(hdr >> 32)) {
+                        const unsigned long long e = ws_ld_slot((const unsigned long long*)stp.ht + 1 + u, pol_keep);
+                        f = (int32_t)(uint32_t)e == v;
+                        pp = (int32_t)(uint32_t)(e >> 32);
+                    }
+                } else {
+                    f = ht_probe_any(stp.ht, stp.ht_log2, stp.ht_layout, v, &pp);
+                }
+            }
             if ((K & kWkD) && f) {
                 cd[s] = (uint32_t)(pp - stp.digit_base);
                 if (cd[s] >= stp.digit_card) {
@@ -693,10 +707,14 @@ __device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* 
             }
             const int32_t v[4] = {(int32_t)w[s].x, (int32_t)w[s].y, (int32_t)w[s].z, (int32_t)w[s].w};
             if (K & kWkF) {
-                const int32_t lo = stp.lo, hi = stp.hi;
+                // lo <= v <= hi as one unsigned comparison of v - lo with hi - lo
+                // (an empty range, hi < lo, keeps nothing)
+                const uint32_t lo = (uint32_t)stp.lo, span = (uint32_t)stp.hi - lo;
+                const uint32_t none = stp.hi < stp.lo ? 0u : 15u;
+                uint32_t pass = 0;
 #pragma unroll
-                for (uint32_t i = 0; i < 4; ++i)
-                    if (!(v[i] >= lo && v[i] <= hi)) kk &= ~(1u << i);
+                for (uint32_t i = 0; i < 4; ++i) pass |= ((uint32_t)v[i] - lo <= span) ? 1u << i : 0u;
+                kk &= pass & none;
             }
             int32_t pp[4] = {v[0], v[1], v[2], v[3]};
             if (K & kWkP) {
@@ -705,7 +723,7 @@ __device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* 
                 const bool dense = htlay == GX_HT_DENSE, bucket = htlay == GX_HT_BUCKET;
                 uint32_t hbase = 0, hspan = 0;
                 if (dense) {
-                    const uint64_t hdr = __ldg((const unsigned long long*)ht);
+                    const uint64_t hdr = s_hdr[s];
                     hbase = (uint32_t)hdr;
                     hspan = (uint32_t)(hdr >> 32);
                 }
@@ -758,17 +776,32 @@ __device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* 
             }
             if (!kk) break;
             if (s + 1 == NS) {
+                if (GR) {
 #pragma unroll
-                for (uint32_t i = 0; i < 4; ++i) {
-                    if (!((kk >> i) & 1u)) continue;
-                    const int64_t val = AGG == GX_AGG_SUM_PRODUCT ? (int64_t)v[i] * carry[i]
-                                        : AGG == GX_AGG_SUM_DIFF  ? (int64_t)v[i] - carry[i]
-                                        : AGG == GX_AGG_COUNT      ? 1
-                                                                   : (int64_t)v[i];
-                    if (GR)
+                    for (uint32_t i = 0; i < 4; ++i) {
+                        if (!((kk >> i) & 1u)) continue;
+                        const int64_t val = AGG == GX_AGG_SUM_PRODUCT ? (int64_t)v[i] * carry[i]
+                                            : AGG == GX_AGG_SUM_DIFF  ? (int64_t)v[i] - carry[i]
+                                            : AGG == GX_AGG_COUNT      ? 1
+                                                                       : (int64_t)v[i];
                         ws_group_add(g[i], val, tkey, tsum, Q.g_keys, Q.g_sums, Q.g_log2);
-                    else
-                        acc += val;
+                    }
+                } else {
+                    // kept rows as multiply-adds by 0 or 1 (one wide multiply-add per row)
+#pragma unroll
+                    for (uint32_t i = 0; i < 4; ++i) {
+                        const int32_t on = (int32_t)((kk >> i) & 1u);
+                        if (AGG == GX_AGG_SUM_PRODUCT) {
+                            acc += (int64_t)v[i] * (int64_t)(on ? carry[i] : 0);
+                        } else if (AGG == GX_AGG_SUM_DIFF) {
+                            acc += (int64_t)v[i] * on;
+                            acc -= (int64_t)carry[i] * on;
+                        } else if (AGG == GX_AGG_COUNT) {
+                            acc += on;
+                        } else {
+                            acc += (int64_t)v[i] * on;
+                        }
+                    }
                 }
             }
         }
@@ -781,6 +814,7 @@ __global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_consta
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ gx_dcol s_cols[kWsMaxCols];
     __shared__ uint32_t s_nsurv;
+    __shared__ uint64_t s_hdr[GX_MAX_STEPS];  // dense join tables' {base, span} headers, per step
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t ncols = P.n_cols;
     const ShQuery& Q = P.q;
@@ -798,6 +832,12 @@ __global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_consta
     unsigned long long* const tsum = (unsigned long long*)(tkey + kWsGroupSlots);
     const uint64_t pol_keep = ws_policy_keep(), pol_stream = ws_policy_stream();
 
+    if (tid < GX_MAX_STEPS) {
+        const ShStep& st = Q.steps[tid];
+        s_hdr[tid] = (tid < Q.n_steps && (st.flags & GX_STEP_PROBE) && st.ht_layout == GX_HT_DENSE)
+                         ? __ldg((const unsigned long long*)st.ht)
+                         : 0ull;
+    }
     for (uint32_t i = tid; i < ncols * (uint32_t)(sizeof(gx_dcol) / 4); i += kWsNT)
         ((uint32_t*)s_cols)[i] = ((const uint32_t*)P.cols)[i];
     // chunk keep (keep_in and the prune predicates' chunk min/max, the
@@ -959,7 +999,7 @@ __global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_consta
                         off[s] = __shfl_sync(0xFFFFFFFFu, roff, c);
                         msk[s] = __shfl_sync(0xFFFFFFFFu, rmask, c);
                     }
-                    local += ws_eval_sig<SIG>(Q, smem, off, msk, keep, tkey, tsum, pol_keep, lane);
+                    local += ws_eval_sig<SIG>(Q, smem, off, msk, keep, tkey, tsum, pol_keep, s_hdr, lane);
                 }
                 uint32_t coff = 0, cmask = 0;  // the carried column (none: carried values are 0)
                 bool carried = false;
