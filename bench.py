@@ -98,7 +98,7 @@ def peaks():
 
 def profile_traffic():
     """dram bytes per launch of the fused scan kernel from the committed ncu summary (or None)."""
-    p = ROOT / "profiles" / "shared_scan_kernel_q1_pruned_60M.md"
+    p = ROOT / "profiles" / "warp_scan_kernel_q1_pruned_60M.md"
     if not p.exists():
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", p.read_text())
@@ -1012,6 +1012,45 @@ def profile_scan(kind, rows, segments):
             print(json.dumps({"profile_scan": kind, "rows": rows, "launch": i, "ms": a.elapsed_time(b)}))
 
 
+def ingest(rows, segments, steps):
+    """Column ingest of the Q1 workload's four columns: the GPU encoder from HBM
+    (gx_column_encode_device: zone maps, plan pass, host layout, write pass, the
+    device metadata and the host copy of the payload) against the host encoder
+    (gx_column_encode, all host threads) with the same options, one JSON line per
+    column.  GB/s are of the uncompressed int32 input."""
+    import ctypes as C
+
+    import torch
+
+    from golap_public_b200 import _lib as L
+    from golap_public_b200 import api, datagen
+
+    f = datagen.fact_q1(rows, True)
+    codecs = {"date_key": "cascaded"}
+    for name, v in f.items():
+        codec = codecs.get(name, "lz4")
+        dev = torch.from_numpy(v).cuda()
+        times = []
+        for i in range(steps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            col = api.Column.from_device(dev, codec, ROWS_PER_CHUNK, ROWS_PER_BLOCK, segments)
+            times.append(time.perf_counter() - t0)
+            comp = col.info.comp_bytes
+            col.free()
+        t_dev = sorted(times[1:])[len(times[1:]) // 2]
+        o = api.Column._opts(codec, ROWS_PER_CHUNK, ROWS_PER_BLOCK, segments, L.GX_LZ4_LITERAL, 16, 0)
+        h = C.c_void_p()
+        t0 = time.perf_counter()
+        L.check(L.lib().gx_column_encode(v.ctypes.data_as(C.c_void_p), len(v), C.byref(o), C.byref(h)))
+        t_host = time.perf_counter() - t0
+        L.lib().gx_column_free(h)
+        print(json.dumps({"ingest": name, "codec": codec, "rows": rows, "comp_bytes": comp,
+                          "device_ms": round(t_dev * 1e3, 3), "device_gbs": round(4 * rows / t_dev / 1e9, 1),
+                          "host_ms": round(t_host * 1e3, 1), "host_gbs": round(4 * rows / t_host / 1e9, 2),
+                          "host_threads": os.cpu_count()}))
+
+
 def main():
     global N_ROWS
     ap = argparse.ArgumentParser()
@@ -1038,6 +1077,8 @@ def main():
     ap.add_argument("--profile-batch", action="store_true",
                     help="only build the batch table and run the 256-query mixed batch (shared form, dense join "
                          "tables, automatic launch shape) three times: the command profiler captures use")
+    ap.add_argument("--ingest", action="store_true",
+                    help="time the GPU column encoder against the host encoder on --rows rows and exit")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     N_ROWS = args.rows
@@ -1049,6 +1090,9 @@ def main():
         return
     if args.profile_batch:
         profile_batch(args.batch_rows)
+        return
+    if args.ingest:
+        ingest(args.rows, args.segments, args.steps)
         return
 
     if args.impl == "reference":

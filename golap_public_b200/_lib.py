@@ -16,6 +16,7 @@ u8p = C.POINTER(C.c_uint8)
 
 GX_OK, GX_ERR_CUDA, GX_ERR_CORRUPT, GX_ERR_CAPACITY, GX_ERR_TIMEOUT, GX_ERR_NOMEM, GX_ERR_INVALID = range(7)
 GX_CODEC_NONE, GX_CODEC_LZ4, GX_CODEC_CASCADED = 0, 1, 2
+GX_LZ4_LITERAL = 0xFFFFFFF0  # lz4_min_match admitting no match: every block one literal run
 GX_STEP_FILTER, GX_STEP_PROBE, GX_STEP_CARRY, GX_STEP_VALUE, GX_STEP_GROUP = 1, 2, 4, 8, 16
 GX_AGG_SUM, GX_AGG_SUM_PRODUCT, GX_AGG_COUNT, GX_AGG_BUILD, GX_AGG_SUM_DIFF = 0, 1, 2, 3, 4
 GX_HT_LINEAR, GX_HT_BUCKET, GX_HT_DENSE = 0, 1, 2
@@ -93,9 +94,11 @@ _SIGS = {
     "gx_device_count": (C.c_int32, [C.POINTER(C.c_int)]),
     "gx_encode_opts_default": (C.c_int32, [C.POINTER(EncodeOpts)]),
     "gx_column_encode": (C.c_int32, [P, C.c_uint64, C.POINTER(EncodeOpts), C.POINTER(P)]),
+    "gx_column_encode_device": (C.c_int32, [P, C.c_uint64, C.POINTER(EncodeOpts), C.POINTER(P), P]),
     "gx_column_free": (C.c_int32, [P]),
     "gx_column_info_get": (C.c_int32, [P, C.POINTER(ColumnInfo)]),
     "gx_column_chunk_minmax": (C.c_int32, [P, P, P]),
+    "gx_column_block_minmax": (C.c_int32, [P, P, P]),
     "gx_column_blocks": (C.c_int32, [P, P]),
     "gx_column_payload": (C.c_int32, [P, C.POINTER(u8p), C.POINTER(C.c_uint64)]),
     "gx_column_seg_index": (C.c_int32, [P, C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64)]),

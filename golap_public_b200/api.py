@@ -48,6 +48,15 @@ class Column:
                  rows_per_block: int = 16384, lz4_segments: int = 128, lz4_min_match: int = 0,
                  lz4_search_depth: int = 16, threads: int = 0, name: str = ""):
         values = np.ascontiguousarray(values, dtype=np.int32)
+        o = self._opts(codec, rows_per_chunk, rows_per_block, lz4_segments, lz4_min_match, lz4_search_depth, threads)
+        h = C.c_void_p()
+        check(L.lib().gx_column_encode(values.ctypes.data_as(C.c_void_p), len(values), C.byref(o), C.byref(h)))
+        self.handle = h
+        self.name = name
+        self.codec = codec
+
+    @staticmethod
+    def _opts(codec, rows_per_chunk, rows_per_block, lz4_segments, lz4_min_match, lz4_search_depth, threads):
         o = L.EncodeOpts()
         check(L.lib().gx_encode_opts_default(C.byref(o)))
         o.codec = CODECS[codec]
@@ -57,11 +66,28 @@ class Column:
         o.lz4_min_match = lz4_min_match
         o.lz4_search_depth = lz4_search_depth
         o.threads = threads
+        return o
+
+    @classmethod
+    def from_device(cls, values, codec: str = "lz4", rows_per_chunk: int = 1_000_000, rows_per_block: int = 16384,
+                    lz4_segments: int = 128, name: str = "", stream=None) -> "Column":
+        """Encodes an int32 CUDA tensor on the GPU (gx_column_encode_device): the column is in HBM on
+        return, byte-identical to Column(values.cpu().numpy(), ...) with the same options.  LZ4 blocks
+        are literal runs (lz4_min_match = GX_LZ4_LITERAL)."""
+        import torch
+
+        if not (isinstance(values, torch.Tensor) and values.is_cuda and values.dtype == torch.int32):
+            raise TypeError("Column.from_device needs an int32 CUDA tensor")
+        values = values.contiguous()
+        o = cls._opts(codec, rows_per_chunk, rows_per_block, lz4_segments, L.GX_LZ4_LITERAL, 0, 0)
         h = C.c_void_p()
-        check(L.lib().gx_column_encode(values.ctypes.data_as(C.c_void_p), len(values), C.byref(o), C.byref(h)))
+        check(L.lib().gx_column_encode_device(_dptr(values), values.numel(), C.byref(o), C.byref(h),
+                                              _stream_handle(stream)))
+        self = cls.__new__(cls)
         self.handle = h
         self.name = name
         self.codec = codec
+        return self
 
     # --- inspection
     @property
@@ -75,6 +101,16 @@ class Column:
         mins = np.zeros(n, np.int32)
         maxs = np.zeros(n, np.int32)
         check(L.lib().gx_column_chunk_minmax(self.handle, mins.ctypes.data_as(C.c_void_p),
+                                             maxs.ctypes.data_as(C.c_void_p)))
+        return mins, maxs
+
+    def block_minmax(self):
+        """Per-block-slot zone maps (n_chunks * blocks_per_chunk entries each)."""
+        i = self.info
+        n = i.n_chunks * i.blocks_per_chunk
+        mins = np.zeros(n, np.int32)
+        maxs = np.zeros(n, np.int32)
+        check(L.lib().gx_column_block_minmax(self.handle, mins.ctypes.data_as(C.c_void_p),
                                              maxs.ctypes.data_as(C.c_void_p)))
         return mins, maxs
 

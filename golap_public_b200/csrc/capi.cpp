@@ -130,6 +130,13 @@ gx_status gx_column_chunk_minmax(const gx_column* c, int32_t* mins, int32_t* max
     return GX_OK;
 }
 
+gx_status gx_column_block_minmax(const gx_column* c, int32_t* mins, int32_t* maxs) {
+    if (!c || !mins || !maxs) return gx::set_error(GX_ERR_INVALID, "gx_column_block_minmax: null argument");
+    memcpy(mins, c->bmins.data(), 4 * c->bmins.size());
+    memcpy(maxs, c->bmaxs.data(), 4 * c->bmaxs.size());
+    return GX_OK;
+}
+
 gx_status gx_column_blocks(const gx_column* c, gx_block_info* out) {
     if (!c || !out) return gx::set_error(GX_ERR_INVALID, "gx_column_blocks: null argument");
     uint64_t k = 0;

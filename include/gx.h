@@ -106,10 +106,27 @@ gx_status gx_encode_opts_default(gx_encode_opts* opts);
 /* Encode n_rows int32 values from host memory into a new column (host side). */
 gx_status gx_column_encode(const int32_t* host_values, uint64_t n_rows,
                            const gx_encode_opts* opts, gx_column** out);
+/* lz4_min_match value that admits no match: every LZ4 block is one literal run
+ * (the decode-cost-aware policy's no-match candidate). */
+#define GX_LZ4_LITERAL 0xFFFFFFF0u
+/* Encode n_rows int32 values already in device memory into a new column that is
+ * resident in HBM on return (as after gx_column_to_device(col, 1, stream)), with
+ * its host copy, per-chunk min/max and per-block zone maps filled in.  The column
+ * is byte-identical to gx_column_encode of the same values and options.  Codecs:
+ * NONE, CASCADED, and LZ4 with lz4_min_match = GX_LZ4_LITERAL (other LZ4 match
+ * policies are GX_ERR_INVALID: use gx_column_encode).  Synchronises `stream`.
+ * Replaces: prepare_compressed's per-chunk compress + MinMaxMeta::init_chunk
+ * (core/apps.cuh:149-255, core/metadata.cuh:157-160) for data already on the GPU. */
+gx_status gx_column_encode_device(const int32_t* values_dev, uint64_t n_rows, const gx_encode_opts* opts,
+                                  gx_column** out, void* stream);
 gx_status gx_column_free(gx_column* col);
 gx_status gx_column_info_get(const gx_column* col, gx_column_info* out);
 /* Per-chunk min/max (host arrays of n_chunks entries; MinMaxMeta mins_hst/maxs_hst). */
 gx_status gx_column_chunk_minmax(const gx_column* col, int32_t* mins, int32_t* maxs);
+/* Per-block zone maps (host arrays of n_chunks * blocks_per_chunk entries, one per
+ * block slot in chunk order; a slot past a short chunk's end holds the empty range
+ * INT32_MAX / INT32_MIN).  The block-level refinement of MinMaxMeta. */
+gx_status gx_column_block_minmax(const gx_column* col, int32_t* mins, int32_t* maxs);
 /* Per-block descriptors (host array of n_blocks entries). */
 gx_status gx_column_blocks(const gx_column* col, gx_block_info* out);
 /* Raw access to the host copy of the compressed payload and the LZ4 segment
