@@ -96,13 +96,24 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """dram bytes per launch of the fused scan kernel from the committed ncu summary (or None)."""
-    p = ROOT / "profiles" / "warp_scan_kernel_q1_pruned_60M.md"
+def profile_traffic(name="warp_scan_kernel_q1_pruned_60M.md", rows=None):
+    """DRAM bytes (read + write) per launch of the fused scan kernel from a committed ncu summary, or
+    None.  With `rows`, a capture of a smaller case (its `captured_rows`) is scaled to `rows`: used
+    only for the full scan, whose traffic grows in proportion to the rows."""
+    p = ROOT / "profiles" / name
     if not p.exists():
         return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", p.read_text())
-    return int(m.group(1)) if m else None
+    text = p.read_text()
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", text)
+    if not m:
+        return None
+    t = int(m.group(1))
+    if rows is not None:
+        r = re.search(r"captured_rows:\s*([0-9]+)", text)
+        if not r:
+            return None
+        t = int(round(t * rows / int(r.group(1))))
+    return t
 
 
 class Clocks:
@@ -430,7 +441,7 @@ def gpu_arm(args, rank, world):
     want_all = int((f["extended_price"][m_all].astype(np.int64) * f["discount"][m_all].astype(np.int64)).sum())
     all_slots = slots_of(range(n_chunks), zone=False)
 
-    def full_scan(fct, label):
+    def full_scan(fct, label, traffic=None):
         qa = queries.Q1Query(fct, dd, ok_all, int(dd["d_key"].min()), int(dd["d_key"].max()), *DISC, *QTY,
                              prune=False)
         if qa.run() != want_all:
@@ -442,10 +453,10 @@ def gpu_arm(args, rank, world):
         nbytes = alg_bytes(fct, Q1_COLS, all_slots, 0, 0)
         return {"ms": avg, "rows_per_s": N_ROWS / (avg * 1e-3), "comp_gbs": nbytes / (avg * 1e-3) / 1e9,
                 "roofline_frac": nbytes / (avg * 1e-3) / 1e9 / pk, "uncomp_gbs": N_ROWS * 16 / (avg * 1e-3) / 1e9,
-                "roofline": roofline(nbytes, avg, pk, pk_kind),
+                "roofline": roofline(nbytes, avg, pk, pk_kind, traffic),
                 "comp_bytes": {k: c.info.comp_bytes for k, c in fct.cols.items()}}
 
-    full = full_scan(fact, "literal policy")
+    full = full_scan(fact, "literal policy", profile_traffic("warp_scan_kernel_q1_fullscan_16M.md", N_ROWS))
     full["lz4_policy"] = "decode-cost-aware (lz4_min_match=0): random-valued columns stored as literal runs"
     # the same data with the LZ4 columns encoded with 4-byte matches
     fact_m = queries.encode_fact({k: f[k] for k in Q1_COLS if k != "date_key"}, {}, ROWS_PER_CHUNK, ROWS_PER_BLOCK,
@@ -1014,10 +1025,11 @@ def profile_scan(kind, rows, segments):
 
 def ingest(rows, segments, steps):
     """Column ingest of the Q1 workload's four columns: the GPU encoder from HBM
-    (gx_column_encode_device: zone maps, plan pass, host layout, write pass, the
-    device metadata and the host copy of the payload) against the host encoder
-    (gx_column_encode, all host threads) with the same options, one JSON line per
-    column.  GB/s are of the uncompressed int32 input."""
+    (gx_column_encode_device: zone maps, plan pass, host layout, write pass and
+    the device metadata, wall time of the call) and, apart, the first read of its
+    host payload copy, against the host encoder (gx_column_encode, all host
+    threads) with the same options; one JSON line per column.  GB/s are of the
+    uncompressed int32 input."""
     import ctypes as C
 
     import torch
@@ -1030,15 +1042,20 @@ def ingest(rows, segments, steps):
     for name, v in f.items():
         codec = codecs.get(name, "lz4")
         dev = torch.from_numpy(v).cuda()
-        times = []
-        for i in range(steps + 1):
+        times, copy_times = [], []
+        for i in range(max(3, steps) + 1):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             col = api.Column.from_device(dev, codec, ROWS_PER_CHUNK, ROWS_PER_BLOCK, segments)
-            times.append(time.perf_counter() - t0)
+            t1 = time.perf_counter()
+            col.payload_view()
+            t2 = time.perf_counter()
+            times.append(t1 - t0)
+            copy_times.append(t2 - t1)
             comp = col.info.comp_bytes
             col.free()
-        t_dev = sorted(times[1:])[len(times[1:]) // 2]
+        t_dev = float(np.median(times[1:]))
+        t_copy = float(np.median(copy_times[1:]))
         o = api.Column._opts(codec, ROWS_PER_CHUNK, ROWS_PER_BLOCK, segments, L.GX_LZ4_LITERAL, 16, 0)
         h = C.c_void_p()
         t0 = time.perf_counter()
@@ -1047,6 +1064,7 @@ def ingest(rows, segments, steps):
         L.lib().gx_column_free(h)
         print(json.dumps({"ingest": name, "codec": codec, "rows": rows, "comp_bytes": comp,
                           "device_ms": round(t_dev * 1e3, 3), "device_gbs": round(4 * rows / t_dev / 1e9, 1),
+                          "host_copy_read_ms": round(t_copy * 1e3, 3),
                           "host_ms": round(t_host * 1e3, 1), "host_gbs": round(4 * rows / t_host / 1e9, 2),
                           "host_threads": os.cpu_count()}))
 

@@ -98,6 +98,7 @@ gx_status gx_column_encode(const int32_t* host_values, uint64_t n_rows, const gx
 
 gx_status gx_column_free(gx_column* col) {
     if (!col) return GX_OK;
+    col->host_pending = false;  // going away: no host copy needed
     gx_column_release_device(col);
     delete col;
     return GX_OK;
@@ -154,6 +155,7 @@ gx_status gx_column_blocks(const gx_column* c, gx_block_info* out) {
 
 gx_status gx_column_payload(const gx_column* c, const uint8_t** payload, uint64_t* bytes) {
     if (!c || !payload || !bytes) return gx::set_error(GX_ERR_INVALID, "gx_column_payload: null argument");
+    if (const int st = gx::host_payload(c)) return st;
     *payload = c->payload.data();
     *bytes = c->payload.size();
     return GX_OK;

@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "../../include/gx.h"
@@ -323,6 +324,30 @@ __global__ void genc_fill_kernel(int32_t* a, int32_t* b, uint32_t n) {
 
 }  // namespace
 
+namespace gx {
+
+int host_payload(const gx_column* col) {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!col->host_pending) return GX_OK;
+    if (!col->d_payload) return set_error(GX_ERR_INVALID, "column payload is neither on the host nor on the device");
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (col->device >= 0 && col->device != dev) cudaSetDevice(col->device);
+    auto& host = const_cast<gx_column*>(col)->payload;
+    host.resize(col->dev_payload_bytes);
+    const cudaError_t e = cudaMemcpy(host.data(), col->d_payload, col->dev_payload_bytes, cudaMemcpyDeviceToHost);
+    if (col->device >= 0 && col->device != dev) cudaSetDevice(dev);
+    if (e != cudaSuccess) {
+        host.clear();
+        return set_error(GX_ERR_CUDA, "reading a column payload back: %s", cudaGetErrorString(e));
+    }
+    col->host_pending = false;
+    return GX_OK;
+}
+
+}  // namespace gx
+
 #define GENC_CK(call)                                                                       \
     do {                                                                                    \
         cudaError_t e_ = (call);                                                            \
@@ -513,9 +538,10 @@ extern "C" gx_status gx_column_encode_device(const int32_t* values_dev, uint64_t
         GENC_CK(cudaMalloc(&col->d_maxs, 4ull * col->n_chunks));
         GENC_CK(cudaMemcpyAsync(col->d_mins, col->mins.data(), 4ull * col->n_chunks, cudaMemcpyHostToDevice, s));
         GENC_CK(cudaMemcpyAsync(col->d_maxs, col->maxs.data(), 4ull * col->n_chunks, cudaMemcpyHostToDevice, s));
-        col->payload.resize(total);
-        GENC_CK(cudaMemcpyAsync(col->payload.data(), col->d_payload, total, cudaMemcpyDeviceToHost, s));
         GENC_CK(cudaStreamSynchronize(s));
+        // the host copy of the payload is read back on first use (host_payload)
+        col->dev_payload_bytes = total;
+        col->host_pending = true;
         cudaGetDevice(&col->device);
         if (codec == GX_CODEC_LZ4) col->lz4_direct = 1;  // every block one literal run, placed aligned
     }

@@ -183,6 +183,10 @@ struct gx_column {
     int32_t* d_bmins = nullptr;
     int32_t* d_bmaxs = nullptr;
     int device = -1;
+    // a column encoded on the device keeps its payload in HBM only until a
+    // caller needs the host copy (gx::host_payload reads it back once)
+    mutable bool host_pending = false;
+    uint64_t dev_payload_bytes = 0;
 
     gx::gx_dcol view() const {
         gx::gx_dcol v{};
@@ -200,15 +204,18 @@ struct gx_column {
         v.blocks_per_chunk = blocks_per_chunk;
         v.n_chunks = n_chunks;
         v.n_slots = n_slots;
-        v.payload_bytes = payload.size();
+        v.payload_bytes = host_pending ? dev_payload_bytes : payload.size();
         v.host_mapped = residency == 2 ? 1u : 0u;
         return v;
     }
 };
 
 namespace gx {
-// Thread-local error message plumbing (implemented in capi.cu).
+// Thread-local error message plumbing (implemented in capi.cpp).
 int set_error(int status, const char* fmt, ...);
+// Fills the host copy of a device-encoded column's payload (once; a no-op for
+// columns encoded on the host).  Implemented in encode_gpu.cu.
+int host_payload(const gx_column* col);
 
 // Host encoders (encode.cpp).
 // Encodes `rows` int32 values as a segmented (S > 1) or plain (S == 1) LZ4

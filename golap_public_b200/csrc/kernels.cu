@@ -1246,6 +1246,7 @@ extern "C" {
 
 gx_status gx_column_to_device(gx_column* col, int residency, void* stream) {
     if (!col || (residency != 1 && residency != 2)) return set_error(GX_ERR_INVALID, "gx_column_to_device: bad args");
+    if (const int st = host_payload(col)) return st;  // a device-encoded column: its host copy first
     gx_column_release_device(col);
     cudaStream_t s = (cudaStream_t)stream;
     const size_t pb = col->payload.size();
@@ -1282,6 +1283,7 @@ gx_status gx_column_to_device(gx_column* col, int residency, void* stream) {
 
 gx_status gx_column_release_device(gx_column* col) {
     if (!col) return set_error(GX_ERR_INVALID, "null column");
+    if (const int st = host_payload(col)) return st;  // keep the payload of a device-encoded column
     if (col->residency == 1 && col->d_payload) cudaFree(col->d_payload);
     if (col->h_pinned) cudaFreeHost(col->h_pinned);
     if (col->d_blocks) cudaFree(col->d_blocks);

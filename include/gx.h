@@ -111,8 +111,10 @@ gx_status gx_column_encode(const int32_t* host_values, uint64_t n_rows,
 #define GX_LZ4_LITERAL 0xFFFFFFF0u
 /* Encode n_rows int32 values already in device memory into a new column that is
  * resident in HBM on return (as after gx_column_to_device(col, 1, stream)), with
- * its host copy, per-chunk min/max and per-block zone maps filled in.  The column
- * is byte-identical to gx_column_encode of the same values and options.  Codecs:
+ * its per-chunk min/max and per-block zone maps filled in.  The host copy of the
+ * payload is read back from HBM on first use (gx_column_payload,
+ * gx_column_to_device, gx_column_release_device).  The column is byte-identical
+ * to gx_column_encode of the same values and options.  Codecs:
  * NONE, CASCADED, and LZ4 with lz4_min_match = GX_LZ4_LITERAL (other LZ4 match
  * policies are GX_ERR_INVALID: use gx_column_encode).  Synchronises `stream`.
  * Replaces: prepare_compressed's per-chunk compress + MinMaxMeta::init_chunk

@@ -172,3 +172,28 @@ def test_device_encode_rejects(cuda):
         api.Column.from_device(v.to(torch.int64))
     with pytest.raises(GxError):
         api.Column.from_device(v, "lz4", lz4_segments=3)
+
+
+def test_device_encoded_host_copy_on_demand(cuda):
+    # the payload stays in HBM until a caller needs the host copy; releasing the
+    # device copy or moving the column to pinned host memory reads it back first
+    torch = cuda
+    rng = np.random.default_rng(11)
+    v = rng.integers(0, 1 << 20, 1_500_001).astype(np.int32)
+    host = api.Column(v, "lz4", lz4_segments=32, lz4_min_match=L.GX_LZ4_LITERAL)
+    for step in ("release", "pinned", "payload"):
+        col = api.Column.from_device(torch.from_numpy(v).cuda(), "lz4", lz4_segments=32)
+        if step == "release":
+            col.release_device()
+            assert col.info.on_device == 0
+            col.to_device("hbm")
+        elif step == "pinned":
+            col.to_device("pinned")
+        else:
+            assert np.array_equal(col.payload_view(), host.payload_view())
+        out = torch.full((len(v),), -7, dtype=torch.int32, device="cuda")
+        api.ChunkDecompressor(col).chunks(0, col.info.n_chunks, out)
+        api.scan_check()
+        assert np.array_equal(out.cpu().numpy(), v), step
+        assert np.array_equal(col.payload_view(), host.payload_view()), step
+        col.free()
