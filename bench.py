@@ -988,8 +988,9 @@ def profile_batch(rows):
 def profile_scan(kind, rows, segments):
     """One single-plan scan of the Q1 workload's shape on `rows` rows, for a
     profiler: "q1full" (every date, no pruning: every tile needs all four
-    columns), "q1pruned" (the headline month) or "q3" (the star join with
-    dense join tables); three untimed launches, then three timed ones."""
+    columns), "q1full_matches" (the same with the LZ4 columns encoded with
+    4-byte matches), "q1pruned" (the headline month) or "q3" (the star join
+    with dense join tables); three untimed launches, then three timed ones."""
     import torch
 
     from golap_public_b200 import api, datagen, queries
@@ -1003,8 +1004,9 @@ def profile_scan(kind, rows, segments):
                             datagen.dim_geo(200_000, datagen.SEED, 22), dd, 2, 1992, 1997, ht_layout="dense")
     else:
         f = datagen.fact_q1(rows, True)
-        fact = queries.encode_fact(f, {"date_key": "cascaded"}, ROWS_PER_CHUNK, ROWS_PER_BLOCK, segments)
-        if kind == "q1full":
+        fact = queries.encode_fact(f, {"date_key": "cascaded"}, ROWS_PER_CHUNK, ROWS_PER_BLOCK, segments,
+                                   **({"lz4_min_match": 4} if kind == "q1full_matches" else {}))
+        if kind in ("q1full", "q1full_matches"):
             ok = np.ones(len(dd["d_key"]), dtype=bool)
             q = queries.Q1Query(fact, dd, ok, int(dd["d_key"].min()), int(dd["d_key"].max()), *DISC, *QTY,
                                 prune=False)
@@ -1090,7 +1092,7 @@ def main():
                     help="fact rows of the Q1 workload (default: the measured 60M-row configuration; smaller "
                          "values are for profiler captures)")
     ap.add_argument("--tune-rows", type=int, default=20_000_000)
-    ap.add_argument("--profile-scan", choices=["q1full", "q1pruned", "q3"],
+    ap.add_argument("--profile-scan", choices=["q1full", "q1full_matches", "q1pruned", "q3"],
                     help="run one single-plan scan six times on --rows rows (for a profiler) and exit")
     ap.add_argument("--profile-batch", action="store_true",
                     help="only build the batch table and run the 256-query mixed batch (shared form, dense join "

@@ -42,6 +42,8 @@ constexpr uint32_t kWsNT = 128;                // threads per CTA (4 independent
 constexpr uint32_t kWsWarps = kWsNT / 32;
 constexpr uint32_t kWsBatch = 128;             // rows of one row group (4 per lane)
 constexpr uint32_t kWsGroups = kWsTile / kWsBatch;  // row groups of a tile (4 keep bits each)
+constexpr uint32_t kWsEvalGroups = 2;               // row groups a scalar compile-time evaluator runs at once
+static_assert(kWsGroups % kWsEvalGroups == 0, "the evaluator's row-group batches cover the tile");
 static_assert(kWsGroups * 4 <= 32, "the keep bits of a tile fit one word");
 constexpr uint32_t kWsMaxCols = kPipeMaxCols;
 constexpr uint32_t kWsGroupLog2 = 9;           // the CTA's group table: 512 slots
@@ -677,18 +679,38 @@ __device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* 
             if (!f) return 0;  // no row of the tile passes
         }
     }
+    // kWsEvalGroups row groups at a time for scalar plans: their column loads
+    // and first-slot probes are all in flight before any is used (grouped
+    // plans, whose group-table inserts are long inlined loops, run one)
+    constexpr uint32_t H = GR ? 1u : kWsEvalGroups;
 #pragma unroll 1
-    for (uint32_t j = 0; j < kWsGroups; ++j) {
-        uint32_t kk = (keep >> (4 * j)) & 15u;
-        if (!kk) continue;
-        const uint32_t ro = (128 * j + 4 * lane) * 4;
-        uint4 w[NS];
+    for (uint32_t j0 = 0; j0 < kWsGroups; j0 += H) {
+        uint32_t kk[H];
+        uint32_t live = 0;
 #pragma unroll
-        for (uint32_t s = 0; s < NS; ++s)
-            w[s] = (s + 1 < NS && msk[s] == 0) ? make_uint4(0, 0, 0, 0)
-                                               : *(const uint4*)(sbase + off[s] + (ro & msk[s]));
-        int32_t carry[4] = {0, 0, 0, 0};
-        uint32_t g[4] = {0, 0, 0, 0};
+        for (uint32_t h = 0; h < H; ++h) {
+            kk[h] = (keep >> (4 * (j0 + h))) & 15u;
+            live |= kk[h];
+        }
+        if (!live) continue;
+        uint4 w[H][NS];
+#pragma unroll
+        for (uint32_t h = 0; h < H; ++h) {
+            const uint32_t ro = (128 * (j0 + h) + 4 * lane) * 4;
+#pragma unroll
+            for (uint32_t s = 0; s < NS; ++s)
+                w[h][s] = (s + 1 < NS && msk[s] == 0) ? make_uint4(0, 0, 0, 0)
+                                                      : *(const uint4*)(sbase + off[s] + (ro & msk[s]));
+        }
+        int32_t carry[H][4];
+        uint32_t g[H][4];
+#pragma unroll
+        for (uint32_t h = 0; h < H; ++h)
+#pragma unroll
+            for (uint32_t i = 0; i < 4; ++i) {
+                carry[h][i] = 0;
+                g[h][i] = 0;
+            }
 #pragma unroll
         for (uint32_t s = 0; s < NS; ++s) {
             const uint32_t K = (SIG >> (7 + 4 * s)) & 15u;
@@ -697,26 +719,44 @@ __device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* 
                 if (K & kWkD) {
                     const uint32_t dcard = stp.digit_card;
 #pragma unroll
-                    for (uint32_t i = 0; i < 4; ++i) g[i] = g[i] * dcard + cd[s];
+                    for (uint32_t h = 0; h < H; ++h)
+#pragma unroll
+                        for (uint32_t i = 0; i < 4; ++i) g[h][i] = g[h][i] * dcard + cd[s];
                 }
                 if (K & kWkC) {
 #pragma unroll
-                    for (uint32_t i = 0; i < 4; ++i) carry[i] = cv[s];
+                    for (uint32_t h = 0; h < H; ++h)
+#pragma unroll
+                        for (uint32_t i = 0; i < 4; ++i) carry[h][i] = cv[s];
                 }
                 continue;
             }
-            const int32_t v[4] = {(int32_t)w[s].x, (int32_t)w[s].y, (int32_t)w[s].z, (int32_t)w[s].w};
+            int32_t v[H][4];
+#pragma unroll
+            for (uint32_t h = 0; h < H; ++h) {
+                v[h][0] = (int32_t)w[h][s].x;
+                v[h][1] = (int32_t)w[h][s].y;
+                v[h][2] = (int32_t)w[h][s].z;
+                v[h][3] = (int32_t)w[h][s].w;
+            }
             if (K & kWkF) {
                 // lo <= v <= hi as one unsigned comparison of v - lo with hi - lo
                 // (an empty range, hi < lo, keeps nothing)
                 const uint32_t lo = (uint32_t)stp.lo, span = (uint32_t)stp.hi - lo;
                 const uint32_t none = stp.hi < stp.lo ? 0u : 15u;
-                uint32_t pass = 0;
 #pragma unroll
-                for (uint32_t i = 0; i < 4; ++i) pass |= ((uint32_t)v[i] - lo <= span) ? 1u << i : 0u;
-                kk &= pass & none;
+                for (uint32_t h = 0; h < H; ++h) {
+                    uint32_t pass = 0;
+#pragma unroll
+                    for (uint32_t i = 0; i < 4; ++i) pass |= ((uint32_t)v[h][i] - lo <= span) ? 1u << i : 0u;
+                    kk[h] &= pass & none;
+                }
             }
-            int32_t pp[4] = {v[0], v[1], v[2], v[3]};
+            int32_t pp[H][4];
+#pragma unroll
+            for (uint32_t h = 0; h < H; ++h)
+#pragma unroll
+                for (uint32_t i = 0; i < 4; ++i) pp[h][i] = v[h][i];
             if (K & kWkP) {
                 const uint64_t* const ht = stp.ht;
                 const uint32_t htlog = stp.ht_log2, htlay = stp.ht_layout;
@@ -728,78 +768,93 @@ __device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* 
                     hspan = (uint32_t)(hdr >> 32);
                 }
                 // the first slot of every kept row's key, all read before any is used
-                uint64_t ee[4];
+                uint64_t ee[H][4];
 #pragma unroll
-                for (uint32_t i = 0; i < 4; ++i) {
-                    const uint32_t u = (uint32_t)v[i] - hbase;
-                    const bool r = ((kk >> i) & 1u) && !bucket && v[i] != kEmptyKey && (!dense || u < hspan);
-                    const unsigned long long* sl =
-                        (const unsigned long long*)ht + (dense ? 1 + u : hash_key32(v[i], htlog));
-                    ee[i] = r ? ws_ld_slot(sl, pol_keep) : (unsigned long long)kEmptySlot;
-                }
+                for (uint32_t h = 0; h < H; ++h)
 #pragma unroll
-                for (uint32_t i = 0; i < 4; ++i) {
-                    if (!((kk >> i) & 1u)) continue;
-                    const int32_t ek = (int32_t)(uint32_t)ee[i];
-                    bool f;
-                    int32_t p = v[i];
-                    if (ek == v[i] && v[i] != kEmptyKey) {
-                        f = true;
-                        p = (int32_t)(uint32_t)(ee[i] >> 32);
-                    } else if (!bucket && (dense || ek == kEmptyKey)) {
-                        f = false;  // an empty first slot, or a dense table's slot of another key
-                    } else {
-                        f = sh_probe(ht, htlog, htlay, v[i], &p);  // a linear chain, or a bucket table
+                    for (uint32_t i = 0; i < 4; ++i) {
+                        const uint32_t u = (uint32_t)v[h][i] - hbase;
+                        const bool r =
+                            ((kk[h] >> i) & 1u) && !bucket && v[h][i] != kEmptyKey && (!dense || u < hspan);
+                        const unsigned long long* sl =
+                            (const unsigned long long*)ht + (dense ? 1 + u : hash_key32(v[h][i], htlog));
+                        ee[h][i] = r ? ws_ld_slot(sl, pol_keep) : (unsigned long long)kEmptySlot;
                     }
-                    pp[i] = p;
-                    if (!f) kk &= ~(1u << i);
-                }
+#pragma unroll
+                for (uint32_t h = 0; h < H; ++h)
+#pragma unroll
+                    for (uint32_t i = 0; i < 4; ++i) {
+                        if (!((kk[h] >> i) & 1u)) continue;
+                        const int32_t ek = (int32_t)(uint32_t)ee[h][i];
+                        bool f;
+                        int32_t p = v[h][i];
+                        if (ek == v[h][i] && v[h][i] != kEmptyKey) {
+                            f = true;
+                            p = (int32_t)(uint32_t)(ee[h][i] >> 32);
+                        } else if (!bucket && (dense || ek == kEmptyKey)) {
+                            f = false;  // an empty first slot, or a dense table's slot of another key
+                        } else {
+                            f = sh_probe(ht, htlog, htlay, v[h][i], &p);  // a linear chain, or a bucket table
+                        }
+                        pp[h][i] = p;
+                        if (!f) kk[h] &= ~(1u << i);
+                    }
             }
             if (K & kWkD) {
                 const uint32_t dcard = stp.digit_card;
                 const int32_t dbase = stp.digit_base;
 #pragma unroll
-                for (uint32_t i = 0; i < 4; ++i) {
-                    if (!((kk >> i) & 1u)) continue;
-                    const uint32_t dgt = (uint32_t)(pp[i] - dbase);
-                    if (dgt >= dcard) {
-                        raise_error(kErrInvalid);
-                        kk &= ~(1u << i);
-                    } else {
-                        g[i] = g[i] * dcard + dgt;
+                for (uint32_t h = 0; h < H; ++h)
+#pragma unroll
+                    for (uint32_t i = 0; i < 4; ++i) {
+                        if (!((kk[h] >> i) & 1u)) continue;
+                        const uint32_t dgt = (uint32_t)(pp[h][i] - dbase);
+                        if (dgt >= dcard) {
+                            raise_error(kErrInvalid);
+                            kk[h] &= ~(1u << i);
+                        } else {
+                            g[h][i] = g[h][i] * dcard + dgt;
+                        }
                     }
-                }
             }
             if (K & kWkC) {
 #pragma unroll
-                for (uint32_t i = 0; i < 4; ++i) carry[i] = v[i];
+                for (uint32_t h = 0; h < H; ++h)
+#pragma unroll
+                    for (uint32_t i = 0; i < 4; ++i) carry[h][i] = v[h][i];
             }
-            if (!kk) break;
+            live = 0;
+#pragma unroll
+            for (uint32_t h = 0; h < H; ++h) live |= kk[h];
+            if (!live) break;
             if (s + 1 == NS) {
-                if (GR) {
 #pragma unroll
-                    for (uint32_t i = 0; i < 4; ++i) {
-                        if (!((kk >> i) & 1u)) continue;
-                        const int64_t val = AGG == GX_AGG_SUM_PRODUCT ? (int64_t)v[i] * carry[i]
-                                            : AGG == GX_AGG_SUM_DIFF  ? (int64_t)v[i] - carry[i]
-                                            : AGG == GX_AGG_COUNT      ? 1
-                                                                       : (int64_t)v[i];
-                        ws_group_add(g[i], val, tkey, tsum, Q.g_keys, Q.g_sums, Q.g_log2);
-                    }
-                } else {
-                    // kept rows as multiply-adds by 0 or 1 (one wide multiply-add per row)
+                for (uint32_t h = 0; h < H; ++h) {
+                    if (GR) {
 #pragma unroll
-                    for (uint32_t i = 0; i < 4; ++i) {
-                        const int32_t on = (int32_t)((kk >> i) & 1u);
-                        if (AGG == GX_AGG_SUM_PRODUCT) {
-                            acc += (int64_t)v[i] * (int64_t)(on ? carry[i] : 0);
-                        } else if (AGG == GX_AGG_SUM_DIFF) {
-                            acc += (int64_t)v[i] * on;
-                            acc -= (int64_t)carry[i] * on;
-                        } else if (AGG == GX_AGG_COUNT) {
-                            acc += on;
-                        } else {
-                            acc += (int64_t)v[i] * on;
+                        for (uint32_t i = 0; i < 4; ++i) {
+                            if (!((kk[h] >> i) & 1u)) continue;
+                            const int64_t val = AGG == GX_AGG_SUM_PRODUCT ? (int64_t)v[h][i] * carry[h][i]
+                                                : AGG == GX_AGG_SUM_DIFF  ? (int64_t)v[h][i] - carry[h][i]
+                                                : AGG == GX_AGG_COUNT      ? 1
+                                                                           : (int64_t)v[h][i];
+                            ws_group_add(g[h][i], val, tkey, tsum, Q.g_keys, Q.g_sums, Q.g_log2);
+                        }
+                    } else {
+                        // kept rows as multiply-adds by 0 or 1 (one wide multiply-add per row)
+#pragma unroll
+                        for (uint32_t i = 0; i < 4; ++i) {
+                            const int32_t on = (int32_t)((kk[h] >> i) & 1u);
+                            if (AGG == GX_AGG_SUM_PRODUCT) {
+                                acc += (int64_t)v[h][i] * (int64_t)(on ? carry[h][i] : 0);
+                            } else if (AGG == GX_AGG_SUM_DIFF) {
+                                acc += (int64_t)v[h][i] * on;
+                                acc -= (int64_t)carry[h][i] * on;
+                            } else if (AGG == GX_AGG_COUNT) {
+                                acc += on;
+                            } else {
+                                acc += (int64_t)v[h][i] * on;
+                            }
                         }
                     }
                 }
@@ -810,7 +865,7 @@ __device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* 
 }
 
 template <uint32_t SIG>
-__global__ void __launch_bounds__(kWsNT, 4) warp_scan_kernel(const __grid_constant__ WsParams P) {
+__global__ void __launch_bounds__(kWsNT, (SIG == 0 || ((SIG >> 6) & 1)) ? 4 : 3) warp_scan_kernel(const __grid_constant__ WsParams P) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ gx_dcol s_cols[kWsMaxCols];
     __shared__ uint32_t s_nsurv;
