@@ -72,7 +72,9 @@ struct WsParams {
 };
 
 // Column read modes of one tile.
-enum : uint32_t { kWmStage = 0, kWmConst = 1, kWmLz4 = 2, kWmCasc = 3, kWmBad = 4 };
+// kWmRuns2: a cascaded tile covered by two runs (value cval on tile rows
+// [0, aux0), value aux1 from there), written out without the page decoder.
+enum : uint32_t { kWmStage = 0, kWmConst = 1, kWmLz4 = 2, kWmCasc = 3, kWmBad = 4, kWmRuns2 = 5 };
 
 __device__ __forceinline__ uint64_t ws_shfl64(uint64_t v, uint32_t src) {
     return ((uint64_t)__shfl_sync(0xFFFFFFFFu, (uint32_t)(v >> 32), src) << 32) |
@@ -372,9 +374,22 @@ __device__ __forceinline__ WsCol ws_column(const WsParams& P, const gx_dcol& col
                                 (delta && k == 0) ? 0u : unpack_bits(vw, k, h.val_bits) + (uint32_t)h.val_base;
                             val = delta ? val + e : e;
                             if (start <= h0 && h0 < end) {
+                                const uint32_t v0 = delta ? val + (uint32_t)h.first : val;
                                 if (h1 <= end) {
                                     C.mode = kWmConst;
-                                    C.cval = (int32_t)(delta ? val + (uint32_t)h.first : val);
+                                    C.cval = (int32_t)v0;
+                                } else if (k + 1 < h.n_runs) {
+                                    // the next run: when it covers the rest of the tile,
+                                    // the tile is two runs
+                                    const uint32_t end2 = end + unpack_bits(lw, k + 1, h.len_bits) + h.len_base;
+                                    const uint32_t e2 = unpack_bits(vw, k + 1, h.val_bits) + (uint32_t)h.val_base;
+                                    const uint32_t v1 = delta ? v0 + e2 : e2;
+                                    if (h1 <= end2) {
+                                        C.mode = kWmRuns2;
+                                        C.cval = (int32_t)v0;
+                                        C.aux0 = end - h0;
+                                        C.aux1 = v1;
+                                    }
                                 }
                                 break;
                             }
@@ -985,8 +1000,21 @@ __global__ void __launch_bounds__(kWsNT, (SIG == 0 || ((SIG >> 6) & 1)) ? 4 : 3)
             }
             for (uint32_t c = 0; c < ncols && !terr; ++c) {
                 const uint32_t m = __shfl_sync(0xFFFFFFFFu, mode, c);
-                if (m != kWmLz4 && m != kWmCasc) continue;
+                if (m != kWmLz4 && m != kWmCasc && m != kWmRuns2) continue;
                 uint32_t* buf = areas + (size_t)P.buf_of[c] * kWsTile;
+                if (m == kWmRuns2) {  // two runs: the rows written out directly
+                    const uint32_t v0 = (uint32_t)__shfl_sync(0xFFFFFFFFu, (uint32_t)cval, c);
+                    const uint32_t split = __shfl_sync(0xFFFFFFFFu, aux0, c), v1 = __shfl_sync(0xFFFFFFFFu, aux1, c);
+#pragma unroll 1
+                    for (uint32_t j = 0; j < kWsTile / 128; ++j) {
+                        const uint32_t r = 128 * j + 4 * lane;
+                        *(uint4*)(buf + r) = make_uint4(r < split ? v0 : v1, r + 1 < split ? v0 : v1,
+                                                        r + 2 < split ? v0 : v1, r + 3 < split ? v0 : v1);
+                    }
+                    __syncwarp();
+                    if (lane == c) roff = (uint32_t)((uint8_t*)buf - smem);
+                    continue;
+                }
                 const uint8_t* cs = (const uint8_t*)ws_shfl64((uint64_t)src, c);
                 const uint32_t x0 = __shfl_sync(0xFFFFFFFFu, aux0, c), x1 = __shfl_sync(0xFFFFFFFFu, aux1, c);
                 int r;

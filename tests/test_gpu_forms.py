@@ -131,8 +131,8 @@ def test_count_and_forced_form_errors(cuda):
 def test_cascaded_page_kinds_every_form(cuda, form):
     # cascaded pages of every kind: increasing with varied steps (delta, no
     # RLE), a staircase (RLE + delta), runs of about six rows (RLE with
-    # hundreds of runs per page), random (bit-packed); SUM of a filtered
-    # column must equal numpy's
+    # hundreds of runs per page), runs longer than a tile (one- and two-run
+    # tiles), random (bit-packed); SUM of a filtered column must equal numpy's
     import torch
 
     from golap_public_b200 import _lib as L
@@ -143,6 +143,10 @@ def test_cascaded_page_kinds_every_form(cuda, form):
         "inc": np.cumsum(rng.integers(1, 60, n)).astype(np.int32),
         "stairs": np.repeat(np.cumsum(rng.integers(1, 9, n // 700 + 2)), 700)[:n].astype(np.int32),
         "runs6": np.repeat(rng.integers(-5000, 5000, n // 6 + 2), 6)[:n].astype(np.int32),
+        # runs longer than a warp tile: tiles of one run and of two runs, with
+        # and without delta between the runs' values
+        "runs1500": np.repeat(rng.integers(-(1 << 30), 1 << 30, n // 1500 + 2), 1500)[:n].astype(np.int32),
+        "stairs3000": np.repeat(np.cumsum(rng.integers(1, 4, n // 3000 + 2)), 3000)[:n].astype(np.int32),
         "rand": rng.integers(-(1 << 20), 1 << 20, n).astype(np.int32),
     }
     fact = queries.encode_fact(cols, {k: "cascaded" for k in cols})
