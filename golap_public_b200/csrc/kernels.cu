@@ -2244,6 +2244,8 @@ static gx_status scan_launch_warp(const gx_scan_plan* plan, const QueryDesc& qd,
     const uint32_t n_range = P.chunk_hi - P.chunk_lo;
     P.chunk_words = ((n_range + 31) / 32 + 3) & ~3u;
     if (P.chunk_words > kWsMaxChunkWords) return GX_OK;
+    // the kernel indexes tiles in 32 bits (with room for its stride)
+    if ((uint64_t)n_range * P.blocks_per_chunk * P.tiles_per_block >= (1ull << 31)) return GX_OK;
     P.n_areas = areas;
     P.grouped_tab = P.q.grouped ? 1u : 0u;
     P.rows_scanned = rows_dev;

@@ -270,11 +270,11 @@ struct WsCol {
 // its tile; false when t is past the end or the tile has no rows of the
 // query's slice.
 __device__ __forceinline__ bool ws_locate(const WsParams& P, const uint32_t* s_kbits, const uint32_t* s_kpre,
-                                          uint64_t t, uint64_t t_end, WsTile& T) {
+                                          uint32_t t, uint32_t t_end, WsTile& T) {
     if (t >= t_end) return false;
     const uint32_t tpb = P.tiles_per_block, bpc = P.blocks_per_chunk;
-    const uint64_t PC = (uint64_t)bpc * tpb;
-    const uint32_t k = (uint32_t)(t / PC), loc = (uint32_t)(t % PC);
+    const uint32_t PC = bpc * tpb;  // the launch keeps tile indices below 2^31
+    const uint32_t k = t / PC, loc = t - k * PC;
     uint32_t lo = 0, hi = P.chunk_words - 1;  // the bitmap word holding the k-th surviving chunk
     while (lo < hi) {
         const uint32_t mid = (lo + hi + 1) >> 1;
@@ -407,7 +407,7 @@ __device__ __forceinline__ WsCol ws_column(const WsParams& P, const gx_dcol& col
 // the four tiles cost one round of dependent loads.  Returns the mask of
 // the tiles to scan; every lane of group q holds tile q in T.
 __device__ __forceinline__ uint32_t ws_decide(const WsParams& P, const gx_dcol* s_cols, const uint32_t* s_kbits,
-                                              const uint32_t* s_kpre, uint64_t t0, uint64_t W, uint64_t t_end,
+                                              const uint32_t* s_kpre, uint32_t t0, uint32_t W, uint32_t t_end,
                                               uint32_t lane, WsTile& T, WsCol& C) {
     const ShQuery& Q = P.q;
     const uint32_t q = lane >> 3, c = lane & 7;
@@ -430,7 +430,7 @@ __device__ __forceinline__ uint32_t ws_decide(const WsParams& P, const gx_dcol* 
 // L2 prefetch of the directory and side-index lines of the four tiles
 // t0 + q*W (lane 8q + c: column c), so that their decisions read L2.
 __device__ __forceinline__ void ws_prefetch_meta(const WsParams& P, const gx_dcol* s_cols, const uint32_t* s_kbits,
-                                                 const uint32_t* s_kpre, uint64_t t0, uint64_t W, uint64_t t_end,
+                                                 const uint32_t* s_kpre, uint32_t t0, uint32_t W, uint32_t t_end,
                                                  uint32_t lane) {
     const uint32_t q = lane >> 3, c = lane & 7;
     WsTile T;
@@ -949,16 +949,16 @@ __global__ void __launch_bounds__(kWsNT, (SIG == 0 || ((SIG >> 6) & 1)) ? 4 : 3)
     }
     __syncthreads();  // the last block-wide barrier: warps are independent from here on
 
-    const uint64_t PC = (uint64_t)P.blocks_per_chunk * P.tiles_per_block;
-    const uint64_t t_end = (uint64_t)s_nsurv * PC;
+    const uint32_t PC = P.blocks_per_chunk * P.tiles_per_block;
+    const uint32_t t_end = s_nsurv * PC;
     const uint32_t ns = Q.n_steps, agg = Q.agg;
     const bool grouped = Q.grouped != 0;
-    const uint64_t W = (uint64_t)gridDim.x * kWsWarps;
+    const uint32_t W = gridDim.x * kWsWarps;
     int64_t local = 0;
     unsigned long long local_rows = 0;
     uint32_t ph = 0;
     bool stop = false;
-    for (uint64_t t0 = (uint64_t)blockIdx.x * kWsWarps + warp; t0 < t_end && !stop; t0 += 4 * W) {
+    for (uint32_t t0 = blockIdx.x * kWsWarps + warp; t0 < t_end && !stop; t0 += 4 * W) {
         WsTile T;
         WsCol C;
         const uint32_t vm = ws_decide(P, s_cols, s_kbits, s_kpre, t0, W, t_end, lane, T, C);
