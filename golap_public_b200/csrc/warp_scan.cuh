@@ -712,10 +712,9 @@ __device__ __forceinline__ int64_t ws_eval_sig(const ShQuery& Q, const uint8_t* 
 #pragma unroll
         for (uint32_t h = 0; h < H; ++h) {
             const uint32_t ro = (128 * (j0 + h) + 4 * lane) * 4;
+            // (a column constant on the tile reads its broadcast slot: mask 0)
 #pragma unroll
-            for (uint32_t s = 0; s < NS; ++s)
-                w[h][s] = (s + 1 < NS && msk[s] == 0) ? make_uint4(0, 0, 0, 0)
-                                                      : *(const uint4*)(sbase + off[s] + (ro & msk[s]));
+            for (uint32_t s = 0; s < NS; ++s) w[h][s] = *(const uint4*)(sbase + off[s] + (ro & msk[s]));
         }
         int32_t carry[H][4];
         uint32_t g[H][4];
