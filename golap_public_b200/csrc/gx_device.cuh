@@ -90,6 +90,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* m, uint32_t phase) {
     return false;
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start while the kernel before it on the stream still
+// runs; griddep_wait blocks the calling thread until that kernel has
+// completed and its writes are visible (at once when there is none), and
+// griddep_launch lets the kernel that follows start early once every CTA of
+// this one has issued it.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 // L2 cache policies: join tables stay (evict last), streamed bytes go first.
 __device__ __forceinline__ uint64_t ws_policy_keep() {
     uint64_t p;

@@ -895,6 +895,7 @@ __device__ __forceinline__ void ht_insert_rows(uint64_t* slots, uint32_t log2cap
 
 __global__ void ht_build_kernel(uint64_t* slots, uint32_t log2cap, const int32_t* keys, const int32_t* payload,
                                 uint64_t n, const __grid_constant__ BuildPreds preds, unsigned long long* counters) {
+    griddep_launch();
     ht_insert_rows(slots, log2cap, keys, payload, blockIdx.x * (uint64_t)blockDim.x + threadIdx.x,
                    (uint64_t)gridDim.x * blockDim.x, n, preds, counters);
 }
@@ -905,6 +906,7 @@ constexpr uint64_t kSmallHtSlots = 1u << 16, kSmallHtRows = 1u << 16;
 __global__ void ht_build_small_kernel(uint64_t* slots, uint32_t log2cap, const int32_t* keys, const int32_t* payload,
                                       uint64_t n, const __grid_constant__ BuildPreds preds,
                                       unsigned long long* counters) {
+    griddep_launch();  // a scan launched after the build may start its table-free work now
     const uint64_t cap = 1ull << log2cap;
     for (uint64_t i = threadIdx.x; i < cap; i += blockDim.x) slots[i] = kEmptySlot;
     if (threadIdx.x < 4) counters[threadIdx.x] = 0;
@@ -942,6 +944,7 @@ __global__ void ht_range_kernel(const int32_t* keys, uint64_t n, const __grid_co
 __global__ void ht_build_dense_kernel(uint64_t* slots, int32_t base, uint32_t span, const int32_t* keys,
                                       const int32_t* payload, uint64_t n, const __grid_constant__ BuildPreds preds,
                                       unsigned long long* counters) {
+    griddep_launch();
     unsigned long long ins = 0, dup = 0, bad = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         bool pass = true;
@@ -972,6 +975,7 @@ __global__ void ht_build_dense_kernel(uint64_t* slots, int32_t base, uint32_t sp
 __global__ void ht_build_bucket_kernel(uint64_t* slots, uint32_t log2cap, const int32_t* keys, const int32_t* payload,
                                        uint64_t n, const __grid_constant__ BuildPreds preds,
                                        unsigned long long* counters) {
+    griddep_launch();
     const uint32_t lb = log2cap - 3, bmask = (1u << lb) - 1;
     unsigned long long ins = 0, dup = 0, bad = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -2277,8 +2281,23 @@ static gx_status scan_launch_warp(const gx_scan_plan* plan, const QueryDesc& qd,
     const uint64_t tiles = (uint64_t)n_range * c0->blocks_per_chunk * P.tiles_per_block;
     const uint64_t want = (tiles + kWsWarps - 1) / kWsWarps;
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count() * per_sm, want));
-    kern<<<grid, kWsNT, smem, s>>>(P);
-    const cudaError_t e = cudaGetLastError();
+    // programmatic dependent launch: the scan's chunk pruning, tile decisions
+    // and first copies overlap the kernel before it on the stream (typically
+    // the join-table build); the kernel waits for it before it reads a join
+    // table or writes a result.  Not for streamed groups, whose staging copies
+    // arrive on another stream.
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kWsNT);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = grp ? 0u : 1u;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, P);
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(GX_ERR_CUDA, "warp scan launch: %s", cudaGetErrorString(e));
     *done = true;
     return GX_OK;

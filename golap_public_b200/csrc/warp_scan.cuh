@@ -52,7 +52,10 @@ constexpr uint32_t kWsGroupProbes = 16;
 constexpr uint32_t kWsNone = 0xFFFFFFFFu;
 constexpr uint32_t kWsMaxDynSmem = 220u << 10;  // dynamic shared memory of one CTA at most
 constexpr uint32_t kWsMaxChunkWords = 1024;     // chunk keep bits of one launch: 32768 chunks
-constexpr uint32_t kWsHead = 36;                // per-warp words before the stage: 8 constant slots, the mbarrier
+// per-warp words before the stage: 8 constant slots (32 words), the mbarrier
+// (2 + 2 padding), the dense join tables' {base, span} headers per step (16)
+constexpr uint32_t kWsHead = 52;
+static_assert(4 * kWsMaxCols + 4 + 2 * GX_MAX_STEPS <= kWsHead && kWsHead % 4 == 0, "the warp head holds its parts");
 static_assert(kWsTile <= kCascPageRows && kCascPageRows % kWsTile == 0, "a warp tile lies in one cascaded page");
 
 struct WsParams {
@@ -883,7 +886,6 @@ __global__ void __launch_bounds__(kWsNT, (SIG == 0 || ((SIG >> 6) & 1)) ? 4 : 3)
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ gx_dcol s_cols[kWsMaxCols];
     __shared__ uint32_t s_nsurv;
-    __shared__ uint64_t s_hdr[GX_MAX_STEPS];  // dense join tables' {base, span} headers, per step
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t ncols = P.n_cols;
     const ShQuery& Q = P.q;
@@ -892,6 +894,7 @@ __global__ void __launch_bounds__(kWsNT, (SIG == 0 || ((SIG >> 6) & 1)) ? 4 : 3)
     uint32_t* const wmem = s_kpre + P.chunk_words + (size_t)warp * P.warp_words;
     uint4* const cslot = (uint4*)wmem;                       // constant columns (4 copies of the value)
     uint64_t* const bar = (uint64_t*)(wmem + 4 * kWsMaxCols);  // the warp's stage mbarrier
+    uint64_t* const whdr = (uint64_t*)(wmem + 4 * kWsMaxCols + 4);  // dense join tables' headers, per step
     uint32_t* const areas = wmem + kWsHead;                  // n_areas x kWsTile words
     // grouped plans: the run-time evaluator's group key of each row of the tile
     // (compile-time evaluators keep keys in registers), then the group table
@@ -901,16 +904,34 @@ __global__ void __launch_bounds__(kWsNT, (SIG == 0 || ((SIG >> 6) & 1)) ? 4 : 3)
     unsigned long long* const tsum = (unsigned long long*)(tkey + kWsGroupSlots);
     const uint64_t pol_keep = ws_policy_keep(), pol_stream = ws_policy_stream();
 
-    if (tid < GX_MAX_STEPS) {
-        const ShStep& st = Q.steps[tid];
-        s_hdr[tid] = (tid < Q.n_steps && (st.flags & GX_STEP_PROBE) && st.ht_layout == GX_HT_DENSE)
-                         ? __ldg((const unsigned long long*)st.ht)
-                         : 0ull;
+    // The launch may overlap the kernel before it on the stream (programmatic
+    // dependent launch): until a thread has passed griddep_wait it reads only
+    // the columns (payload, directory, side index, min/max, zone maps: never
+    // written by kernels), and every read of join tables, keep_in, and every
+    // global write (results, keep_out, group tables) comes after its wait.
+    bool waited = false;
+    if (Q.keep_in) {  // keep flags may come from the kernel before
+        griddep_wait();
+        waited = true;
     }
+    // a warp's first evaluation: the wait, then the dense join tables' headers
+    auto await_tables = [&]() {
+        if (!waited) griddep_wait();
+        waited = true;
+        if (lane < GX_MAX_STEPS) {
+            const ShStep& st = Q.steps[lane];
+            whdr[lane] = (lane < Q.n_steps && (st.flags & GX_STEP_PROBE) && st.ht_layout == GX_HT_DENSE)
+                             ? __ldcg((const unsigned long long*)st.ht)
+                             : 0ull;
+        }
+        __syncwarp();
+    };
+    bool tables = false;  // whdr loaded
     for (uint32_t i = tid; i < ncols * (uint32_t)(sizeof(gx_dcol) / 4); i += kWsNT)
         ((uint32_t*)s_cols)[i] = ((const uint32_t*)P.cols)[i];
     // chunk keep (keep_in and the prune predicates' chunk min/max, the
-    // reference's granularity), one ballot word per 32 chunks; CTA 0 writes keep_out
+    // reference's granularity), one ballot word per 32 chunks; CTA 0 writes
+    // keep_out from them at the end
     const uint32_t n_range = P.chunk_hi - P.chunk_lo;
     for (uint32_t wb = warp * 32; wb < P.chunk_words * 32; wb += kWsNT) {
         const uint32_t i = wb + lane, chunk = P.chunk_lo + i;
@@ -921,7 +942,6 @@ __global__ void __launch_bounds__(kWsNT, (SIG == 0 || ((SIG >> 6) & 1)) ? 4 : 3)
                 const PrunePred& pr = Q.prune[p];
                 ck = ck && pr.lo <= __ldg(pr.maxs + chunk) && pr.hi >= __ldg(pr.mins + chunk);
             }
-            if (blockIdx.x == 0 && Q.keep_out) Q.keep_out[chunk] = ck ? 1 : 0;
         }
         const uint32_t word = __ballot_sync(0xFFFFFFFFu, ck);
         if (lane == 0) s_kbits[wb / 32] = word;
@@ -1072,6 +1092,10 @@ __global__ void __launch_bounds__(kWsNT, (SIG == 0 || ((SIG >> 6) & 1)) ? 4 : 3)
 #pragma unroll 1
                     for (uint32_t j = 0; j < kWsGroups; ++j) *(uint4*)(gkb + 128 * j + 4 * lane) = make_uint4(0, 0, 0, 0);
                 }
+                if (!tables) {
+                    await_tables();
+                    tables = true;
+                }
                 if constexpr (SIG != 0) {
                     constexpr uint32_t NS = SIG & 7;
                     uint32_t off[NS], msk[NS];
@@ -1081,7 +1105,7 @@ __global__ void __launch_bounds__(kWsNT, (SIG == 0 || ((SIG >> 6) & 1)) ? 4 : 3)
                         off[s] = __shfl_sync(0xFFFFFFFFu, roff, c);
                         msk[s] = __shfl_sync(0xFFFFFFFFu, rmask, c);
                     }
-                    local += ws_eval_sig<SIG>(Q, smem, off, msk, keep, tkey, tsum, pol_keep, s_hdr, lane);
+                    local += ws_eval_sig<SIG>(Q, smem, off, msk, keep, tkey, tsum, pol_keep, whdr, lane);
                 }
                 uint32_t coff = 0, cmask = 0;  // the carried column (none: carried values are 0)
                 bool carried = false;
@@ -1113,6 +1137,9 @@ __global__ void __launch_bounds__(kWsNT, (SIG == 0 || ((SIG >> 6) & 1)) ? 4 : 3)
     }
     // ---- results: the CTA's group table once every warp is done, else the warp's sum
     __syncwarp();
+    if (!waited) griddep_wait();
+    if (blockIdx.x == 0 && Q.keep_out)
+        for (uint32_t i = tid; i < n_range; i += kWsNT) Q.keep_out[P.chunk_lo + i] = (s_kbits[i / 32] >> (i % 32)) & 1u;
     if (grouped && P.grouped_tab) {
         __syncthreads();
         for (uint32_t i = tid; i < kWsGroupSlots; i += kWsNT) {
