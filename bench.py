@@ -614,10 +614,11 @@ def star_join_section(args, pk, pk_kind, world=1):
     got = q.run()
 
     def step():
+        q.agg.reset()
         q.build_customer()
         q.hs.build(q._keep_alive[3], q._keep_alive[4], preds=[(q._keep_alive[5], region, region)])
         q.hd.build(q._keep_alive[6], q._keep_alive[7], preds=[(q._keep_alive[7], ylo, yhi)])
-        q.launch()
+        q.scan()
 
     for _ in range(args.warmup):
         step()

@@ -205,6 +205,11 @@ class Q3Query:
 
     def launch(self, stream=None):
         self.agg.reset(stream)
+        self.scan(stream)
+
+    def scan(self, stream=None):
+        """The fused scan alone (group table already reset): launched right after
+        the last join-table build, its table-free work overlaps that build."""
         _launch(self.plan, self.stream_group, stream)
 
     def decode_key(self, k: int):
