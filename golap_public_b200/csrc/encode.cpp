@@ -108,14 +108,20 @@ size_t lz4_encode_block(const int32_t* vals, uint32_t W, uint32_t S, uint32_t se
                         uint32_t* seg, uint32_t* n_seq) {
     constexpr uint32_t HB = 14;
     const size_t base = out.size();
-    std::vector<int32_t> head(1u << HB, -1);
-    std::vector<int32_t> prev(W ? W : 1, -1);
     std::vector<uint32_t> bound(S + 1);
     for (uint32_t j = 0; j <= S; ++j) bound[j] = std::min<uint64_t>((uint64_t)j * seg_rows, W);
     seg[0] = 0;
     seg[1] = 0;
     SeqEmitter em{out, 0, base, (const uint8_t*)vals, seg, bound.data(), S};
     const uint32_t min_w = std::max<uint32_t>(1, (min_match + 3) / 4);
+    if (min_w >= W) {  // no match can be long enough: the block is one literal run
+        em.emit(0, W, false, 0, 0);
+        em.finish(W);
+        if (n_seq) *n_seq = em.n_seq;
+        return out.size() - base;
+    }
+    std::vector<int32_t> head(1u << HB, -1);
+    std::vector<int32_t> prev(W ? W : 1, -1);
     const uint32_t* v = (const uint32_t*)vals;
     auto h = [&](uint32_t x) { return (x * 2654435761u) >> (32 - HB); };
     uint32_t anchor = 0;
