@@ -418,6 +418,10 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
         uint32_t s0 = (uint32_t)((uint64_t)col->n_slots * t / threads);
         uint32_t s1 = (uint32_t)((uint64_t)col->n_slots * (t + 1) / threads);
         auto& buf = bufs[t];
+        // room for the raw bytes of the thread's blocks and their headers, so
+        // that the buffer does not move as it grows (compressed blocks are
+        // smaller, literal-run blocks a few bytes larger)
+        buf.reserve((size_t)(s1 - s0) * ((size_t)rows_per_block * 4 + rows_per_block / 64 + 256));
         std::vector<uint8_t> lz4_tmp;
         for (uint32_t s = s0; s < s1; ++s) {
             uint32_t c = s / col->blocks_per_chunk, j = s % col->blocks_per_chunk;
@@ -471,17 +475,19 @@ int column_encode(const int32_t* vals, uint64_t n_rows, uint32_t codec, uint32_t
     work(0);
     for (auto& th : pool) th.join();
     if (overflow) return set_error(GX_ERR_INVALID, "an LZ4 block exceeds the %u-byte staging buffer", kStageBytes);
-    size_t total = 0;
-    for (auto& b : bufs) total += b.size();
-    col->payload.clear();
-    col->payload.reserve(total + kPayloadSlack);
-    for (uint32_t t = 0; t < threads; ++t) {
-        uint64_t shift = col->payload.size();
-        for (uint64_t s : local_off[t]) col->blocks[s].offset += shift;
-        col->payload.insert(col->payload.end(), bufs[t].begin(), bufs[t].end());
+    // the per-thread buffers in thread order, each copied by its own thread
+    std::vector<uint64_t> shift(threads + 1, 0);
+    for (uint32_t t = 0; t < threads; ++t) shift[t + 1] = shift[t] + bufs[t].size();
+    col->payload.assign(shift[threads] + kPayloadSlack, 0);
+    auto place = [&](uint32_t t) {
+        for (uint64_t s : local_off[t]) col->blocks[s].offset += shift[t];
+        if (!bufs[t].empty()) std::memcpy(col->payload.data() + shift[t], bufs[t].data(), bufs[t].size());
         std::vector<uint8_t>().swap(bufs[t]);
-    }
-    col->payload.resize(col->payload.size() + kPayloadSlack, 0);
+    };
+    pool.clear();
+    for (uint32_t t = 1; t < threads; ++t) pool.emplace_back(place, t);
+    place(0);
+    for (auto& th : pool) th.join();
     col->n_blocks = 0;
     for (auto& b : col->blocks) col->n_blocks += b.n_rows ? 1 : 0;
     return GX_OK;
