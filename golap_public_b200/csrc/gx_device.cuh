@@ -116,105 +116,7 @@ __device__ __forceinline__ unsigned long long ws_ld_slot(const unsigned long lon
     asm("ld.global.nc.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(pol));
     return v;
 }
-// ------------------------------------------------- segmented LZ4, one lane
-// Decodes the K output words of one segment of a segmented LZ4 block (format
-// in gx_internal.h) into out[0..K).  The block's compressed bytes from
-// stream position wbase on are staged in shared memory as the word array A;
-// the lane may read stream positions [lo, hi) only (its tile's window), and
-// the block's stream ends at block_end.
-//
-// One output word per loop iteration: a literal word (rolling funnel shift
-// over the staged words, one shared load per word) or a match word
-// out[k - offw] (LZ4 overlap semantics follow from the word order).  Token
-// and offset parsing happens between words only when a lane needs it, so
-// the 32 lanes of a warp stay in lockstep.  Returns 0 or kErrCorrupt.
-__device__ __forceinline__ int lz4_seg_lane(const uint32_t* __restrict__ A, uint32_t wbase, uint32_t lo,
-                                            uint32_t hi, uint32_t block_end, uint32_t comp_pos, uint32_t info,
-                                            uint32_t K, uint32_t* __restrict__ out) {
-    if (comp_pos < lo || comp_pos > hi) return kErrCorrupt;
-    uint32_t pos = comp_pos;
-    uint32_t litw = 0, mw = 0, offw = 0, mnib = 0;
-    uint32_t phase = 0;  // 0: next is a token, 1: next is a match offset
-    uint32_t lwprev = 0, lsh = 0;
-#define GX_BYTE(i) ((A[((i) - wbase) >> 2] >> ((((i) - wbase) & 3u) * 8)) & 255u)
-    if (info & 16u) {
-        const uint32_t lit = info >> 5;
-        if (lit & 3u) return kErrCorrupt;
-        litw = lit >> 2;
-        mnib = info & 15u;
-        phase = 1;
-        if ((uint64_t)pos + 4ull * min(litw, K) > hi) return kErrCorrupt;
-        if (litw) {
-            const uint32_t r = pos - wbase;
-            lsh = (r & 3u) * 8;
-            lwprev = A[r >> 2];
-        }
-    }
-    for (uint32_t k = 0; k < K; ++k) {
-        while (litw == 0 && mw == 0) {
-            if (phase == 0) {
-                if (pos >= hi) return kErrCorrupt;
-                const uint32_t tok = GX_BYTE(pos);
-                ++pos;
-                uint32_t lit = tok >> 4;
-                mnib = tok & 15u;
-                if (lit == 15) {
-                    uint32_t b;
-                    do {
-                        if (pos >= hi) return kErrCorrupt;
-                        b = GX_BYTE(pos);
-                        ++pos;
-                        lit += b;
-                    } while (b == 255);
-                }
-                if (lit & 3u) return kErrCorrupt;
-                litw = lit >> 2;
-                if ((uint64_t)pos + 4ull * min(litw, K - k) > hi) return kErrCorrupt;
-                if (litw) {
-                    const uint32_t r = pos - wbase;
-                    lsh = (r & 3u) * 8;
-                    lwprev = A[r >> 2];
-                }
-                phase = 1;
-            } else {
-                // literals done: the block may end here (then the segment is short)
-                if (pos == block_end || (uint64_t)pos + 2 > hi) return kErrCorrupt;
-                const uint32_t off = GX_BYTE(pos) | (GX_BYTE(pos + 1) << 8);
-                pos += 2;
-                uint32_t ml = mnib + 4;
-                if (mnib == 15) {
-                    uint32_t b;
-                    do {
-                        if (pos >= hi) return kErrCorrupt;
-                        b = GX_BYTE(pos);
-                        ++pos;
-                        ml += b;
-                    } while (b == 255);
-                }
-                if ((off & 3u) || (ml & 3u) || off == 0) return kErrCorrupt;
-                offw = off >> 2;
-                mw = ml >> 2;
-                if (offw > k || mw > K - k) return kErrCorrupt;
-                phase = 0;
-            }
-        }
-        uint32_t w;
-        if (litw) {
-            const uint32_t nxt = A[((pos - wbase) >> 2) + 1];
-            w = __funnelshift_r(lwprev, nxt, lsh);
-            lwprev = nxt;
-            pos += 4;
-            --litw;
-        } else {
-            w = out[k - offw];
-            --mw;
-        }
-        out[k] = w;
-    }
-    return 0;
-#undef GX_BYTE
-}
-
+// ------------------------------------------------- segmented LZ4
 // 4 bytes at byte offset r of a staged window (little endian, any alignment).
 __device__ __forceinline__ uint32_t fetch4(const uint32_t* __restrict__ A, uint32_t r) {
     const uint32_t w = r >> 2;
