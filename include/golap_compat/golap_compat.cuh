@@ -104,24 +104,23 @@ struct CompInfo {
     }
 };
 
-// Ingest of one int32 column (prepare_compressed, core/apps.cuh:149-255):
-// chunk, compress ("LZ4", "Cascaded" or "Uncompressed"), collect min/max and
-// place the compressed bytes on the device (residency 1 = HBM, 2 = pinned
-// host memory read zero-copy).
-inline CompInfo prepare_compressed(const int32_t* host_col, uint64_t n_rows, uint64_t chunk_bytes,
-                                   const std::string& comp_algo, int residency = 1, cudaStream_t stream = 0,
-                                   uint64_t nvchunk = 1 << 16, uint32_t lz4_segments = 32) {
+namespace detail {
+inline gx_encode_opts ingest_opts(uint64_t chunk_bytes, const std::string& comp_algo, uint64_t nvchunk,
+                                  uint32_t lz4_segments) {
     gx_encode_opts o;
     gx_check(gx_encode_opts_default(&o));
     o.codec = comp_algo == "LZ4" ? GX_CODEC_LZ4 : comp_algo == "Cascaded" ? GX_CODEC_CASCADED : GX_CODEC_NONE;
     o.rows_per_chunk = (uint32_t)(chunk_bytes / 4);
     o.rows_per_block = (uint32_t)(nvchunk / 4);
     o.lz4_segments = lz4_segments;
-    gx_column* c = nullptr;
-    gx_check(gx_column_encode(host_col, n_rows, &o, &c));
+    return o;
+}
+
+// The CompInfo of an encoded column (owns it from here on).
+inline CompInfo comp_info_of(gx_column* c, uint64_t n_rows, uint64_t chunk_bytes, const std::string& comp_algo,
+                             uint64_t nvchunk) {
     CompInfo info;
     info.column = std::shared_ptr<gx_column>(c, [](gx_column* p) { gx_column_free(p); });
-    gx_check(gx_column_to_device(c, residency, (void*)stream));
     gx_column_info ci;
     gx_check(gx_column_info_get(c, &ci));
     info.chunk_bytes = chunk_bytes;
@@ -134,6 +133,35 @@ inline CompInfo prepare_compressed(const int32_t* host_col, uint64_t n_rows, uin
     for (uint64_t r = 0; r < n_rows; r += chunk_bytes / 4)
         info.chunk_size_vec.push_back(4 * std::min<uint64_t>(chunk_bytes / 4, n_rows - r));
     return info;
+}
+}  // namespace detail
+
+// Ingest of one int32 column (prepare_compressed, core/apps.cuh:149-255):
+// chunk, compress ("LZ4", "Cascaded" or "Uncompressed"), collect min/max and
+// place the compressed bytes on the device (residency 1 = HBM, 2 = pinned
+// host memory read zero-copy).
+inline CompInfo prepare_compressed(const int32_t* host_col, uint64_t n_rows, uint64_t chunk_bytes,
+                                   const std::string& comp_algo, int residency = 1, cudaStream_t stream = 0,
+                                   uint64_t nvchunk = 1 << 16, uint32_t lz4_segments = 32) {
+    const gx_encode_opts o = detail::ingest_opts(chunk_bytes, comp_algo, nvchunk, lz4_segments);
+    gx_column* c = nullptr;
+    gx_check(gx_column_encode(host_col, n_rows, &o, &c));
+    CompInfo info = detail::comp_info_of(c, n_rows, chunk_bytes, comp_algo, nvchunk);
+    gx_check(gx_column_to_device(c, residency, (void*)stream));
+    return info;
+}
+
+// The same for a column already in device memory (the reference's
+// prepare_compressed over a device-resident golap::Column): encoded on the
+// GPU, in HBM on return.  "LZ4" writes every block as one literal run.
+inline CompInfo prepare_compressed_device(const int32_t* dev_col, uint64_t n_rows, uint64_t chunk_bytes,
+                                          const std::string& comp_algo, cudaStream_t stream = 0,
+                                          uint64_t nvchunk = 1 << 16, uint32_t lz4_segments = 32) {
+    gx_encode_opts o = detail::ingest_opts(chunk_bytes, comp_algo, nvchunk, lz4_segments);
+    o.lz4_min_match = GX_LZ4_LITERAL;
+    gx_column* c = nullptr;
+    gx_check(gx_column_encode_device(dev_col, n_rows, &o, &c, (void*)stream));
+    return detail::comp_info_of(c, n_rows, chunk_bytes, comp_algo, nvchunk);
 }
 
 // The decoder of one compressed column: what build_gpucomp_manager returns
