@@ -363,7 +363,11 @@ typedef struct gx_scan_plan {
 } gx_scan_plan;
 
 /* Run the plan on `stream`.  Does not clear result_dev or the group table
- * (callers accumulate across calls, like the reference's atomics). */
+ * (callers accumulate across calls, like the reference's atomics).  The
+ * launch may overlap the kernel just before it on the stream (programmatic
+ * dependent launch): until that kernel completes the scan only reads column
+ * data; join tables, keep_chunks_dev, results, group tables and keep_out_dev
+ * are read and written after it, so every write of earlier work is seen. */
 gx_status gx_scan(const gx_scan_plan* plan, void* stream);
 /* Same, then synchronise and report device-side errors (corrupt blocks,
  * table overflow).  *rows_scanned (optional) = rows in surviving tiles. */
