@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 from golap_public_b200 import api, datagen
+from golap_public_b200 import _lib as L
 from golap_public_b200._lib import GxError
 from oracle import oracle as O
 
@@ -185,3 +186,18 @@ def test_block_directory_matches_reference_blockinfo_layout():
     for off, _, used, _ in b:
         _check_alignment("lz4", int(off), pl[int(off):int(off) + int(used)])
     assert np.all(b[1:, 0] >= b[:-1, 0] + b[:-1, 2])
+
+
+@pytest.mark.parametrize("S", [1, 4, 32, 128])
+def test_literal_policy_blocks(S):
+    # lz4_min_match = GX_LZ4_LITERAL (the GPU ingest encoder's LZ4 policy): every
+    # block is one literal run that liblz4 and the oracle decode, placed so that
+    # its first literal byte is 16-byte aligned
+    rng = np.random.default_rng(S)
+    for v in (rng.integers(0, 11, 250_001).astype(np.int32), np.arange(3, dtype=np.int32),
+              np.full(70_000, 5, np.int32)):
+        col = roundtrip(v, "lz4", S=S, lz4_min_match=L.GX_LZ4_LITERAL)
+        pl, blocks = col.payload(), col.blocks()
+        for off, size, used, tuples in blocks.astype(np.int64):
+            lit = _first_literal(pl[off:off + used])
+            assert lit is not None and used == lit + 4 * tuples
